@@ -1,0 +1,190 @@
+#!/usr/bin/env python3
+"""Write the synthetic, GFN2-shaped H/C/O parameter file ``synthetic_hco.tbp``.
+
+The real GFN2-xTB parameter set, tblite's STO-nG expansion tables and the D4
+reference data are not available to this project, and they are not typed in
+from memory.  This script instead produces a clearly labelled *synthetic*
+parameter file that has every field the GFN2 Hamiltonian needs (per-shell
+self-energies, CN shifts, polynomial enhancement, reference occupations,
+shell-resolved Hubbard parameters and their derivatives, repulsion, the
+anisotropic-electrostatics globals) with plausible magnitudes.
+
+Contracted Gaussians are obtained here by a numerical least-squares fit of
+Slater functions r^(n-1) exp(-zeta r) with ``nprim`` Gaussians
+(maximising the normalised radial overlap, exponents optimised in log space,
+coefficients solved linearly).  Coefficients written to the file already
+include the primitive normalisation of the Cartesian component x^l exp(-a r^2)
+and the contraction normalisation, so that every spherical atomic orbital has
+unit self-overlap (the d-shell factor matches the sqrt(3) spherical transform
+used by the integral code).
+
+The file format (``.tbp``) is plain text, one keyword per line:
+
+    format tblite-b200-params 1
+    name <text>
+    global <key> <value>            scalar globals
+    kshell <li> <lj> <value>        angular-momentum pair scaling of H0
+    kpair <sym_i> <sym_j> <value>   optional element-pair scaling of H0
+    element <symbol> <Z>
+      <key> <value>                 element scalars (rad, rcov, en, ...)
+      shell <ang> <nprim>
+        <key> <value>               shell scalars (selfenergy, kcn, ...)
+        alpha <nprim values>
+        coeff <nprim values>
+      end
+    end
+
+Run ``python make_synthetic.py`` to regenerate the file deterministically.
+"""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+from scipy.optimize import minimize
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "synthetic_hco.tbp")
+
+# radial grid for the fits
+_R = np.linspace(1e-6, 40.0, 40001)
+_DR = _R[1] - _R[0]
+
+
+def _radial_overlap(f, g, l):
+    return float(np.sum(f * g * _R ** (2 + 2 * l)) * _DR)
+
+
+def fit_sto(n: int, l: int, zeta: float, nprim: int):
+    """Fit r^(n-1-l) exp(-zeta r) (times r^l Y_lm) with nprim primitives r^l exp(-a r^2).
+
+    Returns exponents (descending) and contraction coefficients for
+    *normalised primitives*, normalised so that the contraction is normalised.
+    """
+    sto = _R ** (n - 1 - l) * np.exp(-zeta * _R)
+    sto = sto / math.sqrt(_radial_overlap(sto, sto, l))
+
+    def prim(a):
+        g = np.exp(-a * _R * _R)
+        return g / math.sqrt(_radial_overlap(g, g, l))
+
+    def solve(loga):
+        a = np.exp(loga)
+        G = np.stack([prim(x) for x in a])
+        M = np.array([[_radial_overlap(G[i], G[j], l) for j in range(nprim)] for i in range(nprim)])
+        b = np.array([_radial_overlap(G[i], sto, l) for i in range(nprim)])
+        c = np.linalg.solve(M, b)
+        ov = float(b @ c) / math.sqrt(float(c @ M @ c))
+        return ov, c, M
+
+    x0 = np.log(zeta * zeta * np.geomspace(0.1, 8.0, nprim))
+    # keep the exponents in a physically sensible window (0.03..60 zeta^2)
+    lo, hi = math.log(0.03 * zeta * zeta), math.log(60.0 * zeta * zeta)
+    res = minimize(lambda x: -solve(x)[0], x0, method="Powell",
+                   bounds=[(lo, hi)] * nprim,
+                   options={"xtol": 1e-10, "ftol": 1e-14, "maxiter": 20000, "maxfev": 40000})
+    ov, c, M = solve(res.x)
+    c = c / math.sqrt(float(c @ M @ c))
+    a = np.exp(res.x)
+    order = np.argsort(-a)
+    return a[order], c[order], ov
+
+
+def cart_norm(a: float, l: int) -> float:
+    """Normalisation of x^l exp(-a r^2) (the 'xx..' Cartesian component)."""
+    dfac = [1.0, 1.0, 3.0, 15.0][l]  # (2l-1)!!
+    return (2.0 * a / math.pi) ** 0.75 * (4.0 * a) ** (0.5 * l) / math.sqrt(dfac)
+
+
+def sph_prim_factor(a: float, l: int) -> float:
+    """Radial-normalised primitive -> Cartesian-normalised primitive factor.
+
+    The fit uses radially normalised primitives; the integral code expects the
+    coefficient multiplying the raw Cartesian primitive x^l exp(-a r^2), whose
+    self-overlap is 1/cart_norm^2.  Both normalisations describe the same
+    function up to a constant, so the contraction coefficient just becomes
+    c * cart_norm(a, l).
+    """
+    return cart_norm(a, l)
+
+
+# ---------------------------------------------------------------------------
+# synthetic values (plausible magnitudes, NOT the GFN2-xTB parameters)
+# ---------------------------------------------------------------------------
+GLOBALS = {
+    "gexp": 2.0,            # exponent of the ES2 gamma kernel
+    "kdmp3": 3.0,           # AES damping exponent, inverse-cubic terms
+    "kdmp5": 4.0,           # AES damping exponent, inverse-quintic terms
+    "mp_shift": 1.0,        # shift of the multipole damping radii
+    "mp_kexp": 4.5,         # steepness of the multipole damping radii
+    "mp_rmax": 5.5,         # maximum multipole damping radius (Bohr)
+    "rep_kexp": 1.5,        # repulsion exponent on R
+    "rep_kexp_light": 1.0,  # repulsion exponent on R for H/He pairs
+    "rep_rexp": 1.0,        # repulsion polynomial exponent
+    "enscale": 0.02,        # electronegativity scaling of H0
+    "wexp": 0.5,            # Slater-exponent weighting exponent of H0
+    "cn_cutoff": 25.0,      # real-space cutoff of the coordination number (Bohr)
+    "rep_cutoff": 25.0,     # real-space cutoff of the repulsion (Bohr)
+}
+KSHELL = {(0, 0): 1.90, (0, 1): 2.05, (1, 1): 2.20, (0, 2): 2.00, (1, 2): 2.10, (2, 2): 2.30}
+
+ELEMENTS = [
+    # symbol, Z, element scalars, shells (n, l, zeta, nprim, shell scalars)
+    ("H", 1,
+     dict(rad=1.10, rcov=0.80, en=2.20, rep_alpha=2.20, rep_zeff=1.10,
+          mp_rad=1.40, mp_vcn=1.0, dkernel=0.0100, qkernel=0.0010),
+     [(1, 0, 1.20, 3, dict(selfenergy=-0.4000, kcn=0.0030, shpoly=-0.050, refocc=1.0,
+                           hubbard=0.4050, hubbard_deriv=0.0800))]),
+    ("C", 6,
+     dict(rad=1.45, rcov=1.90, en=2.55, rep_alpha=2.00, rep_zeff=4.20,
+          mp_rad=3.00, mp_vcn=3.0, dkernel=0.0080, qkernel=0.0020),
+     [(2, 0, 1.70, 4, dict(selfenergy=-0.5000, kcn=0.0040, shpoly=-0.020, refocc=1.0,
+                           hubbard=0.5380, hubbard_deriv=0.1000)),
+      (2, 1, 1.60, 4, dict(selfenergy=-0.3700, kcn=0.0020, shpoly=0.050, refocc=3.0,
+                           hubbard=0.4600, hubbard_deriv=0.0500))]),
+    ("O", 8,
+     dict(rad=1.40, rcov=1.60, en=3.44, rep_alpha=2.30, rep_zeff=5.80,
+          mp_rad=2.50, mp_vcn=2.0, dkernel=0.0150, qkernel=0.0030),
+     [(2, 0, 2.20, 4, dict(selfenergy=-0.7500, kcn=0.0050, shpoly=-0.030, refocc=2.0,
+                           hubbard=0.5700, hubbard_deriv=0.1200)),
+      (2, 1, 2.10, 4, dict(selfenergy=-0.5000, kcn=0.0030, shpoly=0.040, refocc=4.0,
+                           hubbard=0.6200, hubbard_deriv=0.0600))]),
+]
+
+
+def main():
+    lines = [
+        "# SYNTHETIC GFN2-shaped parameters for H, C, O.",
+        "# These are NOT the GFN2-xTB parameters; they only have the same fields and",
+        "# plausible magnitudes. Generated by make_synthetic.py (deterministic).",
+        "format tblite-b200-params 1",
+        "name synthetic-gfn2-shaped-HCO",
+    ]
+    for k, v in GLOBALS.items():
+        lines.append(f"global {k} {v!r}")
+    for (li, lj), v in sorted(KSHELL.items()):
+        lines.append(f"kshell {li} {lj} {v!r}")
+    for sym, z, escal, shells in ELEMENTS:
+        lines.append(f"element {sym} {z}")
+        for k, v in escal.items():
+            lines.append(f"  {k} {v!r}")
+        for n, l, zeta, nprim, sscal in shells:
+            a, c, ov = fit_sto(n, l, zeta, nprim)
+            coeff = [float(ci * sph_prim_factor(ai, l)) for ai, ci in zip(a, c)]
+            lines.append(f"  shell {l} {nprim}")
+            lines.append(f"    # fit of n={n} l={l} Slater zeta={zeta}: overlap {ov:.8f}")
+            lines.append(f"    slater {zeta!r}")
+            for k, v in sscal.items():
+                lines.append(f"    {k} {v!r}")
+            lines.append("    alpha " + " ".join(f"{x:.17g}" for x in a))
+            lines.append("    coeff " + " ".join(f"{x:.17g}" for x in coeff))
+            lines.append("  end")
+        lines.append("end")
+    with open(OUT, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    print("wrote", OUT)
+
+
+if __name__ == "__main__":
+    main()
