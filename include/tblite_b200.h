@@ -1,0 +1,171 @@
+/*
+ * tblite-b200: B200-native (sm_100a) GFN2-xTB singlepoint engine -- C ABI.
+ *
+ * The reference (tornikeo/tblite-cuda) has no host API at all: its only entry
+ * is the device function
+ *   __device__ void xtb_singlepoint(const structure_type &mol,
+ *       const xtb_calculator &calc, wavefunction_type &wfn, float accuracy,
+ *       float energy, float (&gradient)[MAX_NAT][3], float (&sigma)[3][3],
+ *       int verbosity)                                   (src/xtb.cu:188-197)
+ * launched one thread per molecule from a test kernel (src/xtb.cu:436-481).
+ * This header is the drop-in boundary for that path: plain C types, caller
+ * owned host buffers, a status per call and per structure, no exit/trap.
+ * Each declaration names the reference interface it replaces.
+ *
+ * Conventions: coordinates in Bohr, energies in Hartree.  Species indices are
+ * 0-based positions in the parameter file's element list (the reference's
+ * mol%id).  Shell order within an atom follows the parameter file; AOs are
+ * spherical (s; p as y,z,x; d as tblite orders them).  Matrices are row-major.
+ * D[k][mu][nu] and Q[c][mu][nu] are planar with the moment operator on the
+ * atom of the column index nu (tblite's "centered on last index",
+ * src/integral/type.h:13-16); quadrupoles are traceless (xx,xy,yy,xz,yz,zz).
+ *
+ * Thread safety: a calculator may be shared by threads for read-only calls;
+ * tb_singlepoint_batch serialises on the calculator's workspace.  All device
+ * work is ordered on the caller's stream (NULL = default stream).
+ */
+#ifndef TBLITE_B200_H
+#define TBLITE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tb_status {
+  TB_OK = 0,
+  TB_BAD_INPUT = 1,            /* invalid sizes, species or pointers            */
+  TB_NOT_SPD = 2,              /* overlap matrix not positive definite          */
+  TB_SCF_NOT_CONVERGED = 3,    /* max_iter reached                              */
+  TB_FERMI_NOT_CONVERGED = 4,  /* Fermi level solve hit its iteration cap       */
+  TB_EIGEN_FAILED = 5,         /* QL iteration cap reached                      */
+  TB_CAPACITY_EXCEEDED = 6,    /* request larger than a stated maximum          */
+  TB_CUDA_ERROR = 7,           /* CUDA runtime error (see tb_last_error)        */
+  TB_PARAM_ERROR = 8           /* parameter file could not be read              */
+} tb_status;
+
+/* structure_type (src/structure.h:5-15): nat atoms, 0-based species id[nat],
+ * Cartesian xyz[nat][3] in Bohr, total charge and unpaired electrons. */
+typedef struct tb_structure {
+  int32_t nat;
+  int32_t uhf;
+  double charge;
+  const int32_t* id;
+  const double* xyz;
+} tb_structure;
+
+/* Calculator options: accuracy/verbosity arguments of xtb_singlepoint
+ * (src/xtb.cu:192,197) and xtb_calculator%max_iter, %mixer_damping
+ * (src/xtb.h:115-116).  econv = 1e-6*accuracy, pconv = 2e-5*accuracy. */
+typedef struct tb_options {
+  double accuracy;        /* default 1.0                                       */
+  double kt;              /* electronic temperature in Eh, default 300 K       */
+  int32_t max_iter;       /* SCF iterations = Broyden memory, default 32       */
+  double mixer_damping;   /* default 0.4                                       */
+  int32_t verbosity;      /* 0 silent                                          */
+  int32_t use_graphs;     /* 1: replay each SCF iteration as a CUDA graph      */
+  int32_t solver;         /* 0 auto, 1 in-house batched QL, 2 cuSOLVER (large) */
+  int32_t reserved;
+} tb_options;
+
+/* Per-structure results: the energy/wavefunction outputs of xtb_singlepoint.
+ * Array pointers are caller-owned and may be NULL (not written). */
+typedef struct tb_result {
+  double energy;          /* total energy = e_elec + e_rep                     */
+  double e_rep;           /* classical repulsion                               */
+  double e_elec;          /* electronic: band + (-TS) + ES2 + AES2 + ES3        */
+  double e_band, e_ts, e_es2, e_aes2, e_es3;
+  double dipole[3];       /* sum_A q_A R_A + mu_A (a.u.)                       */
+  double scf_error;       /* last RMS charge/multipole change                  */
+  int32_t iterations;
+  int32_t status;         /* tb_status of this structure                       */
+  int32_t nsh, nao;
+  double* qat;            /* [nat]    atomic partial charges                   */
+  double* qsh;            /* [nsh]    shell partial charges                    */
+  double* dpat;           /* [nat][3] atomic dipoles                           */
+  double* qpat;           /* [nat][6] atomic quadrupoles                       */
+} tb_result;
+
+typedef struct tb_calculator tb_calculator;
+
+/* xtb_calculator construction (src/xtb.h:105-126; the reference never builds
+ * one: new_hamiltonian is declared at src/h0.h:80-86 but not defined).  Reads a
+ * tblite-b200 parameter file (.tbp). */
+tb_status tb_calculator_create(const char* param_file, tb_calculator** out);
+void tb_calculator_destroy(tb_calculator* calc);
+int32_t tb_calculator_nspecies(const tb_calculator* calc);
+void tb_default_options(tb_options* opt);
+/* Text of the last error on this thread. */
+const char* tb_last_error(void);
+
+/* basis_type sizes (src/basis/type.h:56-73). */
+tb_status tb_basis_size(const tb_calculator* calc, const tb_structure* mol, int32_t* nsh, int32_t* nao);
+
+/* xtb_singlepoint (src/xtb.cu:188-434) for nmol structures at once, host
+ * buffers in and out.  Returns TB_OK when every structure succeeded, else the
+ * first failing structure's status; per-structure status is in out[i].status. */
+tb_status tb_singlepoint_batch(tb_calculator* calc, const tb_structure* mols, int32_t nmol,
+                               const tb_options* opt, tb_result* out, void* stream);
+
+/* Device-resident batches (for serving and for timing without host copies):
+ * create uploads geometry and sizes workspaces, run executes the full
+ * singlepoint on the device, results copies them back. */
+typedef struct tb_batch tb_batch;
+tb_status tb_batch_create(tb_calculator* calc, const tb_structure* mols, int32_t nmol,
+                          const tb_options* opt, tb_batch** out);
+tb_status tb_batch_run(tb_batch* batch, void* stream);
+tb_status tb_batch_results(tb_batch* batch, tb_result* out, void* stream);
+/* kernels launched by the last tb_batch_run (device work items, not host calls) */
+int64_t tb_batch_launches(const tb_batch* batch);
+void tb_batch_destroy(tb_batch* batch);
+
+/* ---- stage entry points (host buffers; one structure each) ---------------- */
+
+/* get_cutoff (src/basis/type.cu:66-79). */
+double tb_get_cutoff(const tb_calculator* calc, double accuracy);
+
+/* new_adjacency_list / generate (src/adjlist.cu:3-101): half list, jat < iat,
+ * r2 >= eps and r2 <= cutoff^2.  inl[nat], nnl[nat], nlat[cap] (0-based atom
+ * indices), npair out.  Bit-exact with the FP64 restatement. */
+tb_status tb_adjacency_list(const tb_calculator* calc, const tb_structure* mol, double cutoff,
+                            int32_t* inl, int32_t* nnl, int32_t* nlat, int32_t cap, int32_t* npair);
+
+/* ncoord_get_cn (src/coulomb.cu:334-347), get_mrad (:374-408) and
+ * get_selfenergy (src/h0.cu:125-199). cn[nat], mrad[nat], se[nsh]; any NULL. */
+tb_status tb_atomic_properties(const tb_calculator* calc, const tb_structure* mol, double* cn,
+                               double* mrad, double* selfenergy);
+
+/* get_engrad energy part (src/xtb.cu:47-182): erep[nat]. */
+tb_status tb_repulsion(const tb_calculator* calc, const tb_structure* mol, double* erep);
+
+/* get_hamiltonian (src/h0.cu:292-502) incl. on-site blocks: S, H0 [nao][nao],
+ * D [3][nao][nao], Q [6][nao][nao]. */
+tb_status tb_get_hamiltonian(const tb_calculator* calc, const tb_structure* mol, double* S,
+                             double* H0, double* D, double* Q);
+
+/* tb_coulomb::get_potential (src/coulomb.cu:793-809): ES2 + AES2 + ES3
+ * potential shifts for given shell charges and atomic multipoles. */
+tb_status tb_coulomb_potential(const tb_calculator* calc, const tb_structure* mol, const double* qsh,
+                               const double* dpat, const double* qpat, double* vsh, double* vat,
+                               double* vdp, double* vqp);
+
+/* add_pot_to_h1 (src/scf/potential.cu:224-272): F = H0 - potentials. */
+tb_status tb_add_pot_to_h1(const tb_calculator* calc, const tb_structure* mol, const double* S,
+                           const double* H0, const double* D, const double* Q, const double* vsh,
+                           const double* vat, const double* vdp, const double* vqp, double* F);
+
+/* sygvd_solver::solve (src/lapack/sygvd.cu:223-313): batched generalized
+ * symmetric-definite eigenproblems H C = S C e, ascending e, S-orthonormal C.
+ * Matrices packed back to back ([n_i][n_i] each), host buffers. */
+tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const double* S,
+                         double* w, double* C);
+
+/* get_fermi_filling (src/wavefunction/fermi.cu:100-124) for one spin channel. */
+tb_status tb_fermi_filling(int32_t n, double nel, double kt, const double* emo, double* occ,
+                           double* efermi, double* ts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,86 @@
+// Shared device-side types of the tblite-b200 engine.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tb {
+
+constexpr int kMaxL = 2;        // s, p, d
+constexpr int kMaxPrim = 12;    // maxg (reference src/limits.h:18)
+constexpr int kMaxShPerAtom = 3;
+
+// One shell type of one species (cgto_type, src/basis/type.h:18-23, plus the
+// per-shell Hamiltonian parameters of tb_hamiltonian, src/h0.h:27-40).
+struct ShellParam {
+  int ang, nprim, species, local;
+  double alpha[kMaxPrim];
+  double coeff[kMaxPrim];
+  double selfenergy, kcn, shpoly, refocc, hubbard, hubbard_deriv, slater;
+};
+
+struct SpeciesParam {
+  int z, nsh, sh0;  // sh0: index of the first ShellParam of this species
+  double rad, rcov, en, rep_alpha, rep_zeff, mp_rad, mp_vcn, dkernel, qkernel;
+};
+
+// Calculator parameters as seen by kernels (passed by value).
+struct DevParams {
+  const SpeciesParam* sp;
+  const ShellParam* sh;
+  const double* hscale;  // [nshtype][nshtype], hscale(jsh,ish,jzp,izp) by shell type
+  int nsp, nshtype;
+  double gexp, kdmp3, kdmp5, mp_shift, mp_kexp, mp_rmax;
+  double rep_kexp, rep_kexp_light, rep_rexp, cn_cutoff, rep_cutoff;
+  double intcut, cutoff;  // integral screening (25) and neighbour-list cutoff
+};
+
+// Per-batch layout: structures packed back to back.  Offsets are [nmol+1].
+struct DevBatch {
+  int nmol, nat_tot, nsh_tot, nao_tot;
+  const int* aoff;       // atom offset
+  const int* soff;       // shell offset
+  const int* ooff;       // AO offset
+  const long long* moff; // N*N matrix offset
+  const long long* poff; // neighbour pair capacity offset (nat*(nat-1)/2)
+  const int* mixoff;     // Broyden vector offset (nsh + 9 nat)
+  const double* xyz;     // [nat_tot][3]
+  const int* id;         // [nat_tot] species
+  const int* at_mol;     // [nat_tot] owning structure
+  const int* sh_type;    // [nsh_tot] global shell type (ShellParam index)
+  const int* sh_at;      // [nsh_tot] local atom index
+  const int* sh_iao;     // [nsh_tot] local AO offset
+  const int* at_ish;     // [nat_tot] local shell offset of the atom
+  const int* ao_at;      // [nao_tot] local atom index
+  const int* ao_sh;      // [nao_tot] local shell index
+};
+
+__host__ __device__ inline int msao(int l) { return 2 * l + 1; }
+__host__ __device__ inline int mlao(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ inline int lmap(int l) { return l == 0 ? 0 : (l == 1 ? 1 : 4); }
+
+// Status bits per structure (device), mapped to tb_status on the host.
+enum DevStatus : int {
+  kStOk = 0, kStBadInput = 1, kStNotSpd = 2, kStScfNotConverged = 3,
+  kStFermiNotConverged = 4, kStEigenFailed = 5
+};
+
+__device__ inline double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum in a fixed order (deterministic); all threads get the result.
+// `red` must hold blockDim.x/32 doubles.
+__device__ inline double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < nw; ++w) t += red[w];
+  return t;
+}
+
+}  // namespace tb

@@ -1,0 +1,963 @@
+// Host side of the tblite-b200 engine: parameter file, calculator, structure
+// batches (workspace layout in one device allocation), kernel orchestration
+// of xtb_singlepoint (reference src/xtb.cu:188-434) and the C ABI declared in
+// include/tblite_b200.h.  No computation of the singlepoint happens on the
+// host: it only builds index maps (the basis_type bookkeeping of
+// src/basis/type.h:56-73) and launches kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/tblite_b200.h"
+#include "tb_common.cuh"
+#include "tb_kernels.h"
+
+using namespace tb;
+
+namespace {
+
+thread_local std::string g_err;
+
+tb_status fail(tb_status st, const std::string& msg) {
+  g_err = msg;
+  return st;
+}
+
+#define TB_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(TB_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_));        \
+  } while (0)
+
+// ------------------------------------------------------------ parameters
+struct HostParams {
+  std::map<std::string, double> g;
+  double kshell[3][3] = {{0}};
+  std::map<std::pair<int, int>, double> kpair;
+  std::vector<SpeciesParam> sp;
+  std::vector<ShellParam> sh;
+  std::vector<std::string> sym;
+  double min_alpha = 1e300;
+  double glob(const char* k, double dflt = 0.0) const {
+    auto it = g.find(k);
+    return it == g.end() ? dflt : it->second;
+  }
+};
+
+bool parse_params(const char* path, HostParams& P, std::string& err) {
+  std::ifstream f(path);
+  if (!f) { err = std::string("cannot open parameter file ") + path; return false; }
+  std::string line;
+  int cur = -1, csh = -1;
+  bool fmt = false;
+  std::vector<std::vector<ShellParam>> shells;
+  std::vector<std::tuple<std::string, std::string, double>> kp;
+  int lineno = 0;
+  while (std::getline(f, line)) {
+    ++lineno;
+    auto h = line.find('#');
+    if (h != std::string::npos) line = line.substr(0, h);
+    std::istringstream is(line);
+    std::string key;
+    if (!(is >> key)) continue;
+    auto bad = [&](const std::string& m) { err = m + " (line " + std::to_string(lineno) + ")"; return false; };
+    if (key == "format") { std::string n; int v = 0; is >> n >> v; fmt = n == "tblite-b200-params" && v == 1; continue; }
+    if (key == "name") continue;
+    if (csh >= 0) {
+      ShellParam& s = shells[cur][csh];
+      if (key == "end") { csh = -1; continue; }
+      if (key == "alpha") { for (int i = 0; i < s.nprim; ++i) is >> s.alpha[i]; if (!is) return bad("short alpha"); continue; }
+      if (key == "coeff") { for (int i = 0; i < s.nprim; ++i) is >> s.coeff[i]; if (!is) return bad("short coeff"); continue; }
+      double v; if (!(is >> v)) return bad("missing value for " + key);
+      if (key == "selfenergy") s.selfenergy = v;
+      else if (key == "kcn") s.kcn = v;
+      else if (key == "shpoly") s.shpoly = v;
+      else if (key == "refocc") s.refocc = v;
+      else if (key == "hubbard") s.hubbard = v;
+      else if (key == "hubbard_deriv") s.hubbard_deriv = v;
+      else if (key == "slater") s.slater = v;
+      else return bad("unknown shell key " + key);
+      continue;
+    }
+    if (cur >= 0) {
+      SpeciesParam& e = P.sp[cur];
+      if (key == "end") { cur = -1; continue; }
+      if (key == "shell") {
+        ShellParam s{};
+        s.slater = 1.0;
+        if (!(is >> s.ang >> s.nprim)) return bad("bad shell line");
+        if (s.ang < 0 || s.ang > kMaxL || s.nprim < 1 || s.nprim > kMaxPrim) return bad("unsupported shell");
+        if ((int)shells[cur].size() >= kMaxShPerAtom) return bad("too many shells");
+        shells[cur].push_back(s);
+        csh = (int)shells[cur].size() - 1;
+        continue;
+      }
+      double v; if (!(is >> v)) return bad("missing value for " + key);
+      if (key == "rad") e.rad = v;
+      else if (key == "rcov") e.rcov = v;
+      else if (key == "en") e.en = v;
+      else if (key == "rep_alpha") e.rep_alpha = v;
+      else if (key == "rep_zeff") e.rep_zeff = v;
+      else if (key == "mp_rad") e.mp_rad = v;
+      else if (key == "mp_vcn") e.mp_vcn = v;
+      else if (key == "dkernel") e.dkernel = v;
+      else if (key == "qkernel") e.qkernel = v;
+      else return bad("unknown element key " + key);
+      continue;
+    }
+    if (key == "global") { std::string k; double v; if (!(is >> k >> v)) return bad("bad global"); P.g[k] = v; continue; }
+    if (key == "kshell") { int a, b; double v; if (!(is >> a >> b >> v) || a < 0 || b < 0 || a > 2 || b > 2) return bad("bad kshell"); P.kshell[a][b] = P.kshell[b][a] = v; continue; }
+    if (key == "kpair") { std::string a, b; double v; if (!(is >> a >> b >> v)) return bad("bad kpair"); kp.emplace_back(a, b, v); continue; }
+    if (key == "element") {
+      SpeciesParam e{};
+      std::string sym;
+      if (!(is >> sym >> e.z)) return bad("bad element line");
+      P.sp.push_back(e);
+      P.sym.push_back(sym);
+      shells.emplace_back();
+      cur = (int)P.sp.size() - 1;
+      continue;
+    }
+    return bad("unknown key " + key);
+  }
+  if (!fmt) { err = "missing or unsupported 'format' line"; return false; }
+  if (P.sp.empty()) { err = "no elements"; return false; }
+  for (size_t i = 0; i < P.sp.size(); ++i) {
+    P.sp[i].nsh = (int)shells[i].size();
+    P.sp[i].sh0 = (int)P.sh.size();
+    for (size_t s = 0; s < shells[i].size(); ++s) {
+      shells[i][s].species = (int)i;
+      shells[i][s].local = (int)s;
+      P.sh.push_back(shells[i][s]);
+      for (int k = 0; k < shells[i][s].nprim; ++k) P.min_alpha = std::min(P.min_alpha, shells[i][s].alpha[k]);
+    }
+  }
+  for (auto& t : kp) {
+    int a = -1, b = -1;
+    for (size_t i = 0; i < P.sym.size(); ++i) { if (P.sym[i] == std::get<0>(t)) a = (int)i; if (P.sym[i] == std::get<1>(t)) b = (int)i; }
+    if (a < 0 || b < 0) { err = "kpair names an unknown element"; return false; }
+    P.kpair[{a, b}] = P.kpair[{b, a}] = std::get<2>(t);
+  }
+  return true;
+}
+
+// hscale(jsh, ish, jzp, izp) by shell type: GFN2-shaped preprocessing of the
+// parameter file (the reference's gfn2_h0spec is empty, src/h0.h:42-48).
+double hscale_of(const HostParams& P, int ti, int tj) {
+  const ShellParam& a = P.sh[ti];
+  const ShellParam& b = P.sh[tj];
+  const double den = P.sp[a.species].en - P.sp[b.species].en;
+  const double zij = std::pow(2.0 * std::sqrt(a.slater * b.slater) / (a.slater + b.slater), P.glob("wexp"));
+  auto it = P.kpair.find({a.species, b.species});
+  const double kp = it == P.kpair.end() ? 1.0 : it->second;
+  return P.kshell[a.ang][b.ang] * kp * (1.0 + P.glob("enscale") * den * den) * zij;
+}
+
+double integral_cutoff(double acc) {
+  // src/basis/type.cu:17-30 (quoted): clip(acc, min_acc=1e3, max_acc=1e-4)
+  // always yields 1e-4, so intcut = 25 for every accuracy (reproduced literally).
+  auto clip = [](double v, double lo, double hi) { return std::min(std::max(v, lo), hi); };
+  return clip(25.0 - 10.0 * std::log10(clip(acc, 1.0e+3, 1.0e-4)), 5.0, 25.0);
+}
+
+// ------------------------------------------------------------ device arena
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0;
+  ~Arena() { if (base) cudaFree(base); }
+  cudaError_t reserve(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (base) { cudaFree(base); base = nullptr; cap = 0; }
+    cudaError_t e = cudaMalloc(&base, bytes);
+    if (e == cudaSuccess) cap = bytes;
+    return e;
+  }
+};
+
+struct Layout {
+  size_t total = 0;
+  size_t add(size_t bytes) {
+    const size_t off = (total + 255) & ~size_t(255);
+    total = off + bytes;
+    return off;
+  }
+};
+
+}  // namespace
+
+// ====================================================================== calculator
+struct tb_calculator {
+  HostParams hp;
+  DevParams dp{};
+  SpeciesParam* d_sp = nullptr;
+  ShellParam* d_sh = nullptr;
+  double* d_hscale = nullptr;
+  int maxsh = 1;
+  int lmask = 0;  // bit l set when shells of angular momentum l exist
+  std::mutex mu;
+  Arena arena;
+  ~tb_calculator() {
+    if (d_sp) cudaFree(d_sp);
+    if (d_sh) cudaFree(d_sh);
+    if (d_hscale) cudaFree(d_hscale);
+  }
+};
+
+// ====================================================================== batch
+struct tb_batch {
+  tb_calculator* calc = nullptr;
+  tb_options opt{};
+  int nmol = 0, nat_tot = 0, nsh_tot = 0, nao_tot = 0, nmax = 0, natmax = 0, nshmax = 0;
+  long long n2_tot = 0, pair_cap = 0, mix_tot = 0;
+  Arena own;
+  Arena* arena = nullptr;
+  std::vector<int> h_aoff, h_soff, h_ooff, h_mixoff;
+  std::vector<long long> h_moff, h_poff;
+  std::vector<int4> tiles64, tiles32;
+  std::vector<int2> chunks32;
+  std::vector<double> h_xyz;
+  // device views
+  DevBatch db{};
+  MolState ms{};
+  double *cn, *mrad, *erep, *se, *n0sh;
+  int *cnt, *npair, *pair_i, *pair_j;
+  long long* inl;
+  double *S, *H0, *D, *Q, *X, *W, *F, *Z, *P;
+  double *w, *focc, *vsh, *vat, *vdp, *vqp, *colred, *qsh_out, *qat_out, *dpat_out, *qpat_out;
+  int *perm, *kdim;
+  double *q_in, *dq, *dqlast, *qlast, *df, *u, *amat, *omega;
+  double* charge;
+  int* uhf;
+  int4 *d_tiles64, *d_tiles32;
+  int2* d_chunks32;
+  int* h_nactive = nullptr;  // pinned
+  int64_t launches = 0;
+  size_t bytes = 0;
+  ~tb_batch() { if (h_nactive) cudaFreeHost(h_nactive); }
+};
+
+namespace {
+
+template <typename T>
+T* at(char* base, size_t off) { return reinterpret_cast<T*>(base + off); }
+
+// Build index maps, lay out the workspace, allocate, upload.
+tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, const tb_options* opt,
+                      tb_batch* b, Arena* arena) {
+  const HostParams& P = calc->hp;
+  b->calc = calc;
+  b->opt = *opt;
+  b->nmol = nmol;
+  if (nmol <= 0) return fail(TB_BAD_INPUT, "nmol must be positive");
+  if (opt->max_iter < 1 || opt->max_iter > 64) return fail(TB_BAD_INPUT, "max_iter must be in 1..64");
+  b->h_aoff.assign(nmol + 1, 0); b->h_soff.assign(nmol + 1, 0); b->h_ooff.assign(nmol + 1, 0);
+  b->h_mixoff.assign(nmol + 1, 0); b->h_moff.assign(nmol + 1, 0); b->h_poff.assign(nmol + 1, 0);
+  std::vector<int> id, at_mol, sh_type, sh_at, sh_iao, at_ish, ao_at, ao_sh;
+  b->h_xyz.clear();
+  for (int m = 0; m < nmol; ++m) {
+    const tb_structure& s = mols[m];
+    if (s.nat <= 0 || !s.id || !s.xyz) return fail(TB_BAD_INPUT, "structure " + std::to_string(m) + ": empty or null");
+    int nsh = 0, nao = 0;
+    for (int a = 0; a < s.nat; ++a) {
+      const int z = s.id[a];
+      if (z < 0 || z >= (int)P.sp.size()) return fail(TB_BAD_INPUT, "structure " + std::to_string(m) + ": bad species");
+      id.push_back(z);
+      at_mol.push_back(m);
+      at_ish.push_back(nsh);
+      for (int k = 0; k < 3; ++k) {
+        const double x = s.xyz[3 * a + k];
+        if (!std::isfinite(x)) return fail(TB_BAD_INPUT, "structure " + std::to_string(m) + ": non-finite coordinate");
+        b->h_xyz.push_back(x);
+      }
+      const SpeciesParam& sp = P.sp[z];
+      for (int k = 0; k < sp.nsh; ++k) {
+        const ShellParam& sh = P.sh[sp.sh0 + k];
+        sh_type.push_back(sp.sh0 + k);
+        sh_at.push_back(a);
+        sh_iao.push_back(nao);
+        for (int x = 0; x < msao(sh.ang); ++x) { ao_at.push_back(a); ao_sh.push_back(nsh); }
+        nao += msao(sh.ang);
+        nsh += 1;
+      }
+    }
+    b->h_aoff[m + 1] = b->h_aoff[m] + s.nat;
+    b->h_soff[m + 1] = b->h_soff[m] + nsh;
+    b->h_ooff[m + 1] = b->h_ooff[m] + nao;
+    b->h_mixoff[m + 1] = b->h_mixoff[m] + nsh + 9 * s.nat;
+    b->h_moff[m + 1] = b->h_moff[m] + (long long)nao * nao;
+    b->h_poff[m + 1] = b->h_poff[m] + (long long)s.nat * (s.nat - 1) / 2;
+    b->nmax = std::max(b->nmax, nao);
+    b->natmax = std::max(b->natmax, (int)s.nat);
+    b->nshmax = std::max(b->nshmax, nsh);
+    for (int t = 0; t < (nao + 63) / 64; ++t)
+      for (int u = 0; u < (nao + 63) / 64; ++u) b->tiles64.push_back(make_int4(m, t, u, 0));
+    for (int t = 0; t < (nao + 31) / 32; ++t) {
+      b->chunks32.push_back(make_int2(m, t));
+      for (int u = 0; u < (nao + 31) / 32; ++u) b->tiles32.push_back(make_int4(m, t, u, 0));
+    }
+  }
+  if (6 * (size_t)b->nmax * sizeof(double) > 220 * 1024)
+    return fail(TB_CAPACITY_EXCEEDED, "structure with " + std::to_string(b->nmax) +
+                " AOs exceeds the in-house eigensolver limit (4693 AOs)");
+  b->nat_tot = b->h_aoff[nmol];
+  b->nsh_tot = b->h_soff[nmol];
+  b->nao_tot = b->h_ooff[nmol];
+  b->n2_tot = b->h_moff[nmol];
+  b->pair_cap = std::max<long long>(1, b->h_poff[nmol]);
+  b->mix_tot = b->h_mixoff[nmol];
+  const int mem = opt->max_iter;
+
+  // ---- layout
+  Layout L;
+  const size_t D8 = sizeof(double), I4 = sizeof(int);
+  const long long NA = b->nat_tot, NS = b->nsh_tot, NO = b->nao_tot, N2 = b->n2_tot, NM = nmol, MX = b->mix_tot;
+  size_t o_meta_aoff = L.add((NM + 1) * I4), o_meta_soff = L.add((NM + 1) * I4), o_meta_ooff = L.add((NM + 1) * I4),
+         o_meta_mixoff = L.add((NM + 1) * I4), o_meta_moff = L.add((NM + 1) * 8), o_meta_poff = L.add((NM + 1) * 8),
+         o_xyz = L.add(3 * NA * D8), o_id = L.add(NA * I4), o_atmol = L.add(NA * I4), o_shtype = L.add(NS * I4),
+         o_shat = L.add(NS * I4), o_shiao = L.add(NS * I4), o_atish = L.add(NA * I4), o_aoat = L.add(NO * I4),
+         o_aosh = L.add(NO * I4), o_t64 = L.add(b->tiles64.size() * sizeof(int4)),
+         o_t32 = L.add(b->tiles32.size() * sizeof(int4)), o_c32 = L.add(b->chunks32.size() * sizeof(int2)),
+         o_charge = L.add(NM * D8), o_uhf = L.add(NM * I4);
+  const size_t meta_end = L.total;
+  size_t o_cn = L.add(NA * D8), o_mrad = L.add(NA * D8), o_erep = L.add(NA * D8), o_se = L.add(NS * D8),
+         o_n0sh = L.add(NS * D8), o_cnt = L.add(NA * I4), o_inl = L.add(NA * 8), o_npair = L.add(NM * I4),
+         o_pi = L.add(b->pair_cap * I4), o_pj = L.add(b->pair_cap * I4);
+  size_t o_S = L.add(N2 * D8), o_H0 = L.add(N2 * D8), o_D = L.add(3 * N2 * D8), o_Q = L.add(6 * N2 * D8);
+  size_t o_X = L.add(N2 * D8), o_W = L.add(N2 * D8), o_F = L.add(N2 * D8), o_Z = L.add(N2 * D8),
+         o_P = L.add(N2 * D8);
+  size_t o_w = L.add(NO * D8), o_focc = L.add(NO * D8), o_perm = L.add(NO * I4), o_kdim = L.add(NM * I4),
+         o_vsh = L.add(NS * D8), o_vat = L.add(NA * D8), o_vdp = L.add(3 * NA * D8), o_vqp = L.add(6 * NA * D8),
+         o_col = L.add(12 * NO * D8), o_qsho = L.add(NS * D8), o_qato = L.add(NA * D8), o_dpo = L.add(3 * NA * D8),
+         o_qpo = L.add(6 * NA * D8);
+  size_t o_qin = L.add(MX * D8), o_dq = L.add(MX * D8), o_dql = L.add(MX * D8), o_ql = L.add(MX * D8),
+         o_df = L.add((size_t)mem * MX * D8), o_u = L.add((size_t)mem * MX * D8),
+         o_amat = L.add((size_t)mem * mem * NM * D8), o_om = L.add((size_t)mem * NM * D8);
+  size_t o_ms_erep = L.add(NM * D8), o_ms_nel = L.add(2 * NM * D8), o_ms_iscf = L.add(NM * I4),
+         o_ms_mix = L.add(NM * I4), o_ms_eelec = L.add(NM * D8), o_ms_active = L.add(NM * I4),
+         o_ms_status = L.add(NM * I4), o_ms_ets = L.add(NM * D8), o_ms_eband = L.add(NM * D8),
+         o_ms_ees2 = L.add(NM * D8), o_ms_eaes2 = L.add(NM * D8), o_ms_ees3 = L.add(NM * D8),
+         o_ms_err = L.add(NM * D8), o_ms_fw = L.add(NM * I4), o_ms_dip = L.add(3 * NM * D8),
+         o_ms_nact = L.add(I4);
+  b->bytes = L.total;
+  b->arena = arena;
+  {
+    cudaError_t e = arena->reserve(L.total);
+    if (e != cudaSuccess)
+      return fail(TB_CUDA_ERROR, "workspace of " + std::to_string(L.total >> 20) + " MiB: " + cudaGetErrorString(e));
+  }
+  char* base = arena->base;
+  // ---- metadata upload (one host blob, one copy)
+  std::vector<char> blob(meta_end, 0);
+  auto put = [&](size_t off, const void* src, size_t n) { if (n) std::memcpy(blob.data() + off, src, n); };
+  put(o_meta_aoff, b->h_aoff.data(), (NM + 1) * I4);
+  put(o_meta_soff, b->h_soff.data(), (NM + 1) * I4);
+  put(o_meta_ooff, b->h_ooff.data(), (NM + 1) * I4);
+  put(o_meta_mixoff, b->h_mixoff.data(), (NM + 1) * I4);
+  put(o_meta_moff, b->h_moff.data(), (NM + 1) * 8);
+  put(o_meta_poff, b->h_poff.data(), (NM + 1) * 8);
+  put(o_xyz, b->h_xyz.data(), 3 * NA * D8);
+  put(o_id, id.data(), NA * I4);
+  put(o_atmol, at_mol.data(), NA * I4);
+  put(o_shtype, sh_type.data(), NS * I4);
+  put(o_shat, sh_at.data(), NS * I4);
+  put(o_shiao, sh_iao.data(), NS * I4);
+  put(o_atish, at_ish.data(), NA * I4);
+  put(o_aoat, ao_at.data(), NO * I4);
+  put(o_aosh, ao_sh.data(), NO * I4);
+  put(o_t64, b->tiles64.data(), b->tiles64.size() * sizeof(int4));
+  put(o_t32, b->tiles32.data(), b->tiles32.size() * sizeof(int4));
+  put(o_c32, b->chunks32.data(), b->chunks32.size() * sizeof(int2));
+  std::vector<double> ch(nmol);
+  std::vector<int> uh(nmol);
+  for (int m = 0; m < nmol; ++m) { ch[m] = mols[m].charge; uh[m] = mols[m].uhf; }
+  put(o_charge, ch.data(), NM * D8);
+  put(o_uhf, uh.data(), NM * I4);
+  TB_CUDA(cudaMemcpy(base, blob.data(), meta_end, cudaMemcpyHostToDevice));
+
+  DevBatch& d = b->db;
+  d.nmol = nmol; d.nat_tot = (int)NA; d.nsh_tot = (int)NS; d.nao_tot = (int)NO;
+  d.aoff = at<int>(base, o_meta_aoff); d.soff = at<int>(base, o_meta_soff); d.ooff = at<int>(base, o_meta_ooff);
+  d.mixoff = at<int>(base, o_meta_mixoff); d.moff = at<long long>(base, o_meta_moff);
+  d.poff = at<long long>(base, o_meta_poff); d.xyz = at<double>(base, o_xyz); d.id = at<int>(base, o_id);
+  d.at_mol = at<int>(base, o_atmol); d.sh_type = at<int>(base, o_shtype); d.sh_at = at<int>(base, o_shat);
+  d.sh_iao = at<int>(base, o_shiao); d.at_ish = at<int>(base, o_atish); d.ao_at = at<int>(base, o_aoat);
+  d.ao_sh = at<int>(base, o_aosh);
+  b->d_tiles64 = at<int4>(base, o_t64); b->d_tiles32 = at<int4>(base, o_t32); b->d_chunks32 = at<int2>(base, o_c32);
+  b->charge = at<double>(base, o_charge); b->uhf = at<int>(base, o_uhf);
+  b->cn = at<double>(base, o_cn); b->mrad = at<double>(base, o_mrad); b->erep = at<double>(base, o_erep);
+  b->se = at<double>(base, o_se); b->n0sh = at<double>(base, o_n0sh); b->cnt = at<int>(base, o_cnt);
+  b->inl = at<long long>(base, o_inl); b->npair = at<int>(base, o_npair); b->pair_i = at<int>(base, o_pi);
+  b->pair_j = at<int>(base, o_pj);
+  b->S = at<double>(base, o_S); b->H0 = at<double>(base, o_H0); b->D = at<double>(base, o_D);
+  b->Q = at<double>(base, o_Q); b->X = at<double>(base, o_X); b->W = at<double>(base, o_W);
+  b->F = at<double>(base, o_F); b->Z = at<double>(base, o_Z); b->P = at<double>(base, o_P);
+  b->w = at<double>(base, o_w); b->focc = at<double>(base, o_focc); b->perm = at<int>(base, o_perm);
+  b->kdim = at<int>(base, o_kdim); b->vsh = at<double>(base, o_vsh); b->vat = at<double>(base, o_vat);
+  b->vdp = at<double>(base, o_vdp); b->vqp = at<double>(base, o_vqp); b->colred = at<double>(base, o_col);
+  b->qsh_out = at<double>(base, o_qsho); b->qat_out = at<double>(base, o_qato);
+  b->dpat_out = at<double>(base, o_dpo); b->qpat_out = at<double>(base, o_qpo);
+  b->q_in = at<double>(base, o_qin); b->dq = at<double>(base, o_dq); b->dqlast = at<double>(base, o_dql);
+  b->qlast = at<double>(base, o_ql); b->df = at<double>(base, o_df); b->u = at<double>(base, o_u);
+  b->amat = at<double>(base, o_amat); b->omega = at<double>(base, o_om);
+  MolState& s = b->ms;
+  s.e_rep = at<double>(base, o_ms_erep); s.nel = at<double>(base, o_ms_nel); s.iscf = at<int>(base, o_ms_iscf);
+  s.mix_iter = at<int>(base, o_ms_mix); s.eelec = at<double>(base, o_ms_eelec);
+  s.active = at<int>(base, o_ms_active); s.status = at<int>(base, o_ms_status);
+  s.e_ts = at<double>(base, o_ms_ets); s.e_band = at<double>(base, o_ms_eband);
+  s.e_es2 = at<double>(base, o_ms_ees2); s.e_aes2 = at<double>(base, o_ms_eaes2);
+  s.e_es3 = at<double>(base, o_ms_ees3); s.scf_error = at<double>(base, o_ms_err);
+  s.fermi_warn = at<int>(base, o_ms_fw); s.dipole = at<double>(base, o_ms_dip); s.n_active = at<int>(base, o_ms_nact);
+  if (!b->h_nactive) TB_CUDA(cudaMallocHost(&b->h_nactive, sizeof(int)));
+  return TB_OK;
+}
+
+inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
+
+#define TB_LAUNCH_CHECK()                                                                  \
+  do {                                                                                     \
+    cudaError_t e_ = cudaGetLastError();                                                   \
+    if (e_ != cudaSuccess) return fail(TB_CUDA_ERROR, std::string("launch: ") + cudaGetErrorString(e_)); \
+    ++b->launches;                                                                         \
+  } while (0)
+
+tb_status batch_run(tb_batch* b, cudaStream_t st) {
+  tb_calculator* c = b->calc;
+  const DevParams P = c->dp;
+  const DevBatch& B = b->db;
+  MolState& S = b->ms;
+  const int nmol = b->nmol;
+  b->launches = 0;
+  DevParams Pc = P;
+  Pc.intcut = integral_cutoff(b->opt.accuracy);
+  Pc.cutoff = std::min(std::sqrt(2.0 * Pc.intcut / c->hp.min_alpha), 40.0);  // get_cutoff, src/basis/type.cu:43-64
+  TB_CUDA(cudaMemsetAsync(S.status, 0, nmol * sizeof(int), st));
+  TB_CUDA(cudaMemsetAsync(S.fermi_warn, 0, nmol * sizeof(int), st));
+  TB_CUDA(cudaMemsetAsync(S.n_active, 0, sizeof(int), st));
+  // ---- setup
+  k_atoms<<<nblk(B.nat_tot, 128), 128, 0, st>>>(Pc, B, b->cn, b->mrad, b->erep, b->se);
+  TB_LAUNCH_CHECK();
+  k_adj_count<<<nblk((long long)B.nat_tot * 32, 256), 256, 0, st>>>(B, Pc.cutoff, b->cnt);
+  TB_LAUNCH_CHECK();
+  k_adj_scan<<<nmol, 256, 0, st>>>(B, b->cnt, b->inl, b->npair);
+  TB_LAUNCH_CHECK();
+  k_adj_fill<<<nblk((long long)B.nat_tot * 32, 256), 256, 0, st>>>(B, Pc.cutoff, b->inl, b->pair_i, b->pair_j);
+  TB_LAUNCH_CHECK();
+  // S, H0, D, Q are contiguous in the layout: one memset covers 11 N^2
+  TB_CUDA(cudaMemsetAsync(b->S, 0, (size_t)((char*)(b->Q + 6 * b->n2_tot) - (char*)b->S), st));
+  MatOut out{b->S, b->H0, b->D, b->Q};
+  const int maxsp = c->maxsh * c->maxsh;
+  const long long items = b->pair_cap * maxsp;
+  TB_CUDA(launch_integrals(Pc, B, b->npair, b->pair_i, b->pair_j, b->se, out, maxsp, items, c->lmask, st,
+                           &b->launches));
+  k_cholesky<<<nmol, 256, 0, st>>>(B, b->S, b->W, S.status, nullptr);
+  TB_LAUNCH_CHECK();
+  k_trinv<<<nmol, 256, 0, st>>>(B, b->W, b->X, S.status);
+  TB_LAUNCH_CHECK();
+  k_scf_init<<<nmol, 256, 0, st>>>(Pc, B, b->charge, b->uhf, b->erep, b->n0sh, b->q_in, S);
+  TB_LAUNCH_CHECK();
+  // ---- SCF
+  const double econv = 1.0e-6 * b->opt.accuracy, pconv = 2.0e-5 * b->opt.accuracy;
+  const int ntile64 = (int)b->tiles64.size(), ntile32 = (int)b->tiles32.size(), nchunk = (int)b->chunks32.size();
+  const int gemm_grid = std::min(ntile64, 148 * 8);
+  const size_t eig_smem = 6 * (size_t)b->nmax * sizeof(double);
+  if (eig_smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_syev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eig_smem));
+  const size_t fermi_smem = (size_t)b->nmax * sizeof(double);
+  if (fermi_smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_fermi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fermi_smem));
+  const dim3 pot_grid(nmol, nblk(std::max(b->natmax, b->nshmax), 256));
+  for (int it = 0; it < b->opt.max_iter; ++it) {
+    if (it > 0) {
+      k_mix_next<<<nmol, 256, 0, st>>>(B, b->q_in, b->dq, b->dqlast, b->qlast, b->df, b->u, b->amat, b->omega,
+                                       b->opt.max_iter, b->opt.mixer_damping, S);
+      TB_LAUNCH_CHECK();
+    }
+    k_potential<<<pot_grid, 256, 0, st>>>(Pc, B, b->q_in, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, S.active);
+    TB_LAUNCH_CHECK();
+    k_fock<<<ntile32, 256, 0, st>>>(B, b->d_tiles32, ntile32, b->S, b->H0, b->D, b->Q, b->vsh, b->vat, b->vdp,
+                                    b->vqp, b->F, S.active);
+    TB_LAUNCH_CHECK();
+    // F' = X^T F X  (T = F X in W, then F' into F)
+    k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W,
+                                      1.0, 0.0, S.active);
+    TB_LAUNCH_CHECK();
+    k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F,
+                                      1.0, 0.0, S.active);
+    TB_LAUNCH_CHECK();
+    k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->w, b->perm, S.status, S.active);
+    TB_LAUNCH_CHECK();
+    k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S);
+    TB_LAUNCH_CHECK();
+    // C = X Z (eigenvectors in ascending order through perm), P = C diag(f) C^T
+    k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr, b->W,
+                                      1.0, 0.0, S.active);
+    TB_LAUNCH_CHECK();
+    k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P,
+                                      1.0, 0.0, S.active);
+    TB_LAUNCH_CHECK();
+    k_mulliken_cols<<<nchunk, 256, 0, st>>>(B, b->d_chunks32, nchunk, b->P, b->S, b->H0, b->D, b->Q, b->colred,
+                                            S.active);
+    TB_LAUNCH_CHECK();
+    k_finalize<<<nmol, 256, 0, st>>>(Pc, B, b->colred, b->n0sh, b->mrad, b->q_in, b->dq, b->qsh_out, b->qat_out,
+                                     b->dpat_out, b->qpat_out, econv, pconv, b->opt.max_iter, S);
+    TB_LAUNCH_CHECK();
+    TB_CUDA(cudaMemcpyAsync(b->h_nactive, S.n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TB_CUDA(cudaStreamSynchronize(st));
+    if (*b->h_nactive <= 0) break;
+  }
+  return TB_OK;
+}
+
+tb_status batch_results(tb_batch* b, tb_result* out, cudaStream_t st) {
+  const int nmol = b->nmol;
+  const int NA = b->nat_tot, NS = b->nsh_tot;
+  std::vector<double> erep(nmol), eelec(nmol), eband(nmol), ets(nmol), e2(nmol), ea(nmol), e3(nmol), err(nmol),
+      dip(3 * nmol), qat(NA), qsh(NS), dp(3 * NA), qp(6 * NA);
+  std::vector<int> iscf(nmol), status(nmol), fw(nmol);
+  const MolState& S = b->ms;
+  auto cp = [&](void* dst, const void* src, size_t n) {
+    return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, st);
+  };
+  TB_CUDA(cp(erep.data(), S.e_rep, nmol * 8)); TB_CUDA(cp(eelec.data(), S.eelec, nmol * 8));
+  TB_CUDA(cp(eband.data(), S.e_band, nmol * 8)); TB_CUDA(cp(ets.data(), S.e_ts, nmol * 8));
+  TB_CUDA(cp(e2.data(), S.e_es2, nmol * 8)); TB_CUDA(cp(ea.data(), S.e_aes2, nmol * 8));
+  TB_CUDA(cp(e3.data(), S.e_es3, nmol * 8)); TB_CUDA(cp(err.data(), S.scf_error, nmol * 8));
+  TB_CUDA(cp(dip.data(), S.dipole, 3 * nmol * 8)); TB_CUDA(cp(iscf.data(), S.iscf, nmol * 4));
+  TB_CUDA(cp(status.data(), S.status, nmol * 4)); TB_CUDA(cp(fw.data(), S.fermi_warn, nmol * 4));
+  TB_CUDA(cp(qat.data(), b->qat_out, NA * 8)); TB_CUDA(cp(qsh.data(), b->qsh_out, NS * 8));
+  TB_CUDA(cp(dp.data(), b->dpat_out, 3 * NA * 8)); TB_CUDA(cp(qp.data(), b->qpat_out, 6 * NA * 8));
+  TB_CUDA(cudaStreamSynchronize(st));
+  tb_status first = TB_OK;
+  for (int m = 0; m < nmol; ++m) {
+    tb_result& r = out[m];
+    r.e_rep = erep[m]; r.e_elec = eelec[m]; r.energy = eelec[m] + erep[m];
+    r.e_band = eband[m]; r.e_ts = ets[m]; r.e_es2 = e2[m]; r.e_aes2 = ea[m]; r.e_es3 = e3[m];
+    r.scf_error = err[m]; r.iterations = iscf[m];
+    for (int k = 0; k < 3; ++k) r.dipole[k] = dip[3 * m + k];
+    int stt = status[m];
+    if (stt == kStOk && fw[m]) stt = kStFermiNotConverged;
+    r.status = stt;
+    r.nsh = b->h_soff[m + 1] - b->h_soff[m];
+    r.nao = b->h_ooff[m + 1] - b->h_ooff[m];
+    const int a0 = b->h_aoff[m], na = b->h_aoff[m + 1] - a0, s0 = b->h_soff[m];
+    if (r.qat) std::memcpy(r.qat, qat.data() + a0, na * 8);
+    if (r.qsh) std::memcpy(r.qsh, qsh.data() + s0, r.nsh * 8);
+    if (r.dpat) std::memcpy(r.dpat, dp.data() + 3 * a0, 3 * na * 8);
+    if (r.qpat) std::memcpy(r.qpat, qp.data() + 6 * a0, 6 * na * 8);
+    if (stt != kStOk && first == TB_OK) first = (tb_status)stt;
+  }
+  if (first != TB_OK) g_err = "at least one structure did not finish with TB_OK (see tb_result.status)";
+  return first;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char* tb_last_error(void) { return g_err.c_str(); }
+
+void tb_default_options(tb_options* o) {
+  std::memset(o, 0, sizeof(*o));
+  o->accuracy = 1.0;
+  o->kt = 300.0 * 3.166811563455546e-6;
+  o->max_iter = 32;
+  o->mixer_damping = 0.4;
+  o->verbosity = 0;
+  o->use_graphs = 0;
+  o->solver = 0;
+}
+
+tb_status tb_calculator_create(const char* param_file, tb_calculator** out) {
+  if (!param_file || !out) return fail(TB_BAD_INPUT, "null argument");
+  *out = nullptr;
+  auto* c = new tb_calculator();
+  std::string err;
+  if (!parse_params(param_file, c->hp, err)) { delete c; return fail(TB_PARAM_ERROR, err); }
+  const HostParams& P = c->hp;
+  const int nt = (int)P.sh.size();
+  std::vector<double> hs((size_t)nt * nt);
+  for (int i = 0; i < nt; ++i)
+    for (int j = 0; j < nt; ++j) hs[(size_t)i * nt + j] = hscale_of(P, i, j);
+  for (auto& s : P.sp) c->maxsh = std::max(c->maxsh, s.nsh);
+  for (auto& s : P.sh) c->lmask |= 1 << s.ang;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) { delete c; return fail(TB_CUDA_ERROR, std::string("no CUDA device: ") + cudaGetErrorString(e)); }
+  if (cudaMalloc(&c->d_sp, P.sp.size() * sizeof(SpeciesParam)) != cudaSuccess ||
+      cudaMalloc(&c->d_sh, P.sh.size() * sizeof(ShellParam)) != cudaSuccess ||
+      cudaMalloc(&c->d_hscale, hs.size() * sizeof(double)) != cudaSuccess) {
+    delete c;
+    return fail(TB_CUDA_ERROR, "cannot allocate parameter tables");
+  }
+  cudaMemcpy(c->d_sp, P.sp.data(), P.sp.size() * sizeof(SpeciesParam), cudaMemcpyHostToDevice);
+  cudaMemcpy(c->d_sh, P.sh.data(), P.sh.size() * sizeof(ShellParam), cudaMemcpyHostToDevice);
+  e = cudaMemcpy(c->d_hscale, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { delete c; return fail(TB_CUDA_ERROR, cudaGetErrorString(e)); }
+  DevParams& d = c->dp;
+  d.sp = c->d_sp; d.sh = c->d_sh; d.hscale = c->d_hscale;
+  d.nsp = (int)P.sp.size(); d.nshtype = nt;
+  d.gexp = P.glob("gexp", 2.0); d.kdmp3 = P.glob("kdmp3"); d.kdmp5 = P.glob("kdmp5");
+  d.mp_shift = P.glob("mp_shift"); d.mp_kexp = P.glob("mp_kexp"); d.mp_rmax = P.glob("mp_rmax");
+  d.rep_kexp = P.glob("rep_kexp"); d.rep_kexp_light = P.glob("rep_kexp_light"); d.rep_rexp = P.glob("rep_rexp");
+  d.cn_cutoff = P.glob("cn_cutoff", 25.0); d.rep_cutoff = P.glob("rep_cutoff", 25.0);
+  d.intcut = integral_cutoff(1.0);
+  d.cutoff = std::min(std::sqrt(2.0 * d.intcut / P.min_alpha), 40.0);
+  *out = c;
+  return TB_OK;
+}
+
+void tb_calculator_destroy(tb_calculator* c) { delete c; }
+int32_t tb_calculator_nspecies(const tb_calculator* c) { return c ? (int32_t)c->hp.sp.size() : 0; }
+
+double tb_get_cutoff(const tb_calculator* c, double accuracy) {
+  return std::min(std::sqrt(2.0 * integral_cutoff(accuracy) / c->hp.min_alpha), 40.0);
+}
+
+tb_status tb_basis_size(const tb_calculator* c, const tb_structure* mol, int32_t* nsh, int32_t* nao) {
+  if (!c || !mol || !nsh || !nao || !mol->id) return fail(TB_BAD_INPUT, "null argument");
+  int s = 0, o = 0;
+  for (int a = 0; a < mol->nat; ++a) {
+    const int z = mol->id[a];
+    if (z < 0 || z >= (int)c->hp.sp.size()) return fail(TB_BAD_INPUT, "bad species");
+    const SpeciesParam& sp = c->hp.sp[z];
+    for (int k = 0; k < sp.nsh; ++k) o += msao(c->hp.sh[sp.sh0 + k].ang);
+    s += sp.nsh;
+  }
+  *nsh = s; *nao = o;
+  return TB_OK;
+}
+
+tb_status tb_batch_create(tb_calculator* calc, const tb_structure* mols, int32_t nmol, const tb_options* opt,
+                          tb_batch** out) {
+  if (!calc || !mols || !out) return fail(TB_BAD_INPUT, "null argument");
+  tb_options o;
+  if (opt) o = *opt; else tb_default_options(&o);
+  auto* b = new tb_batch();
+  tb_status st = batch_build(calc, mols, nmol, &o, b, &b->own);
+  if (st != TB_OK) { delete b; return st; }
+  *out = b;
+  return TB_OK;
+}
+
+tb_status tb_batch_run(tb_batch* b, void* stream) {
+  if (!b) return fail(TB_BAD_INPUT, "null batch");
+  return batch_run(b, (cudaStream_t)stream);
+}
+
+tb_status tb_batch_results(tb_batch* b, tb_result* out, void* stream) {
+  if (!b || !out) return fail(TB_BAD_INPUT, "null argument");
+  return batch_results(b, out, (cudaStream_t)stream);
+}
+
+int64_t tb_batch_launches(const tb_batch* b) { return b ? b->launches : 0; }
+void tb_batch_destroy(tb_batch* b) { delete b; }
+
+tb_status tb_singlepoint_batch(tb_calculator* calc, const tb_structure* mols, int32_t nmol, const tb_options* opt,
+                               tb_result* out, void* stream) {
+  if (!calc || !mols || !out) return fail(TB_BAD_INPUT, "null argument");
+  tb_options o;
+  if (opt) o = *opt; else tb_default_options(&o);
+  std::lock_guard<std::mutex> lk(calc->mu);
+  tb_batch b;
+  tb_status st = batch_build(calc, mols, nmol, &o, &b, &calc->arena);
+  if (st != TB_OK) return st;
+  st = batch_run(&b, (cudaStream_t)stream);
+  if (st != TB_OK) return st;
+  return batch_results(&b, out, (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+// ====================================================================== stage entry points
+// Each runs the same device kernels as the singlepoint on one structure (or
+// a list of matrices) and copies the stage's outputs back to host buffers.
+namespace {
+
+struct OneBatch {
+  tb_batch b;
+  tb_status st = TB_OK;
+  OneBatch(tb_calculator* c, const tb_structure* mol) {
+    tb_options o;
+    tb_default_options(&o);
+    st = batch_build(c, mol, 1, &o, &b, &b.own);
+  }
+};
+
+DevParams params_for(const tb_calculator* c, double accuracy) {
+  DevParams P = c->dp;
+  P.intcut = integral_cutoff(accuracy);
+  P.cutoff = std::min(std::sqrt(2.0 * P.intcut / c->hp.min_alpha), 40.0);
+  return P;
+}
+
+tb_status d2h(void* dst, const void* src, size_t bytes) {
+  TB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+  return TB_OK;
+}
+
+tb_status run_setup_to_integrals(tb_batch* b, bool with_integrals) {
+  const DevParams P = params_for(b->calc, 1.0);
+  const DevBatch& B = b->db;
+  k_atoms<<<nblk(B.nat_tot, 128), 128>>>(P, B, b->cn, b->mrad, b->erep, b->se);
+  TB_LAUNCH_CHECK();
+  if (!with_integrals) return TB_OK;
+  k_adj_count<<<nblk((long long)B.nat_tot * 32, 256), 256>>>(B, P.cutoff, b->cnt);
+  TB_LAUNCH_CHECK();
+  k_adj_scan<<<b->nmol, 256>>>(B, b->cnt, b->inl, b->npair);
+  TB_LAUNCH_CHECK();
+  k_adj_fill<<<nblk((long long)B.nat_tot * 32, 256), 256>>>(B, P.cutoff, b->inl, b->pair_i, b->pair_j);
+  TB_LAUNCH_CHECK();
+  TB_CUDA(cudaMemset(b->S, 0, (size_t)((char*)(b->Q + 6 * b->n2_tot) - (char*)b->S)));
+  MatOut out{b->S, b->H0, b->D, b->Q};
+  const int maxsp = b->calc->maxsh * b->calc->maxsh;
+  const long long items = b->pair_cap * maxsp;
+  TB_CUDA(launch_integrals(P, B, b->npair, b->pair_i, b->pair_j, b->se, out, maxsp, items, b->calc->lmask, 0,
+                           &b->launches));
+  TB_CUDA(cudaDeviceSynchronize());
+  return TB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+tb_status tb_adjacency_list(const tb_calculator* calc, const tb_structure* mol, double cutoff, int32_t* inl,
+                            int32_t* nnl, int32_t* nlat, int32_t cap, int32_t* npair) {
+  if (!calc || !mol || !inl || !nnl || !npair) return fail(TB_BAD_INPUT, "null argument");
+  OneBatch ob(const_cast<tb_calculator*>(calc), mol);
+  if (ob.st != TB_OK) return ob.st;
+  tb_batch* b = &ob.b;
+  const DevBatch& B = b->db;
+  k_adj_count<<<nblk((long long)B.nat_tot * 32, 256), 256>>>(B, cutoff, b->cnt);
+  TB_LAUNCH_CHECK();
+  k_adj_scan<<<1, 256>>>(B, b->cnt, b->inl, b->npair);
+  TB_LAUNCH_CHECK();
+  k_adj_fill<<<nblk((long long)B.nat_tot * 32, 256), 256>>>(B, cutoff, b->inl, b->pair_i, b->pair_j);
+  TB_LAUNCH_CHECK();
+  const int nat = mol->nat;
+  std::vector<long long> l(nat);
+  int np = 0;
+  if (d2h(l.data(), b->inl, nat * sizeof(long long)) || d2h(nnl, b->cnt, nat * sizeof(int)) ||
+      d2h(&np, b->npair, sizeof(int)))
+    return TB_CUDA_ERROR;
+  for (int a = 0; a < nat; ++a) inl[a] = (int32_t)l[a];
+  *npair = np;
+  if (np > cap) return fail(TB_CAPACITY_EXCEEDED, "nlat capacity too small");
+  if (np > 0 && nlat && d2h(nlat, b->pair_j, np * sizeof(int))) return TB_CUDA_ERROR;
+  return TB_OK;
+}
+
+tb_status tb_atomic_properties(const tb_calculator* calc, const tb_structure* mol, double* cn, double* mrad,
+                               double* se) {
+  if (!calc || !mol) return fail(TB_BAD_INPUT, "null argument");
+  OneBatch ob(const_cast<tb_calculator*>(calc), mol);
+  if (ob.st != TB_OK) return ob.st;
+  tb_batch* b = &ob.b;
+  tb_status st = run_setup_to_integrals(b, false);
+  if (st != TB_OK) return st;
+  if (cn && d2h(cn, b->cn, mol->nat * 8)) return TB_CUDA_ERROR;
+  if (mrad && d2h(mrad, b->mrad, mol->nat * 8)) return TB_CUDA_ERROR;
+  if (se && d2h(se, b->se, b->nsh_tot * 8)) return TB_CUDA_ERROR;
+  return TB_OK;
+}
+
+tb_status tb_repulsion(const tb_calculator* calc, const tb_structure* mol, double* erep) {
+  if (!calc || !mol || !erep) return fail(TB_BAD_INPUT, "null argument");
+  OneBatch ob(const_cast<tb_calculator*>(calc), mol);
+  if (ob.st != TB_OK) return ob.st;
+  tb_status st = run_setup_to_integrals(&ob.b, false);
+  if (st != TB_OK) return st;
+  return d2h(erep, ob.b.erep, mol->nat * 8);
+}
+
+tb_status tb_get_hamiltonian(const tb_calculator* calc, const tb_structure* mol, double* S, double* H0, double* D,
+                             double* Q) {
+  if (!calc || !mol) return fail(TB_BAD_INPUT, "null argument");
+  OneBatch ob(const_cast<tb_calculator*>(calc), mol);
+  if (ob.st != TB_OK) return ob.st;
+  tb_batch* b = &ob.b;
+  tb_status st = run_setup_to_integrals(b, true);
+  if (st != TB_OK) return st;
+  const size_t nn = (size_t)b->n2_tot * 8;
+  if (S && d2h(S, b->S, nn)) return TB_CUDA_ERROR;
+  if (H0 && d2h(H0, b->H0, nn)) return TB_CUDA_ERROR;
+  if (D && d2h(D, b->D, 3 * nn)) return TB_CUDA_ERROR;
+  if (Q && d2h(Q, b->Q, 6 * nn)) return TB_CUDA_ERROR;
+  return TB_OK;
+}
+
+tb_status tb_coulomb_potential(const tb_calculator* calc, const tb_structure* mol, const double* qsh,
+                               const double* dpat, const double* qpat, double* vsh, double* vat, double* vdp,
+                               double* vqp) {
+  if (!calc || !mol || !qsh || !dpat || !qpat) return fail(TB_BAD_INPUT, "null argument");
+  OneBatch ob(const_cast<tb_calculator*>(calc), mol);
+  if (ob.st != TB_OK) return ob.st;
+  tb_batch* b = &ob.b;
+  tb_status st = run_setup_to_integrals(b, false);
+  if (st != TB_OK) return st;
+  const int nat = mol->nat, nsh = b->nsh_tot;
+  TB_CUDA(cudaMemcpy(b->q_in, qsh, nsh * 8, cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMemcpy(b->q_in + nsh, dpat, 3 * nat * 8, cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMemcpy(b->q_in + nsh + 3 * nat, qpat, 6 * nat * 8, cudaMemcpyHostToDevice));
+  const int one = 1;
+  TB_CUDA(cudaMemcpy(b->ms.active, &one, sizeof(int), cudaMemcpyHostToDevice));
+  const DevParams P = params_for(calc, 1.0);
+  k_potential<<<dim3(1, nblk(std::max(nat, nsh), 256)), 256>>>(P, b->db, b->q_in, b->mrad, b->vsh, b->vat, b->vdp,
+                                                               b->vqp, b->ms.active);
+  TB_LAUNCH_CHECK();
+  if (vsh && d2h(vsh, b->vsh, nsh * 8)) return TB_CUDA_ERROR;
+  if (vat && d2h(vat, b->vat, nat * 8)) return TB_CUDA_ERROR;
+  if (vdp && d2h(vdp, b->vdp, 3 * nat * 8)) return TB_CUDA_ERROR;
+  if (vqp && d2h(vqp, b->vqp, 6 * nat * 8)) return TB_CUDA_ERROR;
+  return TB_OK;
+}
+
+tb_status tb_add_pot_to_h1(const tb_calculator* calc, const tb_structure* mol, const double* S, const double* H0,
+                           const double* D, const double* Q, const double* vsh, const double* vat, const double* vdp,
+                           const double* vqp, double* F) {
+  if (!calc || !mol || !S || !H0 || !D || !Q || !vsh || !vat || !vdp || !vqp || !F)
+    return fail(TB_BAD_INPUT, "null argument");
+  OneBatch ob(const_cast<tb_calculator*>(calc), mol);
+  if (ob.st != TB_OK) return ob.st;
+  tb_batch* b = &ob.b;
+  const int nat = mol->nat, nsh = b->nsh_tot;
+  const size_t nn = (size_t)b->n2_tot * 8;
+  TB_CUDA(cudaMemcpy(b->S, S, nn, cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMemcpy(b->H0, H0, nn, cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMemcpy(b->D, D, 3 * nn, cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMemcpy(b->Q, Q, 6 * nn, cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMemcpy(b->vsh, vsh, nsh * 8, cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMemcpy(b->vat, vat, nat * 8, cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMemcpy(b->vdp, vdp, 3 * nat * 8, cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMemcpy(b->vqp, vqp, 6 * nat * 8, cudaMemcpyHostToDevice));
+  const int one = 1;
+  TB_CUDA(cudaMemcpy(b->ms.active, &one, sizeof(int), cudaMemcpyHostToDevice));
+  const int nt = (int)b->tiles32.size();
+  k_fock<<<nt, 256>>>(b->db, b->d_tiles32, nt, b->S, b->H0, b->D, b->Q, b->vsh, b->vat, b->vdp, b->vqp, b->F,
+                      b->ms.active);
+  TB_LAUNCH_CHECK();
+  return d2h(F, b->F, nn);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- matrix batches
+namespace {
+
+// Minimal batch of nmat square matrices (sizes n[i]) for the eigensolver and
+// Fermi entry points: only the AO/matrix offsets are meaningful.
+struct MatBatch {
+  Arena arena;
+  DevBatch db{};
+  MolState ms{};
+  std::vector<int4> tiles;
+  int4* d_tiles = nullptr;
+  double *S = nullptr, *X = nullptr, *W = nullptr, *F = nullptr, *Z = nullptr, *w = nullptr, *focc = nullptr;
+  int *perm = nullptr, *kdim = nullptr;
+  long long n2 = 0, no = 0;
+  int nmax = 0;
+  int64_t launches = 0;
+  tb_status build(int nmat, const int32_t* n) {
+    std::vector<int> ooff(nmat + 1, 0);
+    std::vector<long long> moff(nmat + 1, 0);
+    for (int m = 0; m < nmat; ++m) {
+      if (n[m] <= 0) return fail(TB_BAD_INPUT, "matrix size must be positive");
+      ooff[m + 1] = ooff[m] + n[m];
+      moff[m + 1] = moff[m] + (long long)n[m] * n[m];
+      nmax = std::max(nmax, (int)n[m]);
+      for (int t = 0; t < (n[m] + 63) / 64; ++t)
+        for (int u = 0; u < (n[m] + 63) / 64; ++u) tiles.push_back(make_int4(m, t, u, 0));
+    }
+    if (6 * (size_t)nmax * sizeof(double) > 220 * 1024) return fail(TB_CAPACITY_EXCEEDED, "matrix too large");
+    n2 = moff[nmat];
+    no = ooff[nmat];
+    Layout L;
+    size_t o_ooff = L.add((nmat + 1) * 4), o_moff = L.add((nmat + 1) * 8), o_t = L.add(tiles.size() * sizeof(int4));
+    size_t o_S = L.add(n2 * 8), o_X = L.add(n2 * 8), o_W = L.add(n2 * 8), o_F = L.add(n2 * 8), o_Z = L.add(n2 * 8);
+    size_t o_w = L.add(no * 8), o_f = L.add(no * 8), o_p = L.add(no * 4), o_k = L.add(nmat * 4);
+    size_t o_st = L.add(nmat * 4), o_act = L.add(nmat * 4), o_nel = L.add(2 * nmat * 8), o_ets = L.add(nmat * 8),
+           o_fw = L.add(nmat * 4), o_ef = L.add(nmat * 8), o_na = L.add(4);
+    TB_CUDA(arena.reserve(L.total));
+    char* base = arena.base;
+    TB_CUDA(cudaMemset(base, 0, L.total));
+    TB_CUDA(cudaMemcpy(base + o_ooff, ooff.data(), (nmat + 1) * 4, cudaMemcpyHostToDevice));
+    TB_CUDA(cudaMemcpy(base + o_moff, moff.data(), (nmat + 1) * 8, cudaMemcpyHostToDevice));
+    TB_CUDA(cudaMemcpy(base + o_t, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    db.nmol = nmat;
+    db.ooff = at<int>(base, o_ooff);
+    db.moff = at<long long>(base, o_moff);
+    d_tiles = at<int4>(base, o_t);
+    S = at<double>(base, o_S); X = at<double>(base, o_X); W = at<double>(base, o_W); F = at<double>(base, o_F);
+    Z = at<double>(base, o_Z); w = at<double>(base, o_w); focc = at<double>(base, o_f);
+    perm = at<int>(base, o_p); kdim = at<int>(base, o_k);
+    ms.status = at<int>(base, o_st); ms.active = at<int>(base, o_act); ms.nel = at<double>(base, o_nel);
+    ms.e_ts = at<double>(base, o_ets); ms.fermi_warn = at<int>(base, o_fw); ms.e_fermi = at<double>(base, o_ef);
+    ms.n_active = at<int>(base, o_na);
+    std::vector<int> ones(nmat, 1);
+    TB_CUDA(cudaMemcpy(ms.active, ones.data(), nmat * 4, cudaMemcpyHostToDevice));
+    return TB_OK;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const double* S, double* w, double* C) {
+  if (nmat <= 0 || !n || !H || !S || !w || !C) return fail(TB_BAD_INPUT, "null argument or empty batch");
+  MatBatch mb;
+  tb_status st = mb.build(nmat, n);
+  if (st != TB_OK) return st;
+  TB_CUDA(cudaMemcpy(mb.S, S, mb.n2 * 8, cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMemcpy(mb.F, H, mb.n2 * 8, cudaMemcpyHostToDevice));
+  const DevBatch& B = mb.db;
+  const int nt = (int)mb.tiles.size(), grid = std::min(nt, 148 * 8);
+  k_cholesky<<<nmat, 256>>>(B, mb.S, mb.W, mb.ms.status, nullptr);
+  k_trinv<<<nmat, 256>>>(B, mb.W, mb.X, mb.ms.status);
+  k_gemm<<<grid, 256>>>(B, mb.d_tiles, nt, mb.F, 0, mb.X, 0, nullptr, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);
+  k_gemm<<<grid, 256>>>(B, mb.d_tiles, nt, mb.X, 1, mb.W, 0, nullptr, nullptr, nullptr, mb.F, 1.0, 0.0, mb.ms.active);
+  const size_t smem = 6 * (size_t)mb.nmax * 8;
+  if (smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_syev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_syev<<<nmat, kEigThreads, smem>>>(B, mb.F, mb.Z, mb.w, mb.perm, mb.ms.status, mb.ms.active);
+  k_gemm<<<grid, 256>>>(B, mb.d_tiles, nt, mb.X, 0, mb.Z, 1, mb.perm, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(TB_CUDA_ERROR, cudaGetErrorString(e));
+  TB_CUDA(cudaMemcpy(w, mb.w, mb.no * 8, cudaMemcpyDeviceToHost));
+  TB_CUDA(cudaMemcpy(C, mb.W, mb.n2 * 8, cudaMemcpyDeviceToHost));
+  std::vector<int> status(nmat);
+  TB_CUDA(cudaMemcpy(status.data(), mb.ms.status, nmat * 4, cudaMemcpyDeviceToHost));
+  for (int m = 0; m < nmat; ++m)
+    if (status[m] != kStOk) return fail((tb_status)status[m], "matrix " + std::to_string(m) + " failed");
+  return TB_OK;
+}
+
+tb_status tb_fermi_filling(int32_t n, double nel, double kt, const double* emo, double* occ, double* efermi,
+                           double* ts) {
+  if (n <= 0 || !emo || !occ || !efermi || !ts) return fail(TB_BAD_INPUT, "null argument");
+  MatBatch mb;
+  tb_status st = mb.build(1, &n);
+  if (st != TB_OK) return st;
+  const double nels[2] = {nel, 0.0};
+  TB_CUDA(cudaMemcpy(mb.w, emo, n * 8, cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMemcpy(mb.ms.nel, nels, 16, cudaMemcpyHostToDevice));
+  k_fermi<<<1, 128, (size_t)n * 8>>>(mb.db, mb.w, kt, mb.focc, mb.kdim, mb.ms);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(TB_CUDA_ERROR, cudaGetErrorString(e));
+  TB_CUDA(cudaMemcpy(occ, mb.focc, n * 8, cudaMemcpyDeviceToHost));
+  TB_CUDA(cudaMemcpy(ts, mb.ms.e_ts, 8, cudaMemcpyDeviceToHost));
+  TB_CUDA(cudaMemcpy(efermi, mb.ms.e_fermi, 8, cudaMemcpyDeviceToHost));
+  int fw = 0;
+  TB_CUDA(cudaMemcpy(&fw, mb.ms.fermi_warn, 4, cudaMemcpyDeviceToHost));
+  return fw ? fail(TB_FERMI_NOT_CONVERGED, "Fermi level iteration cap reached") : TB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,74 @@
+// Kernel declarations and per-structure SCF state of the tblite-b200 engine.
+#pragma once
+
+#include "tb_common.cuh"
+
+namespace tb {
+
+constexpr int kEigThreads = 128;
+
+// Per-structure scalars of the SCF (device arrays of length nmol; nel is 2*nmol).
+struct MolState {
+  double* e_rep;
+  double* nel;
+  int* iscf;
+  int* mix_iter;
+  double* eelec;
+  int* active;
+  int* status;
+  double* e_ts;
+  double* e_band;
+  double* e_es2;
+  double* e_aes2;
+  double* e_es3;
+  double* scf_error;
+  int* fermi_warn;
+  double* dipole;   // 3*nmol
+  double* e_fermi;  // optional (may be null): Fermi level of spin channel 0
+  int* n_active;    // single counter
+};
+
+// Matrix outputs of the integral kernels (D, Q planar [3|6][N][N] per structure).
+struct MatOut {
+  double* S;
+  double* H0;
+  double* D;
+  double* Q;
+};
+
+// setup
+__global__ void k_atoms(DevParams P, DevBatch B, double* cn, double* mrad, double* erep, double* se);
+__global__ void k_adj_count(DevBatch B, double cutoff, int* cnt);
+__global__ void k_adj_scan(DevBatch B, const int* cnt, long long* inl, int* npair);
+__global__ void k_adj_fill(DevBatch B, double cutoff, const long long* inl, int* pair_i, int* pair_j);
+cudaError_t launch_integrals(const DevParams& P, const DevBatch& B, const int* npair, const int* pair_i,
+                             const int* pair_j, const double* se, const MatOut& out, int maxsp, long long items,
+                             int lmask, cudaStream_t st, int64_t* launches);
+
+// linear algebra
+__global__ void k_cholesky(DevBatch B, const double* S, double* W, int* status, const int* active);
+__global__ void k_trinv(DevBatch B, const double* W, double* X, const int* status);
+__global__ void k_gemm(DevBatch B, const int4* tiles, int ntiles, const double* Ab, int ta, const double* Bb, int tb_,
+                       const int* perm, const double* ks, const int* kdim, double* Cb, double alpha, double beta,
+                       const int* active);
+__global__ void k_syev(DevBatch B, double* Ab, double* Zb, double* wout, int* perm, int* status, const int* active);
+
+// SCF
+__global__ void k_scf_init(DevParams P, DevBatch B, const double* charge, const int* uhf, const double* erep,
+                           double* n0sh, double* q_in, MolState S);
+__global__ void k_potential(DevParams P, DevBatch B, const double* q_in, const double* mrad, double* vsh, double* vat,
+                            double* vdp, double* vqp, const int* active);
+__global__ void k_fock(DevBatch B, const int4* tiles, int ntiles, const double* S, const double* H0, const double* D,
+                       const double* Q, const double* vsh, const double* vat, const double* vdp, const double* vqp,
+                       double* F, const int* active);
+__global__ void k_fermi(DevBatch B, const double* w, double kt, double* focc, int* kdim, MolState S);
+__global__ void k_mulliken_cols(DevBatch B, const int2* chunks, int nchunks, const double* P, const double* S,
+                                const double* H0, const double* D, const double* Q, double* colred,
+                                const int* active);
+__global__ void k_finalize(DevParams P, DevBatch B, const double* colred, const double* n0sh, const double* mrad,
+                           const double* q_in, double* dq, double* qsh_out, double* qat_out, double* dpat_out,
+                           double* qpat_out, double econv, double pconv, int max_iter, MolState S);
+__global__ void k_mix_next(DevBatch B, double* q_in, const double* dq, double* dqlast, double* qlast, double* df,
+                           double* u, double* amat, double* omega, int memory, double damp, MolState S);
+
+}  // namespace tb

@@ -1,0 +1,619 @@
+// SCF iteration kernels (next_scf, reference src/scf/iterators.cu:317-424 and
+// the quoted Fortran src/scf/iterators.h:53-95), batched over structures.
+//
+// Coulomb interaction matrices are never stored: the ES2 gamma (get_amat_0d,
+// src/coulomb.cu:15-47) and the AES2 multipole tensors
+// (get_multipole_matrix_0d, :409-467) are re-evaluated from the coordinates
+// inside the potential and energy kernels, which replaces 8*(S^2 + 18 A^2)
+// bytes of matrix traffic per iteration by a few flops per pair.
+#include "tb_common.cuh"
+#include "tb_kernels.h"
+
+namespace tb {
+
+__device__ const double kMpScale[6] = {1, 2, 1, 2, 2, 1};
+
+// gamma between shell a (type ta, atom A) and shell b (type tb, atom Bq)
+__device__ inline double gamma_ab(const DevParams& P, int ta, int tbt, bool same_atom, double r2) {
+  const double gam = 0.5 * (P.sh[ta].hubbard + P.sh[tbt].hubbard);
+  if (same_atom) return gam;
+  if (P.gexp == 2.0) return 1.0 / sqrt(r2 + 1.0 / (gam * gam));
+  const double r1 = sqrt(r2);
+  return 1.0 / pow(pow(r1, P.gexp) + pow(gam, -P.gexp), 1.0 / P.gexp);
+}
+
+// AES2 damping functions fdmp3, fdmp5 (quoted Fortran, src/coulomb.cu:449-451)
+__device__ inline void aes_damp(const DevParams& P, double rA, double rB, double g1, double& f3, double& f5) {
+  const double rr = 0.5 * (rA + rB) * g1;
+  const double lr = log(rr);
+  f3 = 1.0 / (1.0 + 6.0 * exp(P.kdmp3 * lr));
+  f5 = 1.0 / (1.0 + 6.0 * exp(P.kdmp5 * lr));
+}
+
+__device__ inline void tcomp(const double* v, double* tc) {
+  tc[0] = v[0] * v[0]; tc[1] = 2 * v[0] * v[1]; tc[2] = v[1] * v[1];
+  tc[3] = 2 * v[0] * v[2]; tc[4] = 2 * v[1] * v[2]; tc[5] = v[2] * v[2];
+}
+
+// ------------------------------------------------------------ initial state
+// Per structure: repulsion sum, reference occupations (get_occupation,
+// src/h0.cu:61-91), alpha/beta split (src/xtb.cu:300-313 and
+// src/wavefunction/type.cu:3-14), charge guess, mixer reset.
+__global__ void k_scf_init(DevParams P, DevBatch B, const double* __restrict__ charge, const int* __restrict__ uhf,
+                           const double* __restrict__ erep, double* __restrict__ n0sh, double* __restrict__ q_in,
+                           MolState S) {
+  const int m = blockIdx.x;
+  __shared__ double red[32];
+  const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0;
+  const int s0 = B.soff[m], nsh = B.soff[m + 1] - s0;
+  double e = 0.0, r = 0.0;
+  for (int a = threadIdx.x; a < nat; a += blockDim.x) e += erep[a0 + a];
+  for (int s = threadIdx.x; s < nsh; s += blockDim.x) {
+    const double ro = P.sh[B.sh_type[s0 + s]].refocc;
+    n0sh[s0 + s] = ro;
+    r += ro;
+  }
+  const double etot = block_sum(e, red);
+  const double nref = block_sum(r, red);
+  const double q = charge[m];
+  // guess: q/nat per atom split over its shells by reference occupation
+  const int mo = B.mixoff[m];
+  for (int a = threadIdx.x; a < nat; a += blockDim.x) {
+    const SpeciesParam& sp = P.sp[B.id[a0 + a]];
+    double tot = 0.0;
+    for (int s = 0; s < sp.nsh; ++s) tot += P.sh[sp.sh0 + s].refocc;
+    const int is = B.at_ish[a0 + a];
+    for (int s = 0; s < sp.nsh; ++s) {
+      const double f = tot > 0.0 ? P.sh[sp.sh0 + s].refocc / tot : 1.0 / sp.nsh;
+      q_in[mo + is + s] = q / nat * f;
+    }
+    for (int k = 0; k < 9; ++k) q_in[mo + nsh + 9 * a + k] = 0.0;
+  }
+  if (threadIdx.x == 0) {
+    S.e_rep[m] = etot;
+    const double nocc = nref - q;
+    const long long inel = llround(nocc);
+    const int nuhf = ((uhf[m] % 2) == (int)(inel % 2)) ? uhf[m] : (int)(inel % 2);
+    const double diff = fmin((double)nuhf, nocc), ntmp = nocc - diff;
+    S.nel[2 * m] = ntmp / 2 + diff;
+    S.nel[2 * m + 1] = ntmp / 2;
+    S.iscf[m] = 0;
+    S.mix_iter[m] = 0;
+    S.eelec[m] = 0.0;
+    S.active[m] = S.status[m] == kStOk ? 1 : 0;
+    if (S.active[m]) atomicAdd(S.n_active, 1);
+  }
+}
+
+// ------------------------------------------------------------ potentials
+// tb_coulomb::get_potential for the mixed input moments q_in = [qsh, dpat,
+// qpat]: ES2 (vsh += gamma qsh), ES3 (vsh += qsh^2 dGamma), AES2 (the five
+// gemv of the quoted Fortran src/coulomb.cu:665-676) and the on-site kernels
+// (get_kernel_potential, :564-589).  grid = (structure, target chunk).
+__global__ void k_potential(DevParams P, DevBatch B, const double* __restrict__ q_in,
+                            const double* __restrict__ mrad, double* __restrict__ vsh, double* __restrict__ vat,
+                            double* __restrict__ vdp, double* __restrict__ vqp, const int* __restrict__ active) {
+  const int m = blockIdx.x;
+  if (!active[m]) return;
+  const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0;
+  const int s0 = B.soff[m], nsh = B.soff[m + 1] - s0;
+  const double* qsh = q_in + B.mixoff[m];
+  const double* dp = qsh + nsh;
+  const double* qp = dp + 3 * nat;
+  const int t = blockIdx.y * blockDim.x + threadIdx.x;
+  const double* xyz = B.xyz + 3 * a0;
+  // shells
+  if (t < nsh) {
+    const int ta = B.sh_type[s0 + t], A = B.sh_at[s0 + t];
+    double v = 0.0;
+    for (int b = 0; b < nsh; ++b) {
+      const int Bq = B.sh_at[s0 + b];
+      const double dx = xyz[3 * A] - xyz[3 * Bq], dy = xyz[3 * A + 1] - xyz[3 * Bq + 1], dz = xyz[3 * A + 2] - xyz[3 * Bq + 2];
+      v += gamma_ab(P, ta, B.sh_type[s0 + b], A == Bq, dx * dx + dy * dy + dz * dz) * qsh[b];
+    }
+    v += qsh[t] * qsh[t] * P.sh[ta].hubbard_deriv;
+    vsh[s0 + t] = v;
+  }
+  // atoms
+  if (t < nat) {
+    const int A = t;
+    double va = 0.0, vd[3] = {0, 0, 0}, vq[6] = {0, 0, 0, 0, 0, 0};
+    const double rA = mrad[a0 + A];
+    for (int Bq = 0; Bq < nat; ++Bq) {
+      if (Bq == A) continue;
+      const double v[3] = {xyz[3 * Bq] - xyz[3 * A], xyz[3 * Bq + 1] - xyz[3 * A + 1], xyz[3 * Bq + 2] - xyz[3 * A + 2]};
+      const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+      const double g1 = 1.0 / sqrt(r2), g3 = g1 * g1 * g1, g5 = g3 * g1 * g1;
+      double f3, f5;
+      aes_damp(P, rA, mrad[a0 + Bq], g1, f3, f5);
+      // qat of atom Bq from its shells
+      const int isb = B.at_ish[a0 + Bq], nsb = P.sp[B.id[a0 + Bq]].nsh;
+      double qb = 0.0;
+      for (int s = 0; s < nsb; ++s) qb += qsh[isb + s];
+      const double* db = dp + 3 * Bq;
+      const double* qpb = qp + 6 * Bq;
+      const double vdb = v[0] * db[0] + v[1] * db[1] + v[2] * db[2];
+      double tc[6];
+      tcomp(v, tc);
+      for (int k = 0; k < 3; ++k) vd[k] += v[k] * g3 * f3 * qb + (g3 * db[k] - 3.0 * v[k] * vdb * g5) * f5;
+      for (int c = 0; c < 6; ++c) vq[c] += tc[c] * g5 * f5 * qb;
+      double tq = 0.0;
+      for (int c = 0; c < 6; ++c) tq += tc[c] * qpb[c];
+      va += -vdb * g3 * f3 + tq * g5 * f5;
+    }
+    const SpeciesParam& sp = P.sp[B.id[a0 + A]];
+    for (int k = 0; k < 3; ++k) vd[k] += 2.0 * sp.dkernel * dp[3 * A + k];
+    for (int c = 0; c < 6; ++c) vq[c] += 2.0 * sp.qkernel * qp[6 * A + c] * kMpScale[c];
+    vat[a0 + A] = va;
+    for (int k = 0; k < 3; ++k) vdp[3 * (a0 + A) + k] = vd[k];
+    for (int c = 0; c < 6; ++c) vqp[6 * (a0 + A) + c] = vq[c];
+  }
+}
+
+// ------------------------------------------------------------ Fock build
+// add_pot_to_h1 (src/scf/potential.cu:224-272 with the quoted add_vat_to_vsh,
+// add_vsh_to_vao, add_vao_to_h1 and add_vmp_to_h1): 32x32 tiles, the
+// transposed D/Q elements staged through shared memory.
+__global__ void __launch_bounds__(256) k_fock(DevBatch B, const int4* __restrict__ tiles, int ntiles,
+                                              const double* __restrict__ S, const double* __restrict__ H0,
+                                              const double* __restrict__ D, const double* __restrict__ Q,
+                                              const double* __restrict__ vsh, const double* __restrict__ vat,
+                                              const double* __restrict__ vdp, const double* __restrict__ vqp,
+                                              double* __restrict__ F, const int* __restrict__ active) {
+  __shared__ double T[32][33];
+  const int t = blockIdx.x;
+  if (t >= ntiles) return;
+  const int4 tl = tiles[t];
+  const int m = tl.x;
+  if (!active[m]) return;
+  const int n = B.ooff[m + 1] - B.ooff[m];
+  const long long mo = B.moff[m], nn = (long long)n * n;
+  const int o0 = B.ooff[m], a0 = B.aoff[m], s0 = B.soff[m];
+  const int r0 = tl.y * 32, c0 = tl.z * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 rows of 32
+  double acc[4];
+  int mu[4];
+  const int nu = c0 + tx;
+  const bool nu_ok = nu < n;
+  const int at_nu = nu_ok ? B.ao_at[o0 + nu] : 0;
+  const double vao_nu = nu_ok ? vsh[s0 + B.ao_sh[o0 + nu]] + vat[a0 + at_nu] : 0.0;
+  for (int r = 0; r < 4; ++r) {
+    mu[r] = r0 + ty + 8 * r;
+    acc[r] = 0.0;
+    if (mu[r] < n && nu_ok) {
+      const int at_mu = B.ao_at[o0 + mu[r]];
+      const double vao_mu = vsh[s0 + B.ao_sh[o0 + mu[r]]] + vat[a0 + at_mu];
+      const long long e = mo + (long long)mu[r] * n + nu;
+      acc[r] = H0[e] - S[e] * 0.5 * (vao_mu + vao_nu);
+    }
+  }
+  // moment planes: -0.5 * (M[k][mu][nu] v[at(nu)][k] + M[k][nu][mu] v[at(mu)][k])
+  for (int plane = 0; plane < 9; ++plane) {
+    const double* M = plane < 3 ? D + 3 * mo + plane * nn : Q + 6 * mo + (plane - 3) * nn;
+    const double* V = plane < 3 ? vdp : vqp;
+    const int stride = plane < 3 ? 3 : 6, k = plane < 3 ? plane : plane - 3;
+    // stage the transposed tile M[c0.., r0..]
+    __syncthreads();
+    for (int r = 0; r < 4; ++r) {
+      const int row = c0 + ty + 8 * r, col = r0 + tx;
+      T[ty + 8 * r][tx] = (row < n && col < n) ? M[(long long)row * n + col] : 0.0;
+    }
+    __syncthreads();
+    const double vnu = nu_ok ? V[stride * (a0 + at_nu) + k] : 0.0;
+    for (int r = 0; r < 4; ++r) {
+      if (mu[r] >= n || !nu_ok) continue;
+      const double vmu = V[stride * (a0 + B.ao_at[o0 + mu[r]]) + k];
+      const double direct = M[(long long)mu[r] * n + nu];
+      const double trans = T[tx][ty + 8 * r];  // M[nu][mu]
+      acc[r] -= 0.5 * (direct * vnu + trans * vmu);
+    }
+  }
+  for (int r = 0; r < 4; ++r)
+    if (mu[r] < n && nu_ok) F[mo + (long long)mu[r] * n + nu] = acc[r];
+}
+
+// ------------------------------------------------------------ Fermi
+// get_fermi_filling (src/wavefunction/fermi.cu:6-124) on the ascending
+// eigenvalues: aufbau guess, Newton on E_F safeguarded by bisection, tolerance
+// |N(E_F) - homo| <= 1e-10, entropy -TS over all 0 < f < 1.  Writes the total
+// occupation per orbital (both spin channels, nspin = 1) and K = number of
+// leading nonzero occupations.
+__device__ double fermi_channel(int n, double nel, double kt, const double* w, double* occ, double* red,
+                                int& ok, double& efermi) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  int homo = (int)floor(nel);
+  const double frac = fmod(nel, 1.0);
+  for (int i = tid; i < n; i += nt) occ[i] = i < homo ? 1.0 : (i == homo ? frac : 0.0);
+  if (frac > 0.5) homo += 1;
+  ok = 1;
+  efermi = 0.0;
+  if (homo <= 0) { __syncthreads(); return 0.0; }
+  const double occt = (double)homo;
+  double ef = 0.5 * (w[max(homo - 1, 0)] + w[min(homo, n - 1)]);
+  double lo = w[0] - 1.0, hi = w[n - 1] + 1.0;
+  ok = 0;
+  for (int cycle = 0; cycle < 200; ++cycle) {
+    double tot = 0.0, dtot = 0.0;
+    for (int i = tid; i < n; i += nt) {
+      const double x = (w[i] - ef) / kt;
+      double f = 0.0, df = 0.0;
+      if (x < 50.0) {
+        const double ex = exp(x);
+        f = 1.0 / (ex + 1.0);
+        df = ex / (kt * (ex + 1.0) * (ex + 1.0));
+      }
+      occ[i] = f;
+      tot += f;
+      dtot += df;
+    }
+    tot = block_sum(tot, red);
+    dtot = block_sum(dtot, red);
+    if (fabs(occt - tot) <= 1e-10) { ok = 1; break; }
+    if (tot < occt) lo = ef; else hi = ef;
+    double next = ef + (occt - tot) / dtot;
+    if (!(dtot > 0.0) || !(next > lo && next < hi)) next = 0.5 * (lo + hi);
+    ef = next;
+  }
+  efermi = ef;
+  double s = 0.0;
+  for (int i = tid; i < n; i += nt) {
+    const double o = occ[i];
+    if (o > 0.0 && o < 1.0) s += o * log(o) + (1.0 - o) * log(1.0 - o);
+  }
+  return block_sum(s, red) * kt;
+}
+
+__global__ void k_fermi(DevBatch B, const double* __restrict__ w, double kt, double* __restrict__ focc,
+                        int* __restrict__ kdim, MolState S) {
+  const int m = blockIdx.x;
+  if (!S.active[m]) return;
+  if (S.status[m] != kStOk) {  // eigensolver failure: retire the structure
+    if (threadIdx.x == 0) { S.active[m] = 0; atomicSub(S.n_active, 1); }
+    return;
+  }
+  const int n = B.ooff[m + 1] - B.ooff[m];
+  const int o0 = B.ooff[m];
+  extern __shared__ double occ[];  // n
+  __shared__ double red[32];
+  __shared__ int last;
+  double* f = focc + o0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) f[i] = 0.0;
+  double ts = 0.0;
+  int ok_all = 1;
+  const double na = S.nel[2 * m], nb = S.nel[2 * m + 1];
+  for (int spin = 0; spin < 2; ++spin) {
+    if (spin == 1 && na == nb) {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) f[i] *= 2.0;
+      ts *= 2.0;
+      break;
+    }
+    int ok;
+    double ef;
+    __syncthreads();
+    ts += fermi_channel(n, spin == 0 ? na : nb, kt, w + o0, occ, red, ok, ef);
+    ok_all &= ok;
+    if (spin == 0 && S.e_fermi && threadIdx.x == 0) S.e_fermi[m] = ef;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) f[i] += occ[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) last = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    if (f[i] > 0.0) atomicMax(&last, i + 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    kdim[m] = last;
+    S.e_ts[m] = ts;
+    if (!ok_all) S.fermi_warn[m] = 1;
+  }
+}
+
+// ------------------------------------------------------------ Mulliken
+// Column sums of P o {S, D, Q, H0} (get_mulliken_shell_charges,
+// src/wavefunction/mulliken.h:8-34; get_mulliken_atomic_multipoles,
+// src/wavefunction/mulliken.cu:40-64; get_electronic_energy,
+// src/scf/iterators.cu:254-272).  One CTA = 32 columns x 8 row groups;
+// results per column in colred[ao][12] (deterministic order).
+__global__ void __launch_bounds__(256) k_mulliken_cols(DevBatch B, const int2* __restrict__ chunks, int nchunks,
+                                                       const double* __restrict__ P, const double* __restrict__ S,
+                                                       const double* __restrict__ H0, const double* __restrict__ D,
+                                                       const double* __restrict__ Q, double* __restrict__ colred,
+                                                       const int* __restrict__ active) {
+  __shared__ double part[8][11][32];
+  const int c = blockIdx.x;
+  if (c >= nchunks) return;
+  const int2 ch = chunks[c];
+  const int m = ch.x;
+  if (!active[m]) return;
+  const int n = B.ooff[m + 1] - B.ooff[m];
+  const long long mo = B.moff[m], nn = (long long)n * n;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int nu = ch.y * 32 + tx;
+  double acc[11];
+  for (int k = 0; k < 11; ++k) acc[k] = 0.0;
+  if (nu < n) {
+    for (int mu = ty; mu < n; mu += 8) {
+      const long long e = (long long)mu * n + nu;
+      const double p = P[mo + e];
+      acc[0] += p * S[mo + e];
+      acc[1] += p * H0[mo + e];
+      for (int k = 0; k < 3; ++k) acc[2 + k] += p * D[3 * mo + k * nn + e];
+      for (int k = 0; k < 6; ++k) acc[5 + k] += p * Q[6 * mo + k * nn + e];
+    }
+  }
+  for (int k = 0; k < 11; ++k) part[ty][k][tx] = acc[k];
+  __syncthreads();
+  if (ty == 0 && nu < n) {
+    double* out = colred + 12 * (long long)(B.ooff[m] + nu);
+    for (int k = 0; k < 11; ++k) {
+      double s = 0.0;
+      for (int g = 0; g < 8; ++g) s += part[g][k][tx];
+      out[k] = s;
+    }
+  }
+}
+
+// ------------------------------------------------------------ finalize
+// Per structure: reduce the column sums to shell charges and atomic
+// multipoles, evaluate the Coulomb energies with the output moments
+// (tb_coulomb::get_energy: ES2 quoted :111-136, AES2 quoted :697-727, ES3
+// quoted :866-899), diff the mixer (diff_mixer), the energy/density
+// convergence test of xtb_singlepoint and the iteration bookkeeping.
+__global__ void k_finalize(DevParams P, DevBatch B, const double* __restrict__ colred, const double* __restrict__ n0sh,
+                           const double* __restrict__ mrad, const double* __restrict__ q_in, double* __restrict__ dq,
+                           double* __restrict__ qsh_out, double* __restrict__ qat_out, double* __restrict__ dpat_out,
+                           double* __restrict__ qpat_out, double econv, double pconv, int max_iter, MolState S) {
+  const int m = blockIdx.x;
+  if (!S.active[m]) return;
+  __shared__ double red[32];
+  const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0;
+  const int s0 = B.soff[m], nsh = B.soff[m + 1] - s0;
+  const int o0 = B.ooff[m], n = B.ooff[m + 1] - o0;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  // shells: qsh = n0sh - sum over the shell's AO columns
+  for (int s = tid; s < nsh; s += nt) {
+    const int i0 = B.sh_iao[s0 + s], na = msao(P.sh[B.sh_type[s0 + s]].ang);
+    double v = 0.0;
+    for (int x = 0; x < na; ++x) v += colred[12 * (long long)(o0 + i0 + x)];
+    qsh_out[s0 + s] = n0sh[s0 + s] - v;
+  }
+  double eb = 0.0;
+  for (int x = tid; x < n; x += nt) eb += colred[12 * (long long)(o0 + x) + 1];
+  const double e_band = block_sum(eb, red);
+  __syncthreads();
+  // atoms: dipole/quadrupole over the atom's AO columns, qat over its shells
+  for (int a = tid; a < nat; a += nt) {
+    const int is = B.at_ish[a0 + a];
+    const SpeciesParam& sp = P.sp[B.id[a0 + a]];
+    double q = 0.0, d[3] = {0, 0, 0}, qq[6] = {0, 0, 0, 0, 0, 0};
+    for (int s = 0; s < sp.nsh; ++s) {
+      q += qsh_out[s0 + is + s];
+      const int i0 = B.sh_iao[s0 + is + s], na = msao(P.sh[sp.sh0 + s].ang);
+      for (int x = 0; x < na; ++x) {
+        const double* c = colred + 12 * (long long)(o0 + i0 + x);
+        for (int k = 0; k < 3; ++k) d[k] -= c[2 + k];
+        for (int k = 0; k < 6; ++k) qq[k] -= c[5 + k];
+      }
+    }
+    qat_out[a0 + a] = q;
+    for (int k = 0; k < 3; ++k) dpat_out[3 * (a0 + a) + k] = d[k];
+    for (int k = 0; k < 6; ++k) qpat_out[6 * (a0 + a) + k] = qq[k];
+  }
+  __syncthreads();
+  const double* xyz = B.xyz + 3 * a0;
+  const double* qs = qsh_out + s0;
+  // ES2 + ES3
+  double e2 = 0.0, e3 = 0.0;
+  for (int a = tid; a < nsh; a += nt) {
+    const int ta = B.sh_type[s0 + a], A = B.sh_at[s0 + a];
+    double v = 0.0;
+    for (int b = 0; b < nsh; ++b) {
+      const int Bq = B.sh_at[s0 + b];
+      const double dx = xyz[3 * A] - xyz[3 * Bq], dy = xyz[3 * A + 1] - xyz[3 * Bq + 1], dz = xyz[3 * A + 2] - xyz[3 * Bq + 2];
+      v += gamma_ab(P, ta, B.sh_type[s0 + b], A == Bq, dx * dx + dy * dy + dz * dz) * qs[b];
+    }
+    e2 += 0.5 * v * qs[a];
+    e3 += qs[a] * qs[a] * qs[a] * P.sh[ta].hubbard_deriv / 3.0;
+  }
+  // AES2: vd = sd q + 0.5 dd dp, vq = sq q; E = dp.vd + qp.vq + kernels
+  double ea = 0.0;
+  for (int A = tid; A < nat; A += nt) {
+    const double* dA = dpat_out + 3 * (a0 + A);
+    const double* qA = qpat_out + 6 * (a0 + A);
+    double vd[3] = {0, 0, 0}, vq[6] = {0, 0, 0, 0, 0, 0};
+    const double rA = mrad[a0 + A];
+    for (int Bq = 0; Bq < nat; ++Bq) {
+      if (Bq == A) continue;
+      const double v[3] = {xyz[3 * Bq] - xyz[3 * A], xyz[3 * Bq + 1] - xyz[3 * A + 1], xyz[3 * Bq + 2] - xyz[3 * A + 2]};
+      const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+      const double g1 = 1.0 / sqrt(r2), g3 = g1 * g1 * g1, g5 = g3 * g1 * g1;
+      double f3, f5;
+      aes_damp(P, rA, mrad[a0 + Bq], g1, f3, f5);
+      const double qb = qat_out[a0 + Bq];
+      const double* db = dpat_out + 3 * (a0 + Bq);
+      const double vdb = v[0] * db[0] + v[1] * db[1] + v[2] * db[2];
+      double tc[6];
+      tcomp(v, tc);
+      for (int k = 0; k < 3; ++k) vd[k] += v[k] * g3 * f3 * qb + 0.5 * (g3 * db[k] - 3.0 * v[k] * vdb * g5) * f5;
+      for (int c = 0; c < 6; ++c) vq[c] += tc[c] * g5 * f5 * qb;
+    }
+    const SpeciesParam& sp = P.sp[B.id[a0 + A]];
+    double dd = 0.0, qq = 0.0;
+    for (int k = 0; k < 3; ++k) { ea += dA[k] * vd[k]; dd += dA[k] * dA[k]; }
+    for (int c = 0; c < 6; ++c) { ea += qA[c] * vq[c]; qq += qA[c] * qA[c] * kMpScale[c]; }
+    ea += sp.dkernel * dd + sp.qkernel * qq;
+  }
+  const double e_es2 = block_sum(e2, red);
+  const double e_es3 = block_sum(e3, red);
+  const double e_aes2 = block_sum(ea, red);
+  // mixer diff: dq = [qsh, dpat, qpat]_out - q_in
+  const int mo = B.mixoff[m], ndim = nsh + 9 * nat;
+  double err = 0.0;
+  for (int i = tid; i < ndim; i += nt) {
+    double out;
+    if (i < nsh) out = qsh_out[s0 + i];
+    else if (i < nsh + 3 * nat) out = dpat_out[3 * a0 + (i - nsh)];
+    else out = qpat_out[6 * a0 + (i - nsh - 3 * nat)];
+    const double x = out - q_in[mo + i];
+    dq[mo + i] = x;
+    err += x * x;
+  }
+  err = block_sum(err, red);
+  if (tid == 0) {
+    const double elast = S.eelec[m];
+    const double eelec = e_band + S.e_ts[m] + e_es2 + e_aes2 + e_es3;
+    const double error = sqrt(err / ndim);
+    S.eelec[m] = eelec;
+    S.e_band[m] = e_band;
+    S.e_es2[m] = e_es2;
+    S.e_aes2[m] = e_aes2;
+    S.e_es3[m] = e_es3;
+    S.scf_error[m] = error;
+    const int it = S.iscf[m] + 1;
+    S.iscf[m] = it;
+    const bool conv = fabs(eelec - elast) < econv && error < pconv;
+    if (conv) {
+      S.active[m] = 0;
+    } else if (it >= max_iter) {
+      S.active[m] = 0;
+      S.status[m] = kStScfNotConverged;
+    }
+    if (!S.active[m]) atomicSub(S.n_active, 1);
+  }
+  // molecular dipole sum_A q_A R_A + mu_A (deterministic fixed-order sum)
+  for (int k = 0; k < 3; ++k) {
+    double dsum = 0.0;
+    for (int a = tid; a < nat; a += nt) dsum += qat_out[a0 + a] * xyz[3 * a + k] + dpat_out[3 * (a0 + a) + k];
+    dsum = block_sum(dsum, red);
+    if (tid == 0) S.dipole[3 * m + k] = dsum;
+  }
+}
+
+// ------------------------------------------------------------ Broyden
+// Modified Broyden mixing (D. D. Johnson, PRB 38, 12807 (1988)); the update
+// step `next` is missing from the reference (D19), set/diff follow
+// src/scf/broyden.cu:47-72.  Runs at the start of every iteration after the
+// first and leaves the new input moments in q_in.
+__global__ void k_mix_next(DevBatch B, double* __restrict__ q_in, const double* __restrict__ dq,
+                           double* __restrict__ dqlast, double* __restrict__ qlast, double* __restrict__ df,
+                           double* __restrict__ u, double* __restrict__ amat, double* __restrict__ omega, int memory,
+                           double damp, MolState S) {
+  const int m = blockIdx.x;
+  if (!S.active[m] || S.iscf[m] == 0) return;
+  const int nat = B.aoff[m + 1] - B.aoff[m], nsh = B.soff[m + 1] - B.soff[m];
+  const int n = nsh + 9 * nat, mo = B.mixoff[m];
+  const long long ho = (long long)mo * memory;  // history slab of this structure
+  double* q = q_in + mo;
+  const double* d = dq + mo;
+  double* dl = dqlast + mo;
+  double* ql = qlast + mo;
+  double* DF = df + ho;
+  double* U = u + ho;
+  double* a = amat + (long long)m * memory * memory;
+  double* om = omega + (long long)m * memory;
+  __shared__ double red[32];
+  __shared__ double cvec[64], gvec[64], M[64 * 64];
+  __shared__ int slot[64];
+  __shared__ double sh_inv;
+  __shared__ int sh_ok;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+  const int iter = S.mix_iter[m] + 1;
+  if (iter == 1) {
+    for (int i = tid; i < n; i += nt) { dl[i] = d[i]; ql[i] = q[i]; q[i] += damp * d[i]; }
+    if (tid == 0) S.mix_iter[m] = iter;
+    return;
+  }
+  const double omega0 = 0.01, minw = 1.0, maxw = 100000.0, wfac = 0.01;
+  const int itn = iter - 1;
+  const int s = (itn - 1) % memory;
+  const int nh = min(itn, memory);
+  double p1 = 0.0, p2 = 0.0;
+  for (int i = tid; i < n; i += nt) {
+    const double x = d[i] - dl[i];
+    DF[(long long)s * n + i] = x;
+    p1 += d[i] * d[i];
+    p2 += x * x;
+  }
+  const double nrm = sqrt(block_sum(p1, red));
+  const double dn = block_sum(p2, red);
+  if (tid == 0) {
+    double w = nrm > wfac / maxw ? wfac / nrm : maxw;
+    if (w < minw) w = minw;
+    om[s] = w;
+    sh_inv = 1.0 / fmax(sqrt(dn), 2.220446049250313e-16);
+  }
+  __syncthreads();
+  const double inv = sh_inv;
+  for (int i = tid; i < n; i += nt) DF[(long long)s * n + i] *= inv;
+  if (tid < nh) slot[tid] = (itn - nh + tid) % memory;
+  __syncthreads();
+  // a(t, s) = df_t . df_s and c_t = w_t df_t . dq (one warp per history entry)
+  for (int h = wid; h < nh; h += nw) {
+    const int t = slot[h];
+    double ad = 0.0, cd = 0.0;
+    for (int i = lane; i < n; i += 32) {
+      const double x = DF[(long long)t * n + i];
+      ad += x * DF[(long long)s * n + i];
+      cd += x * d[i];
+    }
+    ad = warp_sum(ad);
+    cd = warp_sum(cd);
+    if (lane == 0) {
+      a[t * memory + s] = ad;
+      a[s * memory + t] = ad;
+      cvec[h] = om[t] * cd;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int h = 0; h < nh; ++h)
+      for (int k = 0; k < nh; ++k)
+        M[h * nh + k] = om[slot[h]] * om[slot[k]] * a[slot[h] * memory + slot[k]] + (h == k ? omega0 * omega0 : 0.0);
+    for (int h = 0; h < nh; ++h) gvec[h] = cvec[h];
+    int ok = 1;
+    for (int col = 0; col < nh && ok; ++col) {
+      int piv = col;
+      for (int r = col + 1; r < nh; ++r)
+        if (fabs(M[r * nh + col]) > fabs(M[piv * nh + col])) piv = r;
+      if (M[piv * nh + col] == 0.0) { ok = 0; break; }
+      if (piv != col) {
+        for (int k = 0; k < nh; ++k) { const double tmp = M[col * nh + k]; M[col * nh + k] = M[piv * nh + k]; M[piv * nh + k] = tmp; }
+        const double tmp = gvec[col]; gvec[col] = gvec[piv]; gvec[piv] = tmp;
+      }
+      for (int r = col + 1; r < nh; ++r) {
+        const double f = M[r * nh + col] / M[col * nh + col];
+        for (int k = col; k < nh; ++k) M[r * nh + k] -= f * M[col * nh + k];
+        gvec[r] -= f * gvec[col];
+      }
+    }
+    if (ok)
+      for (int r = nh - 1; r >= 0; --r) {
+        double t = gvec[r];
+        for (int k = r + 1; k < nh; ++k) t -= M[r * nh + k] * gvec[k];
+        gvec[r] = t / M[r * nh + r];
+      }
+    for (int h = 0; h < nh; ++h) cvec[h] = om[slot[h]] * gvec[h];  // w_h * gamma_h
+    sh_ok = ok;
+  }
+  __syncthreads();
+  if (!sh_ok) {
+    if (tid == 0) { S.status[m] = kStScfNotConverged; S.active[m] = 0; atomicSub(S.n_active, 1); }
+    return;
+  }
+  for (int i = tid; i < n; i += nt) {
+    U[(long long)s * n + i] = damp * DF[(long long)s * n + i] + inv * (q[i] - ql[i]);
+  }
+  __syncthreads();
+  for (int i = tid; i < n; i += nt) {
+    const double qi = q[i];
+    dl[i] = d[i];
+    ql[i] = qi;
+    double v = qi + damp * d[i];
+    for (int h = 0; h < nh; ++h) v -= cvec[h] * U[(long long)slot[h] * n + i];
+    q[i] = v;
+  }
+  if (tid == 0) S.mix_iter[m] = iter;
+}
+
+}  // namespace tb

@@ -1,0 +1,465 @@
+// Setup kernels of the singlepoint (run once per structure batch): coordination
+// numbers, multipole damping radii, self-energies, repulsion, the half
+// neighbour list, and the overlap/dipole/quadrupole/H0 integral matrices.
+//
+// Layout: every structure of a batch owns contiguous slices of the packed
+// atom/shell/AO vectors and an N x N slice (N = nao) of each matrix arena;
+// D and Q are [3][N][N] / [6][N][N] planar per structure.
+#include "tb_common.cuh"
+#include "tb_kernels.h"
+
+#include <algorithm>
+
+namespace tb {
+
+// ---------------------------------------------------------------- atoms
+// GFN double-exponential counting function (published GFN2-xTB method; the
+// reference calls exp_count without quoting it, src/coulomb.cu:220-222).
+__device__ inline double exp_count(double k, double r, double r0) {
+  return 1.0 / (1.0 + exp(-k * (r0 / r - 1.0)));
+}
+
+// One thread per atom: CN (ncoord_dexp, src/coulomb.cu:173-246), repulsion
+// energy share (get_repulsion_derivs, src/xtb.cu:62-91), multipole damping
+// radius (get_mrad, src/coulomb.cu:387-398) and shell self-energies
+// (get_selfenergy, src/h0.cu:137-170).
+__global__ void k_atoms(DevParams P, DevBatch B, double* __restrict__ cn, double* __restrict__ mrad,
+                        double* __restrict__ erep, double* __restrict__ se) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= B.nat_tot) return;
+  const int m = B.at_mol[a];
+  const int a0 = B.aoff[m], a1 = B.aoff[m + 1];
+  const double xa = B.xyz[3 * a], ya = B.xyz[3 * a + 1], za = B.xyz[3 * a + 2];
+  const SpeciesParam si = P.sp[B.id[a]];
+  const double ka = 10.0, kb = 20.0, rshift = 2.0;
+  const double cn2 = P.cn_cutoff * P.cn_cutoff, rep2 = P.rep_cutoff * P.rep_cutoff;
+  double c = 0.0, e = 0.0;
+  for (int b = a0; b < a1; ++b) {
+    if (b == a) continue;
+    const double dx = xa - B.xyz[3 * b], dy = ya - B.xyz[3 * b + 1], dz = za - B.xyz[3 * b + 2];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 < 1.0e-12) continue;
+    const SpeciesParam& sj = P.sp[B.id[b]];
+    const double r1 = sqrt(r2);
+    if (r2 <= cn2) {
+      const double rc = si.rcov + sj.rcov;
+      c += exp_count(ka, r1, rc) * exp_count(kb, r1, rc + rshift);
+    }
+    if (r2 <= rep2) {
+      const double alpha = sqrt(si.rep_alpha * sj.rep_alpha);
+      const double zeff = si.rep_zeff * sj.rep_zeff;
+      const double kexp = (si.z <= 2 && sj.z <= 2) ? P.rep_kexp_light : P.rep_kexp;
+      const double r1k = pow(r1, kexp);
+      const double r1r = pow(r1, P.rep_rexp);
+      e += 0.5 * zeff * exp(-alpha * r1k) / r1r;
+    }
+  }
+  cn[a] = c;
+  erep[a] = e;
+  const double t1 = exp(-P.mp_kexp * (c - si.mp_vcn - P.mp_shift));
+  mrad[a] = si.mp_rad + (P.mp_rmax - si.mp_rad) / (1.0 + t1);
+  const int s0 = B.soff[m] + B.at_ish[a];
+  for (int s = 0; s < si.nsh; ++s) {
+    const ShellParam& sh = P.sh[si.sh0 + s];
+    se[s0 + s] = sh.selfenergy - sh.kcn * c;
+  }
+}
+
+// ---------------------------------------------------------------- neighbour list
+// Half list of generate() (src/adjlist.cu:15-44): for atom i all j < i with
+// eps <= r2 <= cutoff^2, j ascending.  r2 is evaluated x, y, z in that order
+// with explicit round-to-nearest operations (no contraction) so that the list
+// is bit-identical to the FP64 restatement.
+__device__ inline bool adj_keep(const double* xyz, int i, int j, double cutoff2) {
+  const double v0 = __dsub_rn(xyz[3 * i + 0], xyz[3 * j + 0]);
+  const double v1 = __dsub_rn(xyz[3 * i + 1], xyz[3 * j + 1]);
+  const double v2 = __dsub_rn(xyz[3 * i + 2], xyz[3 * j + 2]);
+  double r2 = __dmul_rn(v0, v0);
+  r2 = __dadd_rn(r2, __dmul_rn(v1, v1));
+  r2 = __dadd_rn(r2, __dmul_rn(v2, v2));
+  return !(r2 < 2.220446049250313e-16 || r2 > cutoff2);
+}
+
+// one warp per atom: number of kept j < i
+__global__ void k_adj_count(DevBatch B, double cutoff, int* __restrict__ cnt) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= B.nat_tot) return;
+  const int a = warp, m = B.at_mol[a], a0 = B.aoff[m];
+  const double c2 = cutoff * cutoff;
+  int n = 0;
+  for (int b = a0 + lane; b < a; b += 32) n += adj_keep(B.xyz, a, b, c2) ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+  if (lane == 0) cnt[a] = n;
+}
+
+// one block per structure: exclusive scan of the counts -> inl (absolute pair
+// offsets inside the structure's pair slice), npair per structure.
+__global__ void k_adj_scan(DevBatch B, const int* __restrict__ cnt, long long* __restrict__ inl,
+                           int* __restrict__ npair) {
+  const int m = blockIdx.x;
+  const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0;
+  __shared__ long long carry;
+  __shared__ int wsum[32];
+  if (threadIdx.x == 0) carry = B.poff[m];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int base = 0; base < nat; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int v = i < nat ? cnt[a0 + i] : 0;
+    int x = v;  // inclusive warp scan
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    int off = 0;
+    for (int w = 0; w < wid; ++w) off += wsum[w];
+    if (i < nat) inl[a0 + i] = carry + off + x - v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int tot = 0;
+      for (int w = 0; w < nw; ++w) tot += wsum[w];
+      carry += tot;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) npair[m] = (int)(carry - B.poff[m]);
+}
+
+// one warp per atom: write kept j (local indices) in ascending order
+__global__ void k_adj_fill(DevBatch B, double cutoff, const long long* __restrict__ inl,
+                           int* __restrict__ pair_i, int* __restrict__ pair_j) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= B.nat_tot) return;
+  const int a = warp, m = B.at_mol[a], a0 = B.aoff[m];
+  const double c2 = cutoff * cutoff;
+  long long pos = inl[a];
+  for (int base = a0; base < a; base += 32) {
+    const int b = base + lane;
+    const bool keep = b < a && adj_keep(B.xyz, a, b, c2);
+    const unsigned mask = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      const int r = __popc(mask & ((1u << lane) - 1u));
+      pair_i[pos + r] = a - a0;
+      pair_j[pos + r] = b - a0;
+    }
+    pos += __popc(mask);
+  }
+}
+
+// ---------------------------------------------------------------- integrals
+// lx ("x (+1), y (-1), z (0)" sorting, src/integral/overlap.h:62-86):
+// p = (y, z, x); d = (xx, yy, zz, xy, xz, yz).
+__device__ constexpr int c_lx[10][3] = {{0, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 0}, {2, 0, 0},
+                                {0, 2, 0}, {0, 0, 2}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+
+// 1-D overlap, dipole and quadrupole moments about centre i for one Cartesian
+// direction: horizontal_shift + form_product + the moment loop of
+// multipole_3d (src/integral/multipole.cu:411-457, quoted Fortran).
+__device__ inline void moments_1d(int li, int lj, double rpi, double rpj, const double* s1d, double* v) {
+  double vi[3] = {0, 0, 0}, vj[3] = {0, 0, 0};
+  vi[li] = 1.0;
+  vj[lj] = 1.0;
+  if (li == 1) vi[0] += rpi * vi[1];
+  if (li == 2) { vi[0] += rpi * rpi * vi[2]; vi[1] += 2.0 * rpi * vi[2]; }
+  if (lj == 1) vj[0] += rpj * vj[1];
+  if (lj == 2) { vj[0] += rpj * rpj * vj[2]; vj[1] += 2.0 * rpj * vj[2]; }
+  double vv[5] = {0, 0, 0, 0, 0};
+  for (int x = 0; x <= li; ++x)
+    for (int y = 0; y <= lj; ++y) vv[x + y] += vi[x] * vj[y];
+  double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+  for (int l = 0; l <= li + lj; ++l) {
+    v0 += s1d[l] * vv[l];
+    v1 += (s1d[l + 1] + rpi * s1d[l]) * vv[l];
+    v2 += (s1d[l + 2] + 2.0 * rpi * s1d[l + 1] + rpi * rpi * s1d[l]) * vv[l];
+  }
+  v[0] = v0; v[1] = v1; v[2] = v2;
+}
+
+// Cartesian -> spherical for one index (dtrafo of src/integral/trafo.h:6-107).
+template <int L>
+__device__ inline void cart_to_sph(const double* c, double* s) {
+  if (L < 2) {
+#pragma unroll
+    for (int i = 0; i < mlao(L); ++i) s[i] = c[i];
+  } else {
+    const double s3 = 1.7320508075688772, s3_4 = 0.8660254037844386;
+    s[0] = c[2] - 0.5 * (c[0] + c[1]);
+    s[1] = s3 * c[4];
+    s[2] = s3 * c[5];
+    s[3] = s3_4 * (c[0] - c[1]);
+    s[4] = s3 * c[3];
+  }
+}
+
+// transform0(lj, li, cart[mli][mlj]) -> sphr[msi][msj]
+template <int LI, int LJ>
+__device__ inline void transform0(const double* cart, double* sphr) {
+  constexpr int MI = (LI + 1) * (LI + 2) / 2, MJ = (LJ + 1) * (LJ + 2) / 2;
+  constexpr int SI = 2 * LI + 1, SJ = 2 * LJ + 1;
+  double tmp[MI][SJ];
+#pragma unroll
+  for (int a = 0; a < MI; ++a) cart_to_sph<LJ>(cart + a * MJ, tmp[a]);
+#pragma unroll
+  for (int b = 0; b < SJ; ++b) {
+    double col[MI], out[SI];
+#pragma unroll
+    for (int a = 0; a < MI; ++a) col[a] = tmp[a][b];
+    cart_to_sph<LI>(col, out);
+#pragma unroll
+    for (int a = 0; a < SI; ++a) sphr[a * SJ + b] = out[a];
+  }
+}
+
+// multipole_cgto(cgtoj, cgtoi, r2, vec, intcut) (src/integral/multipole.h:48-120,
+// quoted Fortran): blocks s[SI][SJ], d[SI][SJ][3], q[SI][SJ][6] with the moment
+// operator on centre i; vec = R_i - R_j.
+template <int LI, int LJ>
+__device__ void multipole_cgto(const ShellParam* __restrict__ ci, const ShellParam* __restrict__ cj, double r2,
+                               const double* vec, double intcut, double* s, double* d, double* q) {
+  constexpr int MI = (LI + 1) * (LI + 2) / 2, MJ = (LJ + 1) * (LJ + 2) / 2;
+  constexpr int SI = 2 * LI + 1, SJ = 2 * LJ + 1;
+  double s3d[MI * MJ], d3d[3][MI * MJ], q3d[6][MI * MJ];
+#pragma unroll
+  for (int x = 0; x < MI * MJ; ++x) {
+    s3d[x] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d3d[k][x] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) q3d[k][x] = 0.0;
+  }
+  const double sqrtpi3 = 5.568327996831708;
+  const int npi = ci->nprim, npj = cj->nprim;
+  for (int ip = 0; ip < npi; ++ip) {
+    const double ai = ci->alpha[ip], cci = ci->coeff[ip];
+    for (int jp = 0; jp < npj; ++jp) {
+      const double aj = cj->alpha[jp];
+      const double eab = ai + aj;
+      const double oab = 1.0 / eab;
+      const double est = ai * aj * r2 * oab;
+      if (est > intcut) continue;
+      const double pre = exp(-est) * sqrtpi3 * oab * sqrt(oab);
+      const double cc = cci * cj->coeff[jp] * pre;
+      double rpi[3], rpj[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) { rpi[k] = -vec[k] * aj * oab; rpj[k] = vec[k] * ai * oab; }
+      double s1d[LI + LJ + 3];
+      const double h = 0.5 * oab;
+      s1d[0] = 1.0;
+#pragma unroll
+      for (int l = 1; l < LI + LJ + 3; ++l) s1d[l] = 0.0;
+      if (LI + LJ + 2 >= 2) s1d[2] = h;
+      if (LI + LJ + 2 >= 4) s1d[4] = 3.0 * h * h;
+      if (LI + LJ + 2 >= 6) s1d[6] = 15.0 * h * h * h;
+      // 1-D moment tables V[k][li][lj][0..2] shared by all Cartesian pairs
+      double V[3][LI + 1][LJ + 1][3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int x = 0; x <= LI; ++x)
+#pragma unroll
+          for (int y = 0; y <= LJ; ++y) moments_1d(x, y, rpi[k], rpj[k], s1d, V[k][x][y]);
+#pragma unroll
+      for (int a = 0; a < MI; ++a) {
+#pragma unroll
+        for (int b = 0; b < MJ; ++b) {
+          const double* vx = V[0][c_lx[lmap(LI) + a][0]][c_lx[lmap(LJ) + b][0]];
+          const double* vy = V[1][c_lx[lmap(LI) + a][1]][c_lx[lmap(LJ) + b][1]];
+          const double* vz = V[2][c_lx[lmap(LI) + a][2]][c_lx[lmap(LJ) + b][2]];
+          const int x = a * MJ + b;
+          s3d[x] += cc * (vx[0] * vy[0] * vz[0]);
+          d3d[0][x] += cc * (vx[1] * vy[0] * vz[0]);
+          d3d[1][x] += cc * (vx[0] * vy[1] * vz[0]);
+          d3d[2][x] += cc * (vx[0] * vy[0] * vz[1]);
+          q3d[0][x] += cc * (vx[2] * vy[0] * vz[0]);
+          q3d[1][x] += cc * (vx[1] * vy[1] * vz[0]);
+          q3d[2][x] += cc * (vx[0] * vy[2] * vz[0]);
+          q3d[3][x] += cc * (vx[1] * vy[0] * vz[1]);
+          q3d[4][x] += cc * (vx[0] * vy[1] * vz[1]);
+          q3d[5][x] += cc * (vx[0] * vy[0] * vz[2]);
+        }
+      }
+    }
+  }
+  double tmp[SI * SJ];
+  transform0<LI, LJ>(s3d, s);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    transform0<LI, LJ>(d3d[k], tmp);
+#pragma unroll
+    for (int x = 0; x < SI * SJ; ++x) d[3 * x + k] = tmp[x];
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    transform0<LI, LJ>(q3d[k], tmp);
+#pragma unroll
+    for (int x = 0; x < SI * SJ; ++x) q[6 * x + k] = tmp[x];
+  }
+#pragma unroll
+  for (int x = 0; x < SI * SJ; ++x) {
+    double* qq = q + 6 * x;
+    const double tr = 0.5 * (qq[0] + qq[2] + qq[5]);
+    qq[0] = 1.5 * qq[0] - tr; qq[1] = 1.5 * qq[1]; qq[2] = 1.5 * qq[2] - tr;
+    qq[3] = 1.5 * qq[3]; qq[4] = 1.5 * qq[4]; qq[5] = 1.5 * qq[5] - tr;
+  }
+}
+
+// shift_operator (src/h0.cu:201-250, quoted Fortran).
+__device__ inline void shift_operator(const double* vec, double s, const double* di, const double* qi,
+                                      double* dj, double* qj) {
+  dj[0] = di[0] + vec[0] * s;
+  dj[1] = di[1] + vec[1] * s;
+  dj[2] = di[2] + vec[2] * s;
+  qj[0] = 2 * vec[0] * di[0] + vec[0] * vec[0] * s;
+  qj[2] = 2 * vec[1] * di[1] + vec[1] * vec[1] * s;
+  qj[5] = 2 * vec[2] * di[2] + vec[2] * vec[2] * s;
+  qj[1] = vec[0] * di[1] + vec[1] * di[0] + vec[0] * vec[1] * s;
+  qj[3] = vec[0] * di[2] + vec[2] * di[0] + vec[0] * vec[2] * s;
+  qj[4] = vec[1] * di[2] + vec[2] * di[1] + vec[1] * vec[2] * s;
+  const double tr = 0.5 * (qj[0] + qj[2] + qj[5]);
+  qj[0] = qi[0] + 1.5 * qj[0] - tr;
+  qj[1] = qi[1] + 1.5 * qj[1];
+  qj[2] = qi[2] + 1.5 * qj[2] - tr;
+  qj[3] = qi[3] + 1.5 * qj[3];
+  qj[4] = qi[4] + 1.5 * qj[4];
+  qj[5] = qi[5] + 1.5 * qj[5] - tr;
+}
+
+// Scatter one shell-pair block into the structure's matrices (the assembly
+// loop of get_hamiltonian, src/h0.cu:306-477, quoted Fortran).  Off-site pairs
+// (onsite=false) also write the transposed block with the operator shifted to
+// centre j; on-site blocks carry no H0 (the diagonal is added separately).
+template <int LI, int LJ>
+__device__ void scatter_block(const MatOut& out, long long mo, int n, int ii, int jj, bool onsite, double hij,
+                              const double* vec, const double* s, const double* d, const double* q) {
+  constexpr int SI = 2 * LI + 1, SJ = 2 * LJ + 1;
+  const long long nn = (long long)n * n;
+#pragma unroll
+  for (int iao = 0; iao < SI; ++iao) {
+#pragma unroll
+    for (int jao = 0; jao < SJ; ++jao) {
+      const int ij = iao * SJ + jao;
+      const long long mu = jj + jao, nu = ii + iao;
+      const long long e1 = mu * n + nu;
+      out.S[mo + e1] = s[ij];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) out.D[3 * mo + k * nn + e1] = d[3 * ij + k];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) out.Q[6 * mo + k * nn + e1] = q[6 * ij + k];
+      if (!onsite) {
+        out.H0[mo + e1] = s[ij] * hij;
+        double dj[3], qj[6];
+        shift_operator(vec, s[ij], d + 3 * ij, q + 6 * ij, dj, qj);
+        const long long e2 = nu * n + mu;
+        out.S[mo + e2] = s[ij];
+        out.H0[mo + e2] = s[ij] * hij;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) out.D[3 * mo + k * nn + e2] = dj[k];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) out.Q[6 * mo + k * nn + e2] = qj[k];
+      }
+    }
+  }
+}
+
+template <int LI, int LJ>
+__device__ void pair_block(const DevParams& P, const MatOut& out, long long mo, int n, int ii, int jj, bool onsite,
+                           double hij, double r2, const double* vec, const ShellParam* ci, const ShellParam* cj) {
+  constexpr int SI = 2 * LI + 1, SJ = 2 * LJ + 1;
+  double s[SI * SJ], d[3 * SI * SJ], q[6 * SI * SJ];
+  multipole_cgto<LI, LJ>(ci, cj, r2, vec, P.intcut, s, d, q);
+  scatter_block<LI, LJ>(out, mo, n, ii, jj, onsite, hij, vec, s, d, q);
+}
+
+// Off-site shell pairs of angular momenta (LI, LJ): one thread per (neighbour
+// pair, shell pair), grid stride over the pair capacity of the whole batch;
+// slots beyond a structure's npair and shell pairs of other (li, lj) are
+// skipped.  One instantiation per (li, lj) keeps the register budget of the
+// s/p kernels independent of the d-shell ones.
+template <int LI, int LJ>
+__global__ void k_integrals_t(DevParams P, DevBatch B, const int* __restrict__ npair, const int* __restrict__ pair_i,
+                              const int* __restrict__ pair_j, const double* __restrict__ se, MatOut out, int maxsp,
+                              long long total_items) {
+  for (long long it = blockIdx.x * (long long)blockDim.x + threadIdx.x; it < total_items;
+       it += (long long)gridDim.x * blockDim.x) {
+    const long long p = it / maxsp;
+    const int sp = (int)(it % maxsp);
+    // structure owning pair slot p (binary search over the capacity offsets)
+    int lo = 0, hi = B.nmol;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (B.poff[mid] <= p) lo = mid; else hi = mid;
+    }
+    const int m = lo;
+    if (p - B.poff[m] >= npair[m]) continue;
+    const int a0 = B.aoff[m];
+    const int iat = pair_i[p], jat = pair_j[p];
+    const SpeciesParam& spi = P.sp[B.id[a0 + iat]];
+    const SpeciesParam& spj = P.sp[B.id[a0 + jat]];
+    if (sp >= spi.nsh * spj.nsh) continue;
+    const int ish = sp / spj.nsh, jsh = sp % spj.nsh;
+    const int ti = spi.sh0 + ish, tj = spj.sh0 + jsh;
+    const ShellParam* ci = P.sh + ti;
+    const ShellParam* cj = P.sh + tj;
+    if (ci->ang != LI || cj->ang != LJ) continue;
+    const int n = B.ooff[m + 1] - B.ooff[m];
+    const long long mo = B.moff[m];
+    const int is = B.soff[m] + B.at_ish[a0 + iat], js = B.soff[m] + B.at_ish[a0 + jat];
+    const int ii = B.sh_iao[is + ish], jj = B.sh_iao[js + jsh];
+    const double vec[3] = {B.xyz[3 * (a0 + iat)] - B.xyz[3 * (a0 + jat)],
+                           B.xyz[3 * (a0 + iat) + 1] - B.xyz[3 * (a0 + jat) + 1],
+                           B.xyz[3 * (a0 + iat) + 2] - B.xyz[3 * (a0 + jat) + 2]};
+    const double r2 = vec[0] * vec[0] + vec[1] * vec[1] + vec[2] * vec[2];
+    const double rr = sqrt(sqrt(r2) / (spj.rad + spi.rad));
+    const double shpoly = (1.0 + ci->shpoly * rr) * (1.0 + cj->shpoly * rr);
+    const double hij = 0.5 * (se[is + ish] + se[js + jsh]) * P.hscale[ti * P.nshtype + tj] * shpoly;
+    pair_block<LI, LJ>(P, out, mo, n, ii, jj, false, hij, r2, vec, ci, cj);
+  }
+}
+
+// On-site blocks (the same-atom step missing from the reference, D8): one
+// thread per (atom, shell pair); the diagonal of H0 gets the self-energies.
+template <int LI, int LJ>
+__global__ void k_onsite_t(DevParams P, DevBatch B, const double* __restrict__ se, MatOut out, int maxsp) {
+  const long long it = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (it >= (long long)B.nat_tot * maxsp) return;
+  const int a = (int)(it / maxsp), sp = (int)(it % maxsp);
+  const int m = B.at_mol[a];
+  const SpeciesParam& spa = P.sp[B.id[a]];
+  if (sp >= spa.nsh * spa.nsh) return;
+  const int ish = sp / spa.nsh, jsh = sp % spa.nsh;
+  const ShellParam* ci = P.sh + spa.sh0 + ish;
+  const ShellParam* cj = P.sh + spa.sh0 + jsh;
+  if (ci->ang != LI || cj->ang != LJ) return;
+  const int n = B.ooff[m + 1] - B.ooff[m];
+  const long long mo = B.moff[m];
+  const int is = B.soff[m] + B.at_ish[a];
+  const int ii = B.sh_iao[is + ish], jj = B.sh_iao[is + jsh];
+  const double vec[3] = {0.0, 0.0, 0.0};
+  pair_block<LI, LJ>(P, out, mo, n, ii, jj, true, 0.0, 0.0, vec, ci, cj);
+  if (ish == jsh) {
+    for (int x = 0; x < msao(LI); ++x) out.H0[mo + (long long)(ii + x) * n + ii + x] = se[is + ish];
+  }
+}
+
+// Launch the integral kernels for every (li, lj) combination in `lmask`
+// (bit l set when the parameter set has shells of angular momentum l).
+cudaError_t launch_integrals(const DevParams& P, const DevBatch& B, const int* npair, const int* pair_i,
+                             const int* pair_j, const double* se, const MatOut& out, int maxsp, long long items,
+                             int lmask, cudaStream_t st, int64_t* launches) {
+  const int grid = (int)std::max(1LL, std::min((items + 127) / 128, 148LL * 32));
+  const int ogrid = (int)std::max(1LL, ((long long)B.nat_tot * maxsp + 127) / 128);
+#define TB_LAUNCH_PAIR(A, C)                                                                              \
+  if ((lmask >> A & 1) && (lmask >> C & 1)) {                                                             \
+    k_integrals_t<A, C><<<grid, 128, 0, st>>>(P, B, npair, pair_i, pair_j, se, out, maxsp, items);        \
+    k_onsite_t<A, C><<<ogrid, 128, 0, st>>>(P, B, se, out, maxsp);                                        \
+    *launches += 2;                                                                                       \
+  }
+  TB_LAUNCH_PAIR(0, 0) TB_LAUNCH_PAIR(0, 1) TB_LAUNCH_PAIR(1, 0) TB_LAUNCH_PAIR(1, 1)
+  TB_LAUNCH_PAIR(0, 2) TB_LAUNCH_PAIR(2, 0) TB_LAUNCH_PAIR(1, 2) TB_LAUNCH_PAIR(2, 1) TB_LAUNCH_PAIR(2, 2)
+#undef TB_LAUNCH_PAIR
+  return cudaGetLastError();
+}
+
+}  // namespace tb

@@ -1,0 +1,316 @@
+"""ctypes binding of the tblite-b200 C ABI (include/tblite_b200.h).
+
+This is the Python mirror of the reference's singlepoint interface: a
+``Calculator`` (xtb_calculator, reference src/xtb.h:105-126) and
+``singlepoint_batch`` (xtb_singlepoint, src/xtb.cu:188-434, batched).  All
+computation happens in ``lib/libtblite_b200.so`` on the GPU; there is no CPU
+fallback -- if the library is missing this module raises on first use.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG, "lib", "libtblite_b200.so")
+DEFAULT_PARAMS = os.path.join(PKG, "params", "synthetic_hco.tbp")
+
+TB_OK, TB_BAD_INPUT, TB_NOT_SPD, TB_SCF_NOT_CONVERGED = 0, 1, 2, 3
+TB_FERMI_NOT_CONVERGED, TB_EIGEN_FAILED, TB_CAPACITY_EXCEEDED = 4, 5, 6
+TB_CUDA_ERROR, TB_PARAM_ERROR = 7, 8
+STATUS_NAMES = {0: "TB_OK", 1: "TB_BAD_INPUT", 2: "TB_NOT_SPD", 3: "TB_SCF_NOT_CONVERGED",
+                4: "TB_FERMI_NOT_CONVERGED", 5: "TB_EIGEN_FAILED", 6: "TB_CAPACITY_EXCEEDED",
+                7: "TB_CUDA_ERROR", 8: "TB_PARAM_ERROR"}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+class Structure(C.Structure):
+    _fields_ = [("nat", C.c_int32), ("uhf", C.c_int32), ("charge", C.c_double),
+                ("id", _ip), ("xyz", _dp)]
+
+
+class Options(C.Structure):
+    _fields_ = [("accuracy", C.c_double), ("kt", C.c_double), ("max_iter", C.c_int32),
+                ("mixer_damping", C.c_double), ("verbosity", C.c_int32), ("use_graphs", C.c_int32),
+                ("solver", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Result(C.Structure):
+    _fields_ = [("energy", C.c_double), ("e_rep", C.c_double), ("e_elec", C.c_double),
+                ("e_band", C.c_double), ("e_ts", C.c_double), ("e_es2", C.c_double),
+                ("e_aes2", C.c_double), ("e_es3", C.c_double), ("dipole", C.c_double * 3),
+                ("scf_error", C.c_double), ("iterations", C.c_int32), ("status", C.c_int32),
+                ("nsh", C.c_int32), ("nao", C.c_int32), ("qat", _dp), ("qsh", _dp), ("dpat", _dp),
+                ("qpat", _dp)]
+
+
+EXPORTS = [
+    "tb_calculator_create", "tb_calculator_destroy", "tb_calculator_nspecies", "tb_default_options",
+    "tb_last_error", "tb_basis_size", "tb_singlepoint_batch", "tb_batch_create", "tb_batch_run",
+    "tb_batch_results", "tb_batch_launches", "tb_batch_destroy", "tb_get_cutoff", "tb_adjacency_list",
+    "tb_atomic_properties", "tb_repulsion", "tb_get_hamiltonian", "tb_coulomb_potential",
+    "tb_add_pot_to_h1", "tb_sygvd_batch", "tb_fermi_filling",
+]
+
+_lib = None
+
+
+class TBError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libtblite_b200.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"tblite-b200 CUDA library not built: {path} (run __graft_entry__.build())")
+    L = C.CDLL(path)
+    L.tb_last_error.restype = C.c_char_p
+    L.tb_get_cutoff.restype = C.c_double
+    L.tb_get_cutoff.argtypes = [C.c_void_p, C.c_double]
+    L.tb_calculator_create.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
+    L.tb_calculator_destroy.argtypes = [C.c_void_p]
+    L.tb_calculator_nspecies.argtypes = [C.c_void_p]
+    L.tb_default_options.argtypes = [C.POINTER(Options)]
+    L.tb_batch_launches.restype = C.c_int64
+    L.tb_batch_launches.argtypes = [C.c_void_p]
+    L.tb_batch_destroy.argtypes = [C.c_void_p]
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return load_library().tb_last_error().decode()
+
+
+def check(st: int, what: str = ""):
+    if st != TB_OK:
+        raise TBError(st, f"{what}: {last_error()}")
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    load_library().tb_default_options(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def _structs(mols):
+    """Pack Molecule-like objects (id, xyz, charge, uhf) into tb_structure records."""
+    keep, arr = [], (Structure * len(mols))()
+    for i, m in enumerate(mols):
+        ids = np.ascontiguousarray(m.id, np.int32)
+        xyz = np.ascontiguousarray(m.xyz, np.float64).reshape(-1, 3)
+        keep.append((ids, xyz))
+        arr[i].nat = ids.shape[0]
+        arr[i].uhf = int(getattr(m, "uhf", 0))
+        arr[i].charge = float(getattr(m, "charge", 0.0))
+        arr[i].id = ids.ctypes.data_as(_ip)
+        arr[i].xyz = xyz.ctypes.data_as(_dp)
+    return arr, keep
+
+
+class Calculator:
+    """GFN2-shaped xTB calculator bound to one parameter file (tb_calculator)."""
+
+    def __init__(self, param_file: str = DEFAULT_PARAMS):
+        L = load_library()
+        h = C.c_void_p()
+        check(L.tb_calculator_create(param_file.encode(), C.byref(h)), "tb_calculator_create")
+        self.h = h
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.h.value:
+                load_library().tb_calculator_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def basis_size(self, mol):
+        arr, keep = _structs([mol])
+        nsh, nao = C.c_int32(), C.c_int32()
+        check(load_library().tb_basis_size(self.h, C.byref(arr[0]), C.byref(nsh), C.byref(nao)),
+              "tb_basis_size")
+        return nsh.value, nao.value
+
+    def cutoff(self, accuracy=1.0):
+        return load_library().tb_get_cutoff(self.h, C.c_double(accuracy))
+
+    def singlepoint_batch(self, mols, stream=None, raise_on_error=False, **opts):
+        """Run xtb_singlepoint for every structure; returns a list of result dicts."""
+        L = load_library()
+        arr, keep = _structs(mols)
+        o = default_options(**opts)
+        res = (Result * len(mols))()
+        bufs = []
+        for i, m in enumerate(mols):
+            nsh, nao = self.basis_size(m)
+            b = dict(qat=np.zeros(m.nat), qsh=np.zeros(nsh), dpat=np.zeros((m.nat, 3)),
+                     qpat=np.zeros((m.nat, 6)))
+            bufs.append(b)
+            res[i].qat = b["qat"].ctypes.data_as(_dp)
+            res[i].qsh = b["qsh"].ctypes.data_as(_dp)
+            res[i].dpat = b["dpat"].ctypes.data_as(_dp)
+            res[i].qpat = b["qpat"].ctypes.data_as(_dp)
+        st = L.tb_singlepoint_batch(self.h, arr, C.c_int32(len(mols)), C.byref(o), res,
+                                    C.c_void_p(stream or 0))
+        if st not in (TB_OK,) and (raise_on_error or st in (TB_BAD_INPUT, TB_CUDA_ERROR,
+                                                            TB_CAPACITY_EXCEEDED, TB_PARAM_ERROR)):
+            check(st, "tb_singlepoint_batch")
+        return [_result_dict(r, b) for r, b in zip(res, bufs)]
+
+
+def _result_dict(r, b):
+    d = dict(energy=r.energy, e_rep=r.e_rep, e_elec=r.e_elec, e_band=r.e_band, e_ts=r.e_ts,
+             e_es2=r.e_es2, e_aes2=r.e_aes2, e_es3=r.e_es3, dipole=np.array(r.dipole[:]),
+             scf_error=r.scf_error, iterations=r.iterations, status=r.status, nsh=r.nsh, nao=r.nao)
+    d.update(b)
+    return d
+
+
+class Batch:
+    """Device-resident batch (tb_batch): geometry uploaded once, run on device."""
+
+    def __init__(self, calc: Calculator, mols, **opts):
+        L = load_library()
+        self.calc = calc
+        self.mols = mols
+        self._arr, self._keep = _structs(mols)
+        o = default_options(**opts)
+        h = C.c_void_p()
+        check(L.tb_batch_create(calc.h, self._arr, C.c_int32(len(mols)), C.byref(o), C.byref(h)),
+              "tb_batch_create")
+        self.h = h
+
+    def run(self, stream=None):
+        st = load_library().tb_batch_run(self.h, C.c_void_p(stream or 0))
+        check(st, "tb_batch_run")
+
+    def launches(self) -> int:
+        return int(load_library().tb_batch_launches(self.h))
+
+    def results(self, stream=None):
+        L = load_library()
+        res = (Result * len(self.mols))()
+        bufs = []
+        for i, m in enumerate(self.mols):
+            nsh, nao = self.calc.basis_size(m)
+            b = dict(qat=np.zeros(m.nat), qsh=np.zeros(nsh), dpat=np.zeros((m.nat, 3)),
+                     qpat=np.zeros((m.nat, 6)))
+            bufs.append(b)
+            res[i].qat = b["qat"].ctypes.data_as(_dp)
+            res[i].qsh = b["qsh"].ctypes.data_as(_dp)
+            res[i].dpat = b["dpat"].ctypes.data_as(_dp)
+            res[i].qpat = b["qpat"].ctypes.data_as(_dp)
+        L.tb_batch_results(self.h, res, C.c_void_p(stream or 0))
+        return [_result_dict(r, b) for r, b in zip(res, bufs)]
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.h.value:
+                load_library().tb_batch_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- stage calls
+def _one(mol):
+    arr, keep = _structs([mol])
+    return arr, keep
+
+
+def adjacency_list(calc: Calculator, mol, cutoff: float):
+    arr, keep = _one(mol)
+    nat = mol.nat
+    cap = max(1, nat * (nat - 1) // 2)
+    inl, nnl = np.zeros(nat, np.int32), np.zeros(nat, np.int32)
+    nlat = np.zeros(cap, np.int32)
+    npair = C.c_int32()
+    check(load_library().tb_adjacency_list(calc.h, C.byref(arr[0]), C.c_double(cutoff), inl.ctypes.data_as(_ip),
+                                           nnl.ctypes.data_as(_ip), nlat.ctypes.data_as(_ip), C.c_int32(cap),
+                                           C.byref(npair)), "tb_adjacency_list")
+    return inl, nnl, nlat[:npair.value].copy()
+
+
+def atomic_properties(calc: Calculator, mol):
+    arr, keep = _one(mol)
+    nsh, _ = calc.basis_size(mol)
+    cn, mrad, se = np.zeros(mol.nat), np.zeros(mol.nat), np.zeros(nsh)
+    check(load_library().tb_atomic_properties(calc.h, C.byref(arr[0]), cn.ctypes.data_as(_dp),
+                                              mrad.ctypes.data_as(_dp), se.ctypes.data_as(_dp)),
+          "tb_atomic_properties")
+    return cn, mrad, se
+
+
+def repulsion(calc: Calculator, mol):
+    arr, keep = _one(mol)
+    e = np.zeros(mol.nat)
+    check(load_library().tb_repulsion(calc.h, C.byref(arr[0]), e.ctypes.data_as(_dp)), "tb_repulsion")
+    return e
+
+
+def get_hamiltonian(calc: Calculator, mol):
+    arr, keep = _one(mol)
+    _, n = calc.basis_size(mol)
+    S, H0, D, Q = np.zeros((n, n)), np.zeros((n, n)), np.zeros((3, n, n)), np.zeros((6, n, n))
+    check(load_library().tb_get_hamiltonian(calc.h, C.byref(arr[0]), *[a.ctypes.data_as(_dp) for a in (S, H0, D, Q)]),
+          "tb_get_hamiltonian")
+    return S, H0, D, Q
+
+
+def coulomb_potential(calc: Calculator, mol, qsh, dpat, qpat):
+    arr, keep = _one(mol)
+    nsh, _ = calc.basis_size(mol)
+    qsh, dpat, qpat = (np.ascontiguousarray(a, np.float64) for a in (qsh, dpat, qpat))
+    vsh, vat, vdp, vqp = np.zeros(nsh), np.zeros(mol.nat), np.zeros((mol.nat, 3)), np.zeros((mol.nat, 6))
+    check(load_library().tb_coulomb_potential(calc.h, C.byref(arr[0]),
+                                              *[a.ctypes.data_as(_dp) for a in (qsh, dpat, qpat, vsh, vat, vdp, vqp)]),
+          "tb_coulomb_potential")
+    return vsh, vat, vdp, vqp
+
+
+def add_pot_to_h1(calc: Calculator, mol, S, H0, D, Q, vsh, vat, vdp, vqp):
+    arr, keep = _one(mol)
+    ins = [np.ascontiguousarray(a, np.float64) for a in (S, H0, D, Q, vsh, vat, vdp, vqp)]
+    F = np.zeros_like(ins[0])
+    check(load_library().tb_add_pot_to_h1(calc.h, C.byref(arr[0]), *[a.ctypes.data_as(_dp) for a in ins],
+                                          F.ctypes.data_as(_dp)), "tb_add_pot_to_h1")
+    return F
+
+
+def sygvd_batch(Hs, Ss):
+    """Generalized eigenproblems H C = S C e for a list of (n_i x n_i) pairs."""
+    n = np.array([h.shape[0] for h in Hs], np.int32)
+    H = np.ascontiguousarray(np.concatenate([np.ravel(h) for h in Hs]), np.float64)
+    S = np.ascontiguousarray(np.concatenate([np.ravel(s) for s in Ss]), np.float64)
+    w = np.zeros(int(n.sum()))
+    Cm = np.zeros_like(H)
+    st = load_library().tb_sygvd_batch(C.c_int32(len(n)), n.ctypes.data_as(_ip), H.ctypes.data_as(_dp),
+                                       S.ctypes.data_as(_dp), w.ctypes.data_as(_dp), Cm.ctypes.data_as(_dp))
+    out, wo, co = [], 0, 0
+    for k in n:
+        out.append((w[wo:wo + k].copy(), Cm[co:co + k * k].reshape(k, k).copy()))
+        wo += k
+        co += k * k
+    return st, out
+
+
+def fermi_filling(nel, kt, emo):
+    emo = np.ascontiguousarray(emo, np.float64)
+    occ = np.zeros_like(emo)
+    ef, ts = C.c_double(), C.c_double()
+    st = load_library().tb_fermi_filling(C.c_int32(len(emo)), C.c_double(nel), C.c_double(kt),
+                                         emo.ctypes.data_as(_dp), occ.ctypes.data_as(_dp), C.byref(ef),
+                                         C.byref(ts))
+    return st, occ, ef.value, ts.value

@@ -1,0 +1,189 @@
+"""CPU tests of the FP64 oracle: pins against the reference's own known-answer
+data (tests/golden/kat_reference.json), scipy, and analytic identities."""
+import json
+import os
+
+import numpy as np
+import pytest
+import scipy.linalg as sl
+
+import pyoracle as po
+from tblite_b200 import geometry as g
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+KAT = json.load(open(os.path.join(HERE, "golden", "kat_reference.json")))
+
+
+# ------------------------------------------------------------ reference KATs
+def test_kat_multipole_3d_ss():
+    k = KAT["multipole_3d_ss"]
+    s3d, d3d, q3d = po.kat_multipole_3d(k["r_other"], k["r_moment"], k["a_other"], k["a_moment"],
+                                        [0, 0, 0], [0, 0, 0], k["s1d"])
+    assert s3d == k["s3d"]
+    np.testing.assert_allclose(d3d, k["d3d"], atol=k["tol"])
+    np.testing.assert_allclose(q3d, k["q3d"], atol=k["tol"])
+    # the restatement is exact for these inputs, far inside the reference's 1e-4
+    np.testing.assert_allclose(q3d, k["q3d"], rtol=1e-12)
+
+
+def test_kat_transform0_sd():
+    k = KAT["transform0_sd"]
+    out = po.kat_transform0(k["lj"], k["li"], k["cart"])
+    np.testing.assert_allclose(out[:5], k["sphr"], atol=1e-15)
+
+
+def test_kat_gemv_case1():
+    k = KAT["gemv_case1"]
+    y = po.kat_gemv(np.array(k["A"]), np.array(k["x"]), np.zeros(2))
+    np.testing.assert_array_equal(y, k["y"])
+
+
+def test_kat_sygvd_2x2_degenerate():
+    k = KAT["sygvd_2x2"]
+    A, B = np.array(k["A"]), np.array(k["B"])
+    st, w, C = po.Oracle.sygvd(A, B)
+    assert st == 0
+    np.testing.assert_allclose(w, k["w"], atol=1e-14)
+    np.testing.assert_allclose(C.T @ B @ C, np.eye(2), atol=1e-14)
+    np.testing.assert_allclose(sl.eigh(A, B, eigvals_only=True), k["w"], atol=1e-12)
+
+
+# ------------------------------------------------------------ eigensolver vs scipy
+@pytest.mark.parametrize("n", [1, 2, 3, 7, 40, 120])
+def test_sygvd_matches_scipy(n):
+    rng = np.random.default_rng(n)
+    M = rng.normal(size=(n, n))
+    H = 0.5 * (M + M.T)
+    R = rng.normal(size=(n, n))
+    S = R @ R.T / n + np.eye(n)
+    st, w, C = po.Oracle.sygvd(H, S)
+    assert st == 0
+    np.testing.assert_allclose(w, sl.eigh(H, S, eigvals_only=True), atol=1e-11)
+    np.testing.assert_allclose(C.T @ S @ C, np.eye(n), atol=1e-11)
+    np.testing.assert_allclose(H @ C, S @ C * w, atol=1e-10)
+
+
+def test_sygvd_degenerate_cluster_density_invariant():
+    # exactly degenerate spectrum: the density of a full degenerate block is unique
+    n = 12
+    rng = np.random.default_rng(3)
+    Qm, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    evals = np.repeat([-1.0, 0.5, 2.0], 4)
+    H = Qm @ np.diag(evals) @ Qm.T
+    st, w, C = po.Oracle.sygvd(H, np.eye(n))
+    assert st == 0
+    np.testing.assert_allclose(w, np.sort(evals), atol=1e-12)
+    P = C[:, :4] @ C[:, :4].T
+    np.testing.assert_allclose(P, Qm[:, :4] @ Qm[:, :4].T, atol=1e-12)
+
+
+def test_sygvd_not_spd():
+    st, _, _ = po.Oracle.sygvd(np.eye(3), -np.eye(3))
+    assert st == 2  # ORC_NOT_SPD
+
+
+# ------------------------------------------------------------ Fermi
+def test_fermi_counts_and_aufbau_limit():
+    emo = np.linspace(-1.0, 1.0, 20)
+    st, occ, ef, ts = po.Oracle.fermi(7.0, 300 * 3.166811563455546e-6, emo)
+    assert st == 0
+    assert abs(occ.sum() - 7.0) < 1e-10
+    np.testing.assert_allclose(occ[:7], 1.0, atol=1e-12)
+    np.testing.assert_allclose(occ[7:], 0.0, atol=1e-12)
+    assert ts <= 0.0
+    # near-degenerate HOMO/LUMO: smeared occupations, entropy nonzero
+    emo2 = emo.copy()
+    emo2[7] = emo2[6] + 1e-5
+    st, occ2, ef2, ts2 = po.Oracle.fermi(7.0, 300 * 3.166811563455546e-6, emo2)
+    assert st == 0 and abs(occ2.sum() - 7.0) < 1e-10 and ts2 < 0.0
+    assert 0.0 < occ2[7] < 1.0
+
+
+# ------------------------------------------------------------ integral identities
+@pytest.fixture(scope="module")
+def octane():
+    return g.octane()
+
+
+def test_overlap_identities(oracle, octane):
+    S, H0, D, Q = oracle.hamiltonian(octane.id, octane.xyz)
+    np.testing.assert_allclose(np.diag(S), 1.0, atol=1e-10)
+    np.testing.assert_array_equal(S, S.T)
+    np.testing.assert_allclose(H0, H0.T, atol=1e-15)
+    assert np.linalg.eigvalsh(S).min() > 0.0
+    # quadrupoles are traceless
+    np.testing.assert_allclose(Q[0] + Q[2] + Q[5], 0.0, atol=1e-12)
+
+
+def test_dipole_shift_relation(oracle, octane):
+    # D[k][nu][mu] (operator on mu's atom) = D[k][mu][nu] + (R_at(nu) - R_at(mu))_k S[mu][nu]
+    S, H0, D, Q = oracle.hamiltonian(octane.id, octane.xyz)
+    maps = oracle.basis_maps(octane.id)
+    R = octane.xyz[maps["ao2at"]]
+    for k in range(3):
+        lhs = D[k].T
+        rhs = D[k] + (R[None, :, k] - R[:, None, k]) * S
+        np.testing.assert_allclose(lhs, rhs, atol=1e-12)
+
+
+def test_adjacency_half_list(octane, oracle):
+    cut = oracle.cutoff()
+    inl, nnl, nlat, nltr = po.Oracle.adjacency_list(octane.xyz, cut)
+    assert nnl.sum() == len(nlat)
+    for i in range(octane.nat):
+        js = nlat[inl[i]:inl[i] + nnl[i]]
+        assert np.all(js < i) and np.all(np.diff(js) > 0)
+        d2 = ((octane.xyz[i] - octane.xyz[js]) ** 2).sum(1)
+        assert np.all(d2 <= cut * cut)
+    assert np.all(nltr == 0)
+
+
+def test_cutoff_is_literal_intcut25(oracle):
+    # integral_cutoff clips acc into [1e-4, 1e-4] (reference quirk): same cutoff for all acc
+    assert oracle.cutoff(1.0) == oracle.cutoff(1e-3) == oracle.cutoff(100.0)
+
+
+# ------------------------------------------------------------ singlepoint
+def test_octane_singlepoint_converges(oracle, octane):
+    r = oracle.singlepoint(octane)
+    assert r["status"] == 0 and 3 <= r["iterations"] < 32
+    assert abs(r["qat"].sum()) < 1e-10  # sum q = charge
+    S, *_ = oracle.hamiltonian(octane.id, octane.xyz)
+    assert abs(np.sum(r["P"] * S) - 50.0) < 1e-9  # Tr(PS) = nel
+
+
+def test_singlepoint_invariances(oracle):
+    m = g.water_cluster(4, np.random.default_rng(5))
+    ref = oracle.singlepoint(m, accuracy=1e-4)
+    # translation
+    mt = g.Molecule(m.id, m.xyz + np.array([3.0, -2.0, 1.5]))
+    rt = oracle.singlepoint(mt, accuracy=1e-4)
+    assert abs(rt["energy"] - ref["energy"]) < 1e-9
+    # rotation (energy and charges invariant, dipole rotates)
+    th = 0.7
+    Rz = np.array([[np.cos(th), -np.sin(th), 0], [np.sin(th), np.cos(th), 0], [0, 0, 1]])
+    mr = g.Molecule(m.id, m.xyz @ Rz.T)
+    rr = oracle.singlepoint(mr, accuracy=1e-4)
+    assert abs(rr["energy"] - ref["energy"]) < 1e-8
+    np.testing.assert_allclose(rr["qat"], ref["qat"], atol=1e-7)
+
+
+def test_charged_and_open_shell(oracle):
+    m = g.octane()
+    cat = g.Molecule(m.id, m.xyz, charge=1.0, uhf=1)
+    r = oracle.singlepoint(cat)
+    assert r["status"] == 0
+    assert abs(r["qat"].sum() - 1.0) < 1e-9
+
+
+def test_max_iter_status(oracle, octane):
+    r = oracle.singlepoint(octane, max_iter=1)
+    assert r["status"] == 3 and r["iterations"] == 1
+
+
+def test_batch_threads_match_single(oracle):
+    mols = g.water_clusters(6, nmin=2, nmax=6)
+    res = oracle.singlepoint_batch(mols, nthreads=3)
+    for m, r in zip(mols, res):
+        assert r["status"] == 0
+        assert r["energy"] == oracle.singlepoint(m)["energy"]
