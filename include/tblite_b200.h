@@ -66,7 +66,7 @@ typedef struct tb_options {
   int32_t verbosity;      /* 0 silent                                          */
   int32_t use_graphs;     /* 1: replay each SCF iteration as a CUDA graph      */
   int32_t solver;         /* 0 auto, 1 in-house batched QL, 2 cuSOLVER (large) */
-  int32_t reserved;
+  int32_t profile;        /* 1: time every kernel class with CUDA events        */
 } tb_options;
 
 /* Per-structure results: the energy/wavefunction outputs of xtb_singlepoint.
@@ -118,6 +118,14 @@ tb_status tb_batch_run(tb_batch* batch, void* stream);
 tb_status tb_batch_results(tb_batch* batch, tb_result* out, void* stream);
 /* kernels launched by the last tb_batch_run (device work items, not host calls) */
 int64_t tb_batch_launches(const tb_batch* batch);
+/* Instrumentation (no counterpart in the reference, which only times its one
+ * launch with cudaEvent, src/xtb.cu:488-506).
+ * With tb_options.profile = 1: per kernel class of the last run, its name
+ * (name[i*32], NUL-terminated), launches, total device time in ms (CUDA events
+ * on the run's stream) and algorithmic work (flops or bytes, see units: 0 none,
+ * 1 FP64 flops, 2 bytes moved).  Returns the number of classes (<= max). */
+int32_t tb_batch_profile(const tb_batch* batch, int32_t max, char* names, int64_t* launches, double* ms,
+                         double* work, int32_t* units);
 void tb_batch_destroy(tb_batch* batch);
 
 /* ---- stage entry points (host buffers; one structure each) ---------------- */

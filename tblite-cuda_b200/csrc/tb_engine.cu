@@ -243,7 +243,22 @@ struct tb_batch {
   int* h_nactive = nullptr;  // pinned
   int64_t launches = 0;
   size_t bytes = 0;
-  ~tb_batch() { if (h_nactive) cudaFreeHost(h_nactive); }
+  std::vector<double> h_nocc;  // closed-shell occupied orbitals per structure (work accounting)
+  // kernel-class profile of the last run (tb_options.profile)
+  struct KClass {
+    std::string name;
+    int64_t launches = 0;
+    double ms = 0.0, work = 0.0;
+    int unit = 0;
+  };
+  std::vector<KClass> kclass;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pend;
+  std::vector<cudaEvent_t> evpool;
+  size_t evused = 0;
+  ~tb_batch() {
+    if (h_nactive) cudaFreeHost(h_nactive);
+    for (cudaEvent_t e : evpool) cudaEventDestroy(e);
+  }
 };
 
 namespace {
@@ -264,6 +279,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   b->h_mixoff.assign(nmol + 1, 0); b->h_moff.assign(nmol + 1, 0); b->h_poff.assign(nmol + 1, 0);
   std::vector<int> id, at_mol, sh_type, sh_at, sh_iao, at_ish, ao_at, ao_sh;
   b->h_xyz.clear();
+  b->h_nocc.clear();
   for (int m = 0; m < nmol; ++m) {
     const tb_structure& s = mols[m];
     if (s.nat <= 0 || !s.id || !s.xyz) return fail(TB_BAD_INPUT, "structure " + std::to_string(m) + ": empty or null");
@@ -289,6 +305,14 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
         nao += msao(sh.ang);
         nsh += 1;
       }
+    }
+    {
+      double nref = -s.charge;
+      for (int a = 0; a < s.nat; ++a) {
+        const SpeciesParam& sp = P.sp[s.id[a]];
+        for (int k = 0; k < sp.nsh; ++k) nref += P.sh[sp.sh0 + k].refocc;
+      }
+      b->h_nocc.push_back(std::ceil(0.5 * nref));
     }
     b->h_aoff[m + 1] = b->h_aoff[m] + s.nat;
     b->h_soff[m + 1] = b->h_soff[m] + nsh;
@@ -423,6 +447,59 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
 
 inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 
+// ---- kernel-class profiling (CUDA events on the run's stream)
+cudaEvent_t prof_event(tb_batch* b) {
+  if (b->evused == b->evpool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    b->evpool.push_back(e);
+  }
+  return b->evpool[b->evused++];
+}
+void prof_start(tb_batch* b, cudaStream_t st, cudaEvent_t* e0) {
+  if (!b->opt.profile) return;
+  *e0 = prof_event(b);
+  cudaEventRecord(*e0, st);
+}
+void prof_stop(tb_batch* b, cudaStream_t st, const char* name, cudaEvent_t e0, double work, int unit) {
+  if (!b->opt.profile) return;
+  cudaEvent_t e1 = prof_event(b);
+  cudaEventRecord(e1, st);
+  int idx = -1;
+  for (size_t i = 0; i < b->kclass.size(); ++i)
+    if (b->kclass[i].name == name) idx = (int)i;
+  if (idx < 0) {
+    b->kclass.push_back({});
+    idx = (int)b->kclass.size() - 1;
+    b->kclass[idx].name = name;
+    b->kclass[idx].unit = unit;
+  }
+  b->kclass[idx].launches += 1;
+  b->kclass[idx].work += work;
+  b->pend.push_back({idx, {e0, e1}});
+}
+tb_status prof_collect(tb_batch* b, cudaStream_t st) {
+  if (!b->opt.profile) return TB_OK;
+  TB_CUDA(cudaStreamSynchronize(st));
+  for (auto& p : b->pend) {
+    float ms = 0.f;
+    TB_CUDA(cudaEventElapsedTime(&ms, p.second.first, p.second.second));
+    b->kclass[p.first].ms += ms;
+  }
+  b->pend.clear();
+  return TB_OK;
+}
+
+// launch + error check + profile record of one kernel class
+#define TB_K(name, work, unit, ...)            \
+  do {                                         \
+    cudaEvent_t e0_ = nullptr;                 \
+    prof_start(b, st, &e0_);                   \
+    __VA_ARGS__;                               \
+    TB_LAUNCH_CHECK();                         \
+    prof_stop(b, st, name, e0_, work, unit);   \
+  } while (0)
+
 #define TB_LAUNCH_CHECK()                                                                  \
   do {                                                                                     \
     cudaError_t e_ = cudaGetLastError();                                                   \
@@ -432,40 +509,43 @@ inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 
 tb_status batch_run(tb_batch* b, cudaStream_t st) {
   tb_calculator* c = b->calc;
-  const DevParams P = c->dp;
   const DevBatch& B = b->db;
   MolState& S = b->ms;
   const int nmol = b->nmol;
   b->launches = 0;
-  DevParams Pc = P;
+  b->kclass.clear();
+  b->pend.clear();
+  b->evused = 0;
+  DevParams Pc = c->dp;
   Pc.intcut = integral_cutoff(b->opt.accuracy);
   Pc.cutoff = std::min(std::sqrt(2.0 * Pc.intcut / c->hp.min_alpha), 40.0);  // get_cutoff, src/basis/type.cu:43-64
   TB_CUDA(cudaMemsetAsync(S.status, 0, nmol * sizeof(int), st));
   TB_CUDA(cudaMemsetAsync(S.fermi_warn, 0, nmol * sizeof(int), st));
   TB_CUDA(cudaMemsetAsync(S.n_active, 0, sizeof(int), st));
-  // ---- setup
-  k_atoms<<<nblk(B.nat_tot, 128), 128, 0, st>>>(Pc, B, b->cn, b->mrad, b->erep, b->se);
-  TB_LAUNCH_CHECK();
-  k_adj_count<<<nblk((long long)B.nat_tot * 32, 256), 256, 0, st>>>(B, Pc.cutoff, b->cnt);
-  TB_LAUNCH_CHECK();
-  k_adj_scan<<<nmol, 256, 0, st>>>(B, b->cnt, b->inl, b->npair);
-  TB_LAUNCH_CHECK();
-  k_adj_fill<<<nblk((long long)B.nat_tot * 32, 256), 256, 0, st>>>(B, Pc.cutoff, b->inl, b->pair_i, b->pair_j);
-  TB_LAUNCH_CHECK();
+  // ---- setup (once per structure)
+  TB_K("atoms", 0, 0, k_atoms<<<nblk(B.nat_tot, 128), 128, 0, st>>>(Pc, B, b->cn, b->mrad, b->erep, b->se));
+  TB_K("adjacency", 0, 0,
+       k_adj_count<<<nblk((long long)B.nat_tot * 32, 256), 256, 0, st>>>(B, Pc.cutoff, b->cnt);
+       TB_LAUNCH_CHECK();
+       k_adj_scan<<<nmol, 256, 0, st>>>(B, b->cnt, b->inl, b->npair);
+       TB_LAUNCH_CHECK();
+       k_adj_fill<<<nblk((long long)B.nat_tot * 32, 256), 256, 0, st>>>(B, Pc.cutoff, b->inl, b->pair_i, b->pair_j));
   // S, H0, D, Q are contiguous in the layout: one memset covers 11 N^2
   TB_CUDA(cudaMemsetAsync(b->S, 0, (size_t)((char*)(b->Q + 6 * b->n2_tot) - (char*)b->S), st));
-  MatOut out{b->S, b->H0, b->D, b->Q};
-  const int maxsp = c->maxsh * c->maxsh;
-  const long long items = b->pair_cap * maxsp;
-  TB_CUDA(launch_integrals(Pc, B, b->npair, b->pair_i, b->pair_j, b->se, out, maxsp, items, c->lmask, st,
-                           &b->launches));
-  k_cholesky<<<nmol, 256, 0, st>>>(B, b->S, b->W, S.status, nullptr);
-  TB_LAUNCH_CHECK();
-  k_trinv<<<nmol, 256, 0, st>>>(B, b->W, b->X, S.status);
-  TB_LAUNCH_CHECK();
-  k_scf_init<<<nmol, 256, 0, st>>>(Pc, B, b->charge, b->uhf, b->erep, b->n0sh, b->q_in, S);
-  TB_LAUNCH_CHECK();
-  // ---- SCF
+  {
+    MatOut out{b->S, b->H0, b->D, b->Q};
+    const int maxsp = c->maxsh * c->maxsh;
+    const long long items = b->pair_cap * maxsp;
+    cudaEvent_t e0 = nullptr;
+    prof_start(b, st, &e0);
+    TB_CUDA(launch_integrals(Pc, B, b->npair, b->pair_i, b->pair_j, b->se, out, maxsp, items, c->lmask, st,
+                             &b->launches));
+    prof_stop(b, st, "integrals", e0, 0, 0);
+  }
+  TB_K("cholesky", 0, 0, k_cholesky<<<nmol, 256, 0, st>>>(B, b->S, b->W, S.status, nullptr));
+  TB_K("trinv", 0, 0, k_trinv<<<nmol, 256, 0, st>>>(B, b->W, b->X, S.status));
+  TB_K("scf_init", 0, 0, k_scf_init<<<nmol, 256, 0, st>>>(Pc, B, b->charge, b->uhf, b->erep, b->n0sh, b->q_in, S));
+  // ---- SCF (next_scf per iteration, src/scf/iterators.cu:317-424)
   const double econv = 1.0e-6 * b->opt.accuracy, pconv = 2.0e-5 * b->opt.accuracy;
   const int ntile64 = (int)b->tiles64.size(), ntile32 = (int)b->tiles32.size(), nchunk = (int)b->chunks32.size();
   const int gemm_grid = std::min(ntile64, 148 * 8);
@@ -474,46 +554,62 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
   const size_t fermi_smem = (size_t)b->nmax * sizeof(double);
   if (fermi_smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_fermi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fermi_smem));
   const dim3 pot_grid(nmol, nblk(std::max(b->natmax, b->nshmax), 256));
+  std::vector<int> act;
   for (int it = 0; it < b->opt.max_iter; ++it) {
-    if (it > 0) {
-      k_mix_next<<<nmol, 256, 0, st>>>(B, b->q_in, b->dq, b->dqlast, b->qlast, b->df, b->u, b->amat, b->omega,
-                                       b->opt.max_iter, b->opt.mixer_damping, S);
-      TB_LAUNCH_CHECK();
+    // algorithmic work of this iteration over the active structures (profile mode only)
+    double n3 = 0, n2 = 0, n2occ = 0;
+    if (b->opt.profile) {
+      act.resize(nmol);
+      TB_CUDA(cudaMemcpyAsync(act.data(), S.active, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
+      TB_CUDA(cudaStreamSynchronize(st));
+      for (int m = 0; m < nmol; ++m) {
+        if (!act[m]) continue;
+        const double n = b->h_ooff[m + 1] - b->h_ooff[m];
+        n3 += n * n * n;
+        n2 += n * n;
+        n2occ += n * n * std::min(n, b->h_nocc[m]);
+      }
     }
-    k_potential<<<pot_grid, 256, 0, st>>>(Pc, B, b->q_in, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, S.active);
-    TB_LAUNCH_CHECK();
-    k_fock<<<ntile32, 256, 0, st>>>(B, b->d_tiles32, ntile32, b->S, b->H0, b->D, b->Q, b->vsh, b->vat, b->vdp,
-                                    b->vqp, b->F, S.active);
-    TB_LAUNCH_CHECK();
-    // F' = X^T F X  (T = F X in W, then F' into F)
-    k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W,
-                                      1.0, 0.0, S.active);
-    TB_LAUNCH_CHECK();
-    k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F,
-                                      1.0, 0.0, S.active);
-    TB_LAUNCH_CHECK();
-    k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->w, b->perm, S.status, S.active);
-    TB_LAUNCH_CHECK();
-    k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S);
-    TB_LAUNCH_CHECK();
-    // C = X Z (eigenvectors in ascending order through perm), P = C diag(f) C^T
-    k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr, b->W,
-                                      1.0, 0.0, S.active);
-    TB_LAUNCH_CHECK();
-    k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P,
-                                      1.0, 0.0, S.active);
-    TB_LAUNCH_CHECK();
-    k_mulliken_cols<<<nchunk, 256, 0, st>>>(B, b->d_chunks32, nchunk, b->P, b->S, b->H0, b->D, b->Q, b->colred,
-                                            S.active);
-    TB_LAUNCH_CHECK();
-    k_finalize<<<nmol, 256, 0, st>>>(Pc, B, b->colred, b->n0sh, b->mrad, b->q_in, b->dq, b->qsh_out, b->qat_out,
-                                     b->dpat_out, b->qpat_out, econv, pconv, b->opt.max_iter, S);
-    TB_LAUNCH_CHECK();
+    if (it > 0)
+      TB_K("mix_next", 0, 0,
+           k_mix_next<<<nmol, 256, 0, st>>>(B, b->q_in, b->dq, b->dqlast, b->qlast, b->df, b->u, b->amat,
+                                            b->omega, b->opt.max_iter, b->opt.mixer_damping, S));
+    TB_K("potential", 0, 0,
+         k_potential<<<pot_grid, 256, 0, st>>>(Pc, B, b->q_in, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, S.active));
+    // Fock build: reads S, H0, D(3), Q(6), writes F -> 12 N^2 doubles
+    TB_K("fock", 96.0 * n2, 2,
+         k_fock<<<ntile32, 256, 0, st>>>(B, b->d_tiles32, ntile32, b->S, b->H0, b->D, b->Q, b->vsh, b->vat, b->vdp,
+                                         b->vqp, b->F, S.active));
+    // F' = X^T F X  (T = F X in W, then F' into F): 2 x 2N^3
+    TB_K("gemm", 2.0 * n3, 1,
+         k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->F, 0, b->X, 0, nullptr, nullptr, nullptr,
+                                           b->W, 1.0, 0.0, S.active));
+    TB_K("gemm", 2.0 * n3, 1,
+         k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 1, b->W, 0, nullptr, nullptr, nullptr,
+                                           b->F, 1.0, 0.0, S.active));
+    // symmetric eigensolve with vectors: canonical 4 N^3
+    TB_K("syev", 4.0 * n3, 1,
+         k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->w, b->perm, S.status, S.active));
+    TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
+    // C = X Z (eigenvectors in ascending order through perm): 2N^3; P = C diag(f) C^T: 2 N^2 n_occ
+    TB_K("gemm", 2.0 * n3, 1,
+         k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr,
+                                           b->W, 1.0, 0.0, S.active));
+    TB_K("gemm", 2.0 * n2occ, 1,
+         k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim,
+                                           b->P, 1.0, 0.0, S.active));
+    // Mulliken + band energy: reads P, S, H0, D(3), Q(6) -> 11 N^2 doubles
+    TB_K("mulliken", 88.0 * n2, 2,
+         k_mulliken_cols<<<nchunk, 256, 0, st>>>(B, b->d_chunks32, nchunk, b->P, b->S, b->H0, b->D, b->Q, b->colred,
+                                                 S.active));
+    TB_K("finalize", 0, 0,
+         k_finalize<<<nmol, 256, 0, st>>>(Pc, B, b->colred, b->n0sh, b->mrad, b->q_in, b->dq, b->qsh_out, b->qat_out,
+                                          b->dpat_out, b->qpat_out, econv, pconv, b->opt.max_iter, S));
     TB_CUDA(cudaMemcpyAsync(b->h_nactive, S.n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
     TB_CUDA(cudaStreamSynchronize(st));
     if (*b->h_nactive <= 0) break;
   }
-  return TB_OK;
+  return prof_collect(b, st);
 }
 
 tb_status batch_results(tb_batch* b, tb_result* out, cudaStream_t st) {
@@ -659,6 +755,21 @@ tb_status tb_batch_results(tb_batch* b, tb_result* out, void* stream) {
 }
 
 int64_t tb_batch_launches(const tb_batch* b) { return b ? b->launches : 0; }
+
+int32_t tb_batch_profile(const tb_batch* b, int32_t max, char* names, int64_t* launches, double* ms, double* work,
+                         int32_t* units) {
+  if (!b) return 0;
+  const int n = std::min<int>(max, (int)b->kclass.size());
+  for (int i = 0; i < n; ++i) {
+    const auto& k = b->kclass[i];
+    if (names) std::snprintf(names + 32 * i, 32, "%s", k.name.c_str());
+    if (launches) launches[i] = k.launches;
+    if (ms) ms[i] = k.ms;
+    if (work) work[i] = k.work;
+    if (units) units[i] = k.unit;
+  }
+  return n;
+}
 void tb_batch_destroy(tb_batch* b) { delete b; }
 
 tb_status tb_singlepoint_batch(tb_calculator* calc, const tb_structure* mols, int32_t nmol, const tb_options* opt,

@@ -36,7 +36,7 @@ class Structure(C.Structure):
 class Options(C.Structure):
     _fields_ = [("accuracy", C.c_double), ("kt", C.c_double), ("max_iter", C.c_int32),
                 ("mixer_damping", C.c_double), ("verbosity", C.c_int32), ("use_graphs", C.c_int32),
-                ("solver", C.c_int32), ("reserved", C.c_int32)]
+                ("solver", C.c_int32), ("profile", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -53,7 +53,7 @@ EXPORTS = [
     "tb_last_error", "tb_basis_size", "tb_singlepoint_batch", "tb_batch_create", "tb_batch_run",
     "tb_batch_results", "tb_batch_launches", "tb_batch_destroy", "tb_get_cutoff", "tb_adjacency_list",
     "tb_atomic_properties", "tb_repulsion", "tb_get_hamiltonian", "tb_coulomb_potential",
-    "tb_add_pot_to_h1", "tb_sygvd_batch", "tb_fermi_filling",
+    "tb_add_pot_to_h1", "tb_sygvd_batch", "tb_fermi_filling", "tb_batch_profile",
 ]
 
 _lib = None
@@ -198,6 +198,21 @@ class Batch:
 
     def launches(self) -> int:
         return int(load_library().tb_batch_launches(self.h))
+
+    def profile(self):
+        """Per kernel class of the last run: {name: (launches, ms, work, unit)} (needs profile=1)."""
+        n = 64
+        names = C.create_string_buffer(32 * n)
+        la = (C.c_int64 * n)()
+        ms = (C.c_double * n)()
+        wk = (C.c_double * n)()
+        un = (C.c_int32 * n)()
+        k = load_library().tb_batch_profile(self.h, C.c_int32(n), names, la, ms, wk, un)
+        out = {}
+        for i in range(k):
+            nm = names.raw[32 * i:32 * (i + 1)].split(b"\0", 1)[0].decode()
+            out[nm] = (int(la[i]), float(ms[i]), float(wk[i]), {0: None, 1: "flop", 2: "byte"}[un[i]])
+        return out
 
     def results(self, stream=None):
         L = load_library()
