@@ -169,6 +169,19 @@ tb_status tb_add_pot_to_h1(const tb_calculator* calc, const tb_structure* mol, c
 tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const double* S,
                          double* w, double* C);
 
+/* Allocation-free variant of tb_sygvd_batch for one problem, for callers that
+ * cannot let a library allocate device memory (frameworks that own all GPU
+ * memory through their own pool, latency-critical loops where cudaMalloc
+ * would synchronise the device, processes with a fixed memory budget).  No
+ * counterpart in the reference.  H, S (n x n, row-major), w (n) and C (n x n)
+ * are DEVICE pointers owned by the caller; every intermediate lives in a
+ * static ~2 MiB device array of the library (held by each GPU that loads the
+ * library until exit).  n <= 256, else TB_CAPACITY_EXCEEDED.  All calls on a
+ * device share that array: calls whose GPU work overlaps race, so serialise
+ * them.  The first call on a device looks up the array's address; make it
+ * before any stream capture.  Synchronous on `stream`. */
+tb_status tb_sygvd_noalloc(int32_t n, const double* H, const double* S, double* w, double* C, void* stream);
+
 /* get_fermi_filling (src/wavefunction/fermi.cu:100-124) for one spin channel. */
 tb_status tb_fermi_filling(int32_t n, double nel, double kt, const double* emo, double* occ,
                            double* efermi, double* ts);

@@ -656,6 +656,12 @@ tb_status batch_results(tb_batch* b, tb_result* out, cudaStream_t st) {
 
 }  // namespace
 
+// error text for the allocation-free entry point (tb_noalloc.cu)
+const char* tb_noalloc_set_error(const char* msg) {
+  g_err = msg;
+  return g_err.c_str();
+}
+
 // ====================================================================== C ABI
 extern "C" {
 
