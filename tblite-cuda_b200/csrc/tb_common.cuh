@@ -53,6 +53,7 @@ struct DevBatch {
   const int* at_ish;     // [nat_tot] local shell offset of the atom
   const int* ao_at;      // [nao_tot] local atom index
   const int* ao_sh;      // [nao_tot] local shell index
+  const int* order;      // [nmol] structures by decreasing N (one-CTA-per-structure kernels), may be null
 };
 
 __host__ __device__ inline int msao(int l) { return 2 * l + 1; }

@@ -330,9 +330,9 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
       for (int u = 0; u < (nao + 31) / 32; ++u) b->tiles32.push_back(make_int4(m, t, u, 0));
     }
   }
-  if (6 * (size_t)b->nmax * sizeof(double) > 220 * 1024)
+  if (b->nmax > kSyevMaxN)
     return fail(TB_CAPACITY_EXCEEDED, "structure with " + std::to_string(b->nmax) +
-                " AOs exceeds the in-house eigensolver limit (4693 AOs)");
+                " AOs exceeds the in-house eigensolver limit (" + std::to_string(kSyevMaxN) + " AOs)");
   b->nat_tot = b->h_aoff[nmol];
   b->nsh_tot = b->h_soff[nmol];
   b->nao_tot = b->h_ooff[nmol];
@@ -351,7 +351,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
          o_shat = L.add(NS * I4), o_shiao = L.add(NS * I4), o_atish = L.add(NA * I4), o_aoat = L.add(NO * I4),
          o_aosh = L.add(NO * I4), o_t64 = L.add(b->tiles64.size() * sizeof(int4)),
          o_t32 = L.add(b->tiles32.size() * sizeof(int4)), o_c32 = L.add(b->chunks32.size() * sizeof(int2)),
-         o_charge = L.add(NM * D8), o_uhf = L.add(NM * I4);
+         o_charge = L.add(NM * D8), o_uhf = L.add(NM * I4), o_order = L.add(NM * I4);
   const size_t meta_end = L.total;
   size_t o_cn = L.add(NA * D8), o_mrad = L.add(NA * D8), o_erep = L.add(NA * D8), o_se = L.add(NS * D8),
          o_n0sh = L.add(NS * D8), o_cnt = L.add(NA * I4), o_inl = L.add(NA * 8), o_npair = L.add(NM * I4),
@@ -406,6 +406,13 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   for (int m = 0; m < nmol; ++m) { ch[m] = mols[m].charge; uh[m] = mols[m].uhf; }
   put(o_charge, ch.data(), NM * D8);
   put(o_uhf, uh.data(), NM * I4);
+  // largest structures first: long eigensolves start early, small ones fill in (LPT)
+  std::vector<int> order(nmol);
+  for (int m = 0; m < nmol; ++m) order[m] = m;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+    return b->h_ooff[a + 1] - b->h_ooff[a] > b->h_ooff[c + 1] - b->h_ooff[c];
+  });
+  put(o_order, order.data(), NM * I4);
   TB_CUDA(cudaMemcpy(base, blob.data(), meta_end, cudaMemcpyHostToDevice));
 
   DevBatch& d = b->db;
@@ -416,6 +423,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   d.at_mol = at<int>(base, o_atmol); d.sh_type = at<int>(base, o_shtype); d.sh_at = at<int>(base, o_shat);
   d.sh_iao = at<int>(base, o_shiao); d.at_ish = at<int>(base, o_atish); d.ao_at = at<int>(base, o_aoat);
   d.ao_sh = at<int>(base, o_aosh);
+  d.order = at<int>(base, o_order);
   b->d_tiles64 = at<int4>(base, o_t64); b->d_tiles32 = at<int4>(base, o_t32); b->d_chunks32 = at<int2>(base, o_c32);
   b->charge = at<double>(base, o_charge); b->uhf = at<int>(base, o_uhf);
   b->cn = at<double>(base, o_cn); b->mrad = at<double>(base, o_mrad); b->erep = at<double>(base, o_erep);
@@ -549,7 +557,7 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
   const double econv = 1.0e-6 * b->opt.accuracy, pconv = 2.0e-5 * b->opt.accuracy;
   const int ntile64 = (int)b->tiles64.size(), ntile32 = (int)b->tiles32.size(), nchunk = (int)b->chunks32.size();
   const int gemm_grid = std::min(ntile64, 148 * 8);
-  const size_t eig_smem = 6 * (size_t)b->nmax * sizeof(double);
+  const size_t eig_smem = syev_smem_bytes(b->nmax);
   if (eig_smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_syev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eig_smem));
   const size_t fermi_smem = (size_t)b->nmax * sizeof(double);
   if (fermi_smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_fermi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fermi_smem));
@@ -994,7 +1002,7 @@ struct MatBatch {
       for (int t = 0; t < (n[m] + 63) / 64; ++t)
         for (int u = 0; u < (n[m] + 63) / 64; ++u) tiles.push_back(make_int4(m, t, u, 0));
     }
-    if (6 * (size_t)nmax * sizeof(double) > 220 * 1024) return fail(TB_CAPACITY_EXCEEDED, "matrix too large");
+    if (nmax > kSyevMaxN) return fail(TB_CAPACITY_EXCEEDED, "matrix too large for the in-house eigensolver");
     n2 = moff[nmat];
     no = ooff[nmat];
     Layout L;
@@ -1042,7 +1050,7 @@ tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const 
   k_trinv<<<nmat, 256>>>(B, mb.W, mb.X, mb.ms.status);
   k_gemm<<<grid, 256>>>(B, mb.d_tiles, nt, mb.F, 0, mb.X, 0, nullptr, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);
   k_gemm<<<grid, 256>>>(B, mb.d_tiles, nt, mb.X, 1, mb.W, 0, nullptr, nullptr, nullptr, mb.F, 1.0, 0.0, mb.ms.active);
-  const size_t smem = 6 * (size_t)mb.nmax * 8;
+  const size_t smem = syev_smem_bytes(mb.nmax);
   if (smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_syev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_syev<<<nmat, kEigThreads, smem>>>(B, mb.F, mb.Z, mb.w, mb.perm, mb.ms.status, mb.ms.active);
   k_gemm<<<grid, 256>>>(B, mb.d_tiles, nt, mb.X, 0, mb.Z, 1, mb.perm, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);

@@ -5,7 +5,11 @@
 
 namespace tb {
 
-constexpr int kEigThreads = 128;
+constexpr int kEigThreads = 256;
+constexpr int kRing = 8;  // QL sweeps buffered between the k_syev producer and consumers
+// shared memory of k_syev: d, e, tau, v, vn, p, w (7n) + the rotation ring (2 n kRing)
+inline size_t syev_smem_bytes(int n) { return (7 + 2 * (size_t)kRing) * (size_t)n * sizeof(double); }
+constexpr int kSyevMaxN = 1216;
 
 // Per-structure scalars of the SCF (device arrays of length nmol; nel is 2*nmol).
 struct MolState {

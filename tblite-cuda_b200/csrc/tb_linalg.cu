@@ -16,7 +16,7 @@ namespace tb {
 // result stored column-major in W (W[k][i] = L[i][k], i >= k).
 __global__ void k_cholesky(DevBatch B, const double* __restrict__ S, double* __restrict__ W,
                            int* __restrict__ status, const int* __restrict__ active) {
-  const int m = blockIdx.x;
+  const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;
   if (active && !active[m]) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
   const long long mo = B.moff[m];
@@ -57,7 +57,7 @@ __global__ void k_cholesky(DevBatch B, const double* __restrict__ S, double* __r
 // W[r][k] is a broadcast and X[k][c] a coalesced read.
 __global__ void k_trinv(DevBatch B, const double* __restrict__ W, double* __restrict__ X,
                         const int* __restrict__ status) {
-  const int m = blockIdx.x;
+  const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;
   if (status[m] != kStOk) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
   const long long mo = B.moff[m];
@@ -83,7 +83,7 @@ __global__ void k_trinv(DevBatch B, const double* __restrict__ W, double* __rest
 // C_m = alpha * op(A_m) * diag(ks_m) * op(B_m) + beta * C_m for every tile in
 // the list (structure, tile row, tile col).  Square n_m x n_m operands with
 // leading dimension n_m at offset moff[m]; K = kdim[m] if kdim != NULL.
-// op(B) may gather rows of B^T through perm (eigenvector reordering).
+// op(B) may gather its columns through perm (eigenvector reordering).
 constexpr int GT = 64, GK = 16;
 
 __global__ void __launch_bounds__(256) k_gemm(DevBatch B, const int4* __restrict__ tiles, int ntiles,
@@ -128,12 +128,8 @@ __global__ void __launch_bounds__(256) k_gemm(DevBatch B, const int4* __restrict
         const int gj = j0 + jj, gk2 = k0 + kb;
         double u = 0.0;
         if (gj < n && gk2 < K) {
-          if (tb_) {
-            const int row = pm ? pm[gj] : gj;
-            u = Bm[(long long)row * n + gk2];
-          } else {
-            u = Bm[(long long)gk2 * n + gj];
-          }
+          const int col = pm ? pm[gj] : gj;  // eigenvector reordering through perm
+          u = tb_ ? Bm[(long long)col * n + gk2] : Bm[(long long)gk2 * n + col];
         }
         Bs[buf][kb][jj] = u;
       }
@@ -174,11 +170,100 @@ __global__ void __launch_bounds__(256) k_gemm(DevBatch B, const int4* __restrict
 
 // ------------------------------------------------------------ eigensolver
 // Symmetric eigenproblem of A (n x n, row-major, overwritten) for every
-// active structure: w ascending, eigenvector j = row perm[j] of Zc.
-__global__ void __launch_bounds__(kEigThreads) k_syev(DevBatch B, double* __restrict__ Ab, double* __restrict__ Zb,
+// active structure, one CTA per structure: w ascending, eigenvector j =
+// row perm[j] of Zc (n x n, one eigenvector per row).
+//
+//  1. Householder tridiagonalisation.  Step k's rank-2 update of the trailing
+//     block and step k+1's product A22 v are done in ONE read+write pass over
+//     the block (thread per column, rows in groups of 8), so each step moves
+//     16 mm^2 bytes instead of 24 mm^2.  Reflector k is kept in row k of A.
+//  2. Q = H_0 ... H_{n-3} accumulated backwards as Zc = Q^T, again with the
+//     update of step k and the dot products of step k-1 in one pass.
+//  3. Implicit QL with Wilkinson shift.  Warp 0 (lane 0) runs the scalar
+//     rotation chain of sweep q+1 while warps 1.. apply sweep q to rows (i,i+1)
+//     of Zc, coalesced across columns; sweeps are handed over through a 2-slot shared-memory ring guarded by
+//     counters.  Every wait is bounded: on timeout the structure is marked
+//     failed and all warps leave.
+//  4. Ascending order by rank (ties by index).
+namespace {
+
+constexpr int kRowBatch = 12;
+constexpr int kWaveK = 4;            // QL sweeps applied per pass over Zc
+constexpr int kWin = 2 * kWaveK;     // rows of Zc in flight per column
+constexpr long long kSpinLimit = 1LL << 24;
+
+__device__ inline double block_sum_syev(double v, double* red) { return block_sum(v, red); }
+
+// Householder reflector of row k: x = A[k][k+1..n-1] -> tau[k], e[k] and v
+// (v[0] = 1), written to `v` and back into row k.
+__device__ void reflector(double* A, int n, int k, double* v, double* tau, double* e, double* red, double* sh) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int mm = n - k - 1;
+  double* rowk = A + (long long)k * n + k + 1;
+  double part = 0.0;
+  for (int i = 1 + tid; i < mm; i += nt) part += rowk[i] * rowk[i];
+  const double sigma = block_sum_syev(part, red);
+  if (tid == 0) {
+    const double alpha = rowk[0];
+    if (sigma == 0.0) {
+      tau[k] = 0.0; e[k] = alpha; sh[0] = 0.0; sh[1] = 0.0;
+    } else {
+      const double r = sqrt(alpha * alpha + sigma);
+      const double beta = alpha <= 0.0 ? r : -r;
+      tau[k] = (beta - alpha) / beta;
+      e[k] = beta;
+      sh[0] = tau[k];
+      sh[1] = 1.0 / (alpha - beta);
+    }
+  }
+  __syncthreads();
+  const double scal = sh[1];
+  const bool refl = sh[0] != 0.0;
+  for (int i = tid; i < mm; i += nt) {
+    const double x = i == 0 ? 1.0 : (refl ? rowk[i] * scal : 0.0);
+    v[i] = x;
+    if (refl) rowk[i] = x;
+  }
+  __syncthreads();
+}
+
+// Column walk over the block rows r0..r0+nr-1, columns c0..c0+nc-1 of a
+// row-major matrix M: optionally M[r][c] -= a_r b_c + b_r a_c (with a, b
+// indexed from the block's origin), and acc_c = sum_r M_new[r][c] * x_r.
+__device__ void colwalk(double* M, int n, int r0, int nr, int c0, int nc, bool upd, const double* a,
+                        const double* b, int aoff, const double* x, double* out, double scale) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int jj = tid; jj < nc; jj += nt) {
+    const int c = c0 + jj;
+    const double aj = upd ? a[aoff + c0 - r0 + jj] : 0.0, bj = upd ? b[aoff + c0 - r0 + jj] : 0.0;
+    double acc = 0.0;
+    for (int i0 = 0; i0 < nr; i0 += kRowBatch) {
+      double q[kRowBatch];
+#pragma unroll
+      for (int u = 0; u < kRowBatch; ++u)
+        q[u] = (i0 + u < nr) ? M[(long long)(r0 + i0 + u) * n + c] : 0.0;
+#pragma unroll
+      for (int u = 0; u < kRowBatch; ++u) {
+        if (i0 + u < nr) {
+          if (upd) {
+            const int ri = aoff + i0 + u;
+            q[u] -= a[ri] * bj + b[ri] * aj;
+            M[(long long)(r0 + i0 + u) * n + c] = q[u];
+          }
+          acc += q[u] * x[i0 + u];
+        }
+      }
+    }
+    out[jj] = scale * acc;
+  }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __restrict__ Ab, double* __restrict__ Zb,
                                                       double* __restrict__ wout, int* __restrict__ perm,
                                                       int* __restrict__ status, const int* __restrict__ active) {
-  const int m = blockIdx.x;
+  const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;  // largest structures first
   if (active && !active[m]) return;
   if (status[m] != kStOk) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
@@ -187,17 +272,19 @@ __global__ void __launch_bounds__(kEigThreads) k_syev(DevBatch B, double* __rest
   double* A = Ab + mo;
   double* Z = Zb + mo;
   extern __shared__ double sm[];
-  double* d = sm;             // n
-  double* e = d + n;          // n
-  double* tau = e + n;        // n
-  double* vs = tau + n;       // n
-  double* ps = vs + n;        // n (reused for rotation cosines)
-  double* ws = ps + n;        // n (reused for rotation sines)
+  double* d = sm;          // n
+  double* e = d + n;       // n
+  double* tau = e + n;     // n
+  double* v = tau + n;     // n
+  double* vn = v + n;      // n
+  double* p = vn + n;      // n
+  double* w = p + n;       // n
+  double* ring = w + n;    // kRing slots x (n cosines + n sines)
   __shared__ double red[kEigThreads / 32];
-  __shared__ double sh_scal, sh_tau;
-  __shared__ int sh_m, sh_cnt, sh_fail;
+  __shared__ double sh[4];
+  __shared__ int q_full, q_end, q_fail, sh_head[kRing][2];
+  __shared__ int q_done[kEigThreads / 32];  // sweeps finished, per consumer warp
   const int tid = threadIdx.x, nt = blockDim.x;
-  const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
 
   // symmetrise
   for (long long x = tid; x < (long long)n * n; x += nt) {
@@ -211,155 +298,285 @@ __global__ void __launch_bounds__(kEigThreads) k_syev(DevBatch B, double* __rest
   for (int i = tid; i < n; i += nt) { e[i] = 0.0; tau[i] = 0.0; }
   __syncthreads();
 
-  // ---- Householder tridiagonalisation; reflector k stored in row k of A
-  for (int k = 0; k + 2 < n; ++k) {
-    const int mm = n - k - 1;
-    double* rowk = A + (long long)k * n + k + 1;
-    double part = 0.0;
-    for (int i = 1 + tid; i < mm; i += nt) part += rowk[i] * rowk[i];
-    const double sigma = block_sum(part, red);
-    if (tid == 0) {
-      const double alpha = rowk[0];
-      if (sigma == 0.0) {
-        tau[k] = 0.0; e[k] = alpha; sh_tau = 0.0; sh_scal = 0.0;
-      } else {
-        const double r = sqrt(alpha * alpha + sigma);
-        const double beta = alpha <= 0.0 ? r : -r;
-        tau[k] = (beta - alpha) / beta;
-        e[k] = beta;
-        sh_tau = tau[k];
-        sh_scal = 1.0 / (alpha - beta);
+  // ---- 1. tridiagonalisation
+  if (n >= 3) {
+    reflector(A, n, 0, v, tau, e, red, sh);
+    // p0 = tau0 * A[1..][1..] v0
+    colwalk(A, n, 1, n - 1, 1, n - 1, false, nullptr, nullptr, 0, v, p, tau[0]);
+    __syncthreads();
+    for (int k = 0; k + 2 < n; ++k) {
+      const int mm = n - k - 1, b0 = k + 1;
+      const double tk = tau[k];
+      // w = p - (tau/2)(p.v) v
+      double part = 0.0;
+      for (int j = tid; j < mm; j += nt) part += p[j] * v[j];
+      const double pv = block_sum_syev(part, red);
+      const double kk = 0.5 * tk * pv;
+      for (int j = tid; j < mm; j += nt) w[j] = p[j] - kk * v[j];
+      __syncthreads();
+      const bool upd = tk != 0.0;
+      // (a) first row of the block
+      if (upd)
+        for (int j = tid; j < mm; j += nt) A[(long long)b0 * n + b0 + j] -= v[0] * w[j] + w[0] * v[j];
+      __syncthreads();
+      if (k + 3 < n) {
+        reflector(A, n, k + 1, vn, tau, e, red, sh);
+        // (c) rest of the block, fused with p_{k+1} = tau_{k+1} A22' v_{k+1}
+        colwalk(A, n, b0 + 1, mm - 1, b0 + 1, mm - 1, upd, v, w, 1, vn, p, tau[k + 1]);
+      } else if (upd) {
+        colwalk(A, n, b0 + 1, mm - 1, b0 + 1, mm - 1, true, v, w, 1, vn, p, 0.0);
       }
+      __syncthreads();
+      double* t = v; v = vn; vn = t;
     }
-    __syncthreads();
-    const double tk = sh_tau;
-    if (tk == 0.0) continue;  // uniform across the block
-    const double scal = sh_scal;
-    for (int i = tid; i < mm; i += nt) {
-      const double v = i == 0 ? 1.0 : rowk[i] * scal;
-      vs[i] = v;
-      rowk[i] = v;
-    }
-    __syncthreads();
-    // p = tau * A22 v (one warp per row)
-    double* A22 = A + (long long)(k + 1) * n + k + 1;
-    for (int i = wid; i < mm; i += nw) {
-      const double* ar = A22 + (long long)i * n;
-      double s = 0.0;
-      for (int j = lane; j < mm; j += 32) s += ar[j] * vs[j];
-      s = warp_sum(s);
-      if (lane == 0) ps[i] = tk * s;
-    }
-    __syncthreads();
-    part = 0.0;
-    for (int i = tid; i < mm; i += nt) part += ps[i] * vs[i];
-    const double pv = block_sum(part, red);
-    const double kk = 0.5 * tk * pv;
-    for (int i = tid; i < mm; i += nt) ws[i] = ps[i] - kk * vs[i];
-    __syncthreads();
-    for (long long x = tid; x < (long long)mm * mm; x += nt) {
-      const int i = (int)(x / mm), j = (int)(x % mm);
-      A22[(long long)i * n + j] -= vs[i] * ws[j] + ws[i] * vs[j];
-    }
-    __syncthreads();
   }
   for (int i = tid; i < n; i += nt) d[i] = A[(long long)i * n + i];
   if (tid == 0 && n >= 2) e[n - 2] = A[(long long)(n - 2) * n + n - 1];
   __syncthreads();
 
-  // ---- Zc = Q^T (row c of Zc = column c of Q), backward accumulation
+  // ---- 2. Zc = Q^T (row c of Zc = column c of Q) by backward accumulation:
+  // Zc22 <- Zc22 (I - tau v v^T), one warp per row of Zc; the dot product
+  // u'_c = Zc_new[c][.] v' of the next step (k-1) is fused into the same pass.
   for (long long x = tid; x < (long long)n * n; x += nt) Z[x] = ((x / n) == (x % n)) ? 1.0 : 0.0;
   __syncthreads();
-  for (int k = n - 3; k >= 0; --k) {
-    const double tk = tau[k];
-    if (tk == 0.0) continue;
-    const int mm = n - k - 1;
-    const double* rowk = A + (long long)k * n + k + 1;
-    for (int i = tid; i < mm; i += nt) vs[i] = rowk[i];
-    __syncthreads();
-    double* Z22 = Z + (long long)(k + 1) * n + k + 1;
-    for (int c = wid; c < mm; c += nw) {
-      double* zr = Z22 + (long long)c * n;
-      double s = 0.0;
-      for (int r = lane; r < mm; r += 32) s += zr[r] * vs[r];
-      s = warp_sum(s) * tk;
-      for (int r = lane; r < mm; r += 32) zr[r] -= s * vs[r];
+  {
+    const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+    int k = n - 3;
+    if (k >= 0) {
+      // first applied step: Zc22 is the identity, so u_c = v_c
+      const int mm = n - k - 1;
+      for (int i = tid; i < mm; i += nt) { v[i] = i == 0 ? 1.0 : A[(long long)k * n + k + 1 + i]; w[i] = v[i]; }
+      __syncthreads();
     }
-    __syncthreads();
-  }
-
-  // ---- implicit QL; rotations of one sweep in (ps, ws), applied to rows of Zc
-  if (tid == 0) { sh_fail = 0; e[n - 1] = 0.0; }
-  __syncthreads();
-  const double eps = 2.220446049250313e-16;
-  for (int l = 0; l < n; ++l) {
-    int iter = 0;
-    for (;;) {
-      if (tid == 0) {
-        int mq = l;
-        for (; mq < n - 1; ++mq) {
-          const double dd = fabs(d[mq]) + fabs(d[mq + 1]);
-          if (fabs(e[mq]) <= eps * dd) break;
-        }
-        sh_m = mq;
-        sh_cnt = 0;
-        if (mq != l) {
-          if (++iter > 60) {
-            sh_fail = 1;
-          } else {
-            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-            double r = sqrt(g * g + 1.0);
-            g = d[mq] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
-            double s = 1.0, c = 1.0, p = 0.0;
-            int i = mq - 1;
-            bool underflow = false;
-            for (; i >= l; --i) {
-              const double f = s * e[i];
-              const double b = c * e[i];
-              r = sqrt(f * f + g * g);
-              e[i + 1] = r;
-              if (r == 0.0) { d[i + 1] -= p; e[mq] = 0.0; underflow = true; break; }
-              const double ri = 1.0 / r;
-              s = f * ri;
-              c = g * ri;
-              g = d[i + 1] - p;
-              r = (d[i] - g) * s + 2.0 * c * b;
-              p = s * r;
-              d[i + 1] = g + p;
-              g = c * r - b;
-              ps[sh_cnt] = c;
-              ws[sh_cnt] = s;
-              ++sh_cnt;
+    for (; k >= 0; --k) {
+      const int mm = n - k - 1, b0 = k + 1;
+      const double tk = tau[k];
+      // v' of step k-1 (its block starts at index k): v'_0 = 1, v'_i = A[k-1][k+i]
+      if (k >= 1)
+        for (int i = tid; i <= mm; i += nt) vn[i] = i == 0 ? 1.0 : A[(long long)(k - 1) * n + k + i];
+      __syncthreads();
+      for (int c = wid; c < mm; c += nw) {
+        double* zr = Z + (long long)(b0 + c) * n + b0;
+        const double tu = tk * w[c];
+        double acc = 0.0;
+        for (int r0 = 0; r0 < mm; r0 += 32 * kRowBatch) {
+          double q[kRowBatch];
+#pragma unroll
+          for (int u = 0; u < kRowBatch; ++u) {
+            const int r = r0 + lane + 32 * u;
+            q[u] = r < mm ? zr[r] : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < kRowBatch; ++u) {
+            const int r = r0 + lane + 32 * u;
+            if (r < mm) {
+              if (tk != 0.0) {
+                q[u] -= tu * v[r];
+                zr[r] = q[u];
+              }
+              acc += q[u] * vn[r + 1];
             }
-            if (!underflow) { d[l] -= p; e[l] = g; e[mq] = 0.0; }
           }
         }
-      }
-      __syncthreads();
-      const int mq = sh_m, cnt = sh_cnt, failed = sh_fail;
-      __syncthreads();  // everyone has read the sweep bounds before thread 0 rewrites them
-      if (mq == l || failed) break;
-      // apply rotations i = mq-1, mq-2, ... (cnt of them) to rows i, i+1 of Zc
-      for (int r = tid; r < n; r += nt) {
-        double f = Z[(long long)mq * n + r];
-        for (int t = 0; t < cnt; ++t) {
-          const int i = mq - 1 - t;
-          const double c = ps[t], s = ws[t];
-          const double z = Z[(long long)i * n + r];
-          Z[(long long)(i + 1) * n + r] = s * z + c * f;
-          f = c * z - s * f;
+        if (k >= 1) {
+          acc = warp_sum(acc);
+          if (lane == 0) p[c + 1] = acc;  // p is free scratch here
         }
-        Z[(long long)(mq - cnt) * n + r] = f;
       }
       __syncthreads();
+      if (k >= 1) {
+        // next step: v <- v'; u'_0 = Zc[k][k..] . v' = 1 (row k of Zc is still e_k)
+        for (int i = tid; i <= mm; i += nt) { v[i] = vn[i]; w[i] = i == 0 ? 1.0 : p[i]; }
+        __syncthreads();
+      }
     }
-    if (sh_fail) break;  // written before the last barrier, uniform
   }
-  if (sh_fail) {
+
+  // ---- 3. implicit QL, producer (warp 0) / consumers (warps 1..)
+  if (tid == 0) { q_full = 0; q_end = 0; q_fail = 0; e[n - 1] = 0.0; }
+  if (tid < kEigThreads / 32) q_done[tid] = 0;
+  __syncthreads();
+  const int ncons = (nt >> 5) - 1;
+  if (tid < 32) {
+    // producer warp: the deflation scan is warp-parallel (ballot over 32
+    // consecutive indices), the rotation chain runs on lane 0
+    const int lane = tid;
+    const double eps = 2.220446049250313e-16;
+    int q = 0;
+    bool fail = false;
+    for (int l = 0; l < n && !fail; ++l) {
+      int iter = 0;
+      for (;;) {
+        int mq = n - 1;
+        for (int base = l; base < n - 1; base += 32) {
+          const int i = base + lane;
+          bool small = false;
+          if (i < n - 1) {
+            const double dd = fabs(d[i]) + fabs(d[i + 1]);
+            small = fabs(e[i]) <= eps * dd;
+          }
+          const unsigned bal = __ballot_sync(0xffffffffu, small);
+          if (bal) { mq = base + __ffs(bal) - 1; break; }
+        }
+        if (mq == l) break;
+        if (++iter > 60) { fail = true; break; }
+        // the ring slot of sweep q held sweep q-kRing: wait until EVERY consumer
+        // warp has finished it (warps progress unevenly)
+        const int slot = q % kRing;
+        if (q >= kRing) {
+          if (lane == 0) {
+            long long spins = 0;
+            for (int cw = 1; cw <= ncons && !fail; ++cw)
+              while (*(volatile int*)&q_done[cw] < q - kRing + 1) {
+                if (++spins > kSpinLimit) { fail = true; break; }
+                __nanosleep(64);
+              }
+          }
+          fail = __shfl_sync(0xffffffffu, fail, 0);
+          if (fail) break;
+          __threadfence_block();
+        }
+        if (lane == 0) {
+          double* rc = ring + (size_t)slot * 2 * n;
+          double* rs = rc + n;
+          double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+          double r = sqrt(g * g + 1.0);
+          g = d[mq] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
+          double s = 1.0, c = 1.0, pp = 0.0;
+          int cnt = 0;
+          bool underflow = false;
+          for (int i = mq - 1; i >= l; --i) {
+            const double f = s * e[i];
+            const double bb = c * e[i];
+            const double rr2 = f * f + g * g;
+            if (rr2 == 0.0) { d[i + 1] -= pp; e[mq] = 0.0; underflow = true; break; }
+            const double ri = rsqrt(rr2);
+            r = rr2 * ri;
+            e[i + 1] = r;
+            s = f * ri;
+            c = g * ri;
+            g = d[i + 1] - pp;
+            r = (d[i] - g) * s + 2.0 * c * bb;
+            pp = s * r;
+            d[i + 1] = g + pp;
+            g = c * r - bb;
+            rc[cnt] = c;
+            rs[cnt] = s;
+            ++cnt;
+          }
+          if (!underflow) { d[l] -= pp; e[l] = g; e[mq] = 0.0; }
+          sh_head[slot][0] = mq;
+          sh_head[slot][1] = cnt;
+          __threadfence_block();
+          *(volatile int*)&q_full = q + 1;
+        }
+        __syncwarp();  // d and e of this sweep are visible to the whole warp
+        ++q;
+      }
+    }
+    if (lane == 0) {
+      if (fail) *(volatile int*)&q_fail = 1;
+      __threadfence_block();
+      *(volatile int*)&q_end = 1;
+    }
+  } else {
+    // consumers: every column r of Zc owned by this thread (r = tid - 32 + k*(nt-32)).
+    // Sweeps are taken in groups of kWaveK and applied as a wavefront: sweep k
+    // of the group lags sweep k-1 by two rows, so each column streams through
+    // a window of 2*kWaveK rows held in registers and every element is loaded
+    // and stored once per group instead of once per sweep.
+    const int lane = tid & 31;
+    int q0 = 0;
+    for (;;) {
+      long long spins = 0;
+      int full;
+      bool quit = false;
+      while ((full = *(volatile int*)&q_full) < q0 + kWaveK) {
+        if (*(volatile int*)&q_end) {
+          __threadfence_block();
+          full = *(volatile int*)&q_full;
+          if (full <= q0) quit = true;
+          break;
+        }
+        if (++spins > kSpinLimit) { *(volatile int*)&q_fail = 1; quit = true; break; }
+        __nanosleep(32);
+      }
+      if (quit) break;
+      __threadfence_block();
+      const int kg = min(kWaveK, full - q0);
+      int mk[kWaveK], lk[kWaveK];
+      const double* ck[kWaveK];
+      int mx = 0, lmin = n;
+#pragma unroll
+      for (int k = 0; k < kWaveK; ++k) {
+        const int slot = (q0 + k) % kRing;
+        ck[k] = ring + (size_t)slot * 2 * n;
+        if (k < kg) {
+          mk[k] = sh_head[slot][0];
+          lk[k] = mk[k] - sh_head[slot][1];
+          mx = max(mx, mk[k]);
+          lmin = min(lmin, lk[k]);
+        } else {
+          mk[k] = -1;  // inactive: no index satisfies lk <= i <= mk - 1
+          lk[k] = 0;
+        }
+      }
+      const int J = mx - lmin + 2 * (kg - 1);
+      const int nblk = (J + kWin - 1) / kWin;
+      for (int r = tid - 32; r < n; r += nt - 32) {
+        double* zr = Z + r;
+        double wv[kWin];
+        wv[0] = 0.0;
+#pragma unroll
+        for (int a = 1; a < kWin; ++a) {
+          const int row = mx - 1 + a;
+          wv[a] = row <= n - 1 ? zr[(long long)row * n] : 0.0;
+        }
+        for (int blk = 0; blk < nblk; ++blk) {
+#pragma unroll
+          for (int p = 0; p < kWin; ++p) {
+            const int j = blk * kWin + p;
+            const int sl = (kWin - p) % kWin;
+            const int row_out = mx + kWin - 1 - j;
+            if (j >= 1 && row_out >= 0 && row_out <= n - 1) zr[(long long)row_out * n] = wv[sl];
+            const int row_in = mx - 1 - j;
+            wv[sl] = row_in >= 0 ? zr[(long long)row_in * n] : 0.0;
+#pragma unroll
+            for (int k = 0; k < kWaveK; ++k) {
+              const int i = mx - 1 - j + 2 * k;
+              if (i >= lk[k] && i <= mk[k] - 1) {
+                const int t = mk[k] - 1 - i;
+                const double c = ck[k][t], sn = ck[k][n + t];
+                const int ia = (2 * k - p + 2 * kWin) % kWin, ib = (2 * k + 1 - p + 2 * kWin) % kWin;
+                const double x = wv[ia], y = wv[ib];
+                wv[ib] = sn * x + c * y;
+                wv[ia] = c * x - sn * y;
+              }
+            }
+          }
+        }
+        // flush the final window (last step has phase kWin - 1)
+        const int jl = nblk * kWin - 1;
+#pragma unroll
+        for (int a = 0; a < kWin; ++a) {
+          const int row = mx - 1 - jl + a;
+          if (row >= 0 && row <= n - 1) zr[(long long)row * n] = wv[(a + 1) % kWin];
+        }
+      }
+      __syncwarp();
+      q0 += kg;
+      if (lane == 0) {
+        __threadfence_block();
+        *(volatile int*)&q_done[tid >> 5] = q0;
+      }
+    }
+  }
+  __syncthreads();
+  if (q_fail) {
     if (tid == 0) status[m] = kStEigenFailed;  // k_fermi retires the structure
     return;
   }
-  // ---- ascending order by rank (ties by index)
+  // ---- 4. ascending order by rank (ties by index)
   for (int i = tid; i < n; i += nt) {
     const double di = d[i];
     int rank = 0;
