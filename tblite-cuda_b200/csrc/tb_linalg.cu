@@ -187,7 +187,8 @@ __global__ void __launch_bounds__(256) k_gemm(DevBatch B, const int4* __restrict
 //  4. Ascending order by rank (ties by index).
 namespace {
 
-constexpr int kRowBatch = 12;
+constexpr int kWalkBatch = 12;  // rows per load batch in the Householder column walk
+constexpr int kQBatch = 8;      // 32-wide row segments per load batch in the Q accumulation
 constexpr int kWaveK = 4;            // QL sweeps applied per pass over Zc
 constexpr int kWin = 2 * kWaveK;     // rows of Zc in flight per column
 constexpr long long kSpinLimit = 1LL << 24;
@@ -229,7 +230,9 @@ __device__ void reflector(double* A, int n, int k, double* v, double* tau, doubl
 
 // Column walk over the block rows r0..r0+nr-1, columns c0..c0+nc-1 of a
 // row-major matrix M: optionally M[r][c] -= a_r b_c + b_r a_c (with a, b
-// indexed from the block's origin), and acc_c = sum_r M_new[r][c] * x_r.
+// indexed from the block's origin), and out_c = scale * sum_r M_new[r][c] x_r.
+// One thread per column; rows are loaded in batches of kWalkBatch before any
+// of them is written back, so a batch costs about one L2 round trip.
 __device__ void colwalk(double* M, int n, int r0, int nr, int c0, int nc, bool upd, const double* a,
                         const double* b, int aoff, const double* x, double* out, double scale) {
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -237,13 +240,13 @@ __device__ void colwalk(double* M, int n, int r0, int nr, int c0, int nc, bool u
     const int c = c0 + jj;
     const double aj = upd ? a[aoff + c0 - r0 + jj] : 0.0, bj = upd ? b[aoff + c0 - r0 + jj] : 0.0;
     double acc = 0.0;
-    for (int i0 = 0; i0 < nr; i0 += kRowBatch) {
-      double q[kRowBatch];
+    for (int i0 = 0; i0 < nr; i0 += kWalkBatch) {
+      double q[kWalkBatch];
 #pragma unroll
-      for (int u = 0; u < kRowBatch; ++u)
+      for (int u = 0; u < kWalkBatch; ++u)
         q[u] = (i0 + u < nr) ? M[(long long)(r0 + i0 + u) * n + c] : 0.0;
 #pragma unroll
-      for (int u = 0; u < kRowBatch; ++u) {
+      for (int u = 0; u < kWalkBatch; ++u) {
         if (i0 + u < nr) {
           if (upd) {
             const int ri = aoff + i0 + u;
@@ -355,32 +358,46 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
       if (k >= 1)
         for (int i = tid; i <= mm; i += nt) vn[i] = i == 0 ? 1.0 : A[(long long)(k - 1) * n + k + i];
       __syncthreads();
-      for (int c = wid; c < mm; c += nw) {
-        double* zr = Z + (long long)(b0 + c) * n + b0;
-        const double tu = tk * w[c];
-        double acc = 0.0;
-        for (int r0 = 0; r0 < mm; r0 += 32 * kRowBatch) {
-          double q[kRowBatch];
+      for (int c = wid; c < mm; c += 2 * nw) {
+        // rows c and c + nw of the block (the second may not exist)
+        const int c2 = c + nw;
+        const bool two = c2 < mm;
+        double* za = Z + (long long)(b0 + c) * n + b0;
+        double* zb = Z + (long long)(b0 + (two ? c2 : c)) * n + b0;
+        const double ta = tk * w[c], tb = two ? tk * w[c2] : 0.0;
+        double acca = 0.0, accb = 0.0;
+        for (int r0 = 0; r0 < mm; r0 += 32 * kQBatch) {
+          double qa[kQBatch], qb[kQBatch];
 #pragma unroll
-          for (int u = 0; u < kRowBatch; ++u) {
+          for (int u = 0; u < kQBatch; ++u) {
             const int r = r0 + lane + 32 * u;
-            q[u] = r < mm ? zr[r] : 0.0;
+            qa[u] = r < mm ? za[r] : 0.0;
+            qb[u] = (two && r < mm) ? zb[r] : 0.0;
           }
 #pragma unroll
-          for (int u = 0; u < kRowBatch; ++u) {
+          for (int u = 0; u < kQBatch; ++u) {
             const int r = r0 + lane + 32 * u;
             if (r < mm) {
               if (tk != 0.0) {
-                q[u] -= tu * v[r];
-                zr[r] = q[u];
+                qa[u] -= ta * v[r];
+                za[r] = qa[u];
+                if (two) {
+                  qb[u] -= tb * v[r];
+                  zb[r] = qb[u];
+                }
               }
-              acc += q[u] * vn[r + 1];
+              acca += qa[u] * vn[r + 1];
+              accb += qb[u] * vn[r + 1];
             }
           }
         }
         if (k >= 1) {
-          acc = warp_sum(acc);
-          if (lane == 0) p[c + 1] = acc;  // p is free scratch here
+          acca = warp_sum(acca);
+          accb = warp_sum(accb);
+          if (lane == 0) {
+            p[c + 1] = acca;  // p is free scratch here
+            if (two) p[c2 + 1] = accb;
+          }
         }
       }
       __syncthreads();
