@@ -54,7 +54,12 @@ struct DevBatch {
   const int* ao_at;      // [nao_tot] local atom index
   const int* ao_sh;      // [nao_tot] local shell index
   const int* order;      // [nmol] structures by decreasing N (one-CTA-per-structure kernels), may be null
+  int lib_above;         // 0: every structure on the in-house kernels; else structures with N > lib_above
+                         // (all of them when -1) are factorised and diagonalised by the library path
 };
+
+// True when structure size n is handled by the library (cuSOLVER) path.
+__host__ __device__ inline bool on_library(const DevBatch& B, int n) { return B.lib_above != 0 && n > B.lib_above; }
 
 __host__ __device__ inline int msao(int l) { return 2 * l + 1; }
 __host__ __device__ inline int mlao(int l) { return (l + 1) * (l + 2) / 2; }

@@ -241,6 +241,14 @@ struct tb_batch {
   int4 *d_tiles64, *d_tiles32;
   int2* d_chunks32;
   int* h_nactive = nullptr;  // pinned
+  // structures above the in-house size bound: cuSOLVER path (tb_large.cu)
+  std::vector<int> big;
+  int nmax_in = 0;           // largest N on the in-house eigensolver
+  LargeSolver lib;
+  void* lib_work = nullptr;
+  size_t lib_bytes = 0;
+  int* lib_info = nullptr;   // 2 per library structure
+  std::vector<int> h_active, h_status;
   int64_t launches = 0;
   size_t bytes = 0;
   std::vector<double> h_nocc;  // closed-shell occupied orbitals per structure (work accounting)
@@ -330,9 +338,31 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
       for (int u = 0; u < (nao + 31) / 32; ++u) b->tiles32.push_back(make_int4(m, t, u, 0));
     }
   }
-  if (b->nmax > kSyevMaxN)
+  // solver choice: 0 auto (in-house up to kSyevMaxN AOs, library above), 1 in-house only, 2 library only
+  int lib_above = 0;
+  if (opt->solver == 0) lib_above = kSyevMaxN;
+  else if (opt->solver == 2) lib_above = -1;
+  else if (opt->solver != 1) return fail(TB_BAD_INPUT, "solver must be 0, 1 or 2");
+  if (opt->solver == 1 && b->nmax > kSyevMaxN)
     return fail(TB_CAPACITY_EXCEEDED, "structure with " + std::to_string(b->nmax) +
                 " AOs exceeds the in-house eigensolver limit (" + std::to_string(kSyevMaxN) + " AOs)");
+  b->big.clear();
+  b->nmax_in = 0;
+  int nbig_max = 0;
+  for (int m = 0; m < nmol; ++m) {
+    const int n = b->h_ooff[m + 1] - b->h_ooff[m];
+    if (lib_above != 0 && n > lib_above) {
+      b->big.push_back(m);
+      nbig_max = std::max(nbig_max, n);
+    } else {
+      b->nmax_in = std::max(b->nmax_in, n);
+    }
+  }
+  b->lib_bytes = 0;
+  if (!b->big.empty()) {
+    const std::string e = b->lib.workspace(nbig_max, &b->lib_bytes);
+    if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
+  }
   b->nat_tot = b->h_aoff[nmol];
   b->nsh_tot = b->h_soff[nmol];
   b->nao_tot = b->h_ooff[nmol];
@@ -372,6 +402,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
          o_ms_ees2 = L.add(NM * D8), o_ms_eaes2 = L.add(NM * D8), o_ms_ees3 = L.add(NM * D8),
          o_ms_err = L.add(NM * D8), o_ms_fw = L.add(NM * I4), o_ms_dip = L.add(3 * NM * D8),
          o_ms_nact = L.add(I4);
+  size_t o_lwork = L.add(std::max<size_t>(b->lib_bytes, 16)), o_linfo = L.add((2 * b->big.size() + 2) * I4);
   b->bytes = L.total;
   b->arena = arena;
   {
@@ -424,6 +455,9 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   d.sh_iao = at<int>(base, o_shiao); d.at_ish = at<int>(base, o_atish); d.ao_at = at<int>(base, o_aoat);
   d.ao_sh = at<int>(base, o_aosh);
   d.order = at<int>(base, o_order);
+  d.lib_above = lib_above;
+  b->lib_work = base + o_lwork;
+  b->lib_info = at<int>(base, o_linfo);
   b->d_tiles64 = at<int4>(base, o_t64); b->d_tiles32 = at<int4>(base, o_t32); b->d_chunks32 = at<int2>(base, o_c32);
   b->charge = at<double>(base, o_charge); b->uhf = at<int>(base, o_uhf);
   b->cn = at<double>(base, o_cn); b->mrad = at<double>(base, o_mrad); b->erep = at<double>(base, o_erep);
@@ -552,17 +586,43 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
   }
   TB_K("cholesky", 0, 0, k_cholesky<<<nmol, 256, 0, st>>>(B, b->S, b->W, S.status, nullptr));
   TB_K("trinv", 0, 0, k_trinv<<<nmol, 256, 0, st>>>(B, b->W, b->X, S.status));
+  for (size_t k = 0; k < b->big.size(); ++k) {
+    const int m = b->big[k], n = b->h_ooff[m + 1] - b->h_ooff[m];
+    const long long mo = b->h_moff[m];
+    cudaEvent_t e0 = nullptr;
+    prof_start(b, st, &e0);
+    const std::string e = b->lib.factor(st, b->S + mo, b->X + mo, n, b->lib_work, b->lib_bytes, b->lib_info + 2 * k,
+                                        S.status + m);
+    if (!e.empty()) return fail(TB_CUDA_ERROR, "library Cholesky: " + e);
+    ++b->launches;
+    prof_stop(b, st, "factor_lib", e0, 0, 0);
+  }
   TB_K("scf_init", 0, 0, k_scf_init<<<nmol, 256, 0, st>>>(Pc, B, b->charge, b->uhf, b->erep, b->n0sh, b->q_in, S));
   // ---- SCF (next_scf per iteration, src/scf/iterators.cu:317-424)
   const double econv = 1.0e-6 * b->opt.accuracy, pconv = 2.0e-5 * b->opt.accuracy;
   const int ntile64 = (int)b->tiles64.size(), ntile32 = (int)b->tiles32.size(), nchunk = (int)b->chunks32.size();
   const int gemm_grid = std::min(ntile64, 148 * 8);
-  const size_t eig_smem = syev_smem_bytes(b->nmax);
+  const size_t eig_smem = syev_smem_bytes(std::max(b->nmax_in, 1));
   if (eig_smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_syev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eig_smem));
   const size_t fermi_smem = (size_t)b->nmax * sizeof(double);
   if (fermi_smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_fermi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fermi_smem));
   const dim3 pot_grid(nmol, nblk(std::max(b->natmax, b->nshmax), 256));
   std::vector<int> act;
+  // host copy of active/status, read where the loop synchronises anyway, so
+  // that converged or failed library structures are not diagonalised again
+  auto read_flags = [&]() -> tb_status {
+    if (b->big.empty()) return TB_OK;
+    b->h_active.resize(nmol);
+    b->h_status.resize(nmol);
+    TB_CUDA(cudaMemcpyAsync(b->h_active.data(), S.active, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
+    TB_CUDA(cudaMemcpyAsync(b->h_status.data(), S.status, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
+    TB_CUDA(cudaStreamSynchronize(st));
+    return TB_OK;
+  };
+  {
+    const tb_status fs = read_flags();
+    if (fs != TB_OK) return fs;
+  }
   for (int it = 0; it < b->opt.max_iter; ++it) {
     // algorithmic work of this iteration over the active structures (profile mode only)
     double n3 = 0, n2 = 0, n2occ = 0;
@@ -598,6 +658,18 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
     // symmetric eigensolve with vectors: canonical 4 N^3
     TB_K("syev", 4.0 * n3, 1,
          k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->w, b->perm, S.status, S.active));
+    for (size_t k = 0; k < b->big.size(); ++k) {
+      const int m = b->big[k], n = b->h_ooff[m + 1] - b->h_ooff[m];
+      if (!b->h_active[m] || b->h_status[m] != kStOk) continue;
+      const long long mo = b->h_moff[m], vo = b->h_ooff[m];
+      cudaEvent_t e0 = nullptr;
+      prof_start(b, st, &e0);
+      const std::string e = b->lib.syev(st, b->F + mo, b->Z + mo, b->w + vo, b->perm + vo, n, b->lib_work,
+                                        b->lib_bytes, b->lib_info + 2 * k, S.status + m);
+      if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
+      ++b->launches;
+      prof_stop(b, st, "syev_lib", e0, 4.0 * n * n * n, 1);
+    }
     TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
     // C = X Z (eigenvectors in ascending order through perm): 2N^3; P = C diag(f) C^T: 2 N^2 n_occ
     TB_K("gemm", 2.0 * n3, 1,
@@ -616,6 +688,8 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
     TB_CUDA(cudaMemcpyAsync(b->h_nactive, S.n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
     TB_CUDA(cudaStreamSynchronize(st));
     if (*b->h_nactive <= 0) break;
+    const tb_status fs = read_flags();
+    if (fs != TB_OK) return fs;
   }
   return prof_collect(b, st);
 }
@@ -989,8 +1063,16 @@ struct MatBatch {
   double *S = nullptr, *X = nullptr, *W = nullptr, *F = nullptr, *Z = nullptr, *w = nullptr, *focc = nullptr;
   int *perm = nullptr, *kdim = nullptr;
   long long n2 = 0, no = 0;
-  int nmax = 0;
+  int nmax = 0, nmax_in = 0;
   int64_t launches = 0;
+  // matrices above the in-house size bound go to the library path (tb_large.cu)
+  std::vector<int> big;
+  std::vector<long long> h_moff;
+  std::vector<int> h_ooff;
+  LargeSolver lib;
+  void* lib_work = nullptr;
+  size_t lib_bytes = 0;
+  int* lib_info = nullptr;
   tb_status build(int nmat, const int32_t* n) {
     std::vector<int> ooff(nmat + 1, 0);
     std::vector<long long> moff(nmat + 1, 0);
@@ -1002,7 +1084,17 @@ struct MatBatch {
       for (int t = 0; t < (n[m] + 63) / 64; ++t)
         for (int u = 0; u < (n[m] + 63) / 64; ++u) tiles.push_back(make_int4(m, t, u, 0));
     }
-    if (nmax > kSyevMaxN) return fail(TB_CAPACITY_EXCEEDED, "matrix too large for the in-house eigensolver");
+    int nbig_max = 0;
+    for (int m = 0; m < nmat; ++m) {
+      if (n[m] > kSyevMaxN) { big.push_back(m); nbig_max = std::max(nbig_max, (int)n[m]); }
+      else nmax_in = std::max(nmax_in, (int)n[m]);
+    }
+    if (!big.empty()) {
+      const std::string e = lib.workspace(nbig_max, &lib_bytes);
+      if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
+    }
+    h_moff = moff;
+    h_ooff = ooff;
     n2 = moff[nmat];
     no = ooff[nmat];
     Layout L;
@@ -1011,6 +1103,7 @@ struct MatBatch {
     size_t o_w = L.add(no * 8), o_f = L.add(no * 8), o_p = L.add(no * 4), o_k = L.add(nmat * 4);
     size_t o_st = L.add(nmat * 4), o_act = L.add(nmat * 4), o_nel = L.add(2 * nmat * 8), o_ets = L.add(nmat * 8),
            o_fw = L.add(nmat * 4), o_ef = L.add(nmat * 8), o_na = L.add(4);
+    size_t o_lw = L.add(std::max<size_t>(lib_bytes, 16)), o_li = L.add((2 * big.size() + 2) * 4);
     TB_CUDA(arena.reserve(L.total));
     char* base = arena.base;
     TB_CUDA(cudaMemset(base, 0, L.total));
@@ -1020,6 +1113,9 @@ struct MatBatch {
     db.nmol = nmat;
     db.ooff = at<int>(base, o_ooff);
     db.moff = at<long long>(base, o_moff);
+    db.lib_above = kSyevMaxN;
+    lib_work = base + o_lw;
+    lib_info = at<int>(base, o_li);
     d_tiles = at<int4>(base, o_t);
     S = at<double>(base, o_S); X = at<double>(base, o_X); W = at<double>(base, o_W); F = at<double>(base, o_F);
     Z = at<double>(base, o_Z); w = at<double>(base, o_w); focc = at<double>(base, o_f);
@@ -1048,11 +1144,28 @@ tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const 
   const int nt = (int)mb.tiles.size(), grid = std::min(nt, 148 * 8);
   k_cholesky<<<nmat, 256>>>(B, mb.S, mb.W, mb.ms.status, nullptr);
   k_trinv<<<nmat, 256>>>(B, mb.W, mb.X, mb.ms.status);
+  for (size_t k = 0; k < mb.big.size(); ++k) {
+    const int m = mb.big[k];
+    const long long mo = mb.h_moff[m];
+    const std::string e = mb.lib.factor(0, mb.S + mo, mb.X + mo, n[m], mb.lib_work, mb.lib_bytes, mb.lib_info + 2 * k,
+                                        mb.ms.status + m);
+    if (!e.empty()) return fail(TB_CUDA_ERROR, "library Cholesky: " + e);
+  }
   k_gemm<<<grid, 256>>>(B, mb.d_tiles, nt, mb.F, 0, mb.X, 0, nullptr, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);
   k_gemm<<<grid, 256>>>(B, mb.d_tiles, nt, mb.X, 1, mb.W, 0, nullptr, nullptr, nullptr, mb.F, 1.0, 0.0, mb.ms.active);
-  const size_t smem = syev_smem_bytes(mb.nmax);
+  const size_t smem = syev_smem_bytes(std::max(mb.nmax_in, 1));
   if (smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_syev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_syev<<<nmat, kEigThreads, smem>>>(B, mb.F, mb.Z, mb.w, mb.perm, mb.ms.status, mb.ms.active);
+  std::vector<int> fstat(nmat, 0);
+  if (!mb.big.empty()) TB_CUDA(cudaMemcpy(fstat.data(), mb.ms.status, nmat * 4, cudaMemcpyDeviceToHost));
+  for (size_t k = 0; k < mb.big.size(); ++k) {
+    const int m = mb.big[k];
+    if (fstat[m] != kStOk) continue;  // S not positive definite: reported below
+    const long long mo = mb.h_moff[m], vo = mb.h_ooff[m];
+    const std::string e = mb.lib.syev(0, mb.F + mo, mb.Z + mo, mb.w + vo, mb.perm + vo, n[m], mb.lib_work,
+                                      mb.lib_bytes, mb.lib_info + 2 * k + 1, mb.ms.status + m);
+    if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
+  }
   k_gemm<<<grid, 256>>>(B, mb.d_tiles, nt, mb.X, 0, mb.Z, 1, mb.perm, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(TB_CUDA_ERROR, cudaGetErrorString(e));

@@ -1,6 +1,9 @@
 // Kernel declarations and per-structure SCF state of the tblite-b200 engine.
 #pragma once
 
+#include <string>
+#include <vector>
+
 #include "tb_common.cuh"
 
 namespace tb {
@@ -10,6 +13,24 @@ constexpr int kRing = 8;  // QL sweeps buffered between the k_syev producer and 
 // shared memory of k_syev: d, e, tau, v, vn, p, w (7n) + the rotation ring (2 n kRing)
 inline size_t syev_smem_bytes(int n) { return (7 + 2 * (size_t)kRing) * (size_t)n * sizeof(double); }
 constexpr int kSyevMaxN = 1216;
+
+// cuSOLVER dense path for structures above the in-house size bound
+// (tb_large.cu); one instance per batch, used from one host thread at a time.
+struct LargeSolver {
+  void* handle = nullptr;  // cusolverDnHandle_t
+  void* params = nullptr;  // cusolverDnParams_t
+  std::vector<char> host;  // host workspace
+  ~LargeSolver();
+  std::string init();
+  // device workspace in bytes for potrf, trtri and syevd of order n
+  std::string workspace(int n, size_t* dev_bytes);
+  // X = L^-T of S (row-major, both n x n); info[0..1], status: device ints
+  std::string factor(cudaStream_t st, const double* S, double* X, int n, void* dwork, size_t dbytes, int* info,
+                     int* status);
+  // eigenpairs of A: eigenvector j in row j of Z, w ascending, perm = identity
+  std::string syev(cudaStream_t st, const double* A, double* Z, double* w, int* perm, int n, void* dwork,
+                   size_t dbytes, int* info, int* status);
+};
 
 // Per-structure scalars of the SCF (device arrays of length nmol; nel is 2*nmol).
 struct MolState {

@@ -19,6 +19,7 @@ __global__ void k_cholesky(DevBatch B, const double* __restrict__ S, double* __r
   const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;
   if (active && !active[m]) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
+  if (on_library(B, n)) return;
   const long long mo = B.moff[m];
   const double* s = S + mo;
   double* w = W + mo;
@@ -60,6 +61,7 @@ __global__ void k_trinv(DevBatch B, const double* __restrict__ W, double* __rest
   const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;
   if (status[m] != kStOk) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
+  if (on_library(B, n)) return;
   const long long mo = B.moff[m];
   const double* w = W + mo;
   double* x = X + mo;
@@ -270,6 +272,7 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
   if (active && !active[m]) return;
   if (status[m] != kStOk) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
+  if (on_library(B, n)) return;
   const long long mo = B.moff[m];
   const long long vo = B.ooff[m];
   double* A = Ab + mo;
