@@ -65,8 +65,14 @@ typedef struct tb_options {
   double mixer_damping;   /* default 0.4                                       */
   int32_t verbosity;      /* 0 silent                                          */
   int32_t use_graphs;     /* 1: replay each SCF iteration as a CUDA graph      */
-  int32_t solver;         /* 0 auto, 1 in-house batched QL, 2 cuSOLVER (large) */
+  int32_t solver;         /* 0 auto: in-house batched eigensolver up to 1216 AOs,
+                             cuSOLVER Xsyevd above; 1 in-house only (larger
+                             structures: TB_CAPACITY_EXCEEDED); 2 cuSOLVER only */
   int32_t profile;        /* 1: time every kernel class with CUDA events        */
+  int32_t precision;      /* 0 plain FP64; 1 mixed: FP32 eigensolve refined in
+                             FP64 and FP32-product contractions until the SCF
+                             nearly converges, then at least two FP64
+                             iterations before the final convergence test     */
 } tb_options;
 
 /* Per-structure results: the energy/wavefunction outputs of xtb_singlepoint.

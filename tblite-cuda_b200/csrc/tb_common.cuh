@@ -71,20 +71,22 @@ enum DevStatus : int {
   kStFermiNotConverged = 4, kStEigenFailed = 5
 };
 
-__device__ inline double warp_sum(double v) {
+template <typename T>
+__device__ inline T warp_sum(T v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
 
 // Block-wide sum in a fixed order (deterministic); all threads get the result.
-// `red` must hold blockDim.x/32 doubles.
-__device__ inline double block_sum(double v, double* red) {
+// `red` must hold blockDim.x/32 values.
+template <typename T>
+__device__ inline T block_sum(T v, T* red) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
   v = warp_sum(v);
   __syncthreads();
   if (lane == 0) red[wid] = v;
   __syncthreads();
-  double t = 0.0;
+  T t = T(0);
   for (int w = 0; w < nw; ++w) t += red[w];
   return t;
 }

@@ -249,6 +249,11 @@ struct tb_batch {
   size_t lib_bytes = 0;
   int* lib_info = nullptr;   // 2 per library structure
   std::vector<int> h_active, h_status;
+  // mixed-precision form (tb_options.precision = 1)
+  bool mixed = false;
+  float *Af = nullptr, *Zf = nullptr, *wf = nullptr;
+  double *Vn = nullptr, *G = nullptr;
+  int *act_lo = nullptr, *act_hi = nullptr;
   int64_t launches = 0;
   size_t bytes = 0;
   std::vector<double> h_nocc;  // closed-shell occupied orbitals per structure (work accounting)
@@ -283,6 +288,8 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   b->nmol = nmol;
   if (nmol <= 0) return fail(TB_BAD_INPUT, "nmol must be positive");
   if (opt->max_iter < 1 || opt->max_iter > 64) return fail(TB_BAD_INPUT, "max_iter must be in 1..64");
+  if (opt->precision != 0 && opt->precision != 1) return fail(TB_BAD_INPUT, "precision must be 0 or 1");
+  b->mixed = opt->precision == 1;
   b->h_aoff.assign(nmol + 1, 0); b->h_soff.assign(nmol + 1, 0); b->h_ooff.assign(nmol + 1, 0);
   b->h_mixoff.assign(nmol + 1, 0); b->h_moff.assign(nmol + 1, 0); b->h_poff.assign(nmol + 1, 0);
   std::vector<int> id, at_mol, sh_type, sh_at, sh_iao, at_ish, ao_at, ao_sh;
@@ -403,6 +410,11 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
          o_ms_err = L.add(NM * D8), o_ms_fw = L.add(NM * I4), o_ms_dip = L.add(3 * NM * D8),
          o_ms_nact = L.add(I4);
   size_t o_lwork = L.add(std::max<size_t>(b->lib_bytes, 16)), o_linfo = L.add((2 * b->big.size() + 2) * I4);
+  // mixed-precision form: FP32 eigensolver input/output, refinement buffers, phase state
+  const long long MXN2 = b->mixed ? N2 : 0, MXNO = b->mixed ? NO : 0, MXNM = b->mixed ? NM : 0;
+  size_t o_Af = L.add(MXN2 * 4), o_Zf = L.add(MXN2 * 4), o_wf = L.add(MXNO * 4), o_Vn = L.add(MXN2 * D8),
+         o_G = L.add(MXN2 * D8), o_lo = L.add(MXNM * I4), o_hi = L.add(MXNM * I4), o_phase = L.add(MXNM * I4),
+         o_n64 = L.add(MXNM * I4);
   b->bytes = L.total;
   b->arena = arena;
   {
@@ -458,6 +470,11 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   d.lib_above = lib_above;
   b->lib_work = base + o_lwork;
   b->lib_info = at<int>(base, o_linfo);
+  if (b->mixed) {
+    b->Af = at<float>(base, o_Af); b->Zf = at<float>(base, o_Zf); b->wf = at<float>(base, o_wf);
+    b->Vn = at<double>(base, o_Vn); b->G = at<double>(base, o_G);
+    b->act_lo = at<int>(base, o_lo); b->act_hi = at<int>(base, o_hi);
+  }
   b->d_tiles64 = at<int4>(base, o_t64); b->d_tiles32 = at<int4>(base, o_t32); b->d_chunks32 = at<int2>(base, o_c32);
   b->charge = at<double>(base, o_charge); b->uhf = at<int>(base, o_uhf);
   b->cn = at<double>(base, o_cn); b->mrad = at<double>(base, o_mrad); b->erep = at<double>(base, o_erep);
@@ -483,6 +500,8 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   s.e_es2 = at<double>(base, o_ms_ees2); s.e_aes2 = at<double>(base, o_ms_eaes2);
   s.e_es3 = at<double>(base, o_ms_ees3); s.scf_error = at<double>(base, o_ms_err);
   s.fermi_warn = at<int>(base, o_ms_fw); s.dipole = at<double>(base, o_ms_dip); s.n_active = at<int>(base, o_ms_nact);
+  s.phase = b->mixed ? at<int>(base, o_phase) : nullptr;
+  s.n64 = b->mixed ? at<int>(base, o_n64) : nullptr;
   if (!b->h_nactive) TB_CUDA(cudaMallocHost(&b->h_nactive, sizeof(int)));
   return TB_OK;
 }
@@ -549,6 +568,90 @@ tb_status prof_collect(tb_batch* b, cudaStream_t st) {
     ++b->launches;                                                                         \
   } while (0)
 
+// The mixed phase hands over to FP64 once |dE| and the charge error are below
+// this multiple of the final thresholds, but never below the floors: the FP32
+// contractions leave iteration-to-iteration noise of about 1e-6 in charges.
+constexpr double kMixedSwitchScale = 10.0, kMixedSwitchFloorE = 1e-5, kMixedSwitchFloorQ = 2e-4;
+
+// Eigen-decomposition and density of one SCF iteration in the mixed-precision
+// form (tb_mixed.cu).  Every matrix is stored in FP64.  F', C and P are
+// FP32-product GEMMs (k_gemm_mx) for structures in the mixed phase and FP64
+// GEMMs in the FP64 phase; the eigenpairs come from the FP32 eigensolver and
+// FP64 refinement (one step in the mixed phase, two in the FP64 phase).
+// Leaves w, focc, kdim and P as the plain form does.
+tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, double n2occ_lo, double n2occ_hi,
+                     int gemm_grid, size_t fermi_smem) {
+  const DevBatch& B = b->db;
+  MolState& S = b->ms;
+  const int nmol = b->nmol, nt = (int)b->tiles64.size();
+  const int4* T = b->d_tiles64;
+  const size_t smem32 = syev_smem_bytes(std::max(b->nmax_in, 1), sizeof(float));
+  int *lo = b->act_lo, *hi = b->act_hi;
+  TB_K("masks", 0, 0, k_phase_masks<<<nblk(nmol, 256), 256, 0, st>>>(nmol, S.active, S.phase, lo, hi));
+  // F' = X^T F X into F (T = F X in W), each phase in its precision
+  TB_K("gemm_mx", 2.0 * n3_lo, 1,
+       k_gemm_mx<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.f, 0.f,
+                                            lo));
+  TB_K("gemm", 2.0 * n3_hi, 1,
+       k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi));
+  TB_K("gemm_mx", 2.0 * n3_lo, 1,
+       k_gemm_mx<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.f, 0.f,
+                                            lo));
+  TB_K("gemm", 2.0 * n3_hi, 1,
+       k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, hi));
+  // FP32 eigensolve of every active structure
+  TB_K("convert", 0, 0, k_to_f32<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, b->Af, S.active));
+  TB_K("syev_f32", 4.0 * (n3_lo + n3_hi), 1,
+       k_syev_f32<<<nmol, kEigThreads, smem32, st>>>(B, b->Af, b->Zf, b->w, b->perm, S.status, S.active));
+  for (size_t k = 0; k < b->big.size(); ++k) {
+    const int m = b->big[k], n = b->h_ooff[m + 1] - b->h_ooff[m];
+    if (!b->h_active[m] || b->h_status[m] != kStOk) continue;
+    const long long mo = b->h_moff[m], vo = b->h_ooff[m];
+    cudaEvent_t e0 = nullptr;
+    prof_start(b, st, &e0);
+    const std::string e = b->lib.syev32(st, b->Af + mo, b->Zf + mo, b->wf + vo, b->w + vo, b->perm + vo, n,
+                                        b->lib_work, b->lib_bytes, b->lib_info + 2 * k, S.status + m);
+    if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
+    ++b->launches;
+    prof_stop(b, st, "syev_lib_f32", e0, 4.0 * n * n * n, 1);
+  }
+  // refinement in FP64 (GEMMs included): V = eigenvectors as columns in
+  // ascending order.  Step 1 (every active structure) Z -> Vn; step 2 (FP64
+  // phase only) Vn -> Z.
+  const size_t oa_smem = oa_smem_bytes(b->nmax);
+  TB_K("refine", 0, 0, k_gather_vectors<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->Zf, b->perm, b->Z, S.active));
+  for (int r = 0; r < 2; ++r) {
+    double* V = r == 0 ? b->Z : b->Vn;
+    double* Vo = r == 0 ? b->Vn : b->Z;
+    int* mk = r == 0 ? S.active : hi;
+    const double wk = 2.0 * (r == 0 ? n3_lo + n3_hi : n3_hi);
+    TB_K("gemm", wk, 1,  // G = V^T V
+         k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, V, 1, V, 0, nullptr, nullptr, nullptr, b->G, 1.0, 0.0, mk));
+    TB_K("gemm", wk, 1,  // W = F' V
+         k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, 0, V, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, mk));
+    TB_K("gemm", wk, 1,  // Sm = V^T W (in P)
+         k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, V, 1, b->W, 0, nullptr, nullptr, nullptr, b->P, 1.0, 0.0, mk));
+    TB_K("refine", 0, 0, k_oa_step<<<nmol, 256, oa_smem, st>>>(B, b->G, b->P, V, b->w, mk));
+    TB_CUDA(cudaMemcpyAsync(Vo, V, (size_t)b->n2_tot * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    TB_K("gemm", wk, 1,  // Vo = V + V E
+         k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, V, 0, b->G, 0, nullptr, nullptr, nullptr, Vo, 1.0, 1.0, mk));
+  }
+  TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
+  // C = X V into W (mixed phase: V after one step, in Vn; FP64 phase: after two, in Z)
+  TB_K("gemm_mx", 2.0 * n3_lo, 1,
+       k_gemm_mx<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->X, 0, b->Vn, 0, nullptr, nullptr, nullptr, b->W, 1.f, 0.f,
+                                            lo));
+  TB_K("gemm", 2.0 * n3_hi, 1,
+       k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->X, 0, b->Z, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi));
+  // P = C diag(f) C^T
+  TB_K("gemm_mx", 2.0 * n2occ_lo, 1,
+       k_gemm_mx<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.f, 0.f,
+                                            lo));
+  TB_K("gemm", 2.0 * n2occ_hi, 1,
+       k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.0, 0.0, hi));
+  return TB_OK;
+}
+
 tb_status batch_run(tb_batch* b, cudaStream_t st) {
   tb_calculator* c = b->calc;
   const DevBatch& B = b->db;
@@ -607,7 +710,13 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
   const size_t fermi_smem = (size_t)b->nmax * sizeof(double);
   if (fermi_smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_fermi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fermi_smem));
   const dim3 pot_grid(nmol, nblk(std::max(b->natmax, b->nshmax), 256));
-  std::vector<int> act;
+  std::vector<int> act, phase;
+  if (b->mixed) {
+    const size_t smem32 = syev_smem_bytes(std::max(b->nmax_in, 1), sizeof(float));
+    if (smem32 > 48 * 1024)
+      TB_CUDA(cudaFuncSetAttribute(k_syev_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
+    TB_CUDA(cudaFuncSetAttribute(k_oa_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)oa_smem_bytes(b->nmax)));
+  }
   // host copy of active/status, read where the loop synchronises anyway, so
   // that converged or failed library structures are not diagonalised again
   auto read_flags = [&]() -> tb_status {
@@ -625,17 +734,23 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
   }
   for (int it = 0; it < b->opt.max_iter; ++it) {
     // algorithmic work of this iteration over the active structures (profile mode only)
-    double n3 = 0, n2 = 0, n2occ = 0;
+    double n3 = 0, n2 = 0, n2occ = 0, n3_lo = 0, n3_hi = 0, n2occ_lo = 0, n2occ_hi = 0;
     if (b->opt.profile) {
       act.resize(nmol);
+      phase.assign(nmol, 1);
       TB_CUDA(cudaMemcpyAsync(act.data(), S.active, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
+      if (b->mixed)
+        TB_CUDA(cudaMemcpyAsync(phase.data(), S.phase, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
       TB_CUDA(cudaStreamSynchronize(st));
       for (int m = 0; m < nmol; ++m) {
         if (!act[m]) continue;
         const double n = b->h_ooff[m + 1] - b->h_ooff[m];
+        const double occ = n * n * std::min(n, b->h_nocc[m]);
         n3 += n * n * n;
         n2 += n * n;
-        n2occ += n * n * std::min(n, b->h_nocc[m]);
+        n2occ += occ;
+        (phase[m] ? n3_hi : n3_lo) += n * n * n;
+        (phase[m] ? n2occ_hi : n2occ_lo) += occ;
       }
     }
     if (it > 0)
@@ -648,43 +763,50 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
     TB_K("fock", 96.0 * n2, 2,
          k_fock<<<ntile32, 256, 0, st>>>(B, b->d_tiles32, ntile32, b->S, b->H0, b->D, b->Q, b->vsh, b->vat, b->vdp,
                                          b->vqp, b->F, S.active));
-    // F' = X^T F X  (T = F X in W, then F' into F): 2 x 2N^3
-    TB_K("gemm", 2.0 * n3, 1,
-         k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->F, 0, b->X, 0, nullptr, nullptr, nullptr,
-                                           b->W, 1.0, 0.0, S.active));
-    TB_K("gemm", 2.0 * n3, 1,
-         k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 1, b->W, 0, nullptr, nullptr, nullptr,
-                                           b->F, 1.0, 0.0, S.active));
-    // symmetric eigensolve with vectors: canonical 4 N^3
-    TB_K("syev", 4.0 * n3, 1,
-         k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->w, b->perm, S.status, S.active));
-    for (size_t k = 0; k < b->big.size(); ++k) {
-      const int m = b->big[k], n = b->h_ooff[m + 1] - b->h_ooff[m];
-      if (!b->h_active[m] || b->h_status[m] != kStOk) continue;
-      const long long mo = b->h_moff[m], vo = b->h_ooff[m];
-      cudaEvent_t e0 = nullptr;
-      prof_start(b, st, &e0);
-      const std::string e = b->lib.syev(st, b->F + mo, b->Z + mo, b->w + vo, b->perm + vo, n, b->lib_work,
-                                        b->lib_bytes, b->lib_info + 2 * k, S.status + m);
-      if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
-      ++b->launches;
-      prof_stop(b, st, "syev_lib", e0, 4.0 * n * n * n, 1);
+    if (!b->mixed) {
+      // F' = X^T F X  (T = F X in W, then F' into F): 2 x 2N^3
+      TB_K("gemm", 2.0 * n3, 1,
+           k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->F, 0, b->X, 0, nullptr, nullptr, nullptr,
+                                             b->W, 1.0, 0.0, S.active));
+      TB_K("gemm", 2.0 * n3, 1,
+           k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 1, b->W, 0, nullptr, nullptr, nullptr,
+                                             b->F, 1.0, 0.0, S.active));
+      // symmetric eigensolve with vectors: canonical 4 N^3
+      TB_K("syev", 4.0 * n3, 1,
+           k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->w, b->perm, S.status, S.active));
+      for (size_t k = 0; k < b->big.size(); ++k) {
+        const int m = b->big[k], n = b->h_ooff[m + 1] - b->h_ooff[m];
+        if (!b->h_active[m] || b->h_status[m] != kStOk) continue;
+        const long long mo = b->h_moff[m], vo = b->h_ooff[m];
+        cudaEvent_t e0 = nullptr;
+        prof_start(b, st, &e0);
+        const std::string e = b->lib.syev(st, b->F + mo, b->Z + mo, b->w + vo, b->perm + vo, n, b->lib_work,
+                                          b->lib_bytes, b->lib_info + 2 * k, S.status + m);
+        if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
+        ++b->launches;
+        prof_stop(b, st, "syev_lib", e0, 4.0 * n * n * n, 1);
+      }
+      TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
+      // C = X Z (eigenvectors in ascending order through perm): 2N^3; P = C diag(f) C^T: 2 N^2 n_occ
+      TB_K("gemm", 2.0 * n3, 1,
+           k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr,
+                                             b->W, 1.0, 0.0, S.active));
+      TB_K("gemm", 2.0 * n2occ, 1,
+           k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim,
+                                             b->P, 1.0, 0.0, S.active));
+    } else {
+      const tb_status ms = mixed_core(b, st, n3_lo, n3_hi, n2occ_lo, n2occ_hi, gemm_grid, fermi_smem);
+      if (ms != TB_OK) return ms;
     }
-    TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
-    // C = X Z (eigenvectors in ascending order through perm): 2N^3; P = C diag(f) C^T: 2 N^2 n_occ
-    TB_K("gemm", 2.0 * n3, 1,
-         k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr,
-                                           b->W, 1.0, 0.0, S.active));
-    TB_K("gemm", 2.0 * n2occ, 1,
-         k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim,
-                                           b->P, 1.0, 0.0, S.active));
     // Mulliken + band energy: reads P, S, H0, D(3), Q(6) -> 11 N^2 doubles
     TB_K("mulliken", 88.0 * n2, 2,
          k_mulliken_cols<<<nchunk, 256, 0, st>>>(B, b->d_chunks32, nchunk, b->P, b->S, b->H0, b->D, b->Q, b->colred,
                                                  S.active));
     TB_K("finalize", 0, 0,
          k_finalize<<<nmol, 256, 0, st>>>(Pc, B, b->colred, b->n0sh, b->mrad, b->q_in, b->dq, b->qsh_out, b->qat_out,
-                                          b->dpat_out, b->qpat_out, econv, pconv, b->opt.max_iter, S));
+                                          b->dpat_out, b->qpat_out, econv, pconv, b->opt.max_iter, S,
+                                          std::max(kMixedSwitchScale * econv, kMixedSwitchFloorE),
+                                          std::max(kMixedSwitchScale * pconv, kMixedSwitchFloorQ)));
     TB_CUDA(cudaMemcpyAsync(b->h_nactive, S.n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
     TB_CUDA(cudaStreamSynchronize(st));
     if (*b->h_nactive <= 0) break;

@@ -11,7 +11,7 @@ namespace tb {
 constexpr int kEigThreads = 256;
 constexpr int kRing = 8;  // QL sweeps buffered between the k_syev producer and consumers
 // shared memory of k_syev: d, e, tau, v, vn, p, w (7n) + the rotation ring (2 n kRing)
-inline size_t syev_smem_bytes(int n) { return (7 + 2 * (size_t)kRing) * (size_t)n * sizeof(double); }
+inline size_t syev_smem_bytes(int n, size_t elem = sizeof(double)) { return (7 + 2 * (size_t)kRing) * (size_t)n * elem; }
 constexpr int kSyevMaxN = 1216;
 
 // cuSOLVER dense path for structures above the in-house size bound
@@ -30,6 +30,9 @@ struct LargeSolver {
   // eigenpairs of A: eigenvector j in row j of Z, w ascending, perm = identity
   std::string syev(cudaStream_t st, const double* A, double* Z, double* w, int* perm, int n, void* dwork,
                    size_t dbytes, int* info, int* status);
+  // the same in FP32 (mixed-precision form); wtmp: n floats of scratch, w written as double
+  std::string syev32(cudaStream_t st, const float* A, float* Z, float* wtmp, double* w, int* perm, int n,
+                     void* dwork, size_t dbytes, int* info, int* status);
 };
 
 // Per-structure scalars of the SCF (device arrays of length nmol; nel is 2*nmol).
@@ -51,6 +54,8 @@ struct MolState {
   double* dipole;   // 3*nmol
   double* e_fermi;  // optional (may be null): Fermi level of spin channel 0
   int* n_active;    // single counter
+  int* phase;       // mixed-precision form only (else null): 0 mixed phase, 1 FP64 phase
+  int* n64;         // mixed-precision form only: FP64 iterations done
 };
 
 // Matrix outputs of the integral kernels (D, Q planar [3|6][N][N] per structure).
@@ -77,6 +82,25 @@ __global__ void k_gemm(DevBatch B, const int4* tiles, int ntiles, const double* 
                        const int* perm, const double* ks, const int* kdim, double* Cb, double alpha, double beta,
                        const int* active);
 __global__ void k_syev(DevBatch B, double* Ab, double* Zb, double* wout, int* perm, int* status, const int* active);
+// the same eigensolver in FP32 (A and Z float, eigenvalues written as double)
+__global__ void k_syev_f32(DevBatch B, float* Ab, float* Zb, double* wout, int* perm, int* status, const int* active);
+
+// mixed-precision form (tb_mixed.cu)
+// k_gemm with FP32 products and accumulation on FP64-stored operands
+__global__ void k_gemm_mx(DevBatch B, const int4* tiles, int ntiles, const double* Ab, int ta, const double* Bb,
+                          int tb_, const int* perm, const double* ks, const int* kdim, double* Cb, float alpha,
+                          float beta, const int* active);
+__global__ void k_phase_masks(int nmol, const int* active, const int* phase, int* lo, int* hi);
+__global__ void k_to_f32(DevBatch B, const int4* tiles, int ntiles, const double* F, float* Af, const int* mask);
+__global__ void k_gather_vectors(DevBatch B, const int4* tiles, int ntiles, const float* Zf, const int* perm,
+                                 double* V, const int* mask);
+// refinement step (Rayleigh-Ritz in clusters + Ogita-Aishima coefficients)
+constexpr int kClusterMax = 64;
+inline size_t oa_smem_bytes(int nmax) {
+  return (3 * (size_t)kClusterMax * kClusterMax + 2 * kClusterMax) * sizeof(double) +
+         2 * ((size_t)nmax + 1) * sizeof(int);
+}
+__global__ void k_oa_step(DevBatch B, double* G, double* Sm, double* V, double* w, const int* mask);
 
 // SCF
 __global__ void k_scf_init(DevParams P, DevBatch B, const double* charge, const int* uhf, const double* erep,
@@ -92,7 +116,8 @@ __global__ void k_mulliken_cols(DevBatch B, const int2* chunks, int nchunks, con
                                 const int* active);
 __global__ void k_finalize(DevParams P, DevBatch B, const double* colred, const double* n0sh, const double* mrad,
                            const double* q_in, double* dq, double* qsh_out, double* qat_out, double* dpat_out,
-                           double* qpat_out, double econv, double pconv, int max_iter, MolState S);
+                           double* qpat_out, double econv, double pconv, int max_iter, MolState S,
+                           double econv_lo, double pconv_lo);
 __global__ void k_mix_next(DevBatch B, double* q_in, const double* dq, double* dqlast, double* qlast, double* df,
                            double* u, double* amat, double* omega, int memory, double damp, MolState S);
 

@@ -70,6 +70,16 @@ __global__ void k_lib_syev_post(int* __restrict__ perm, int n, const int* __rest
   if (blockIdx.x == 0 && threadIdx.x == 0 && info[0] != 0) *status = kStEigenFailed;
 }
 
+// FP32 variant: ascending eigenvalues widened to FP64.
+__global__ void k_lib_syev32_post(int* __restrict__ perm, const float* __restrict__ wtmp, double* __restrict__ w,
+                                  int n, const int* __restrict__ info, int* __restrict__ status) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    perm[j] = j;
+    w[j] = (double)wtmp[j];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && info[0] != 0) *status = kStEigenFailed;
+}
+
 inline int grid_for(long long items) {
   const long long g = (items + 255) / 256;
   return (int)(g < 148 * 16 ? (g < 1 ? 1 : g) : 148 * 16);
@@ -105,10 +115,15 @@ std::string LargeSolver::workspace(int n, size_t* dev_bytes) {
                                        &h2));
   LS_CHECK(cusolverDnXsyevd_bufferSize(h, p, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, CUDA_R_64F, nullptr,
                                        n, CUDA_R_64F, nullptr, CUDA_R_64F, &d3, &h3));
+  size_t d4 = 0, h4 = 0;
+  LS_CHECK(cusolverDnXsyevd_bufferSize(h, p, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, CUDA_R_32F, nullptr,
+                                       n, CUDA_R_32F, nullptr, CUDA_R_32F, &d4, &h4));
   size_t d = d1 > d2 ? d1 : d2;
   d = d > d3 ? d : d3;
+  d = d > d4 ? d : d4;
   size_t hb = h1 > h2 ? h1 : h2;
   hb = hb > h3 ? hb : h3;
+  hb = hb > h4 ? hb : h4;
   if (host.size() < hb) host.resize(hb);
   *dev_bytes = d;
   return "";
@@ -144,6 +159,22 @@ std::string LargeSolver::syev(cudaStream_t st, const double* A, double* Z, doubl
   LS_CHECK(cusolverDnXsyevd(h, p, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, CUDA_R_64F, Z, n, CUDA_R_64F,
                             w, CUDA_R_64F, dwork, dbytes, hw, host.size(), info));
   k_lib_syev_post<<<grid_for(n), 256, 0, st>>>(perm, n, info, status);
+  LS_CUDA(cudaGetLastError());
+  return "";
+}
+
+std::string LargeSolver::syev32(cudaStream_t st, const float* A, float* Z, float* wtmp, double* w, int* perm, int n,
+                                void* dwork, size_t dbytes, int* info, int* status) {
+  std::string err = init();
+  if (!err.empty()) return err;
+  auto h = static_cast<cusolverDnHandle_t>(handle);
+  auto p = static_cast<cusolverDnParams_t>(params);
+  LS_CHECK(cusolverDnSetStream(h, st));
+  LS_CUDA(cudaMemcpyAsync(Z, A, (size_t)n * n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  void* hw = host.empty() ? nullptr : host.data();
+  LS_CHECK(cusolverDnXsyevd(h, p, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, CUDA_R_32F, Z, n, CUDA_R_32F,
+                            wtmp, CUDA_R_32F, dwork, dbytes, hw, host.size(), info));
+  k_lib_syev32_post<<<grid_for(n), 256, 0, st>>>(perm, wtmp, w, n, info, status);
   LS_CUDA(cudaGetLastError());
   return "";
 }

@@ -195,35 +195,51 @@ constexpr int kWaveK = 4;            // QL sweeps applied per pass over Zc
 constexpr int kWin = 2 * kWaveK;     // rows of Zc in flight per column
 constexpr long long kSpinLimit = 1LL << 24;
 
-__device__ inline double block_sum_syev(double v, double* red) { return block_sum(v, red); }
+template <typename T> struct Eps;
+template <> struct Eps<double> { static constexpr double v = 2.220446049250313e-16; };
+template <> struct Eps<float> { static constexpr float v = 1.1920929e-07f; };
+__device__ inline double tb_sqrt(double x) { return sqrt(x); }
+__device__ inline float tb_sqrt(float x) { return sqrtf(x); }
+__device__ inline double tb_abs(double x) { return fabs(x); }
+__device__ inline float tb_abs(float x) { return fabsf(x); }
+__device__ inline double tb_rsqrt(double x) { return rsqrt(x); }
+// one Newton step y(3 - x y^2)/2 on the hardware estimate keeps Givens pairs orthogonal to ~1 ulp
+__device__ inline float tb_rsqrt(float x) {
+  const float y = rsqrtf(x);
+  return y * (1.5f - 0.5f * x * y * y);
+}
+
+template <typename T>
+__device__ inline T block_sum_syev(T v, T* red) { return block_sum(v, red); }
 
 // Householder reflector of row k: x = A[k][k+1..n-1] -> tau[k], e[k] and v
 // (v[0] = 1), written to `v` and back into row k.
-__device__ void reflector(double* A, int n, int k, double* v, double* tau, double* e, double* red, double* sh) {
+template <typename T>
+__device__ void reflector(T* A, int n, int k, T* v, T* tau, T* e, T* red, T* sh) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int mm = n - k - 1;
-  double* rowk = A + (long long)k * n + k + 1;
-  double part = 0.0;
+  T* rowk = A + (long long)k * n + k + 1;
+  T part = T(0);
   for (int i = 1 + tid; i < mm; i += nt) part += rowk[i] * rowk[i];
-  const double sigma = block_sum_syev(part, red);
+  const T sigma = block_sum_syev(part, red);
   if (tid == 0) {
-    const double alpha = rowk[0];
-    if (sigma == 0.0) {
-      tau[k] = 0.0; e[k] = alpha; sh[0] = 0.0; sh[1] = 0.0;
+    const T alpha = rowk[0];
+    if (sigma == T(0)) {
+      tau[k] = T(0); e[k] = alpha; sh[0] = T(0); sh[1] = T(0);
     } else {
-      const double r = sqrt(alpha * alpha + sigma);
-      const double beta = alpha <= 0.0 ? r : -r;
+      const T r = tb_sqrt(alpha * alpha + sigma);
+      const T beta = alpha <= T(0) ? r : -r;
       tau[k] = (beta - alpha) / beta;
       e[k] = beta;
       sh[0] = tau[k];
-      sh[1] = 1.0 / (alpha - beta);
+      sh[1] = T(1) / (alpha - beta);
     }
   }
   __syncthreads();
-  const double scal = sh[1];
-  const bool refl = sh[0] != 0.0;
+  const T scal = sh[1];
+  const bool refl = sh[0] != T(0);
   for (int i = tid; i < mm; i += nt) {
-    const double x = i == 0 ? 1.0 : (refl ? rowk[i] * scal : 0.0);
+    const T x = i == 0 ? T(1) : (refl ? rowk[i] * scal : T(0));
     v[i] = x;
     if (refl) rowk[i] = x;
   }
@@ -235,18 +251,19 @@ __device__ void reflector(double* A, int n, int k, double* v, double* tau, doubl
 // indexed from the block's origin), and out_c = scale * sum_r M_new[r][c] x_r.
 // One thread per column; rows are loaded in batches of kWalkBatch before any
 // of them is written back, so a batch costs about one L2 round trip.
-__device__ void colwalk(double* M, int n, int r0, int nr, int c0, int nc, bool upd, const double* a,
-                        const double* b, int aoff, const double* x, double* out, double scale) {
+template <typename T>
+__device__ void colwalk(T* M, int n, int r0, int nr, int c0, int nc, bool upd, const T* a,
+                        const T* b, int aoff, const T* x, T* out, T scale) {
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int jj = tid; jj < nc; jj += nt) {
     const int c = c0 + jj;
-    const double aj = upd ? a[aoff + c0 - r0 + jj] : 0.0, bj = upd ? b[aoff + c0 - r0 + jj] : 0.0;
-    double acc = 0.0;
+    const T aj = upd ? a[aoff + c0 - r0 + jj] : T(0), bj = upd ? b[aoff + c0 - r0 + jj] : T(0);
+    T acc = T(0);
     for (int i0 = 0; i0 < nr; i0 += kWalkBatch) {
-      double q[kWalkBatch];
+      T q[kWalkBatch];
 #pragma unroll
       for (int u = 0; u < kWalkBatch; ++u)
-        q[u] = (i0 + u < nr) ? M[(long long)(r0 + i0 + u) * n + c] : 0.0;
+        q[u] = (i0 + u < nr) ? M[(long long)(r0 + i0 + u) * n + c] : T(0);
 #pragma unroll
       for (int u = 0; u < kWalkBatch; ++u) {
         if (i0 + u < nr) {
@@ -263,11 +280,10 @@ __device__ void colwalk(double* M, int n, int r0, int nr, int c0, int nc, bool u
   }
 }
 
-}  // namespace
-
-__global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __restrict__ Ab, double* __restrict__ Zb,
-                                                      double* __restrict__ wout, int* __restrict__ perm,
-                                                      int* __restrict__ status, const int* __restrict__ active) {
+template <typename T>
+__device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab, T* __restrict__ Zb,
+                                          double* __restrict__ wout, int* __restrict__ perm,
+                                          int* __restrict__ status, const int* __restrict__ active) {
   const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;  // largest structures first
   if (active && !active[m]) return;
   if (status[m] != kStOk) return;
@@ -275,19 +291,20 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
   if (on_library(B, n)) return;
   const long long mo = B.moff[m];
   const long long vo = B.ooff[m];
-  double* A = Ab + mo;
-  double* Z = Zb + mo;
-  extern __shared__ double sm[];
-  double* d = sm;          // n
-  double* e = d + n;       // n
-  double* tau = e + n;     // n
-  double* v = tau + n;     // n
-  double* vn = v + n;      // n
-  double* p = vn + n;      // n
-  double* w = p + n;       // n
-  double* ring = w + n;    // kRing slots x (n cosines + n sines)
-  __shared__ double red[kEigThreads / 32];
-  __shared__ double sh[4];
+  T* A = Ab + mo;
+  T* Z = Zb + mo;
+  extern __shared__ __align__(16) unsigned char syev_smem[];
+  T* sm = reinterpret_cast<T*>(syev_smem);
+  T* d = sm;          // n
+  T* e = d + n;       // n
+  T* tau = e + n;     // n
+  T* v = tau + n;     // n
+  T* vn = v + n;      // n
+  T* p = vn + n;      // n
+  T* w = p + n;       // n
+  T* ring = w + n;    // kRing slots x (n cosines + n sines)
+  __shared__ T red[kEigThreads / 32];
+  __shared__ T sh[4];
   __shared__ int q_full, q_end, q_fail, sh_head[kRing][2];
   __shared__ int q_done[kEigThreads / 32];  // sweeps finished, per consumer warp
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -296,31 +313,31 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
   for (long long x = tid; x < (long long)n * n; x += nt) {
     const int i = (int)(x / n), j = (int)(x % n);
     if (i < j) {
-      const double s = 0.5 * (A[(long long)i * n + j] + A[(long long)j * n + i]);
+      const T s = T(0.5) * (A[(long long)i * n + j] + A[(long long)j * n + i]);
       A[(long long)i * n + j] = s;
       A[(long long)j * n + i] = s;
     }
   }
-  for (int i = tid; i < n; i += nt) { e[i] = 0.0; tau[i] = 0.0; }
+  for (int i = tid; i < n; i += nt) { e[i] = T(0); tau[i] = T(0); }
   __syncthreads();
 
   // ---- 1. tridiagonalisation
   if (n >= 3) {
     reflector(A, n, 0, v, tau, e, red, sh);
     // p0 = tau0 * A[1..][1..] v0
-    colwalk(A, n, 1, n - 1, 1, n - 1, false, nullptr, nullptr, 0, v, p, tau[0]);
+    colwalk<T>(A, n, 1, n - 1, 1, n - 1, false, nullptr, nullptr, 0, v, p, tau[0]);
     __syncthreads();
     for (int k = 0; k + 2 < n; ++k) {
       const int mm = n - k - 1, b0 = k + 1;
-      const double tk = tau[k];
+      const T tk = tau[k];
       // w = p - (tau/2)(p.v) v
-      double part = 0.0;
+      T part = T(0);
       for (int j = tid; j < mm; j += nt) part += p[j] * v[j];
-      const double pv = block_sum_syev(part, red);
-      const double kk = 0.5 * tk * pv;
+      const T pv = block_sum_syev(part, red);
+      const T kk = T(0.5) * tk * pv;
       for (int j = tid; j < mm; j += nt) w[j] = p[j] - kk * v[j];
       __syncthreads();
-      const bool upd = tk != 0.0;
+      const bool upd = tk != T(0);
       // (a) first row of the block
       if (upd)
         for (int j = tid; j < mm; j += nt) A[(long long)b0 * n + b0 + j] -= v[0] * w[j] + w[0] * v[j];
@@ -328,12 +345,12 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
       if (k + 3 < n) {
         reflector(A, n, k + 1, vn, tau, e, red, sh);
         // (c) rest of the block, fused with p_{k+1} = tau_{k+1} A22' v_{k+1}
-        colwalk(A, n, b0 + 1, mm - 1, b0 + 1, mm - 1, upd, v, w, 1, vn, p, tau[k + 1]);
+        colwalk<T>(A, n, b0 + 1, mm - 1, b0 + 1, mm - 1, upd, v, w, 1, vn, p, tau[k + 1]);
       } else if (upd) {
-        colwalk(A, n, b0 + 1, mm - 1, b0 + 1, mm - 1, true, v, w, 1, vn, p, 0.0);
+        colwalk<T>(A, n, b0 + 1, mm - 1, b0 + 1, mm - 1, true, v, w, 1, vn, p, T(0));
       }
       __syncthreads();
-      double* t = v; v = vn; vn = t;
+      T* t = v; v = vn; vn = t;
     }
   }
   for (int i = tid; i < n; i += nt) d[i] = A[(long long)i * n + i];
@@ -343,7 +360,7 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
   // ---- 2. Zc = Q^T (row c of Zc = column c of Q) by backward accumulation:
   // Zc22 <- Zc22 (I - tau v v^T), one warp per row of Zc; the dot product
   // u'_c = Zc_new[c][.] v' of the next step (k-1) is fused into the same pass.
-  for (long long x = tid; x < (long long)n * n; x += nt) Z[x] = ((x / n) == (x % n)) ? 1.0 : 0.0;
+  for (long long x = tid; x < (long long)n * n; x += nt) Z[x] = ((x / n) == (x % n)) ? T(1) : T(0);
   __syncthreads();
   {
     const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
@@ -351,37 +368,37 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
     if (k >= 0) {
       // first applied step: Zc22 is the identity, so u_c = v_c
       const int mm = n - k - 1;
-      for (int i = tid; i < mm; i += nt) { v[i] = i == 0 ? 1.0 : A[(long long)k * n + k + 1 + i]; w[i] = v[i]; }
+      for (int i = tid; i < mm; i += nt) { v[i] = i == 0 ? T(1) : A[(long long)k * n + k + 1 + i]; w[i] = v[i]; }
       __syncthreads();
     }
     for (; k >= 0; --k) {
       const int mm = n - k - 1, b0 = k + 1;
-      const double tk = tau[k];
+      const T tk = tau[k];
       // v' of step k-1 (its block starts at index k): v'_0 = 1, v'_i = A[k-1][k+i]
       if (k >= 1)
-        for (int i = tid; i <= mm; i += nt) vn[i] = i == 0 ? 1.0 : A[(long long)(k - 1) * n + k + i];
+        for (int i = tid; i <= mm; i += nt) vn[i] = i == 0 ? T(1) : A[(long long)(k - 1) * n + k + i];
       __syncthreads();
       for (int c = wid; c < mm; c += 2 * nw) {
         // rows c and c + nw of the block (the second may not exist)
         const int c2 = c + nw;
         const bool two = c2 < mm;
-        double* za = Z + (long long)(b0 + c) * n + b0;
-        double* zb = Z + (long long)(b0 + (two ? c2 : c)) * n + b0;
-        const double ta = tk * w[c], tb = two ? tk * w[c2] : 0.0;
-        double acca = 0.0, accb = 0.0;
+        T* za = Z + (long long)(b0 + c) * n + b0;
+        T* zb = Z + (long long)(b0 + (two ? c2 : c)) * n + b0;
+        const T ta = tk * w[c], tb = two ? tk * w[c2] : T(0);
+        T acca = T(0), accb = T(0);
         for (int r0 = 0; r0 < mm; r0 += 32 * kQBatch) {
-          double qa[kQBatch], qb[kQBatch];
+          T qa[kQBatch], qb[kQBatch];
 #pragma unroll
           for (int u = 0; u < kQBatch; ++u) {
             const int r = r0 + lane + 32 * u;
-            qa[u] = r < mm ? za[r] : 0.0;
-            qb[u] = (two && r < mm) ? zb[r] : 0.0;
+            qa[u] = r < mm ? za[r] : T(0);
+            qb[u] = (two && r < mm) ? zb[r] : T(0);
           }
 #pragma unroll
           for (int u = 0; u < kQBatch; ++u) {
             const int r = r0 + lane + 32 * u;
             if (r < mm) {
-              if (tk != 0.0) {
+              if (tk != T(0)) {
                 qa[u] -= ta * v[r];
                 za[r] = qa[u];
                 if (two) {
@@ -406,14 +423,14 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
       __syncthreads();
       if (k >= 1) {
         // next step: v <- v'; u'_0 = Zc[k][k..] . v' = 1 (row k of Zc is still e_k)
-        for (int i = tid; i <= mm; i += nt) { v[i] = vn[i]; w[i] = i == 0 ? 1.0 : p[i]; }
+        for (int i = tid; i <= mm; i += nt) { v[i] = vn[i]; w[i] = i == 0 ? T(1) : p[i]; }
         __syncthreads();
       }
     }
   }
 
   // ---- 3. implicit QL, producer (warp 0) / consumers (warps 1..)
-  if (tid == 0) { q_full = 0; q_end = 0; q_fail = 0; e[n - 1] = 0.0; }
+  if (tid == 0) { q_full = 0; q_end = 0; q_fail = 0; e[n - 1] = T(0); }
   if (tid < kEigThreads / 32) q_done[tid] = 0;
   __syncthreads();
   const int ncons = (nt >> 5) - 1;
@@ -421,7 +438,7 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
     // producer warp: the deflation scan is warp-parallel (ballot over 32
     // consecutive indices), the rotation chain runs on lane 0
     const int lane = tid;
-    const double eps = 2.220446049250313e-16;
+    const T eps = Eps<T>::v;
     int q = 0;
     bool fail = false;
     for (int l = 0; l < n && !fail; ++l) {
@@ -432,8 +449,8 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
           const int i = base + lane;
           bool small = false;
           if (i < n - 1) {
-            const double dd = fabs(d[i]) + fabs(d[i + 1]);
-            small = fabs(e[i]) <= eps * dd;
+            const T dd = tb_abs(d[i]) + tb_abs(d[i + 1]);
+            small = tb_abs(e[i]) <= eps * dd;
           }
           const unsigned bal = __ballot_sync(0xffffffffu, small);
           if (bal) { mq = base + __ffs(bal) - 1; break; }
@@ -457,26 +474,26 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
           __threadfence_block();
         }
         if (lane == 0) {
-          double* rc = ring + (size_t)slot * 2 * n;
-          double* rs = rc + n;
-          double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-          double r = sqrt(g * g + 1.0);
-          g = d[mq] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
-          double s = 1.0, c = 1.0, pp = 0.0;
+          T* rc = ring + (size_t)slot * 2 * n;
+          T* rs = rc + n;
+          T g = (d[l + 1] - d[l]) / (T(2) * e[l]);
+          T r = tb_sqrt(g * g + T(1));
+          g = d[mq] - d[l] + e[l] / (g + (g >= T(0) ? r : -r));
+          T s = T(1), c = T(1), pp = T(0);
           int cnt = 0;
           bool underflow = false;
           for (int i = mq - 1; i >= l; --i) {
-            const double f = s * e[i];
-            const double bb = c * e[i];
-            const double rr2 = f * f + g * g;
-            if (rr2 == 0.0) { d[i + 1] -= pp; e[mq] = 0.0; underflow = true; break; }
-            const double ri = rsqrt(rr2);
+            const T f = s * e[i];
+            const T bb = c * e[i];
+            const T rr2 = f * f + g * g;
+            if (rr2 == T(0)) { d[i + 1] -= pp; e[mq] = T(0); underflow = true; break; }
+            const T ri = tb_rsqrt(rr2);
             r = rr2 * ri;
             e[i + 1] = r;
             s = f * ri;
             c = g * ri;
             g = d[i + 1] - pp;
-            r = (d[i] - g) * s + 2.0 * c * bb;
+            r = (d[i] - g) * s + T(2) * c * bb;
             pp = s * r;
             d[i + 1] = g + pp;
             g = c * r - bb;
@@ -484,7 +501,7 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
             rs[cnt] = s;
             ++cnt;
           }
-          if (!underflow) { d[l] -= pp; e[l] = g; e[mq] = 0.0; }
+          if (!underflow) { d[l] -= pp; e[l] = g; e[mq] = T(0); }
           sh_head[slot][0] = mq;
           sh_head[slot][1] = cnt;
           __threadfence_block();
@@ -525,7 +542,7 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
       __threadfence_block();
       const int kg = min(kWaveK, full - q0);
       int mk[kWaveK], lk[kWaveK];
-      const double* ck[kWaveK];
+      const T* ck[kWaveK];
       int mx = 0, lmin = n;
 #pragma unroll
       for (int k = 0; k < kWaveK; ++k) {
@@ -544,13 +561,13 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
       const int J = mx - lmin + 2 * (kg - 1);
       const int nblk = (J + kWin - 1) / kWin;
       for (int r = tid - 32; r < n; r += nt - 32) {
-        double* zr = Z + r;
-        double wv[kWin];
-        wv[0] = 0.0;
+        T* zr = Z + r;
+        T wv[kWin];
+        wv[0] = T(0);
 #pragma unroll
         for (int a = 1; a < kWin; ++a) {
           const int row = mx - 1 + a;
-          wv[a] = row <= n - 1 ? zr[(long long)row * n] : 0.0;
+          wv[a] = row <= n - 1 ? zr[(long long)row * n] : T(0);
         }
         for (int blk = 0; blk < nblk; ++blk) {
 #pragma unroll
@@ -560,15 +577,15 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
             const int row_out = mx + kWin - 1 - j;
             if (j >= 1 && row_out >= 0 && row_out <= n - 1) zr[(long long)row_out * n] = wv[sl];
             const int row_in = mx - 1 - j;
-            wv[sl] = row_in >= 0 ? zr[(long long)row_in * n] : 0.0;
+            wv[sl] = row_in >= 0 ? zr[(long long)row_in * n] : T(0);
 #pragma unroll
             for (int k = 0; k < kWaveK; ++k) {
               const int i = mx - 1 - j + 2 * k;
               if (i >= lk[k] && i <= mk[k] - 1) {
                 const int t = mk[k] - 1 - i;
-                const double c = ck[k][t], sn = ck[k][n + t];
+                const T c = ck[k][t], sn = ck[k][n + t];
                 const int ia = (2 * k - p + 2 * kWin) % kWin, ib = (2 * k + 1 - p + 2 * kWin) % kWin;
-                const double x = wv[ia], y = wv[ib];
+                const T x = wv[ia], y = wv[ib];
                 wv[ib] = sn * x + c * y;
                 wv[ia] = c * x - sn * y;
               }
@@ -598,15 +615,30 @@ __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __r
   }
   // ---- 4. ascending order by rank (ties by index)
   for (int i = tid; i < n; i += nt) {
-    const double di = d[i];
+    const T di = d[i];
     int rank = 0;
     for (int j = 0; j < n; ++j) {
-      const double dj = d[j];
+      const T dj = d[j];
       rank += (dj < di || (dj == di && j < i)) ? 1 : 0;
     }
     perm[vo + rank] = i;
     wout[vo + rank] = di;
   }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __restrict__ Ab, double* __restrict__ Zb,
+                                                      double* __restrict__ wout, int* __restrict__ perm,
+                                                      int* __restrict__ status, const int* __restrict__ active) {
+  syev_body<double>(B, Ab, Zb, wout, perm, status, active);
+}
+
+__global__ void __launch_bounds__(kEigThreads, 4) k_syev_f32(DevBatch B, float* __restrict__ Ab,
+                                                          float* __restrict__ Zb, double* __restrict__ wout,
+                                                          int* __restrict__ perm, int* __restrict__ status,
+                                                          const int* __restrict__ active) {
+  syev_body<float>(B, Ab, Zb, wout, perm, status, active);
 }
 
 }  // namespace tb

@@ -81,6 +81,7 @@ __global__ void k_scf_init(DevParams P, DevBatch B, const double* __restrict__ c
     S.mix_iter[m] = 0;
     S.eelec[m] = 0.0;
     S.active[m] = S.status[m] == kStOk ? 1 : 0;
+    if (S.phase) { S.phase[m] = 0; S.n64[m] = 0; }  // mixed-precision form starts in the mixed phase
     if (S.active[m]) atomicAdd(S.n_active, 1);
   }
 }
@@ -363,7 +364,8 @@ __global__ void __launch_bounds__(256) k_mulliken_cols(DevBatch B, const int2* _
 __global__ void k_finalize(DevParams P, DevBatch B, const double* __restrict__ colred, const double* __restrict__ n0sh,
                            const double* __restrict__ mrad, const double* __restrict__ q_in, double* __restrict__ dq,
                            double* __restrict__ qsh_out, double* __restrict__ qat_out, double* __restrict__ dpat_out,
-                           double* __restrict__ qpat_out, double econv, double pconv, int max_iter, MolState S) {
+                           double* __restrict__ qpat_out, double econv, double pconv, int max_iter, MolState S,
+                           double econv_lo, double pconv_lo) {
   const int m = blockIdx.x;
   if (!S.active[m]) return;
   __shared__ double red[32];
@@ -472,7 +474,21 @@ __global__ void k_finalize(DevParams P, DevBatch B, const double* __restrict__ c
     S.scf_error[m] = error;
     const int it = S.iscf[m] + 1;
     S.iscf[m] = it;
-    const bool conv = fabs(eelec - elast) < econv && error < pconv;
+    bool conv = fabs(eelec - elast) < econv && error < pconv;
+    if (S.phase) {
+      // mixed-precision form: the mixed phase ends at the loosened test (or
+      // after half the iteration budget), the mixer restarts from the current
+      // point, then at least two FP64 iterations run and the full test decides
+      if (S.phase[m] == 0) {
+        if ((fabs(eelec - elast) < econv_lo && error < pconv_lo) || 2 * it >= max_iter) {
+          S.phase[m] = 1;
+          S.mix_iter[m] = 0;
+        }
+        conv = false;
+      } else if (++S.n64[m] < 2) {
+        conv = false;
+      }
+    }
     if (conv) {
       S.active[m] = 0;
     } else if (it >= max_iter) {

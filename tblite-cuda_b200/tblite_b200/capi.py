@@ -36,7 +36,8 @@ class Structure(C.Structure):
 class Options(C.Structure):
     _fields_ = [("accuracy", C.c_double), ("kt", C.c_double), ("max_iter", C.c_int32),
                 ("mixer_damping", C.c_double), ("verbosity", C.c_int32), ("use_graphs", C.c_int32),
-                ("solver", C.c_int32), ("profile", C.c_int32)]
+                ("solver", C.c_int32), ("profile", C.c_int32),
+                ("precision", C.c_int32)]
 
 
 class Result(C.Structure):
