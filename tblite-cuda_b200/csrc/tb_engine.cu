@@ -593,12 +593,12 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
        k_gemm_mx<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.f, 0.f,
                                             lo));
   TB_K("gemm", 2.0 * n3_hi, 1,
-       k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi));
+       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi));
   TB_K("gemm_mx", 2.0 * n3_lo, 1,
        k_gemm_mx<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.f, 0.f,
                                             lo));
   TB_K("gemm", 2.0 * n3_hi, 1,
-       k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, hi));
+       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, hi));
   // FP32 eigensolve of every active structure
   TB_K("convert", 0, 0, k_to_f32<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, b->Af, S.active));
   TB_K("syev_f32", 4.0 * (n3_lo + n3_hi), 1,
@@ -626,15 +626,16 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
     int* mk = r == 0 ? S.active : hi;
     const double wk = 2.0 * (r == 0 ? n3_lo + n3_hi : n3_hi);
     TB_K("gemm", wk, 1,  // G = V^T V
-         k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, V, 1, V, 0, nullptr, nullptr, nullptr, b->G, 1.0, 0.0, mk));
+         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, V, 1, V, 0, nullptr, nullptr, nullptr, b->G, 1.0, 0.0, mk));
     TB_K("gemm", wk, 1,  // W = F' V
-         k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, 0, V, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, mk));
+         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->F, 0, V, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, mk));
     TB_K("gemm", wk, 1,  // Sm = V^T W (in P)
-         k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, V, 1, b->W, 0, nullptr, nullptr, nullptr, b->P, 1.0, 0.0, mk));
-    TB_K("refine", 0, 0, k_oa_step<<<nmol, 256, oa_smem, st>>>(B, b->G, b->P, V, b->w, mk));
+         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, V, 1, b->W, 0, nullptr, nullptr, nullptr, b->P, 1.0, 0.0, mk));
+    // Rayleigh-Ritz in clusters only in the first of the FP64 phase's two steps
+    TB_K("refine", 0, 0, k_oa_step<<<nmol, 256, oa_smem, st>>>(B, b->G, b->P, V, b->w, mk, r == 0 ? hi : nullptr));
     TB_CUDA(cudaMemcpyAsync(Vo, V, (size_t)b->n2_tot * sizeof(double), cudaMemcpyDeviceToDevice, st));
     TB_K("gemm", wk, 1,  // Vo = V + V E
-         k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, V, 0, b->G, 0, nullptr, nullptr, nullptr, Vo, 1.0, 1.0, mk));
+         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, V, 0, b->G, 0, nullptr, nullptr, nullptr, Vo, 1.0, 1.0, mk));
   }
   TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
   // C = X V into W (mixed phase: V after one step, in Vn; FP64 phase: after two, in Z)
@@ -642,13 +643,13 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
        k_gemm_mx<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->X, 0, b->Vn, 0, nullptr, nullptr, nullptr, b->W, 1.f, 0.f,
                                             lo));
   TB_K("gemm", 2.0 * n3_hi, 1,
-       k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->X, 0, b->Z, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi));
+       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 0, b->Z, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi));
   // P = C diag(f) C^T
   TB_K("gemm_mx", 2.0 * n2occ_lo, 1,
        k_gemm_mx<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.f, 0.f,
                                             lo));
   TB_K("gemm", 2.0 * n2occ_hi, 1,
-       k_gemm<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.0, 0.0, hi));
+       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.0, 0.0, hi));
   return TB_OK;
 }
 
@@ -766,10 +767,10 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
     if (!b->mixed) {
       // F' = X^T F X  (T = F X in W, then F' into F): 2 x 2N^3
       TB_K("gemm", 2.0 * n3, 1,
-           k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->F, 0, b->X, 0, nullptr, nullptr, nullptr,
+           k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->F, 0, b->X, 0, nullptr, nullptr, nullptr,
                                              b->W, 1.0, 0.0, S.active));
       TB_K("gemm", 2.0 * n3, 1,
-           k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 1, b->W, 0, nullptr, nullptr, nullptr,
+           k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 1, b->W, 0, nullptr, nullptr, nullptr,
                                              b->F, 1.0, 0.0, S.active));
       // symmetric eigensolve with vectors: canonical 4 N^3
       TB_K("syev", 4.0 * n3, 1,
@@ -789,10 +790,10 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
       TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
       // C = X Z (eigenvectors in ascending order through perm): 2N^3; P = C diag(f) C^T: 2 N^2 n_occ
       TB_K("gemm", 2.0 * n3, 1,
-           k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr,
+           k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr,
                                              b->W, 1.0, 0.0, S.active));
       TB_K("gemm", 2.0 * n2occ, 1,
-           k_gemm<<<gemm_grid, 256, 0, st>>>(B, b->d_tiles64, ntile64, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim,
+           k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim,
                                              b->P, 1.0, 0.0, S.active));
     } else {
       const tb_status ms = mixed_core(b, st, n3_lo, n3_hi, n2occ_lo, n2occ_hi, gemm_grid, fermi_smem);
@@ -1273,8 +1274,8 @@ tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const 
                                         mb.ms.status + m);
     if (!e.empty()) return fail(TB_CUDA_ERROR, "library Cholesky: " + e);
   }
-  k_gemm<<<grid, 256>>>(B, mb.d_tiles, nt, mb.F, 0, mb.X, 0, nullptr, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);
-  k_gemm<<<grid, 256>>>(B, mb.d_tiles, nt, mb.X, 1, mb.W, 0, nullptr, nullptr, nullptr, mb.F, 1.0, 0.0, mb.ms.active);
+  k_gemm<<<grid, kGemmThreads>>>(B, mb.d_tiles, nt, mb.F, 0, mb.X, 0, nullptr, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);
+  k_gemm<<<grid, kGemmThreads>>>(B, mb.d_tiles, nt, mb.X, 1, mb.W, 0, nullptr, nullptr, nullptr, mb.F, 1.0, 0.0, mb.ms.active);
   const size_t smem = syev_smem_bytes(std::max(mb.nmax_in, 1));
   if (smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_syev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_syev<<<nmat, kEigThreads, smem>>>(B, mb.F, mb.Z, mb.w, mb.perm, mb.ms.status, mb.ms.active);
@@ -1288,7 +1289,7 @@ tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const 
                                       mb.lib_bytes, mb.lib_info + 2 * k + 1, mb.ms.status + m);
     if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
   }
-  k_gemm<<<grid, 256>>>(B, mb.d_tiles, nt, mb.X, 0, mb.Z, 1, mb.perm, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);
+  k_gemm<<<grid, kGemmThreads>>>(B, mb.d_tiles, nt, mb.X, 0, mb.Z, 1, mb.perm, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(TB_CUDA_ERROR, cudaGetErrorString(e));
   TB_CUDA(cudaMemcpy(w, mb.w, mb.no * 8, cudaMemcpyDeviceToHost));

@@ -13,6 +13,7 @@ constexpr int kRing = 8;  // QL sweeps buffered between the k_syev producer and 
 // shared memory of k_syev: d, e, tau, v, vn, p, w (7n) + the rotation ring (2 n kRing)
 inline size_t syev_smem_bytes(int n, size_t elem = sizeof(double)) { return (7 + 2 * (size_t)kRing) * (size_t)n * elem; }
 constexpr int kSyevMaxN = 1216;
+constexpr int kGemmThreads = 128;  // block size of k_gemm
 
 // cuSOLVER dense path for structures above the in-house size bound
 // (tb_large.cu); one instance per batch, used from one host thread at a time.
@@ -100,7 +101,8 @@ inline size_t oa_smem_bytes(int nmax) {
   return (3 * (size_t)kClusterMax * kClusterMax + 2 * kClusterMax) * sizeof(double) +
          2 * ((size_t)nmax + 1) * sizeof(int);
 }
-__global__ void k_oa_step(DevBatch B, double* G, double* Sm, double* V, double* w, const int* mask);
+__global__ void k_oa_step(DevBatch B, double* G, double* Sm, double* V, double* w, const int* mask,
+                          const int* rr_mask);
 
 // SCF
 __global__ void k_scf_init(DevParams P, DevBatch B, const double* charge, const int* uhf, const double* erep,

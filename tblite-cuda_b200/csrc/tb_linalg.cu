@@ -86,15 +86,45 @@ __global__ void k_trinv(DevBatch B, const double* __restrict__ W, double* __rest
 // the list (structure, tile row, tile col).  Square n_m x n_m operands with
 // leading dimension n_m at offset moff[m]; K = kdim[m] if kdim != NULL.
 // op(B) may gather its columns through perm (eigenvector reordering).
-constexpr int GT = 64, GK = 16;
+// 64 x 64 tiles on the FP64 tensor instruction mma.sync.m8n8k4.f64: four warps,
+// each owning a 32 x 32 quarter as 4 x 4 fragments of 8 x 8 (32 accumulators
+// per lane).  K slabs of 16 are staged by cp.async in a two-stage ring (zero
+// fill past the matrix edge); the shared tiles are padded by 4 doubles so the
+// 64-bit fragment loads of a half-warp hit 16 distinct bank pairs.
+constexpr int GT = 64, GK = 16, GP = GT + 4;
+static_assert(kGemmThreads == 128, "k_gemm assumes four warps");
 
-__global__ void __launch_bounds__(256) k_gemm(DevBatch B, const int4* __restrict__ tiles, int ntiles,
-                                              const double* __restrict__ Ab, int ta, const double* __restrict__ Bb,
-                                              int tb_, const int* __restrict__ perm, const double* __restrict__ ks,
-                                              const int* __restrict__ kdim, double* __restrict__ Cb, double alpha,
-                                              double beta, const int* __restrict__ active) {
-  __shared__ double As[2][GK][GT + 1];
-  __shared__ double Bs[2][GK][GT + 1];
+namespace {
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 8 : 0;  // bytes read; the rest of the 8 is zero-filled
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+// D = A B + D for one 8 x 8 x 4 step.  Lane l = 4 g + t holds A[g][t], B[t][g]
+// and D[g][2t], D[g][2t+1].
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+}  // namespace
+
+__global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* __restrict__ tiles, int ntiles,
+                                                       const double* __restrict__ Ab, int ta,
+                                                       const double* __restrict__ Bb, int tb_,
+                                                       const int* __restrict__ perm, const double* __restrict__ ks,
+                                                       const int* __restrict__ kdim, double* __restrict__ Cb,
+                                                       double alpha, double beta, const int* __restrict__ active) {
+  __shared__ __align__(16) double As[2][GK][GP];
+  __shared__ __align__(16) double Bs[2][GK][GP];
+  __shared__ __align__(16) double Ks[2][GK];
+  __shared__ int colS[GT];  // columns of op(B) for this tile (through perm)
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, tg = lane & 3;              // fragment coordinates
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;  // this warp's quarter of the tile
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int4 tl = tiles[t];
     const int m = tl.x;
@@ -108,63 +138,99 @@ __global__ void __launch_bounds__(256) k_gemm(DevBatch B, const int4* __restrict
     const int* pm = perm ? perm + vo : nullptr;
     const double* kv = ks ? ks + vo : nullptr;
     const int i0 = tl.y * GT, j0 = tl.z * GT;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    double acc[4][4];
+    double acc[4][4][2];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-
-    auto load = [&](int buf, int k0) {
-      // A tile: op(A)[i0+ii][k0+kk] -> As[kk][ii]; B tile: op(B)[k0+kk][j0+jj] -> Bs[kk][jj]
-      for (int e = threadIdx.x; e < GT * GK; e += blockDim.x) {
-        int ii, kk;
-        if (ta) { ii = e % GT; kk = e / GT; } else { kk = e % GK; ii = e / GK; }
-        const int gi = i0 + ii, gk = k0 + kk;
-        double v = 0.0;
-        if (gi < n && gk < K) v = ta ? A[(long long)gk * n + gi] : A[(long long)gi * n + gk];
-        if (kv && gk < K) v *= kv[gk];
-        As[buf][kk][ii] = v;
-        int jj, kb;
-        if (tb_) { kb = e % GK; jj = e / GK; } else { jj = e % GT; kb = e / GT; }
-        const int gj = j0 + jj, gk2 = k0 + kb;
-        double u = 0.0;
-        if (gj < n && gk2 < K) {
-          const int col = pm ? pm[gj] : gj;  // eigenvector reordering through perm
-          u = tb_ ? Bm[(long long)col * n + gk2] : Bm[(long long)gk2 * n + col];
+      for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    __syncthreads();  // colS and the ring of the previous tile are free
+    if (tid < GT) colS[tid] = pm ? (j0 + tid < n ? pm[j0 + tid] : 0) : j0 + tid;
+    __syncthreads();
+    // Element r (0..7) of a slab for this thread:
+    //   op(A) not transposed: kk = tid & 15, ii = (tid >> 4) + 8 r;  transposed: ii = tid & 63, kk = (tid >> 6) + 2 r
+    //   op(B) not transposed: jj = tid & 63, kb = (tid >> 6) + 2 r;  transposed: kb = tid & 15, jj = (tid >> 4) + 8 r
+    const int lo16 = tid & 15, hi8 = tid >> 4, lo64 = tid & 63, hi2 = tid >> 6;
+    auto issue = [&](int buf, int k0) {
+      if (!ta) {
+        const int gk = k0 + lo16;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const int gi = i0 + hi8 + 8 * r;
+          const bool v = gi < n && gk < K;
+          cp_async8(&As[buf][lo16][hi8 + 8 * r], v ? A + (long long)gi * n + gk : A, v);
         }
-        Bs[buf][kb][jj] = u;
+      } else {
+        const int gi = i0 + lo64;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const int gk = k0 + hi2 + 2 * r;
+          const bool v = gi < n && gk < K;
+          cp_async8(&As[buf][hi2 + 2 * r][lo64], v ? A + (long long)gk * n + gi : A, v);
+        }
       }
+      if (!tb_) {
+        const bool vj = j0 + lo64 < n;
+        const int col = colS[lo64];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const int gk = k0 + hi2 + 2 * r;
+          const bool v = vj && gk < K;
+          cp_async8(&Bs[buf][hi2 + 2 * r][lo64], v ? Bm + (long long)gk * n + col : Bm, v);
+        }
+      } else {
+        const int gk = k0 + lo16;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const int jj = hi8 + 8 * r;
+          const bool v = j0 + jj < n && gk < K;
+          cp_async8(&Bs[buf][lo16][jj], v ? Bm + (long long)colS[jj] * n + gk : Bm, v);
+        }
+      }
+      if (kv && tid < GK) cp_async8(&Ks[buf][tid], k0 + tid < K ? kv + k0 + tid : kv, k0 + tid < K);
+      cp_async_commit();
     };
     const int nk = (K + GK - 1) / GK;
-    __syncthreads();
-    if (nk > 0) load(0, 0);
-    __syncthreads();
+    if (nk > 0) issue(0, 0);
     for (int kt = 0; kt < nk; ++kt) {
       const int cur = kt & 1;
-      if (kt + 1 < nk) load(cur ^ 1, (kt + 1) * GK);
+      if (kt + 1 < nk) {
+        issue(cur ^ 1, (kt + 1) * GK);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();
+      if (kv) {  // diag(ks) between the factors: scale the slab of op(B) once
+        for (int e = tid; e < GK * GT; e += kGemmThreads) Bs[cur][e / GT][e % GT] *= Ks[cur][e / GT];
+        __syncthreads();
+      }
 #pragma unroll
-      for (int kk = 0; kk < GK; ++kk) {
-        double a[4], b[4];
+      for (int k4 = 0; k4 < GK; k4 += 4) {
+        double af[4], bf[4];
 #pragma unroll
-        for (int x = 0; x < 4; ++x) { a[x] = As[cur][kk][ty + 16 * x]; b[x] = Bs[cur][kk][tx + 16 * x]; }
+        for (int x = 0; x < 4; ++x) af[x] = As[cur][k4 + tg][wr + 8 * x + g];
+#pragma unroll
+        for (int y = 0; y < 4; ++y) bf[y] = Bs[cur][k4 + tg][wc + 8 * y + g];
 #pragma unroll
         for (int x = 0; x < 4; ++x)
 #pragma unroll
-          for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+          for (int y = 0; y < 4; ++y) dmma(acc[x][y][0], acc[x][y][1], af[x], bf[y]);
       }
-      __syncthreads();
+      __syncthreads();  // buffer cur is refilled two slabs later
     }
 #pragma unroll
     for (int x = 0; x < 4; ++x) {
-      const int gi = i0 + ty + 16 * x;
+      const int gi = i0 + wr + 8 * x + g;
       if (gi >= n) continue;
 #pragma unroll
       for (int y = 0; y < 4; ++y) {
-        const int gj = j0 + tx + 16 * y;
-        if (gj >= n) continue;
-        double* c = Cb + mo + (long long)gi * n + gj;
-        *c = beta == 0.0 ? alpha * acc[x][y] : alpha * acc[x][y] + beta * (*c);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int gj = j0 + wc + 8 * y + 2 * tg + h;
+          if (gj >= n) continue;
+          double* c = Cb + mo + (long long)gi * n + gj;
+          *c = beta == 0.0 ? alpha * acc[x][y][h] : alpha * acc[x][y][h] + beta * (*c);
+        }
       }
     }
   }

@@ -188,11 +188,14 @@ __global__ void k_gather_vectors(DevBatch B, const int4* __restrict__ tiles, int
 //  4. lambda recomputed, E (overwrites G) with R = I - G:
 //       E_ij = (Sm_ij + lambda_j R_ij) / (lambda_j - lambda_i)  if |lambda_j - lambda_i| > delta
 //            = R_ij / 2                                          otherwise (and on the diagonal).
-// The caller then forms V + V E.  Refined eigenvalues go to w.
+// The caller then forms V + V E.  Refined eigenvalues go to w.  Steps 2-3 run
+// only for structures with rr_mask set: a single step (or a second step after
+// one with Rayleigh-Ritz) needs no cluster solve, since clustered pairs then
+// only carry rotations inside the cluster, which leave the density unchanged.
 // Dynamic shared memory: oa_smem_bytes(nmax).
 __global__ void __launch_bounds__(256) k_oa_step(DevBatch B, double* __restrict__ G, double* __restrict__ Sm,
                                                  double* __restrict__ Vb, double* __restrict__ w,
-                                                 const int* __restrict__ mask) {
+                                                 const int* __restrict__ mask, const int* __restrict__ rr_mask) {
   const int m = blockIdx.x;
   if (!mask[m]) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
@@ -243,8 +246,9 @@ __global__ void __launch_bounds__(256) k_oa_step(DevBatch B, double* __restrict_
   rr = block_sum(rr, red);
   const double delta = 2.0 * (sqrt(so) + sh_amax * sqrt(rr));
 
-  // ---- 2. clusters
-  if (tid == 0) {
+  // ---- 2. clusters (only where rr_mask asks for the Rayleigh-Ritz solve)
+  if (tid == 0 && !(rr_mask && rr_mask[m])) ncl = 0;
+  if (tid == 0 && rr_mask && rr_mask[m]) {
     int c = 0, i = 0;
     while (i < n) {
       int j = i;
