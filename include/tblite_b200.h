@@ -134,6 +134,34 @@ int32_t tb_batch_profile(const tb_batch* batch, int32_t max, char* names, int64_
                          double* work, int32_t* units);
 void tb_batch_destroy(tb_batch* batch);
 
+/* ---- serving: continuous batching of singlepoint requests ------------------
+ * No counterpart in the reference (its driver runs one fixed batch,
+ * src/xtb.cu:483-509).  Requests are queued by tb_server_submit.  Each
+ * tb_server_step admits queued requests (first in, first out) as one new
+ * resident micro-batch while the device workspace of all resident
+ * micro-batches stays within hbm_budget_bytes (at most max_batch per
+ * micro-batch), runs ONE SCF iteration of every resident micro-batch, each on
+ * its own stream so that their work overlaps on the device, and retires the
+ * structures that finished; a micro-batch's workspace is freed when its last
+ * structure finishes.  tb_server_poll hands out finished results in completion
+ * order.  Each result equals the one tb_singlepoint_batch gives for the same
+ * structure alone (the kernels treat every structure independently).
+ * Calls on one server must come from one host thread at a time. */
+typedef struct tb_server tb_server;
+tb_status tb_server_create(tb_calculator* calc, const tb_options* opt, int64_t hbm_budget_bytes,
+                           int32_t max_batch, tb_server** out);
+/* Copies the structure into the queue; *ticket identifies its result.
+ * TB_CAPACITY_EXCEEDED if the structure alone needs more than the budget. */
+tb_status tb_server_submit(tb_server* server, const tb_structure* mol, int64_t* ticket);
+/* One scheduling step (see above); optional outputs: requests resident on the
+ * device, requests still queued, workspace bytes resident. */
+tb_status tb_server_step(tb_server* server, int32_t* n_resident, int32_t* n_queued, int64_t* bytes_resident);
+/* Up to max finished results: tickets[i], results[i] (scalar fields; the array
+ * pointers of results[i], when not NULL, receive that structure's qat / qsh /
+ * dpat / qpat).  Returns the number written. */
+int32_t tb_server_poll(tb_server* server, int32_t max, int64_t* tickets, tb_result* results);
+void tb_server_destroy(tb_server* server);
+
 /* ---- stage entry points (host buffers; one structure each) ---------------- */
 
 /* get_cutoff (src/basis/type.cu:66-79). */

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <fstream>
 #include <map>
 #include <mutex>
@@ -254,6 +255,12 @@ struct tb_batch {
   float *Af = nullptr, *Zf = nullptr, *wf = nullptr;
   double *Vn = nullptr, *G = nullptr;
   int *act_lo = nullptr, *act_hi = nullptr;
+  // stepping state (tb_batch_begin / tb_batch_step) and the captured iteration
+  DevParams Pc{};
+  int it = 0;
+  cudaStream_t cap = nullptr;       // capture stream of the iteration graph
+  cudaGraphExec_t gexec = nullptr;  // one SCF iteration (tb_options.use_graphs)
+  int64_t launches_per_iter = 0;
   int64_t launches = 0;
   size_t bytes = 0;
   std::vector<double> h_nocc;  // closed-shell occupied orbitals per structure (work accounting)
@@ -269,6 +276,8 @@ struct tb_batch {
   std::vector<cudaEvent_t> evpool;
   size_t evused = 0;
   ~tb_batch() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (cap) cudaStreamDestroy(cap);
     if (h_nactive) cudaFreeHost(h_nactive);
     for (cudaEvent_t e : evpool) cudaEventDestroy(e);
   }
@@ -653,7 +662,39 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
   return TB_OK;
 }
 
-tb_status batch_run(tb_batch* b, cudaStream_t st) {
+// Dynamic shared memory of the one-CTA-per-structure kernels grows with N.
+// The opt-in limit is a per-kernel attribute shared by every batch of the
+// process (batches of different sizes can be resident at once), so it is
+// raised once to the device maximum rather than set per batch.
+tb_status raise_smem_limits() {
+  int dev = 0, optin = 0;
+  TB_CUDA(cudaGetDevice(&dev));
+  TB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const void* ks[] = {(const void*)k_syev, (const void*)k_syev_f32, (const void*)k_fermi, (const void*)k_oa_step};
+  for (const void* k : ks) {
+    cudaFuncAttributes a;
+    TB_CUDA(cudaFuncGetAttributes(&a, k));
+    TB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes));
+  }
+  return TB_OK;
+}
+
+// Host copy of active/status, read where a run synchronises anyway, so that
+// converged or failed library structures are not diagonalised again.
+tb_status read_flags(tb_batch* b, cudaStream_t st) {
+  if (b->big.empty()) return TB_OK;
+  const int nmol = b->nmol;
+  b->h_active.resize(nmol);
+  b->h_status.resize(nmol);
+  TB_CUDA(cudaMemcpyAsync(b->h_active.data(), b->ms.active, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
+  TB_CUDA(cudaMemcpyAsync(b->h_status.data(), b->ms.status, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
+  TB_CUDA(cudaStreamSynchronize(st));
+  return TB_OK;
+}
+
+// Setup of a run: status reset, per-structure setup kernels (CN, neighbour
+// list, integrals, S = L L^T and X = L^-T) and the SCF start (k_scf_init).
+tb_status batch_setup(tb_batch* b, cudaStream_t st) {
   tb_calculator* c = b->calc;
   const DevBatch& B = b->db;
   MolState& S = b->ms;
@@ -662,9 +703,11 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
   b->kclass.clear();
   b->pend.clear();
   b->evused = 0;
-  DevParams Pc = c->dp;
+  b->Pc = c->dp;
+  DevParams& Pc = b->Pc;
   Pc.intcut = integral_cutoff(b->opt.accuracy);
   Pc.cutoff = std::min(std::sqrt(2.0 * Pc.intcut / c->hp.min_alpha), 40.0);  // get_cutoff, src/basis/type.cu:43-64
+  b->it = 0;
   TB_CUDA(cudaMemsetAsync(S.status, 0, nmol * sizeof(int), st));
   TB_CUDA(cudaMemsetAsync(S.fermi_warn, 0, nmol * sizeof(int), st));
   TB_CUDA(cudaMemsetAsync(S.n_active, 0, sizeof(int), st));
@@ -702,117 +745,164 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
     prof_stop(b, st, "factor_lib", e0, 0, 0);
   }
   TB_K("scf_init", 0, 0, k_scf_init<<<nmol, 256, 0, st>>>(Pc, B, b->charge, b->uhf, b->erep, b->n0sh, b->q_in, S));
-  // ---- SCF (next_scf per iteration, src/scf/iterators.cu:317-424)
+  {
+    const tb_status ss = raise_smem_limits();
+    if (ss != TB_OK) return ss;
+  }
+  return read_flags(b, st);
+}
+
+// One SCF iteration (next_scf, src/scf/iterators.cu:317-424) for every
+// active structure: launches only, no host synchronisation, so that the same
+// sequence can be captured once as a CUDA graph.
+tb_status iterate_body(tb_batch* b, cudaStream_t st) {
+  const DevBatch& B = b->db;
+  MolState& S = b->ms;
+  const DevParams& Pc = b->Pc;
+  const int nmol = b->nmol;
   const double econv = 1.0e-6 * b->opt.accuracy, pconv = 2.0e-5 * b->opt.accuracy;
   const int ntile64 = (int)b->tiles64.size(), ntile32 = (int)b->tiles32.size(), nchunk = (int)b->chunks32.size();
   const int gemm_grid = std::min(ntile64, 148 * 8);
   const size_t eig_smem = syev_smem_bytes(std::max(b->nmax_in, 1));
-  if (eig_smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_syev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eig_smem));
   const size_t fermi_smem = (size_t)b->nmax * sizeof(double);
-  if (fermi_smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_fermi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fermi_smem));
   const dim3 pot_grid(nmol, nblk(std::max(b->natmax, b->nshmax), 256));
   std::vector<int> act, phase;
-  if (b->mixed) {
-    const size_t smem32 = syev_smem_bytes(std::max(b->nmax_in, 1), sizeof(float));
-    if (smem32 > 48 * 1024)
-      TB_CUDA(cudaFuncSetAttribute(k_syev_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32));
-    TB_CUDA(cudaFuncSetAttribute(k_oa_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)oa_smem_bytes(b->nmax)));
-  }
-  // host copy of active/status, read where the loop synchronises anyway, so
-  // that converged or failed library structures are not diagonalised again
-  auto read_flags = [&]() -> tb_status {
-    if (b->big.empty()) return TB_OK;
-    b->h_active.resize(nmol);
-    b->h_status.resize(nmol);
-    TB_CUDA(cudaMemcpyAsync(b->h_active.data(), S.active, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
-    TB_CUDA(cudaMemcpyAsync(b->h_status.data(), S.status, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
+  // algorithmic work of this iteration over the active structures (profile mode only)
+  double n3 = 0, n2 = 0, n2occ = 0, n3_lo = 0, n3_hi = 0, n2occ_lo = 0, n2occ_hi = 0;
+  if (b->opt.profile) {
+    act.resize(nmol);
+    phase.assign(nmol, 1);
+    TB_CUDA(cudaMemcpyAsync(act.data(), S.active, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (b->mixed)
+      TB_CUDA(cudaMemcpyAsync(phase.data(), S.phase, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
     TB_CUDA(cudaStreamSynchronize(st));
-    return TB_OK;
-  };
-  {
-    const tb_status fs = read_flags();
-    if (fs != TB_OK) return fs;
+    for (int m = 0; m < nmol; ++m) {
+      if (!act[m]) continue;
+      const double n = b->h_ooff[m + 1] - b->h_ooff[m];
+      const double occ = n * n * std::min(n, b->h_nocc[m]);
+      n3 += n * n * n;
+      n2 += n * n;
+      n2occ += occ;
+      (phase[m] ? n3_hi : n3_lo) += n * n * n;
+      (phase[m] ? n2occ_hi : n2occ_lo) += occ;
+    }
   }
+  // (k_mix_next leaves structures in their first iteration alone)
+  TB_K("mix_next", 0, 0,
+         k_mix_next<<<nmol, 256, 0, st>>>(B, b->q_in, b->dq, b->dqlast, b->qlast, b->df, b->u, b->amat,
+                                          b->omega, b->opt.max_iter, b->opt.mixer_damping, S));
+  TB_K("potential", 0, 0,
+       k_potential<<<pot_grid, 256, 0, st>>>(Pc, B, b->q_in, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, S.active));
+  // Fock build: reads S, H0, D(3), Q(6), writes F -> 12 N^2 doubles
+  TB_K("fock", 96.0 * n2, 2,
+       k_fock<<<ntile32, 256, 0, st>>>(B, b->d_tiles32, ntile32, b->S, b->H0, b->D, b->Q, b->vsh, b->vat, b->vdp,
+                                       b->vqp, b->F, S.active));
+  if (!b->mixed) {
+    // F' = X^T F X  (T = F X in W, then F' into F): 2 x 2N^3
+    TB_K("gemm", 2.0 * n3, 1,
+         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->F, 0, b->X, 0, nullptr, nullptr, nullptr,
+                                           b->W, 1.0, 0.0, S.active));
+    TB_K("gemm", 2.0 * n3, 1,
+         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 1, b->W, 0, nullptr, nullptr, nullptr,
+                                           b->F, 1.0, 0.0, S.active));
+    // symmetric eigensolve with vectors: canonical 4 N^3
+    TB_K("syev", 4.0 * n3, 1,
+         k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->w, b->perm, S.status, S.active));
+    for (size_t k = 0; k < b->big.size(); ++k) {
+      const int m = b->big[k], n = b->h_ooff[m + 1] - b->h_ooff[m];
+      if (!b->h_active[m] || b->h_status[m] != kStOk) continue;
+      const long long mo = b->h_moff[m], vo = b->h_ooff[m];
+      cudaEvent_t e0 = nullptr;
+      prof_start(b, st, &e0);
+      const std::string e = b->lib.syev(st, b->F + mo, b->Z + mo, b->w + vo, b->perm + vo, n, b->lib_work,
+                                        b->lib_bytes, b->lib_info + 2 * k, S.status + m);
+      if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
+      ++b->launches;
+      prof_stop(b, st, "syev_lib", e0, 4.0 * n * n * n, 1);
+    }
+    TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
+    // C = X Z (eigenvectors in ascending order through perm): 2N^3; P = C diag(f) C^T: 2 N^2 n_occ
+    TB_K("gemm", 2.0 * n3, 1,
+         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr,
+                                           b->W, 1.0, 0.0, S.active));
+    TB_K("gemm", 2.0 * n2occ, 1,
+         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim,
+                                           b->P, 1.0, 0.0, S.active));
+  } else {
+    const tb_status ms = mixed_core(b, st, n3_lo, n3_hi, n2occ_lo, n2occ_hi, gemm_grid, fermi_smem);
+    if (ms != TB_OK) return ms;
+  }
+  // Mulliken + band energy: reads P, S, H0, D(3), Q(6) -> 11 N^2 doubles
+  TB_K("mulliken", 88.0 * n2, 2,
+       k_mulliken_cols<<<nchunk, 256, 0, st>>>(B, b->d_chunks32, nchunk, b->P, b->S, b->H0, b->D, b->Q, b->colred,
+                                               S.active));
+  TB_K("finalize", 0, 0,
+       k_finalize<<<nmol, 256, 0, st>>>(Pc, B, b->colred, b->n0sh, b->mrad, b->q_in, b->dq, b->qsh_out, b->qat_out,
+                                        b->dpat_out, b->qpat_out, econv, pconv, b->opt.max_iter, S,
+                                        std::max(kMixedSwitchScale * econv, kMixedSwitchFloorE),
+                                        std::max(kMixedSwitchScale * pconv, kMixedSwitchFloorQ)));
+  return TB_OK;
+}
+
+
+// One iteration plus the host read of the active count; *n_active = structures
+// still iterating.  With tb_options.use_graphs (and no structure on the
+// library path, whose calls depend on host-side flags) the launches of
+// iterate_body are captured once per batch and replayed.
+tb_status launch_iteration(tb_batch* b, cudaStream_t st) {
+  const bool graphs = b->opt.use_graphs && !b->opt.profile && b->big.empty();
+  if (graphs) {
+    if (!b->gexec) {
+      if (!b->cap) TB_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+      const int64_t l0 = b->launches;
+      TB_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+      const tb_status bs = iterate_body(b, b->cap);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(b->cap, &g);
+      if (bs != TB_OK) {
+        if (g) cudaGraphDestroy(g);
+        return bs;
+      }
+      TB_CUDA(ce);
+      const cudaError_t ie = cudaGraphInstantiate(&b->gexec, g, 0);
+      cudaGraphDestroy(g);
+      TB_CUDA(ie);
+      b->launches_per_iter = b->launches - l0;
+      b->launches = l0;
+    }
+    TB_CUDA(cudaGraphLaunch(b->gexec, st));
+    b->launches += b->launches_per_iter;
+  } else {
+    const tb_status bs = iterate_body(b, st);
+    if (bs != TB_OK) return bs;
+  }
+  ++b->it;
+  TB_CUDA(cudaMemcpyAsync(b->h_nactive, b->ms.n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
+  return TB_OK;
+}
+
+// Waits for the iteration launched on st and reads the active count.
+tb_status finish_iteration(tb_batch* b, cudaStream_t st, int* n_active) {
+  TB_CUDA(cudaStreamSynchronize(st));
+  *n_active = *b->h_nactive;
+  if (*n_active > 0) return read_flags(b, st);
+  return TB_OK;
+}
+
+tb_status batch_iterate(tb_batch* b, cudaStream_t st, int* n_active) {
+  const tb_status s = launch_iteration(b, st);
+  if (s != TB_OK) return s;
+  return finish_iteration(b, st, n_active);
+}
+
+tb_status batch_run(tb_batch* b, cudaStream_t st) {
+  tb_status s = batch_setup(b, st);
+  if (s != TB_OK) return s;
   for (int it = 0; it < b->opt.max_iter; ++it) {
-    // algorithmic work of this iteration over the active structures (profile mode only)
-    double n3 = 0, n2 = 0, n2occ = 0, n3_lo = 0, n3_hi = 0, n2occ_lo = 0, n2occ_hi = 0;
-    if (b->opt.profile) {
-      act.resize(nmol);
-      phase.assign(nmol, 1);
-      TB_CUDA(cudaMemcpyAsync(act.data(), S.active, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
-      if (b->mixed)
-        TB_CUDA(cudaMemcpyAsync(phase.data(), S.phase, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
-      TB_CUDA(cudaStreamSynchronize(st));
-      for (int m = 0; m < nmol; ++m) {
-        if (!act[m]) continue;
-        const double n = b->h_ooff[m + 1] - b->h_ooff[m];
-        const double occ = n * n * std::min(n, b->h_nocc[m]);
-        n3 += n * n * n;
-        n2 += n * n;
-        n2occ += occ;
-        (phase[m] ? n3_hi : n3_lo) += n * n * n;
-        (phase[m] ? n2occ_hi : n2occ_lo) += occ;
-      }
-    }
-    if (it > 0)
-      TB_K("mix_next", 0, 0,
-           k_mix_next<<<nmol, 256, 0, st>>>(B, b->q_in, b->dq, b->dqlast, b->qlast, b->df, b->u, b->amat,
-                                            b->omega, b->opt.max_iter, b->opt.mixer_damping, S));
-    TB_K("potential", 0, 0,
-         k_potential<<<pot_grid, 256, 0, st>>>(Pc, B, b->q_in, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, S.active));
-    // Fock build: reads S, H0, D(3), Q(6), writes F -> 12 N^2 doubles
-    TB_K("fock", 96.0 * n2, 2,
-         k_fock<<<ntile32, 256, 0, st>>>(B, b->d_tiles32, ntile32, b->S, b->H0, b->D, b->Q, b->vsh, b->vat, b->vdp,
-                                         b->vqp, b->F, S.active));
-    if (!b->mixed) {
-      // F' = X^T F X  (T = F X in W, then F' into F): 2 x 2N^3
-      TB_K("gemm", 2.0 * n3, 1,
-           k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->F, 0, b->X, 0, nullptr, nullptr, nullptr,
-                                             b->W, 1.0, 0.0, S.active));
-      TB_K("gemm", 2.0 * n3, 1,
-           k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 1, b->W, 0, nullptr, nullptr, nullptr,
-                                             b->F, 1.0, 0.0, S.active));
-      // symmetric eigensolve with vectors: canonical 4 N^3
-      TB_K("syev", 4.0 * n3, 1,
-           k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->w, b->perm, S.status, S.active));
-      for (size_t k = 0; k < b->big.size(); ++k) {
-        const int m = b->big[k], n = b->h_ooff[m + 1] - b->h_ooff[m];
-        if (!b->h_active[m] || b->h_status[m] != kStOk) continue;
-        const long long mo = b->h_moff[m], vo = b->h_ooff[m];
-        cudaEvent_t e0 = nullptr;
-        prof_start(b, st, &e0);
-        const std::string e = b->lib.syev(st, b->F + mo, b->Z + mo, b->w + vo, b->perm + vo, n, b->lib_work,
-                                          b->lib_bytes, b->lib_info + 2 * k, S.status + m);
-        if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
-        ++b->launches;
-        prof_stop(b, st, "syev_lib", e0, 4.0 * n * n * n, 1);
-      }
-      TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
-      // C = X Z (eigenvectors in ascending order through perm): 2N^3; P = C diag(f) C^T: 2 N^2 n_occ
-      TB_K("gemm", 2.0 * n3, 1,
-           k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr,
-                                             b->W, 1.0, 0.0, S.active));
-      TB_K("gemm", 2.0 * n2occ, 1,
-           k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim,
-                                             b->P, 1.0, 0.0, S.active));
-    } else {
-      const tb_status ms = mixed_core(b, st, n3_lo, n3_hi, n2occ_lo, n2occ_hi, gemm_grid, fermi_smem);
-      if (ms != TB_OK) return ms;
-    }
-    // Mulliken + band energy: reads P, S, H0, D(3), Q(6) -> 11 N^2 doubles
-    TB_K("mulliken", 88.0 * n2, 2,
-         k_mulliken_cols<<<nchunk, 256, 0, st>>>(B, b->d_chunks32, nchunk, b->P, b->S, b->H0, b->D, b->Q, b->colred,
-                                                 S.active));
-    TB_K("finalize", 0, 0,
-         k_finalize<<<nmol, 256, 0, st>>>(Pc, B, b->colred, b->n0sh, b->mrad, b->q_in, b->dq, b->qsh_out, b->qat_out,
-                                          b->dpat_out, b->qpat_out, econv, pconv, b->opt.max_iter, S,
-                                          std::max(kMixedSwitchScale * econv, kMixedSwitchFloorE),
-                                          std::max(kMixedSwitchScale * pconv, kMixedSwitchFloorQ)));
-    TB_CUDA(cudaMemcpyAsync(b->h_nactive, S.n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
-    TB_CUDA(cudaStreamSynchronize(st));
-    if (*b->h_nactive <= 0) break;
-    const tb_status fs = read_flags();
-    if (fs != TB_OK) return fs;
+    int na = 0;
+    s = batch_iterate(b, st, &na);
+    if (s != TB_OK) return s;
+    if (na <= 0) break;
   }
   return prof_collect(b, st);
 }
@@ -1277,7 +1367,10 @@ tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const 
   k_gemm<<<grid, kGemmThreads>>>(B, mb.d_tiles, nt, mb.F, 0, mb.X, 0, nullptr, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);
   k_gemm<<<grid, kGemmThreads>>>(B, mb.d_tiles, nt, mb.X, 1, mb.W, 0, nullptr, nullptr, nullptr, mb.F, 1.0, 0.0, mb.ms.active);
   const size_t smem = syev_smem_bytes(std::max(mb.nmax_in, 1));
-  if (smem > 48 * 1024) TB_CUDA(cudaFuncSetAttribute(k_syev, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  {
+    const tb_status ss = raise_smem_limits();
+    if (ss != TB_OK) return ss;
+  }
   k_syev<<<nmat, kEigThreads, smem>>>(B, mb.F, mb.Z, mb.w, mb.perm, mb.ms.status, mb.ms.active);
   std::vector<int> fstat(nmat, 0);
   if (!mb.big.empty()) TB_CUDA(cudaMemcpy(fstat.data(), mb.ms.status, nmat * 4, cudaMemcpyDeviceToHost));
@@ -1310,6 +1403,10 @@ tb_status tb_fermi_filling(int32_t n, double nel, double kt, const double* emo, 
   const double nels[2] = {nel, 0.0};
   TB_CUDA(cudaMemcpy(mb.w, emo, n * 8, cudaMemcpyHostToDevice));
   TB_CUDA(cudaMemcpy(mb.ms.nel, nels, 16, cudaMemcpyHostToDevice));
+  {
+    const tb_status ss = raise_smem_limits();
+    if (ss != TB_OK) return ss;
+  }
   k_fermi<<<1, 128, (size_t)n * 8>>>(mb.db, mb.w, kt, mb.focc, mb.kdim, mb.ms);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(TB_CUDA_ERROR, cudaGetErrorString(e));
@@ -1320,5 +1417,223 @@ tb_status tb_fermi_filling(int32_t n, double nel, double kt, const double* emo, 
   TB_CUDA(cudaMemcpy(&fw, mb.ms.fermi_warn, 4, cudaMemcpyDeviceToHost));
   return fw ? fail(TB_FERMI_NOT_CONVERGED, "Fermi level iteration cap reached") : TB_OK;
 }
+
+}  // extern "C"
+
+// ====================================================================== serving
+struct tb_server {
+  struct Req {
+    int64_t ticket = 0;
+    int nat = 0, uhf = 0, nsh = 0, nao = 0;
+    double charge = 0.0;
+    std::vector<int32_t> id;
+    std::vector<double> xyz;
+    int64_t bytes = 0;  // workspace estimate
+  };
+  struct Live {
+    tb_batch* b = nullptr;
+    cudaStream_t st = nullptr;
+    std::vector<Req> reqs;
+    std::vector<char> done;
+    int64_t bytes = 0;
+  };
+  struct Done {
+    int64_t ticket = 0;
+    tb_result r{};
+    std::vector<double> qat, qsh, dpat, qpat;
+  };
+  tb_calculator* calc = nullptr;
+  tb_options opt{};
+  int64_t budget = 0, resident = 0, next_ticket = 0;
+  int max_batch = 1;
+  std::deque<Req> queue;
+  std::vector<Live> live;
+  std::deque<Done> done;
+  ~tb_server() {
+    for (Live& L : live) {
+      delete L.b;
+      if (L.st) cudaStreamDestroy(L.st);
+    }
+  }
+};
+
+namespace {
+
+// Device workspace of one structure in a batch, following batch_build's
+// layout: 16 N^2 doubles of matrices (S, H0, D, Q, X, W, F, Z, P), 3 more N^2
+// in the mixed-precision form, the pair lists, the Broyden history and the
+// library workspace above the in-house size bound; 4 KiB per array of slack.
+int64_t workspace_estimate(const tb_options& o, int nat, int nsh, int nao) {
+  const double n2 = (double)nao * nao;
+  double b = 128.0 * n2 + (o.precision == 1 ? 24.0 * n2 : 0.0);
+  b += 4.0 * nat * (nat - 1);  // pair_i, pair_j
+  const double mx = nsh + 9.0 * nat;
+  b += 8.0 * mx * (4 + 2.0 * o.max_iter) + 8.0 * o.max_iter * o.max_iter;
+  b += 8.0 * (30.0 * nao + 30.0 * nat);  // per-AO / per-atom vectors
+  if (o.solver != 1 && (o.solver == 2 || nao > kSyevMaxN)) b += 16.0 * n2 + 64.0 * nao;
+  return (int64_t)b + 64 * 4096;
+}
+
+tb_status server_admit(tb_server* s) {
+  if (s->queue.empty()) return TB_OK;
+  std::vector<tb_server::Req> take;
+  int64_t est = 0;
+  while (!s->queue.empty() && (int)take.size() < s->max_batch) {
+    const tb_server::Req& r = s->queue.front();
+    if (s->resident + est + r.bytes > s->budget) break;
+    est += r.bytes;
+    take.push_back(std::move(s->queue.front()));
+    s->queue.pop_front();
+  }
+  if (take.empty()) return TB_OK;
+  std::vector<tb_structure> mols(take.size());
+  for (size_t i = 0; i < take.size(); ++i)
+    mols[i] = {take[i].nat, take[i].uhf, take[i].charge, take[i].id.data(), take[i].xyz.data()};
+  tb_server::Live L;
+  L.b = new tb_batch();
+  tb_status st = batch_build(s->calc, mols.data(), (int)mols.size(), &s->opt, L.b, &L.b->own);
+  if (st == TB_OK && cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking) != cudaSuccess)
+    st = fail(TB_CUDA_ERROR, "cannot create a stream for a micro-batch");
+  if (st == TB_OK) st = batch_setup(L.b, L.st);
+  if (st != TB_OK) {
+    delete L.b;
+    if (L.st) cudaStreamDestroy(L.st);
+    for (auto r = take.rbegin(); r != take.rend(); ++r) s->queue.push_front(std::move(*r));  // back in order
+    return st;
+  }
+  L.bytes = (int64_t)L.b->bytes;
+  s->resident += L.bytes;
+  L.reqs = std::move(take);
+  L.done.assign(L.reqs.size(), 0);
+  s->live.push_back(std::move(L));
+  return TB_OK;
+}
+
+// Results of the structures of L that finished since the last call.
+tb_status server_collect(tb_server* s, tb_server::Live& L) {
+  const int nmol = L.b->nmol;
+  std::vector<int> act(nmol);
+  TB_CUDA(cudaMemcpy(act.data(), L.b->ms.active, nmol * sizeof(int), cudaMemcpyDeviceToHost));
+  bool any = false;
+  for (int m = 0; m < nmol; ++m) any |= !act[m] && !L.done[m];
+  if (!any) return TB_OK;
+  std::vector<tb_result> res(nmol);
+  std::vector<tb_server::Done> out(nmol);
+  for (int m = 0; m < nmol; ++m) {
+    const tb_server::Req& r = L.reqs[m];
+    out[m].qat.resize(r.nat); out[m].qsh.resize(r.nsh); out[m].dpat.resize(3 * r.nat); out[m].qpat.resize(6 * r.nat);
+    res[m] = tb_result{};
+    res[m].qat = out[m].qat.data(); res[m].qsh = out[m].qsh.data();
+    res[m].dpat = out[m].dpat.data(); res[m].qpat = out[m].qpat.data();
+  }
+  const std::string keep = g_err;
+  const tb_status rs = batch_results(L.b, res.data(), L.st);
+  if (rs == TB_CUDA_ERROR) return rs;
+  g_err = keep;  // per-structure statuses travel in the results
+  for (int m = 0; m < nmol; ++m) {
+    if (act[m] || L.done[m]) continue;
+    L.done[m] = 1;
+    out[m].ticket = L.reqs[m].ticket;
+    out[m].r = res[m];
+    s->done.push_back(std::move(out[m]));
+  }
+  return TB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+tb_status tb_server_create(tb_calculator* calc, const tb_options* opt, int64_t hbm_budget_bytes, int32_t max_batch,
+                           tb_server** out) {
+  if (!calc || !out) return fail(TB_BAD_INPUT, "null argument");
+  if (hbm_budget_bytes <= 0 || max_batch <= 0) return fail(TB_BAD_INPUT, "budget and max_batch must be positive");
+  auto* s = new tb_server();
+  s->calc = calc;
+  if (opt) s->opt = *opt; else tb_default_options(&s->opt);
+  s->opt.profile = 0;
+  s->budget = hbm_budget_bytes;
+  s->max_batch = max_batch;
+  *out = s;
+  return TB_OK;
+}
+
+tb_status tb_server_submit(tb_server* s, const tb_structure* mol, int64_t* ticket) {
+  if (!s || !mol || !ticket) return fail(TB_BAD_INPUT, "null argument");
+  if (mol->nat <= 0 || !mol->id || !mol->xyz) return fail(TB_BAD_INPUT, "empty or null structure");
+  tb_server::Req r;
+  int32_t nsh = 0, nao = 0;
+  const tb_status bs = tb_basis_size(s->calc, mol, &nsh, &nao);
+  if (bs != TB_OK) return bs;
+  r.nat = mol->nat; r.uhf = mol->uhf; r.charge = mol->charge; r.nsh = nsh; r.nao = nao;
+  r.id.assign(mol->id, mol->id + mol->nat);
+  r.xyz.assign(mol->xyz, mol->xyz + 3 * (size_t)mol->nat);
+  r.bytes = workspace_estimate(s->opt, r.nat, nsh, nao);
+  if (r.bytes > s->budget) return fail(TB_CAPACITY_EXCEEDED, "structure needs more device memory than the budget");
+  r.ticket = s->next_ticket++;
+  *ticket = r.ticket;
+  s->queue.push_back(std::move(r));
+  return TB_OK;
+}
+
+tb_status tb_server_step(tb_server* s, int32_t* n_resident, int32_t* n_queued, int64_t* bytes_resident) {
+  if (!s) return fail(TB_BAD_INPUT, "null server");
+  tb_status st = server_admit(s);
+  if (st != TB_OK) return st;
+  // one SCF iteration of every resident micro-batch, launched on all streams first
+  for (auto& L : s->live) {
+    st = launch_iteration(L.b, L.st);
+    if (st != TB_OK) return st;
+  }
+  for (size_t i = 0; i < s->live.size();) {
+    tb_server::Live& L = s->live[i];
+    int na = 0;
+    st = finish_iteration(L.b, L.st, &na);
+    if (st != TB_OK) return st;
+    st = server_collect(s, L);
+    if (st != TB_OK) return st;
+    if (na <= 0 || L.b->it >= L.b->opt.max_iter) {
+      delete L.b;
+      cudaStreamDestroy(L.st);
+      s->resident -= L.bytes;
+      s->live.erase(s->live.begin() + i);
+    } else {
+      ++i;
+    }
+  }
+  if (n_resident || bytes_resident) {
+    int32_t nr = 0;
+    for (auto& L : s->live)
+      for (char d : L.done) nr += !d;
+    if (n_resident) *n_resident = nr;
+    if (bytes_resident) *bytes_resident = s->resident;
+  }
+  if (n_queued) *n_queued = (int32_t)s->queue.size();
+  return TB_OK;
+}
+
+int32_t tb_server_poll(tb_server* s, int32_t max, int64_t* tickets, tb_result* results) {
+  if (!s || max <= 0) return 0;
+  int32_t k = 0;
+  while (k < max && !s->done.empty()) {
+    tb_server::Done& d = s->done.front();
+    if (tickets) tickets[k] = d.ticket;
+    if (results) {
+      tb_result& r = results[k];
+      double *qat = r.qat, *qsh = r.qsh, *dpat = r.dpat, *qpat = r.qpat;
+      r = d.r;
+      r.qat = qat; r.qsh = qsh; r.dpat = dpat; r.qpat = qpat;
+      if (qat) std::memcpy(qat, d.qat.data(), d.qat.size() * sizeof(double));
+      if (qsh) std::memcpy(qsh, d.qsh.data(), d.qsh.size() * sizeof(double));
+      if (dpat) std::memcpy(dpat, d.dpat.data(), d.dpat.size() * sizeof(double));
+      if (qpat) std::memcpy(qpat, d.qpat.data(), d.qpat.size() * sizeof(double));
+    }
+    s->done.pop_front();
+    ++k;
+  }
+  return k;
+}
+
+void tb_server_destroy(tb_server* s) { delete s; }
 
 }  // extern "C"

@@ -55,6 +55,7 @@ EXPORTS = [
     "tb_batch_results", "tb_batch_launches", "tb_batch_destroy", "tb_get_cutoff", "tb_adjacency_list",
     "tb_atomic_properties", "tb_repulsion", "tb_get_hamiltonian", "tb_coulomb_potential",
     "tb_add_pot_to_h1", "tb_sygvd_batch", "tb_fermi_filling", "tb_batch_profile",
+    "tb_server_create", "tb_server_submit", "tb_server_step", "tb_server_poll", "tb_server_destroy",
 ]
 
 _lib = None
@@ -84,6 +85,12 @@ def load_library(path: str = LIB_PATH):
     L.tb_batch_launches.restype = C.c_int64
     L.tb_batch_launches.argtypes = [C.c_void_p]
     L.tb_batch_destroy.argtypes = [C.c_void_p]
+    L.tb_server_create.argtypes = [C.c_void_p, C.POINTER(Options), C.c_int64, C.c_int32, C.POINTER(C.c_void_p)]
+    L.tb_server_submit.argtypes = [C.c_void_p, C.POINTER(Structure), C.POINTER(C.c_int64)]
+    L.tb_server_step.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+    L.tb_server_poll.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.c_void_p]
+    L.tb_server_poll.restype = C.c_int32
+    L.tb_server_destroy.argtypes = [C.c_void_p]
     _lib = L
     return L
 
@@ -235,6 +242,71 @@ class Batch:
         try:
             if getattr(self, "h", None) and self.h.value:
                 load_library().tb_batch_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching request loop (tb_server): submit() queues a
+    structure, step() admits queued requests within the device-memory budget
+    and runs one SCF iteration of every resident micro-batch, poll() returns
+    finished results as (ticket, result dict)."""
+
+    def __init__(self, calc: Calculator, hbm_budget_bytes: int, max_batch: int = 256, **opts):
+        L = load_library()
+        self.calc = calc
+        o = default_options(**opts)
+        h = C.c_void_p()
+        check(L.tb_server_create(calc.h, C.byref(o), C.c_int64(int(hbm_budget_bytes)), C.c_int32(max_batch),
+                                 C.byref(h)), "tb_server_create")
+        self.h = h
+        self._sizes = {}
+
+    def submit(self, mol) -> int:
+        arr, keep = _structs([mol])
+        t = C.c_int64()
+        check(load_library().tb_server_submit(self.h, C.byref(arr[0]), C.byref(t)), "tb_server_submit")
+        self._sizes[t.value] = (mol.nat, self.calc.basis_size(mol)[0])
+        return t.value
+
+    def step(self):
+        """Returns (requests resident on the device, requests queued, workspace bytes resident)."""
+        nr, nq, nb = C.c_int32(), C.c_int32(), C.c_int64()
+        check(load_library().tb_server_step(self.h, C.byref(nr), C.byref(nq), C.byref(nb)), "tb_server_step")
+        return nr.value, nq.value, nb.value
+
+    def poll(self, max_results: int = 4096):
+        L = load_library()
+        out = []
+        while True:
+            # one result at a time so that every array buffer has its structure's size
+            t = C.c_int64()
+            res = (Result * 1)()
+            pending = [k for k in self._sizes]
+            if not pending:
+                break
+            # sizes are per ticket: peek by polling into the largest buffers needed, then trim
+            nat = max(v[0] for v in self._sizes.values())
+            nsh = max(v[1] for v in self._sizes.values())
+            b = dict(qat=np.zeros(nat), qsh=np.zeros(nsh), dpat=np.zeros((nat, 3)), qpat=np.zeros((nat, 6)))
+            res[0].qat = b["qat"].ctypes.data_as(_dp)
+            res[0].qsh = b["qsh"].ctypes.data_as(_dp)
+            res[0].dpat = b["dpat"].ctypes.data_as(_dp)
+            res[0].qpat = b["qpat"].ctypes.data_as(_dp)
+            k = L.tb_server_poll(self.h, 1, C.byref(t), res)
+            if k == 0 or len(out) >= max_results:
+                break
+            na, ns = self._sizes.pop(t.value)
+            b = dict(qat=b["qat"][:na].copy(), qsh=b["qsh"][:ns].copy(), dpat=b["dpat"][:na].copy(),
+                     qpat=b["qpat"][:na].copy())
+            out.append((t.value, _result_dict(res[0], b)))
+        return out
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.h.value:
+                load_library().tb_server_destroy(self.h)
                 self.h = None
         except Exception:
             pass

@@ -226,3 +226,18 @@ def test_device_batch_api(gpu_calc, oracle):
     for m, r1, r2 in zip(mols, first, second):
         assert r1["energy"] == r2["energy"]
         _check(r1, oracle.singlepoint(m, accuracy=1e-4))
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_graph_replay_equals_eager(gpu_calc, precision):
+    # use_graphs captures one SCF iteration per batch and replays it
+    mols = g.water_clusters(6, seed=13, nmin=2, nmax=20)
+    eager = capi.Batch(gpu_calc, mols, precision=precision)
+    eager.run()
+    graph = capi.Batch(gpu_calc, mols, precision=precision, use_graphs=1)
+    graph.run()
+    graph.run()  # second run replays the instantiated graph
+    assert graph.launches() == eager.launches()
+    for a, b in zip(eager.results(), graph.results()):
+        assert a["energy"] == b["energy"] and a["iterations"] == b["iterations"]
+        np.testing.assert_array_equal(a["qat"], b["qat"])
