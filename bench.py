@@ -1,14 +1,20 @@
 #!/usr/bin/env python3
-"""Benchmark: batched GFN2-shaped singlepoints/s on B200.
+"""Benchmark: batched GFN2-shaped singlepoints/s on B200, plain FP64 and mixed forms.
 
 Workload (default): 1024 water clusters of U{8..64} rigid waters (24-192 atoms,
 48-384 AOs), seeded synthetic inputs built by the cluster rules (no dataset).
 One step = the full singlepoint (setup + SCF to convergence) of the whole
-batch.  `value` times tb_batch_run with the geometry already resident on the
-device; `e2e` times the public tb_singlepoint_batch with host buffers (the
-upload of the inputs and the download of every result inside the timed
-region).  The working set (about 7 GB of matrices) is far larger than L2, so no
-flush is needed between steps.
+batch.  Both forms are timed (tb_options.precision 0 and 1) with the geometry
+already resident on the device and one captured SCF iteration replayed as a
+CUDA graph; `value` is the faster form whose energies agree with the FP64 form
+to 1e-6 Eh (config.form names it, `forms` lists both).  `e2e` times the public
+tb_singlepoint_batch of that form with host buffers (the upload of the inputs
+and the download of every result inside the timed region).  The working set
+(about 7 GB of matrices) is far larger than L2, so no flush is needed between
+steps.  `serving` is a bounded sample of the request stream (Poisson arrivals,
+log-uniform 10-600 atoms) through tb_server with p50/p99 latency;
+--workload serving runs the full stream report for both forms and
+--workload water_box_1000 the 6000-AO structure.
 
 Multi-GPU (torchrun): one replica per GPU, each rank its own seeded batch
 (weak scaling, no data-path collective); value = all structures / max time.
@@ -29,7 +35,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "tblite-cuda_b200"))
 
-METRIC = "GFN2 singlepoints/s at |dE|<=1e-6 Eh (plain FP64 batched form), 1 GPU"
+METRIC = "GFN2 singlepoints/s at |dE|<=1e-6 Eh, mixed vs FP64 on 1 GPU; p50/p99 ms"
 UNIT = "singlepoints/s"
 WORKLOAD = "water_clusters_1024"
 
@@ -42,8 +48,12 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--count", type=int, default=1024, help="structures per batch")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "water_box_1000"],
-                    help="water_box_1000: one 3000-atom / 6000-AO structure, time per SCF iteration")
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "water_box_1000", "serving"],
+                    help="water_box_1000: one 3000-atom / 6000-AO structure, time per SCF iteration; "
+                         "serving: the request stream through tb_server, both forms")
+    ap.add_argument("--serving-requests", type=int, default=300,
+                    help="requests of the bounded serving sample (0: skip)")
+    ap.add_argument("--serving-rate", type=float, default=30.0, help="Poisson arrival rate per second")
     return ap.parse_args()
 
 
@@ -153,6 +163,72 @@ def cpu_baseline(mols, nthreads, target_s=12.0):
             "sample": f"first {count} of the {len(mols)} water clusters, one structure per thread, {dt:.1f} s"}, res, count
 
 
+def time_form(capi, torch, calc, mols, args, stream, precision):
+    """Device-resident batch of one form: W warm-up runs, K timed runs (CUDA events)."""
+    sh = stream.cuda_stream
+    batch = capi.Batch(calc, mols, profile=1, precision=precision, use_graphs=0)
+    for _ in range(args.warmup):
+        batch.run(sh)
+    torch.cuda.synchronize()
+    res = batch.results(sh)
+    prof_tot, launches = {}, 0
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        t0.record(stream)
+        for _ in range(args.steps):
+            batch.run(sh)
+            launches += batch.launches()
+            for k, (la, ms, wk, un) in batch.profile().items():
+                p = prof_tot.setdefault(k, [0, 0.0, 0.0, un])
+                p[0] += la; p[1] += ms; p[2] += wk
+        t1.record(stream)
+    torch.cuda.synchronize()
+    # graph-replayed runs (what a user gets with use_graphs = 1), without per-kernel events
+    gb = capi.Batch(calc, mols, precision=precision, use_graphs=1)
+    for _ in range(args.warmup):
+        gb.run(sh)
+    torch.cuda.synchronize()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        g0.record(stream)
+        for _ in range(args.steps):
+            gb.run(sh)
+        g1.record(stream)
+    torch.cuda.synchronize()
+    return dict(res=res, prof=prof_tot, launches=launches, elapsed_events=t0.elapsed_time(t1) * 1e-3,
+                elapsed=g0.elapsed_time(g1) * 1e-3)
+
+
+def serving_run(capi, calc, count, rate, precision, budget):
+    """Poisson arrivals of log-uniform 10-600 atom water/alkane requests through tb_server."""
+    from tblite_b200 import geometry
+    reqs = geometry.request_stream(count=count, seed=1003, rate=rate)
+    srv = capi.Server(calc, budget, max_batch=512, precision=precision, use_graphs=1)
+    arrival, lat, i = {}, [], 0
+    t0 = time.perf_counter()
+    while len(lat) < count:
+        now = time.perf_counter() - t0
+        while i < count and reqs[i][0] <= now:
+            arrival[srv.submit(reqs[i][1])] = reqs[i][0]
+            i += 1
+        resident, queued, _ = srv.step()
+        now = time.perf_counter() - t0
+        for t, r in srv.poll():
+            lat.append(now - arrival[t])
+        if resident == 0 and queued == 0 and i < count:
+            time.sleep(max(0.0, min(0.002, reqs[i][0] - (time.perf_counter() - t0))))
+        else:
+            time.sleep(0.0002)  # the step polls; micro-batches run on their own streams
+    total = time.perf_counter() - t0
+    lat_ms = sorted(x * 1e3 for x in lat)
+    q = lambda f: lat_ms[min(len(lat_ms) - 1, int(f * len(lat_ms)))]
+    return {"requests": count, "arrival_rate_per_s": rate, "throughput": count / total, "unit": UNIT,
+            "p50_ms": q(0.50), "p99_ms": q(0.99), "wall_s": total,
+            "sizes": "log-uniform 10-600 atoms, 50/50 water clusters / alkanes, seed 1003"}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup(args)
@@ -164,10 +240,12 @@ def main():
     torch.cuda.set_device(local)
     if args.workload == "water_box_1000":
         return run_water_box(args, torch)
+    if args.workload == "serving":
+        return run_serving(args, torch)
     if ws > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+                               device_id=torch.device("cuda", local))
     from tblite_b200 import Calculator, capi, geometry
     calc = Calculator()
     mols = geometry.water_clusters(args.count, seed=1001 + rank)
@@ -176,51 +254,46 @@ def main():
     nat = sum(m.nat for m in mols)
     nao = sum(calc.basis_size(m)[1] for m in mols)
 
-    # ---------------- device-resident batch (value)
-    batch = capi.Batch(calc, mols, profile=1)
-    for _ in range(args.warmup):
-        batch.run(sh)
-    torch.cuda.synchronize()
-    res = batch.results(sh)
+    # ---------------- both forms, device-resident batches (value)
     sampler = ClockSampler(local)
     sampler.start()
     if ws > 1:
         dist.barrier()
-    torch.cuda.synchronize()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    prof_tot = {}
-    launches = 0
-    with torch.cuda.stream(stream):
-        t0.record(stream)
-        for _ in range(args.steps):
-            batch.run(sh)
-            launches += batch.launches()
-            for k, (la, ms, wk, un) in batch.profile().items():
-                p = prof_tot.setdefault(k, [0, 0.0, 0.0, un])
-                p[0] += la; p[1] += ms; p[2] += wk
-        t1.record(stream)
-    torch.cuda.synchronize()
+    forms = {}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        forms[name] = time_form(capi, torch, calc, mols, args, stream, prec)
     if ws > 1:
         dist.barrier()
     clocks = sampler.stop()
-    elapsed = t0.elapsed_time(t1) * 1e-3
-    if ws > 1:
-        tt = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed = float(tt.item())
-    value = ws * args.steps * len(mols) / elapsed
+    for name, f in forms.items():
+        el = f["elapsed"]
+        if ws > 1:
+            tt = torch.tensor([el], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            el = float(tt.item())
+        f["value"] = ws * args.steps * len(mols) / el
+        f["ms_per_step"] = el / args.steps * 1e3
+    e_fp = np.array([r["energy"] for r in forms["fp64"]["res"]])
+    e_mx = np.array([r["energy"] for r in forms["mixed"]["res"]])
+    forms["mixed"]["max_abs_dE_vs_fp64"] = float(np.max(np.abs(e_mx - e_fp)))
+    forms["fp64"]["max_abs_dE_vs_fp64"] = 0.0
+    ok = {k: f for k, f in forms.items() if f["max_abs_dE_vs_fp64"] <= 1e-6 and
+          all(r["status"] == 0 for r in f["res"])}
+    head_name = max(ok, key=lambda k: ok[k]["value"]) if ok else "fp64"
+    head = forms[head_name]
+    head_prec = 0 if head_name == "fp64" else 1
+    value = head["value"]
 
-    # ---------------- end to end through the public API (host buffers)
+    # ---------------- end to end through the public API (host buffers), headline form
     ids_bytes = sum(m.nat * (3 * 8 + 4) + 12 for m in mols)
     out_bytes = sum(8 * (13 + m.nat * 10) + 8 * calc.basis_size(m)[0] for m in mols)
-    calc.singlepoint_batch(mols)  # warm the workspace
+    calc.singlepoint_batch(mols, precision=head_prec, use_graphs=1)  # warm the workspace
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()
     te = time.perf_counter()
     for _ in range(args.steps):
-        e2e_res = calc.singlepoint_batch(mols, stream=sh)
+        calc.singlepoint_batch(mols, stream=sh, precision=head_prec, use_graphs=1)
     torch.cuda.synchronize()
     e2e_t = time.perf_counter() - te
     if ws > 1:
@@ -230,16 +303,17 @@ def main():
     e2e = {"value": ws * args.steps * len(mols) / e2e_t, "unit": UNIT, "h2d_bytes_per_step": ids_bytes,
            "d2h_bytes_per_step": out_bytes}
 
-    # ---------------- roofline of the dominant kernel class (live CUDA-event times)
-    dom = max(prof_tot.items(), key=lambda kv: kv[1][1])
-    name, (la, ms, wk, un) = dom
+    # ---------------- roofline of the dominant kernel class (live CUDA-event times, headline form)
+    prof_tot = head["prof"]
+    name, (la, ms, wk, un) = max(prof_tot.items(), key=lambda kv: kv[1][1])
     peaks, src = measured_peaks()
     if un == "flop":
         peak = fp64_peak_tflops(torch)
         achieved = wk / (ms * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "pipe": "fp64",
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)"}
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
+                "work": "canonical 4 N^3 flops per eigensolve"}
     elif un == "byte":
         peak = peaks["hbm_gbs"]
         achieved = wk / (ms * 1e-3) / 1e9
@@ -258,13 +332,31 @@ def main():
     kernels = {k: {"launches": v[0], "ms": round(v[1], 3), "share": round(v[1] / total_ms, 4)}
                for k, v in sorted(prof_tot.items(), key=lambda kv: -kv[1][1])}
 
+    # ---------------- serving latency (bounded sample of the request stream), headline form
+    serving = None
+    if rank == 0 and args.serving_requests > 0:
+        free, _ = torch.cuda.mem_get_info()
+        serving = serving_run(capi, calc, args.serving_requests, args.serving_rate, head_prec, int(0.5 * free))
+
+    res = head["res"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "structures_per_gpu": len(mols), "waters": "U{8..64}",
-                       "atoms": nat, "aos": nao, "seed": 1001, "parallelism": f"replicas x{ws}",
-                       "l2": "inputs larger than L2 (no flush needed)", "accuracy": 1.0},
-            "e2e": e2e, "gpu_launches": launches, "roofline": roof, "kernels": kernels, "clocks": clocks}
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if head_prec == 0 else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "form": head_name, "structures_per_gpu": len(mols),
+                       "waters": "U{8..64}", "atoms": nat, "aos": nao, "seed": 1001,
+                       "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (no flush needed)",
+                       "accuracy": 1.0, "graphs": "one captured SCF iteration replayed"},
+            "e2e": e2e, "gpu_launches": launches_of(forms, head_name), "roofline": roof, "kernels": kernels,
+            "clocks": clocks,
+            "forms": {k: {"value": f["value"], "ms_per_step": f["ms_per_step"],
+                          "ms_per_step_with_kernel_events": f["elapsed_events"] / args.steps * 1e3,
+                          "max_abs_dE_vs_fp64": f["max_abs_dE_vs_fp64"],
+                          "scf_iterations_mean": float(np.mean([r["iterations"] for r in f["res"]])),
+                          "status_ok": int(sum(r["status"] == 0 for r in f["res"]))} for k, f in forms.items()},
+            "mixed_vs_fp64": forms["mixed"]["value"] / forms["fp64"]["value"]}
+    if serving is not None:
+        line["serving"] = serving
     iters = [r["iterations"] for r in res]
     line["scf_iterations"] = {"mean": float(np.mean(iters)), "max": int(max(iters))}
     line["status_ok"] = int(sum(r["status"] == 0 for r in res))
@@ -281,6 +373,27 @@ def main():
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+def launches_of(forms, name):
+    return int(forms[name]["launches"])
+
+
+def run_serving(args, torch):
+    """The request-stream workload: throughput and p50/p99 latency of both forms."""
+    from tblite_b200 import Calculator, capi
+    calc = Calculator()
+    free, _ = torch.cuda.mem_get_info()
+    out = {}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        serving_run(capi, calc, min(64, args.serving_requests), args.serving_rate, prec, int(0.5 * free))  # warm-up
+        out[name] = serving_run(capi, calc, args.serving_requests, args.serving_rate, prec, int(0.5 * free))
+    line = {"metric": "GFN2 singlepoints/s and p50/p99 latency, request stream, 1 GPU",
+            "value": out["fp64"]["throughput"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "data": "synthetic", "config": {"workload": "request_stream", "requests": args.serving_requests,
+                                            "rate_per_s": args.serving_rate},
+            "forms": out}
+    print(json.dumps(line))
 
 
 def run_water_box(args, torch):

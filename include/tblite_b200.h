@@ -140,10 +140,11 @@ void tb_batch_destroy(tb_batch* batch);
  * tb_server_step admits queued requests (first in, first out) as one new
  * resident micro-batch while the device workspace of all resident
  * micro-batches stays within hbm_budget_bytes (at most max_batch per
- * micro-batch), runs ONE SCF iteration of every resident micro-batch, each on
- * its own stream so that their work overlaps on the device, and retires the
- * structures that finished; a micro-batch's workspace is freed when its last
- * structure finishes.  tb_server_poll hands out finished results in completion
+ * micro-batch) and advances every resident micro-batch without waiting for
+ * any: each runs its SCF iterations on its own stream, so their work overlaps
+ * on the device; one whose iteration has finished is collected (structures
+ * that converged are retired) and given its next iteration.  A micro-batch's
+ * workspace is freed when its last structure finishes.  Call it in a loop.  tb_server_poll hands out finished results in completion
  * order.  Each result equals the one tb_singlepoint_batch gives for the same
  * structure alone (the kernels treat every structure independently).
  * Calls on one server must come from one host thread at a time. */

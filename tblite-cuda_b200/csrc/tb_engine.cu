@@ -7,12 +7,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <deque>
 #include <fstream>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <sstream>
 #include <string>
@@ -207,6 +209,13 @@ struct tb_calculator {
   int lmask = 0;  // bit l set when shells of angular momentum l exist
   std::mutex mu;
   Arena arena;
+  // eigensolver cost models for the automatic per-size choice (see choose_lib_above)
+  struct EigModel {
+    bool ready = false;
+    double a = 0, b = 0;  // in-house latency of one structure: a N^2 + b N^3 seconds
+    double c = 0, d = 0;  // one cuSOLVER call: c + d N^3 seconds
+  } eig;
+  std::mutex tune_mu;
   ~tb_calculator() {
     if (d_sp) cudaFree(d_sp);
     if (d_sh) cudaFree(d_sh);
@@ -288,6 +297,44 @@ namespace {
 template <typename T>
 T* at(char* base, size_t off) { return reinterpret_cast<T*>(base + off); }
 
+tb_status calibrate_eigensolvers(tb_calculator* c);
+
+// Automatic eigensolver choice for a batch (tb_options.solver = 0): the k
+// largest structures go to cuSOLVER, the rest to the batched in-house solver,
+// with k minimising the modelled time of one SCF iteration's eigensolve:
+//   sum_{i<k} t_lib(N_i) + max(t_in(N_k), sum_{i>=k} t_in(N_i) / slots)
+// (library calls run one after another; in-house structures run concurrently,
+// one CTA each, up to `slots` at a time; t_in and t_lib are measured once per
+// calculator).  Returns lib_above: structures with more AOs go to the library.
+int choose_lib_above(tb_calculator* c, std::vector<int> sizes) {
+  std::sort(sizes.begin(), sizes.end(), std::greater<int>());
+  const int nmol = (int)sizes.size();
+  int k0 = 0;
+  while (k0 < nmol && sizes[k0] > kSyevMaxN) ++k0;
+  if (k0 == nmol) return -1;
+  if (sizes[k0] < 384) return kSyevMaxN;  // small structures: the batched solver always wins
+  if (calibrate_eigensolvers(c) != TB_OK) return kSyevMaxN;
+  const auto& M = c->eig;
+  auto t_in = [&](double n) { return M.a * n * n + M.b * n * n * n; };
+  auto t_lib = [&](double n) { return M.c + M.d * n * n * n; };
+  auto slots = [&](int n) {
+    const int per = (int)std::min<size_t>(3, (227 * 1024) / std::max<size_t>(syev_smem_bytes(n), 1));
+    return 148.0 * std::max(per, 1);
+  };
+  std::vector<double> tail(nmol + 1, 0.0);
+  for (int i = nmol - 1; i >= 0; --i) tail[i] = tail[i + 1] + t_in(sizes[i]);
+  double lib_sum = 0.0, best = 1e300;
+  int best_k = k0;
+  for (int i = 0; i < k0; ++i) lib_sum += t_lib(sizes[i]);
+  for (int k = k0; k <= nmol; ++k) {
+    const double in_t = k == nmol ? 0.0 : std::max(t_in(sizes[k]), tail[k] / slots(sizes[k]));
+    if (lib_sum + in_t < best) { best = lib_sum + in_t; best_k = k; }
+    if (k < nmol) lib_sum += t_lib(sizes[k]);
+  }
+  if (best_k == nmol) return -1;
+  return best_k == 0 ? kSyevMaxN : sizes[best_k];
+}
+
 // Build index maps, lay out the workspace, allocate, upload.
 tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, const tb_options* opt,
                       tb_batch* b, Arena* arena) {
@@ -356,8 +403,13 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   }
   // solver choice: 0 auto (in-house up to kSyevMaxN AOs, library above), 1 in-house only, 2 library only
   int lib_above = 0;
-  if (opt->solver == 0) lib_above = kSyevMaxN;
-  else if (opt->solver == 2) lib_above = -1;
+  if (opt->solver == 0) {
+    std::vector<int> sizes(nmol);
+    for (int m = 0; m < nmol; ++m) sizes[m] = b->h_ooff[m + 1] - b->h_ooff[m];
+    lib_above = choose_lib_above(calc, sizes);
+  } else if (opt->solver == 2) {
+    lib_above = -1;
+  }
   else if (opt->solver != 1) return fail(TB_BAD_INPUT, "solver must be 0, 1 or 2");
   if (opt->solver == 1 && b->nmax > kSyevMaxN)
     return fail(TB_CAPACITY_EXCEEDED, "structure with " + std::to_string(b->nmax) +
@@ -676,6 +728,104 @@ tb_status raise_smem_limits() {
     TB_CUDA(cudaFuncGetAttributes(&a, k));
     TB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes));
   }
+  return TB_OK;
+}
+
+// Measures the two eigensolvers once per calculator: the in-house k_syev on
+// one structure (latency, at 256 and 512 AOs, fitted by a N^2 + b N^3) and one
+// cuSOLVER syevd call (at 256 and 1024 AOs, fitted by c + d N^3), on
+// deterministic random symmetric matrices.
+tb_status calibrate_eigensolvers(tb_calculator* c) {
+  std::lock_guard<std::mutex> lk(c->tune_mu);
+  if (c->eig.ready) return TB_OK;
+  {
+    const tb_status ss = raise_smem_limits();
+    if (ss != TB_OK) return ss;
+  }
+  const int NL = 1024;
+  Arena ar;
+  const size_t nn = (size_t)NL * NL;
+  LargeSolver ls;
+  size_t wbytes = 0;
+  const std::string we = ls.workspace(NL, &wbytes);
+  if (!we.empty()) return fail(TB_CUDA_ERROR, "eigensolver calibration: " + we);
+  Layout L;
+  const size_t oA = L.add(nn * 8), oZ = L.add(nn * 8), ow = L.add(NL * 8), op = L.add(NL * 4), os = L.add(16),
+               oo = L.add(16), om = L.add(16), owk = L.add(std::max<size_t>(wbytes, 16)), oi = L.add(16);
+  TB_CUDA(ar.reserve(L.total));
+  char* base = ar.base;
+  std::vector<double> h(nn);
+  uint64_t x = 0x9e3779b97f4a7c15ull;
+  auto rnd = [&]() {  // xorshift64*, uniform in (-1, 1)
+    x ^= x >> 12; x ^= x << 25; x ^= x >> 27;
+    return (double)((x * 0x2545f4914f6cdd1dull) >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+  };
+  cudaEvent_t e0, e1;
+  TB_CUDA(cudaEventCreate(&e0));
+  TB_CUDA(cudaEventCreate(&e1));
+  auto upload = [&](int n) -> tb_status {
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j <= i; ++j) h[(size_t)i * n + j] = h[(size_t)j * n + i] = rnd() / std::sqrt((double)n);
+    TB_CUDA(cudaMemcpy(base + oA, h.data(), (size_t)n * n * 8, cudaMemcpyHostToDevice));
+    const int oo_h[2] = {0, n};
+    const long long om_h[2] = {0, (long long)n * n};
+    TB_CUDA(cudaMemcpy(base + oo, oo_h, 8, cudaMemcpyHostToDevice));
+    TB_CUDA(cudaMemcpy(base + om, om_h, 16, cudaMemcpyHostToDevice));
+    TB_CUDA(cudaMemset(base + os, 0, 16));
+    return TB_OK;
+  };
+  auto inhouse = [&](int n, double* sec) -> tb_status {
+    DevBatch B{};
+    B.nmol = 1;
+    B.ooff = at<int>(base, oo);
+    B.moff = at<long long>(base, om);
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
+      const tb_status us = upload(n);
+      if (us != TB_OK) return us;
+      TB_CUDA(cudaEventRecord(e0));
+      k_syev<<<1, kEigThreads, syev_smem_bytes(n)>>>(B, at<double>(base, oA), at<double>(base, oZ),
+                                                     at<double>(base, ow), at<int>(base, op), at<int>(base, os),
+                                                     nullptr);
+      TB_CUDA(cudaEventRecord(e1));
+      TB_CUDA(cudaEventSynchronize(e1));
+      TB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    }
+    *sec = ms * 1e-3;
+    return TB_OK;
+  };
+  auto library = [&](int n, double* sec) -> tb_status {
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
+      const tb_status us = upload(n);
+      if (us != TB_OK) return us;
+      TB_CUDA(cudaEventRecord(e0));
+      const std::string e = ls.syev(0, at<double>(base, oA), at<double>(base, oZ), at<double>(base, ow),
+                                    at<int>(base, op), n, base + owk, wbytes, at<int>(base, oi), at<int>(base, os));
+      if (!e.empty()) return fail(TB_CUDA_ERROR, "eigensolver calibration: " + e);
+      TB_CUDA(cudaEventRecord(e1));
+      TB_CUDA(cudaEventSynchronize(e1));
+      TB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    }
+    *sec = ms * 1e-3;
+    return TB_OK;
+  };
+  double t1 = 0, t2 = 0, l1 = 0, l2 = 0;
+  tb_status st = inhouse(256, &t1);
+  if (st == TB_OK) st = inhouse(512, &t2);
+  if (st == TB_OK) st = library(256, &l1);
+  if (st == TB_OK) st = library(NL, &l2);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != TB_OK) return st;
+  // t = a n^2 + b n^3 through (256, t1), (512, t2); t = c + d n^3 through (256, l1), (1024, l2)
+  const double n1 = 256, n2 = 512, m1 = 256, m2 = NL;
+  const double det = n1 * n1 * n2 * n2 * n2 - n2 * n2 * n1 * n1 * n1;
+  c->eig.a = std::max(0.0, (t1 * n2 * n2 * n2 - t2 * n1 * n1 * n1) / det);
+  c->eig.b = std::max(0.0, (n1 * n1 * t2 - n2 * n2 * t1) / det);
+  c->eig.d = std::max(0.0, (l2 - l1) / (m2 * m2 * m2 - m1 * m1 * m1));
+  c->eig.c = std::max(0.0, l1 - c->eig.d * m1 * m1 * m1);
+  c->eig.ready = true;
   return TB_OK;
 }
 
@@ -1429,6 +1579,7 @@ struct tb_server {
     std::vector<int32_t> id;
     std::vector<double> xyz;
     int64_t bytes = 0;  // workspace estimate
+    std::chrono::steady_clock::time_point t_submit;
   };
   struct Live {
     tb_batch* b = nullptr;
@@ -1436,6 +1587,8 @@ struct tb_server {
     std::vector<Req> reqs;
     std::vector<char> done;
     int64_t bytes = 0;
+    bool inflight = false;  // an SCF iteration of this micro-batch is queued on st
+    std::unique_ptr<Arena> ar;  // its workspace (from the pool)
   };
   struct Done {
     int64_t ticket = 0;
@@ -1449,11 +1602,20 @@ struct tb_server {
   std::deque<Req> queue;
   std::vector<Live> live;
   std::deque<Done> done;
+  // Workspaces and streams of retired micro-batches are kept for reuse:
+  // cudaFree would synchronise the whole device and stall the other streams.
+  std::vector<std::unique_ptr<Arena>> pool;
+  int64_t pooled = 0;
+  std::vector<cudaStream_t> streams;
+  // arrivals are collected this long (or until max_batch are queued, or while
+  // nothing is resident) so that micro-batches hold more than one request
+  double window_s = 0.002;
   ~tb_server() {
     for (Live& L : live) {
       delete L.b;
       if (L.st) cudaStreamDestroy(L.st);
     }
+    for (cudaStream_t st : streams) cudaStreamDestroy(st);
   }
 };
 
@@ -1476,6 +1638,9 @@ int64_t workspace_estimate(const tb_options& o, int nat, int nsh, int nao) {
 
 tb_status server_admit(tb_server* s) {
   if (s->queue.empty()) return TB_OK;
+  const double waited =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - s->queue.front().t_submit).count();
+  if ((int)s->queue.size() < s->max_batch && waited < s->window_s && !s->live.empty()) return TB_OK;
   std::vector<tb_server::Req> take;
   int64_t est = 0;
   while (!s->queue.empty() && (int)take.size() < s->max_batch) {
@@ -1486,14 +1651,40 @@ tb_status server_admit(tb_server* s) {
     s->queue.pop_front();
   }
   if (take.empty()) return TB_OK;
+  // release pooled workspaces that would push the total held past the budget
+  while (!s->pool.empty() && s->resident + s->pooled + est > s->budget) {
+    s->pooled -= (int64_t)s->pool.back()->cap;
+    s->pool.pop_back();  // Arena frees its buffer
+  }
+  // smallest pooled workspace that fits, else a new one
+  std::unique_ptr<Arena> ar;
+  {
+    int best = -1;
+    for (int i = 0; i < (int)s->pool.size(); ++i)
+      if ((int64_t)s->pool[i]->cap >= est && (best < 0 || s->pool[i]->cap < s->pool[best]->cap)) best = i;
+    if (best >= 0) {
+      ar = std::move(s->pool[best]);
+      s->pool.erase(s->pool.begin() + best);
+      s->pooled -= (int64_t)ar->cap;
+    } else {
+      ar.reset(new Arena());
+    }
+  }
   std::vector<tb_structure> mols(take.size());
   for (size_t i = 0; i < take.size(); ++i)
     mols[i] = {take[i].nat, take[i].uhf, take[i].charge, take[i].id.data(), take[i].xyz.data()};
   tb_server::Live L;
   L.b = new tb_batch();
-  tb_status st = batch_build(s->calc, mols.data(), (int)mols.size(), &s->opt, L.b, &L.b->own);
-  if (st == TB_OK && cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking) != cudaSuccess)
-    st = fail(TB_CUDA_ERROR, "cannot create a stream for a micro-batch");
+  L.ar = std::move(ar);
+  tb_status st = batch_build(s->calc, mols.data(), (int)mols.size(), &s->opt, L.b, L.ar.get());
+  if (st == TB_OK) {
+    if (!s->streams.empty()) {
+      L.st = s->streams.back();
+      s->streams.pop_back();
+    } else if (cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking) != cudaSuccess) {
+      st = fail(TB_CUDA_ERROR, "cannot create a stream for a micro-batch");
+    }
+  }
   if (st == TB_OK) st = batch_setup(L.b, L.st);
   if (st != TB_OK) {
     delete L.b;
@@ -1501,7 +1692,7 @@ tb_status server_admit(tb_server* s) {
     for (auto r = take.rbegin(); r != take.rend(); ++r) s->queue.push_front(std::move(*r));  // back in order
     return st;
   }
-  L.bytes = (int64_t)L.b->bytes;
+  L.bytes = (int64_t)L.ar->cap;
   s->resident += L.bytes;
   L.reqs = std::move(take);
   L.done.assign(L.reqs.size(), 0);
@@ -1571,6 +1762,7 @@ tb_status tb_server_submit(tb_server* s, const tb_structure* mol, int64_t* ticke
   r.bytes = workspace_estimate(s->opt, r.nat, nsh, nao);
   if (r.bytes > s->budget) return fail(TB_CAPACITY_EXCEEDED, "structure needs more device memory than the budget");
   r.ticket = s->next_ticket++;
+  r.t_submit = std::chrono::steady_clock::now();
   *ticket = r.ticket;
   s->queue.push_back(std::move(r));
   return TB_OK;
@@ -1580,33 +1772,42 @@ tb_status tb_server_step(tb_server* s, int32_t* n_resident, int32_t* n_queued, i
   if (!s) return fail(TB_BAD_INPUT, "null server");
   tb_status st = server_admit(s);
   if (st != TB_OK) return st;
-  // one SCF iteration of every resident micro-batch, launched on all streams first
-  for (auto& L : s->live) {
-    st = launch_iteration(L.b, L.st);
-    if (st != TB_OK) return st;
-  }
+  // Micro-batches progress independently: a micro-batch whose iteration has
+  // finished on its stream is collected and given its next iteration at once;
+  // one still running is left alone (the step does not wait for it).
   for (size_t i = 0; i < s->live.size();) {
     tb_server::Live& L = s->live[i];
-    int na = 0;
-    st = finish_iteration(L.b, L.st, &na);
-    if (st != TB_OK) return st;
-    st = server_collect(s, L);
-    if (st != TB_OK) return st;
-    if (na <= 0 || L.b->it >= L.b->opt.max_iter) {
-      delete L.b;
-      cudaStreamDestroy(L.st);
-      s->resident -= L.bytes;
-      s->live.erase(s->live.begin() + i);
-    } else {
-      ++i;
+    if (L.inflight) {
+      const cudaError_t q = cudaStreamQuery(L.st);
+      if (q == cudaErrorNotReady) { ++i; continue; }
+      if (q != cudaSuccess) return fail(TB_CUDA_ERROR, std::string("micro-batch: ") + cudaGetErrorString(q));
+      int na = 0;
+      st = finish_iteration(L.b, L.st, &na);
+      if (st != TB_OK) return st;
+      st = server_collect(s, L);
+      if (st != TB_OK) return st;
+      L.inflight = false;
+      if (na <= 0 || L.b->it >= L.b->opt.max_iter) {
+        delete L.b;
+        s->streams.push_back(L.st);
+        s->resident -= L.bytes;
+        s->pooled += (int64_t)L.ar->cap;
+        s->pool.push_back(std::move(L.ar));
+        s->live.erase(s->live.begin() + i);
+        continue;
+      }
     }
+    st = launch_iteration(L.b, L.st);
+    if (st != TB_OK) return st;
+    L.inflight = true;
+    ++i;
   }
   if (n_resident || bytes_resident) {
     int32_t nr = 0;
     for (auto& L : s->live)
       for (char d : L.done) nr += !d;
     if (n_resident) *n_resident = nr;
-    if (bytes_resident) *bytes_resident = s->resident;
+    if (bytes_resident) *bytes_resident = s->resident + s->pooled;
   }
   if (n_queued) *n_queued = (int32_t)s->queue.size();
   return TB_OK;

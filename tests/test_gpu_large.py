@@ -89,3 +89,16 @@ def test_water_box_6000_aos(gpu_calc):
     # rigid, nearly neutral waters: each molecule's net charge stays small
     qmol = r["qat"].reshape(-1, 3).sum(axis=1)
     assert np.max(np.abs(qmol)) < 0.2
+
+
+def test_automatic_solver_choice_matches_inhouse(gpu_calc):
+    # a few large alkanes among small structures: the automatic choice (timed
+    # cost models) may send the large ones to cuSOLVER; results must agree
+    rng = np.random.default_rng(9)
+    mols = [g.alkane(n, rng) for n in (140, 160)] + g.water_clusters(4, seed=31, nmin=4, nmax=12)
+    auto = gpu_calc.singlepoint_batch(mols, solver=0)
+    inhouse = gpu_calc.singlepoint_batch(mols, solver=1)
+    for a, b in zip(auto, inhouse):
+        assert a["status"] == b["status"] == 0
+        assert abs(a["energy"] - b["energy"]) < E_TOL
+        np.testing.assert_allclose(a["qat"], b["qat"], atol=Q_TOL)

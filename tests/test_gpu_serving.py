@@ -3,6 +3,8 @@ sizes arrive while others are on the device; every result must equal the
 singlepoint of the same structure alone (bit for bit: each kernel treats a
 structure independently of its batch), and the resident workspace must stay
 within the budget."""
+import time
+
 import numpy as np
 import pytest
 
@@ -33,8 +35,9 @@ def _serve(calc, mols, budget, max_batch, per_step=2, **opts):
         peak = max(peak, nbytes)
         for t, r in srv.poll():
             got[t] = r
+        time.sleep(0.0005)  # step() only polls the micro-batches' streams
         steps += 1
-        assert steps < 500
+        assert steps < 200000
     return tickets, got, peak
 
 
