@@ -233,7 +233,7 @@ struct tb_batch {
   Arena* arena = nullptr;
   std::vector<int> h_aoff, h_soff, h_ooff, h_mixoff;
   std::vector<long long> h_moff, h_poff;
-  std::vector<int4> tiles64, tiles32;
+  std::vector<int4> tiles64, tiles32, tiles128;
   std::vector<int2> chunks32;
   std::vector<double> h_xyz;
   // device views
@@ -248,7 +248,7 @@ struct tb_batch {
   double *q_in, *dq, *dqlast, *qlast, *df, *u, *amat, *omega;
   double* charge;
   int* uhf;
-  int4 *d_tiles64, *d_tiles32;
+  int4 *d_tiles64, *d_tiles32, *d_tiles128;
   int2* d_chunks32;
   int* h_nactive = nullptr;  // pinned
   // structures above the in-house size bound: cuSOLVER path (tb_large.cu)
@@ -396,6 +396,8 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
     b->nshmax = std::max(b->nshmax, nsh);
     for (int t = 0; t < (nao + 63) / 64; ++t)
       for (int u = 0; u < (nao + 63) / 64; ++u) b->tiles64.push_back(make_int4(m, t, u, 0));
+    for (int t = 0; t < (nao + kTcTile - 1) / kTcTile; ++t)
+      for (int u = 0; u < (nao + kTcTile - 1) / kTcTile; ++u) b->tiles128.push_back(make_int4(m, t, u, 0));
     for (int t = 0; t < (nao + 31) / 32; ++t) {
       b->chunks32.push_back(make_int2(m, t));
       for (int u = 0; u < (nao + 31) / 32; ++u) b->tiles32.push_back(make_int4(m, t, u, 0));
@@ -448,6 +450,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
          o_xyz = L.add(3 * NA * D8), o_id = L.add(NA * I4), o_atmol = L.add(NA * I4), o_shtype = L.add(NS * I4),
          o_shat = L.add(NS * I4), o_shiao = L.add(NS * I4), o_atish = L.add(NA * I4), o_aoat = L.add(NO * I4),
          o_aosh = L.add(NO * I4), o_t64 = L.add(b->tiles64.size() * sizeof(int4)),
+         o_t128 = L.add(b->tiles128.size() * sizeof(int4)),
          o_t32 = L.add(b->tiles32.size() * sizeof(int4)), o_c32 = L.add(b->chunks32.size() * sizeof(int2)),
          o_charge = L.add(NM * D8), o_uhf = L.add(NM * I4), o_order = L.add(NM * I4);
   const size_t meta_end = L.total;
@@ -503,6 +506,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   put(o_aoat, ao_at.data(), NO * I4);
   put(o_aosh, ao_sh.data(), NO * I4);
   put(o_t64, b->tiles64.data(), b->tiles64.size() * sizeof(int4));
+  put(o_t128, b->tiles128.data(), b->tiles128.size() * sizeof(int4));
   put(o_t32, b->tiles32.data(), b->tiles32.size() * sizeof(int4));
   put(o_c32, b->chunks32.data(), b->chunks32.size() * sizeof(int2));
   std::vector<double> ch(nmol);
@@ -536,7 +540,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
     b->Vn = at<double>(base, o_Vn); b->G = at<double>(base, o_G);
     b->act_lo = at<int>(base, o_lo); b->act_hi = at<int>(base, o_hi);
   }
-  b->d_tiles64 = at<int4>(base, o_t64); b->d_tiles32 = at<int4>(base, o_t32); b->d_chunks32 = at<int2>(base, o_c32);
+  b->d_tiles64 = at<int4>(base, o_t64); b->d_tiles128 = at<int4>(base, o_t128); b->d_tiles32 = at<int4>(base, o_t32); b->d_chunks32 = at<int2>(base, o_c32);
   b->charge = at<double>(base, o_charge); b->uhf = at<int>(base, o_uhf);
   b->cn = at<double>(base, o_cn); b->mrad = at<double>(base, o_mrad); b->erep = at<double>(base, o_erep);
   b->se = at<double>(base, o_se); b->n0sh = at<double>(base, o_n0sh); b->cnt = at<int>(base, o_cnt);
@@ -636,8 +640,8 @@ constexpr double kMixedSwitchScale = 10.0, kMixedSwitchFloorE = 1e-5, kMixedSwit
 
 // Eigen-decomposition and density of one SCF iteration in the mixed-precision
 // form (tb_mixed.cu).  Every matrix is stored in FP64.  F', C and P are
-// FP32-product GEMMs (k_gemm_mx) for structures in the mixed phase and FP64
-// GEMMs in the FP64 phase; the eigenpairs come from the FP32 eigensolver and
+// TF32x3 tensor-core GEMMs (k_gemm_tc, tcgen05) for structures in the mixed
+// phase and FP64 GEMMs in the FP64 phase; the eigenpairs come from the FP32 eigensolver and
 // FP64 refinement (one step in the mixed phase, two in the FP64 phase).
 // Leaves w, focc, kdim and P as the plain form does.
 tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, double n2occ_lo, double n2occ_hi,
@@ -648,16 +652,17 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
   const int4* T = b->d_tiles64;
   const size_t smem32 = syev_smem_bytes(std::max(b->nmax_in, 1), sizeof(float));
   int *lo = b->act_lo, *hi = b->act_hi;
+  const int nt128 = (int)b->tiles128.size(), tc_grid = std::min(nt128, 148);
+  const int4* T128 = b->d_tiles128;
+  const size_t tc_smem = gemm_tc_smem_bytes();
   TB_K("masks", 0, 0, k_phase_masks<<<nblk(nmol, 256), 256, 0, st>>>(nmol, S.active, S.phase, lo, hi));
   // F' = X^T F X into F (T = F X in W), each phase in its precision
-  TB_K("gemm_mx", 2.0 * n3_lo, 1,
-       k_gemm_mx<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.f, 0.f,
-                                            lo));
+  TB_K("gemm_tc", 2.0 * n3_lo, 1,
+       k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, lo, S.status));
   TB_K("gemm", 2.0 * n3_hi, 1,
        k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi));
-  TB_K("gemm_mx", 2.0 * n3_lo, 1,
-       k_gemm_mx<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.f, 0.f,
-                                            lo));
+  TB_K("gemm_tc", 2.0 * n3_lo, 1,
+       k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, lo, S.status));
   TB_K("gemm", 2.0 * n3_hi, 1,
        k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, hi));
   // FP32 eigensolve of every active structure
@@ -700,15 +705,13 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
   }
   TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
   // C = X V into W (mixed phase: V after one step, in Vn; FP64 phase: after two, in Z)
-  TB_K("gemm_mx", 2.0 * n3_lo, 1,
-       k_gemm_mx<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->X, 0, b->Vn, 0, nullptr, nullptr, nullptr, b->W, 1.f, 0.f,
-                                            lo));
+  TB_K("gemm_tc", 2.0 * n3_lo, 1,
+       k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->X, 0, b->Vn, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, lo, S.status));
   TB_K("gemm", 2.0 * n3_hi, 1,
        k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 0, b->Z, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi));
   // P = C diag(f) C^T
-  TB_K("gemm_mx", 2.0 * n2occ_lo, 1,
-       k_gemm_mx<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.f, 0.f,
-                                            lo));
+  TB_K("gemm_tc", 2.0 * n2occ_lo, 1,
+       k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.0, 0.0, lo, S.status));
   TB_K("gemm", 2.0 * n2occ_hi, 1,
        k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.0, 0.0, hi));
   return TB_OK;
@@ -722,7 +725,8 @@ tb_status raise_smem_limits() {
   int dev = 0, optin = 0;
   TB_CUDA(cudaGetDevice(&dev));
   TB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  const void* ks[] = {(const void*)k_syev, (const void*)k_syev_f32, (const void*)k_fermi, (const void*)k_oa_step};
+  const void* ks[] = {(const void*)k_syev, (const void*)k_syev_f32, (const void*)k_fermi, (const void*)k_oa_step,
+                      (const void*)k_gemm_tc};
   for (const void* k : ks) {
     cudaFuncAttributes a;
     TB_CUDA(cudaFuncGetAttributes(&a, k));

@@ -87,11 +87,15 @@ __global__ void k_syev(DevBatch B, double* Ab, double* Zb, double* wout, int* pe
 __global__ void k_syev_f32(DevBatch B, float* Ab, float* Zb, double* wout, int* perm, int* status, const int* active);
 
 // mixed-precision form (tb_mixed.cu)
-// k_gemm with FP32 products and accumulation on FP64-stored operands
-__global__ void k_gemm_mx(DevBatch B, const int4* tiles, int ntiles, const double* Ab, int ta, const double* Bb,
-                          int tb_, const int* perm, const double* ks, const int* kdim, double* Cb, float alpha,
-                          float beta, const int* active);
 __global__ void k_phase_masks(int nmol, const int* active, const int* phase, int* lo, int* hi);
+// the same contractions as TF32x3 (split precision) tcgen05 GEMMs over 128 x 128 tiles (tb_tc.cu);
+// kTcThreads threads, dynamic shared memory gemm_tc_smem_bytes(), status marks a structure whose waits ran out
+constexpr int kTcTile = 128;
+constexpr int kTcThreads = 256;
+__global__ void k_gemm_tc(DevBatch B, const int4* tiles, int ntiles, const double* Ab, int ta, const double* Bb,
+                          int tb_, const int* perm, const double* ks, const int* kdim, double* Cb, double alpha,
+                          double beta, const int* active, int* status);
+size_t gemm_tc_smem_bytes();
 __global__ void k_to_f32(DevBatch B, const int4* tiles, int ntiles, const double* F, float* Af, const int* mask);
 __global__ void k_gather_vectors(DevBatch B, const int4* tiles, int ntiles, const float* Zf, const int* perm,
                                  double* V, const int* mask);

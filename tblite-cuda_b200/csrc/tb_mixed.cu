@@ -2,8 +2,8 @@
 //
 // Each structure runs in one of two phases (MolState::phase):
 //  * mixed (0): the contractions F' = X^T F X, C = X V and P = C f C^T are
-//    FP32-product GEMMs accumulated in FP32 on FP64-stored operands
-//    (k_gemm_mx);
+//    TF32x3 split-precision tensor-core GEMMs accumulated in FP32 on
+//    FP64-stored operands (k_gemm_tc, tb_tc.cu);
 //  * FP64 (1): entered once the mixed phase meets the (loosened) convergence
 //    test; the same contractions as FP64 GEMMs.  A structure retires only
 //    after at least two FP64 iterations and the full-accuracy convergence test.
@@ -26,98 +26,8 @@
 namespace tb {
 
 namespace {
-constexpr int MT = 64, MK = 16;
-
-__device__ inline void store_c(double* c, float v, float alpha, float beta) {
-  *c = beta == 0.0f ? (double)(alpha * v) : (double)(alpha * v) + (double)beta * (*c);
-}
+constexpr int MT = 64;
 }  // namespace
-
-// C_m = alpha op(A_m) diag(ks_m) op(B_m) + beta C_m with FP32 products and FP32
-// accumulation on FP64-stored operands (rounded to FP32 when staged in shared
-// memory); with beta = 1 the FP32 result is added to C in FP64.  Same tiling
-// and arguments as k_gemm.
-__global__ void __launch_bounds__(256) k_gemm_mx(DevBatch B, const int4* __restrict__ tiles, int ntiles,
-                                                 const double* __restrict__ Ab, int ta, const double* __restrict__ Bb,
-                                                 int tb_, const int* __restrict__ perm, const double* __restrict__ ks,
-                                                 const int* __restrict__ kdim, double* __restrict__ Cb, float alpha,
-                                                 float beta, const int* __restrict__ active) {
-  __shared__ float As[2][MK][MT + 4];
-  __shared__ float Bs[2][MK][MT + 4];
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int4 tl = tiles[t];
-    const int m = tl.x;
-    if (active && !active[m]) continue;
-    const int n = B.ooff[m + 1] - B.ooff[m];
-    const int K = kdim ? kdim[m] : n;
-    const long long mo = B.moff[m];
-    const long long vo = B.ooff[m];
-    const double* A = Ab + mo;
-    const double* Bm = Bb + mo;
-    const int* pm = perm ? perm + vo : nullptr;
-    const double* kv = ks ? ks + vo : nullptr;
-    const int i0 = tl.y * MT, j0 = tl.z * MT;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    float acc[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0f;
-    auto load = [&](int buf, int k0) {
-      for (int e = threadIdx.x; e < MT * MK; e += blockDim.x) {
-        int ii, kk;
-        if (ta) { ii = e % MT; kk = e / MT; } else { kk = e % MK; ii = e / MK; }
-        const int gi = i0 + ii, gk = k0 + kk;
-        float v = 0.0f;
-        if (gi < n && gk < K) {
-          double x = ta ? A[(long long)gk * n + gi] : A[(long long)gi * n + gk];
-          if (kv) x *= kv[gk];
-          v = (float)x;
-        }
-        As[buf][kk][ii] = v;
-        int jj, kb;
-        if (tb_) { kb = e % MK; jj = e / MK; } else { jj = e % MT; kb = e / MT; }
-        const int gj = j0 + jj, gk2 = k0 + kb;
-        float u = 0.0f;
-        if (gj < n && gk2 < K) {
-          const int col = pm ? pm[gj] : gj;
-          u = (float)(tb_ ? Bm[(long long)col * n + gk2] : Bm[(long long)gk2 * n + col]);
-        }
-        Bs[buf][kb][jj] = u;
-      }
-    };
-    const int nk = (K + MK - 1) / MK;
-    __syncthreads();
-    if (nk > 0) load(0, 0);
-    __syncthreads();
-    for (int kt = 0; kt < nk; ++kt) {
-      const int cur = kt & 1;
-      if (kt + 1 < nk) load(cur ^ 1, (kt + 1) * MK);
-#pragma unroll
-      for (int kk = 0; kk < MK; ++kk) {
-        float a[4], b[4];
-#pragma unroll
-        for (int x = 0; x < 4; ++x) { a[x] = As[cur][kk][ty + 16 * x]; b[x] = Bs[cur][kk][tx + 16 * x]; }
-#pragma unroll
-        for (int x = 0; x < 4; ++x)
-#pragma unroll
-          for (int y = 0; y < 4; ++y) acc[x][y] = fmaf(a[x], b[y], acc[x][y]);
-      }
-      __syncthreads();
-    }
-#pragma unroll
-    for (int x = 0; x < 4; ++x) {
-      const int gi = i0 + ty + 16 * x;
-      if (gi >= n) continue;
-#pragma unroll
-      for (int y = 0; y < 4; ++y) {
-        const int gj = j0 + tx + 16 * y;
-        if (gj >= n) continue;
-        store_c(Cb + mo + (long long)gi * n + gj, acc[x][y], alpha, beta);
-      }
-    }
-  }
-}
 
 // lo[m] = active and in the mixed phase; hi[m] = active and in the FP64 phase.
 __global__ void k_phase_masks(int nmol, const int* __restrict__ active, const int* __restrict__ phase,
