@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
 namespace {
 
 constexpr int kWalkBatch = 12;  // rows per load batch in the Householder column walk
-constexpr int kQBatch = 8;      // 32-wide row segments per load batch in the Q accumulation
+constexpr int kQBlock = 16;     // reflectors per compact-WY block of the Q accumulation
 constexpr int kWaveK = 4;            // QL sweeps applied per pass over Zc
 constexpr int kWin = 2 * kWaveK;     // rows of Zc in flight per column
 constexpr long long kSpinLimit = 1LL << 24;
@@ -423,75 +423,91 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
   if (tid == 0 && n >= 2) e[n - 2] = A[(long long)(n - 2) * n + n - 1];
   __syncthreads();
 
-  // ---- 2. Zc = Q^T (row c of Zc = column c of Q) by backward accumulation:
-  // Zc22 <- Zc22 (I - tau v v^T), one warp per row of Zc; the dot product
-  // u'_c = Zc_new[c][.] v' of the next step (k-1) is fused into the same pass.
+  // ---- 2. Zc = Q^T (row c of Zc = column c of Q), Q = H_0 H_1 ... H_{n-3},
+  // accumulated backwards in blocks of kQBlock reflectors in compact WY form:
+  // H_k0 ... H_k1 = I - V T V^T (V = [v_k0 .. v_k1], T upper triangular), so
+  // Zc <- Zc H_k1 ... H_k0 = Zc - (Zc V) T^T V^T on rows and columns >= k0+1.
+  // Each row of that block is read twice and written once per block instead of
+  // once per reflector.  V is staged in shared memory (the rotation ring is not
+  // in use yet); one warp per row: partial dots of the row with the kQBlock
+  // reflectors, a warp reduction, T^T applied by kQBlock lanes, then the update.
   for (long long x = tid; x < (long long)n * n; x += nt) Z[x] = ((x / n) == (x % n)) ? T(1) : T(0);
   __syncthreads();
   {
     const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
-    int k = n - 3;
-    if (k >= 0) {
-      // first applied step: Zc22 is the identity, so u_c = v_c
-      const int mm = n - k - 1;
-      for (int i = tid; i < mm; i += nt) { v[i] = i == 0 ? T(1) : A[(long long)k * n + k + 1 + i]; w[i] = v[i]; }
+    __shared__ T Ts[kQBlock][kQBlock];          // T of the block
+    __shared__ T yv[kQBlock][kQBlock];          // V^T V (upper part)
+    __shared__ T wps[kEigThreads / 32][kQBlock];  // per warp: (row . V) T^T
+    T* Vs = ring;                               // kQBlock x m, m <= n - 1
+    const int nref = n - 2;
+    for (int k1 = nref - 1; k1 >= 0; k1 -= kQBlock) {
+      const int k0 = k1 - kQBlock + 1 > 0 ? k1 - kQBlock + 1 : 0, bb = k1 - k0 + 1;
+      const int c0 = k0 + 1, m = n - c0;
+      // Vs[j][cc] = v_{k0+j}[c0 + cc]: row k0+j of A from column k0+j+1 (which holds 1), zero before
+      for (int e = tid; e < kQBlock * m; e += nt) {
+        const int j = e / m, cc = e - j * m, c = c0 + cc;
+        Vs[e] = (j < bb && c >= k0 + j + 1) ? A[(long long)(k0 + j) * n + c] : T(0);
+      }
       __syncthreads();
-    }
-    for (; k >= 0; --k) {
-      const int mm = n - k - 1, b0 = k + 1;
-      const T tk = tau[k];
-      // v' of step k-1 (its block starts at index k): v'_0 = 1, v'_i = A[k-1][k+i]
-      if (k >= 1)
-        for (int i = tid; i <= mm; i += nt) vn[i] = i == 0 ? T(1) : A[(long long)(k - 1) * n + k + i];
+      for (int pq = wid; pq < kQBlock * kQBlock; pq += nw) {
+        const int j = pq / kQBlock, i = pq - j * kQBlock;
+        if (j >= i || i >= bb) continue;  // warp-uniform
+        T acc = T(0);
+        for (int cc = lane; cc < m; cc += 32) acc += Vs[j * m + cc] * Vs[i * m + cc];
+        acc = warp_sum(acc);
+        if (lane == 0) yv[j][i] = acc;
+      }
       __syncthreads();
-      for (int c = wid; c < mm; c += 2 * nw) {
-        // rows c and c + nw of the block (the second may not exist)
-        const int c2 = c + nw;
-        const bool two = c2 < mm;
-        T* za = Z + (long long)(b0 + c) * n + b0;
-        T* zb = Z + (long long)(b0 + (two ? c2 : c)) * n + b0;
-        const T ta = tk * w[c], tb = two ? tk * w[c2] : T(0);
-        T acca = T(0), accb = T(0);
-        for (int r0 = 0; r0 < mm; r0 += 32 * kQBatch) {
-          T qa[kQBatch], qb[kQBatch];
-#pragma unroll
-          for (int u = 0; u < kQBatch; ++u) {
-            const int r = r0 + lane + 32 * u;
-            qa[u] = r < mm ? za[r] : T(0);
-            qb[u] = (two && r < mm) ? zb[r] : T(0);
-          }
-#pragma unroll
-          for (int u = 0; u < kQBatch; ++u) {
-            const int r = r0 + lane + 32 * u;
-            if (r < mm) {
-              if (tk != T(0)) {
-                qa[u] -= ta * v[r];
-                za[r] = qa[u];
-                if (two) {
-                  qb[u] -= tb * v[r];
-                  zb[r] = qb[u];
-                }
+      if (tid == 0) {  // T column by column: T[i][i] = tau, T[0:i][i] = -tau T[0:i][0:i] (V^T v_i)[0:i]
+        for (int i = 0; i < kQBlock; ++i) {
+          const T ti = i < bb ? tau[k0 + i] : T(0);
+          for (int r = 0; r < kQBlock; ++r) {
+            T x = T(0);
+            if (i < bb) {
+              if (r == i) {
+                x = ti;
+              } else if (r < i) {
+                T sacc = T(0);
+                for (int q = r; q < i; ++q) sacc += Ts[r][q] * yv[q][i];
+                x = -ti * sacc;
               }
-              acca += qa[u] * vn[r + 1];
-              accb += qb[u] * vn[r + 1];
             }
-          }
-        }
-        if (k >= 1) {
-          acca = warp_sum(acca);
-          accb = warp_sum(accb);
-          if (lane == 0) {
-            p[c + 1] = acca;  // p is free scratch here
-            if (two) p[c2 + 1] = accb;
+            Ts[r][i] = x;
           }
         }
       }
       __syncthreads();
-      if (k >= 1) {
-        // next step: v <- v'; u'_0 = Zc[k][k..] . v' = 1 (row k of Zc is still e_k)
-        for (int i = tid; i <= mm; i += nt) { v[i] = vn[i]; w[i] = i == 0 ? T(1) : p[i]; }
-        __syncthreads();
+      for (int r = c0 + wid; r < n; r += nw) {
+        T* zr = Z + (long long)r * n + c0;
+        T acc[kQBlock];
+#pragma unroll
+        for (int j = 0; j < kQBlock; ++j) acc[j] = T(0);
+        for (int cc = lane; cc < m; cc += 32) {
+          const T z = zr[cc];
+#pragma unroll
+          for (int j = 0; j < kQBlock; ++j) acc[j] += z * Vs[j * m + cc];
+        }
+#pragma unroll
+        for (int j = 0; j < kQBlock; ++j) acc[j] = warp_sum(acc[j]);
+        if (lane < kQBlock) {  // (row . V) T^T, entry lane
+          T x = T(0);
+#pragma unroll
+          for (int q = 0; q < kQBlock; ++q) x += acc[q] * Ts[lane][q];
+          wps[wid][lane] = x;
+        }
+        __syncwarp();
+        T wp[kQBlock];
+#pragma unroll
+        for (int j = 0; j < kQBlock; ++j) wp[j] = wps[wid][j];
+        for (int cc = lane; cc < m; cc += 32) {
+          T z = zr[cc];
+#pragma unroll
+          for (int j = 0; j < kQBlock; ++j) z -= wp[j] * Vs[j * m + cc];
+          zr[cc] = z;
+        }
+        __syncwarp();
       }
+      __syncthreads();
     }
   }
 
