@@ -256,6 +256,14 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
 namespace {
 
 constexpr int kWalkBatch = 12;  // rows per load batch in the Householder column walk
+// Tridiagonalisation panel: reflectors per panel (2 panel n <= ring) and rows
+// per load batch of the panel-closing walk.  FP64 moves twice the bytes per
+// element, so the walk is traffic-bound and wide panels pay; in FP32 a panel
+// of one (each step's update fused with the next product) is as fast.
+template <typename T> struct PanelCfg;
+template <> struct PanelCfg<double> { static constexpr int width = 8, batch = 4; };
+template <> struct PanelCfg<float> { static constexpr int width = 1, batch = 12; };
+static_assert(PanelCfg<double>::width <= kRing && PanelCfg<float>::width <= kRing, "panel exceeds the ring");
 constexpr int kQBlock = 16;     // reflectors per compact-WY block of the Q accumulation
 constexpr int kWaveK = 4;            // QL sweeps applied per pass over Zc
 constexpr int kWin = 2 * kWaveK;     // rows of Zc in flight per column
@@ -268,12 +276,15 @@ __device__ inline double tb_sqrt(double x) { return sqrt(x); }
 __device__ inline float tb_sqrt(float x) { return sqrtf(x); }
 __device__ inline double tb_abs(double x) { return fabs(x); }
 __device__ inline float tb_abs(float x) { return fabsf(x); }
-__device__ inline double tb_rsqrt(double x) { return rsqrt(x); }
 // one Newton step y(3 - x y^2)/2 on the hardware estimate keeps Givens pairs orthogonal to ~1 ulp
 __device__ inline float tb_rsqrt(float x) {
   const float y = rsqrtf(x);
   return y * (1.5f - 0.5f * x * y * y);
 }
+
+// reciprocal square root on the QL rotation chain (FP32: one Newton step on the estimate)
+__device__ inline double chain_rsqrt(double x) { return rsqrt(x); }
+__device__ inline float chain_rsqrt(float x) { return tb_rsqrt(x); }
 
 template <typename T>
 __device__ inline T block_sum_syev(T v, T* red) { return block_sum(v, red); }
@@ -346,6 +357,45 @@ __device__ void colwalk(T* M, int n, int r0, int nr, int c0, int nc, bool upd, c
   }
 }
 
+// Closing walk of a tridiagonalisation panel over rows and columns
+// r0..r0+nm-1 (both relative to the matrix origin, the block is square):
+// M -= sum_i PV_i PW_i^T + PW_i PV_i^T over the panel's pairs (absolute
+// index), and out_c = scale * sum_r M_new[r][c] x_{r-r0}.  One thread per
+// column keeps its column's pair entries in registers.
+template <typename T>
+__device__ void panel_walk(T* M, int n, int r0, int nm, const T* PV, const T* PW, const T* x, T* out, T scale) {
+  constexpr int kPanel = PanelCfg<T>::width, kPanelBatch = PanelCfg<T>::batch;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int jj = tid; jj < nm; jj += nt) {
+    const int c = r0 + jj;
+    T vc[kPanel], wc[kPanel];
+#pragma unroll
+    for (int i = 0; i < kPanel; ++i) {
+      vc[i] = PV[(long long)i * n + c];
+      wc[i] = PW[(long long)i * n + c];
+    }
+    T acc = T(0);
+    for (int i0 = 0; i0 < nm; i0 += kPanelBatch) {
+      T q[kPanelBatch];
+#pragma unroll
+      for (int u = 0; u < kPanelBatch; ++u)
+        q[u] = (i0 + u < nm) ? M[(long long)(r0 + i0 + u) * n + c] : T(0);
+#pragma unroll
+      for (int u = 0; u < kPanelBatch; ++u) {
+        if (i0 + u < nm) {
+          const int rr = r0 + i0 + u;
+          T y = q[u];
+#pragma unroll
+          for (int i = 0; i < kPanel; ++i) y -= PV[(long long)i * n + rr] * wc[i] + PW[(long long)i * n + rr] * vc[i];
+          M[(long long)rr * n + c] = y;
+          acc += y * x[i0 + u];
+        }
+      }
+    }
+    out[jj] = scale * acc;
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab, T* __restrict__ Zb,
                                           double* __restrict__ wout, int* __restrict__ perm,
@@ -387,35 +437,78 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
   for (int i = tid; i < n; i += nt) { e[i] = T(0); tau[i] = T(0); }
   __syncthreads();
 
-  // ---- 1. tridiagonalisation
+  // ---- 1. tridiagonalisation in panels of PanelCfg<T>::width reflectors.  Within a
+  // panel the trailing block keeps its value A0 from the panel start; step k
+  // forms p = tau A0 v and corrects it with the open pairs (v_i, w_i):
+  // A = A0 - sum_i (v_i w_i^T + w_i v_i^T).  Only the row that yields the next
+  // reflector is brought up to date; the block itself is rewritten once, when
+  // the panel closes, fused with the next step's product.
   if (n >= 3) {
+    const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+    constexpr int kPanel = PanelCfg<T>::width;
+    T* PV = ring;               // kPanel x n: v_i of the open panel (absolute index)
+    T* PW = ring + kPanel * n;  // kPanel x n: w_i
+    __shared__ T dots[2 * kPanel];
+    const int nref = n - 2;     // reflectors 0 .. n-3
     reflector(A, n, 0, v, tau, e, red, sh);
     // p0 = tau0 * A[1..][1..] v0
     colwalk<T>(A, n, 1, n - 1, 1, n - 1, false, nullptr, nullptr, 0, v, p, tau[0]);
     __syncthreads();
-    for (int k = 0; k + 2 < n; ++k) {
+    int np = 0;  // pairs in the open panel
+    for (int k = 0; k < nref; ++k) {
       const int mm = n - k - 1, b0 = k + 1;
       const T tk = tau[k];
-      // w = p - (tau/2)(p.v) v
+      if (np > 0) {  // dots[i] = w_i . v, dots[np + i] = v_i . v over the block, one warp per dot
+        for (int q = wid; q < 2 * np; q += nw) {
+          const T* src = (q < np ? PW + (long long)q * n : PV + (long long)(q - np) * n) + b0;
+          T acc = T(0);
+          for (int j = lane; j < mm; j += 32) acc += src[j] * v[j];
+          acc = warp_sum(acc);
+          if (lane == 0) dots[q] = acc;
+        }
+        __syncthreads();
+      }
+      // p = tau (A0 v - sum_i v_i (w_i.v) + w_i (v_i.v)); w = p - (tau/2)(p.v) v
       T part = T(0);
-      for (int j = tid; j < mm; j += nt) part += p[j] * v[j];
+      for (int j = tid; j < mm; j += nt) {
+        T pj = p[j];
+        for (int i = 0; i < np; ++i)
+          pj -= tk * (PV[(long long)i * n + b0 + j] * dots[i] + PW[(long long)i * n + b0 + j] * dots[np + i]);
+        p[j] = pj;
+        part += pj * v[j];
+      }
       const T pv = block_sum_syev(part, red);
       const T kk = T(0.5) * tk * pv;
-      for (int j = tid; j < mm; j += nt) w[j] = p[j] - kk * v[j];
+      for (int j = tid; j < mm; j += nt) {
+        PV[(long long)np * n + b0 + j] = v[j];
+        PW[(long long)np * n + b0 + j] = p[j] - kk * v[j];
+      }
+      ++np;
       __syncthreads();
-      const bool upd = tk != T(0);
-      // (a) first row of the block
-      if (upd)
-        for (int j = tid; j < mm; j += nt) A[(long long)b0 * n + b0 + j] -= v[0] * w[j] + w[0] * v[j];
-      __syncthreads();
-      if (k + 3 < n) {
-        reflector(A, n, k + 1, vn, tau, e, red, sh);
-        // (c) rest of the block, fused with p_{k+1} = tau_{k+1} A22' v_{k+1}
-        colwalk<T>(A, n, b0 + 1, mm - 1, b0 + 1, mm - 1, upd, v, w, 1, vn, p, tau[k + 1]);
-      } else if (upd) {
-        colwalk<T>(A, n, b0 + 1, mm - 1, b0 + 1, mm - 1, true, v, w, 1, vn, p, T(0));
+      // row r = k+1 (columns r..n-1) brought up to date; the last step also row n-1's diagonal
+      const int r = k + 1;
+      for (int c = r + tid; c < n; c += nt) {
+        T x = A[(long long)r * n + c];
+        for (int i = 0; i < np; ++i)
+          x -= PV[(long long)i * n + r] * PW[(long long)i * n + c] + PW[(long long)i * n + r] * PV[(long long)i * n + c];
+        A[(long long)r * n + c] = x;
+      }
+      if (r == nref && tid == 0) {
+        T x = A[(long long)(n - 1) * n + n - 1];
+        for (int i = 0; i < np; ++i) x -= T(2) * PV[(long long)i * n + n - 1] * PW[(long long)i * n + n - 1];
+        A[(long long)(n - 1) * n + n - 1] = x;
       }
       __syncthreads();
+      if (r < nref) {
+        reflector(A, n, r, vn, tau, e, red, sh);
+        if (np == kPanel) {  // close the panel: A -= V W^T + W V^T on the block, fused with p_r = tau_r A vn
+          panel_walk<T>(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r]);
+          np = 0;
+        } else {  // p_r = tau_r A0 vn
+          colwalk<T>(A, n, r + 1, n - r - 1, r + 1, n - r - 1, false, nullptr, nullptr, 0, vn, p, tau[r]);
+        }
+        __syncthreads();
+      }
       T* t = v; v = vn; vn = t;
     }
   }
@@ -564,24 +657,34 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
           T s = T(1), c = T(1), pp = T(0);
           int cnt = 0;
           bool underflow = false;
+          // d[i+1], d[i], e[i] of the current rotation are carried in registers
+          // and the next rotation's d[i-1], e[i-1] are loaded one step ahead, so
+          // no shared-memory latency sits on the dependency chain (the sweep
+          // writes only d[i+1] and e[i+1], never an entry still to be read).
+          T dn = d[mq], di = d[mq - 1], ei = e[mq - 1];
           for (int i = mq - 1; i >= l; --i) {
-            const T f = s * e[i];
-            const T bb = c * e[i];
+            const T di_next = i > l ? d[i - 1] : T(0);
+            const T ei_next = i > l ? e[i - 1] : T(0);
+            const T f = s * ei;
+            const T bb = c * ei;
             const T rr2 = f * f + g * g;
-            if (rr2 == T(0)) { d[i + 1] -= pp; e[mq] = T(0); underflow = true; break; }
-            const T ri = tb_rsqrt(rr2);
+            if (rr2 == T(0)) { d[i + 1] = dn - pp; e[mq] = T(0); underflow = true; break; }
+            const T ri = chain_rsqrt(rr2);
             r = rr2 * ri;
             e[i + 1] = r;
             s = f * ri;
             c = g * ri;
-            g = d[i + 1] - pp;
-            r = (d[i] - g) * s + T(2) * c * bb;
+            g = dn - pp;
+            r = (di - g) * s + T(2) * c * bb;
             pp = s * r;
             d[i + 1] = g + pp;
             g = c * r - bb;
             rc[cnt] = c;
             rs[cnt] = s;
             ++cnt;
+            dn = di;
+            di = di_next;
+            ei = ei_next;
           }
           if (!underflow) { d[l] -= pp; e[l] = g; e[mq] = T(0); }
           sh_head[slot][0] = mq;

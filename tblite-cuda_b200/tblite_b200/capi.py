@@ -402,3 +402,4 @@ def fermi_filling(nel, kt, emo):
                                          emo.ctypes.data_as(_dp), occ.ctypes.data_as(_dp), C.byref(ef),
                                          C.byref(ts))
     return st, occ, ef.value, ts.value
+

@@ -130,6 +130,22 @@ def test_sygvd_degenerate_and_kat():
     np.testing.assert_allclose(C[:, :4] @ C[:, :4].T, Qm[:, :4] @ Qm[:, :4].T, atol=1e-12)
 
 
+def test_sygvd_tridiagonal_panel_sizes(oracle):
+    # sizes around the FP64 panel width (8 reflectors) and its multiples
+    rng = np.random.default_rng(5)
+    sizes = [3, 4, 9, 10, 11, 17, 18, 19, 66, 67]
+    Hs = []
+    for n in sizes:
+        M = rng.normal(size=(n, n))
+        Hs.append(0.5 * (M + M.T))
+    st, out = capi.sygvd_batch(Hs, [np.eye(n) for n in sizes])
+    assert st == capi.TB_OK
+    for H, (w, C) in zip(Hs, out):
+        np.testing.assert_allclose(w, np.linalg.eigvalsh(H), atol=1e-12)
+        np.testing.assert_allclose(C.T @ C, np.eye(len(w)), atol=1e-12)
+        np.testing.assert_allclose(H @ C, C * w, atol=1e-11)
+
+
 def test_sygvd_not_spd_status():
     st, _ = capi.sygvd_batch([np.eye(3)], [-np.eye(3)])
     assert st == capi.TB_NOT_SPD
