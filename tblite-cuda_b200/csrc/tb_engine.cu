@@ -754,7 +754,7 @@ tb_status calibrate_eigensolvers(tb_calculator* c) {
   const std::string we = ls.workspace(NL, &wbytes);
   if (!we.empty()) return fail(TB_CUDA_ERROR, "eigensolver calibration: " + we);
   Layout L;
-  const size_t oA = L.add(nn * 8), oZ = L.add(nn * 8), ow = L.add(NL * 8), op = L.add(NL * 4), os = L.add(16),
+  const size_t oA = L.add(nn * 8), oZ = L.add(nn * 8), oW = L.add(nn * 8), ow = L.add(NL * 8), op = L.add(NL * 4), os = L.add(16),
                oo = L.add(16), om = L.add(16), owk = L.add(std::max<size_t>(wbytes, 16)), oi = L.add(16);
   TB_CUDA(ar.reserve(L.total));
   char* base = ar.base;
@@ -789,8 +789,8 @@ tb_status calibrate_eigensolvers(tb_calculator* c) {
       if (us != TB_OK) return us;
       TB_CUDA(cudaEventRecord(e0));
       k_syev<<<1, kEigThreads, syev_smem_bytes(n)>>>(B, at<double>(base, oA), at<double>(base, oZ),
-                                                     at<double>(base, ow), at<int>(base, op), at<int>(base, os),
-                                                     nullptr);
+                                                     at<double>(base, oW), at<double>(base, ow), at<int>(base, op),
+                                                     at<int>(base, os), nullptr);
       TB_CUDA(cudaEventRecord(e1));
       TB_CUDA(cudaEventSynchronize(e1));
       TB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
@@ -961,7 +961,7 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
                                            b->F, 1.0, 0.0, S.active));
     // symmetric eigensolve with vectors: canonical 4 N^3
     TB_K("syev", 4.0 * n3, 1,
-         k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->w, b->perm, S.status, S.active));
+         k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->W, b->w, b->perm, S.status, S.active));
     for (size_t k = 0; k < b->big.size(); ++k) {
       const int m = b->big[k], n = b->h_ooff[m + 1] - b->h_ooff[m];
       if (!b->h_active[m] || b->h_status[m] != kStOk) continue;
@@ -1525,7 +1525,7 @@ tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const 
     const tb_status ss = raise_smem_limits();
     if (ss != TB_OK) return ss;
   }
-  k_syev<<<nmat, kEigThreads, smem>>>(B, mb.F, mb.Z, mb.w, mb.perm, mb.ms.status, mb.ms.active);
+  k_syev<<<nmat, kEigThreads, smem>>>(B, mb.F, mb.Z, mb.W, mb.w, mb.perm, mb.ms.status, mb.ms.active);
   std::vector<int> fstat(nmat, 0);
   if (!mb.big.empty()) TB_CUDA(cudaMemcpy(fstat.data(), mb.ms.status, nmat * 4, cudaMemcpyDeviceToHost));
   for (size_t k = 0; k < mb.big.size(); ++k) {

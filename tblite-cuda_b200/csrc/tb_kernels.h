@@ -82,7 +82,10 @@ __global__ void k_trinv(DevBatch B, const double* W, double* X, const int* statu
 __global__ void k_gemm(DevBatch B, const int4* tiles, int ntiles, const double* Ab, int ta, const double* Bb, int tb_,
                        const int* perm, const double* ks, const int* kdim, double* Cb, double alpha, double beta,
                        const int* active);
-__global__ void k_syev(DevBatch B, double* Ab, double* Zb, double* wout, int* perm, int* status, const int* active);
+// Sb: optional n x n scratch per structure (same offsets as Ab); with it,
+// structures of at least 128 AOs take divide and conquer instead of QL
+__global__ void k_syev(DevBatch B, double* Ab, double* Zb, double* Sb, double* wout, int* perm, int* status,
+                       const int* active);
 // the same eigensolver in FP32 (A and Z float, eigenvalues written as double)
 __global__ void k_syev_f32(DevBatch B, float* Ab, float* Zb, double* wout, int* perm, int* status, const int* active);
 

@@ -396,9 +396,329 @@ __device__ void panel_walk(T* M, int n, int r0, int nm, const T* PV, const T* PW
   }
 }
 
+// ------------------------------------------------ divide and conquer (Cuppen)
+// Tridiagonal T (d, e) = diag(T_left, T_right) + rho v v^T torn at every node
+// of a halving tree down to 1 x 1 leaves; the eigenvector matrix G of each
+// node (rows = eigenvectors in T's index space, an m x m diagonal block of an
+// n x n buffer) is built bottom-up by rank-one merges:
+//  * z = [last column of G_left ; sign(e) * first column of G_right], unit
+//    norm, rho' = |e| |z|^2; eigenvalues sorted;
+//  * deflation (tolerance 8 eps max(|delta|max, rho')): entries with rho'|z_i|
+//    below it keep their eigenpair; adjacent close pairs are rotated so that
+//    one z entry vanishes (LAPACK dlaed2's two tests);
+//  * roots of the secular equation 1 + rho' sum z_i^2 / (delta_i - lambda) = 0
+//    by bracketed two-pole rational interpolation (Bunch, Nielsen and Sorensen
+//    1978), each root kept as (nearest pole, offset) so that delta_i - lambda
+//    keeps full relative accuracy;
+//  * z recomputed from the roots (Gu and Eisenstat 1994) so the eigenvectors
+//    w_j = z_i / (delta_i - lambda_j) are orthogonal to working accuracy;
+//  * G_node = W G_children as a tiled product with W generated on the fly.
+// Finally Zc <- G Zc (Zc = Q^T), and the eigenvalues are left in d.
+constexpr int kDcMin = 128;  // smallest structure solved this way (shared memory, see dc_ws_ok)
+constexpr int kDcK = 8;      // reduction slab of the tiled products
+
+// workspace of one merge of m entries, in units of T (the ints after the T arrays)
+template <typename T>
+__host__ __device__ constexpr int dc_ws_elems(int m) {
+  return 8 * m + 2 * 64 * kDcK + (7 * m * (int)sizeof(int) + (int)sizeof(T) - 1) / (int)sizeof(T);
+}
+
+// the workspace starts at tau: 5 n vectors + the ring are free after Q is formed
+static_assert(dc_ws_elems<double>(kDcMin) <= (5 + 2 * kRing) * kDcMin,
+              "divide-and-conquer workspace exceeds the free shared memory");
+
+// Root j of 1 + rho sum_i z_i^2 / (dl_i - lambda) = 0 (dl strictly ascending,
+// rho > 0): lambda = dl[*o] + *tau.
+template <typename T>
+__device__ void secular_root(int j, int k, const T* dl, const T* z, T rho, int* o_out, T* tau_out) {
+  const T eps = Eps<T>::v;
+  int o;
+  T lo, hi;
+  if (j < k - 1) {
+    const T mid = T(0.5) * (dl[j + 1] - dl[j]);
+    T f = T(1);
+    for (int i = 0; i < k; ++i) f += rho * z[i] * z[i] / ((dl[i] - dl[j]) - mid);
+    if (f >= T(0)) { o = j; lo = T(0); hi = mid; }
+    else { o = j + 1; lo = -mid; hi = T(0); }
+  } else {
+    T s = T(0);
+    for (int i = 0; i < k; ++i) s += z[i] * z[i];
+    o = k - 1; lo = T(0); hi = rho * s;
+  }
+  const T base = dl[o];
+  T tau = T(0.5) * (lo + hi);
+  for (int it = 0; it < 100; ++it) {
+    T psi = T(0), phi = T(0), dpsi = T(0), dphi = T(0);
+    for (int i = 0; i < k; ++i) {
+      const T r = T(1) / ((dl[i] - base) - tau);
+      const T q = z[i] * z[i] * r;
+      if (i <= j) { psi += q; dpsi += q * r; }
+      else { phi += q; dphi += q * r; }
+    }
+    psi *= rho; phi *= rho; dpsi *= rho; dphi *= rho;
+    const T f = T(1) + psi + phi;
+    const T err = eps * (T(8) * (tb_abs(psi) + tb_abs(phi)) + T(3) + tb_abs(tau) * (dpsi + dphi));
+    if (tb_abs(f) <= err) break;
+    if (f < T(0)) lo = tau; else hi = tau;
+    if (hi - lo <= T(2) * eps * fmax(tb_abs(lo), tb_abs(hi))) break;
+    const T a = (dl[j] - base) - tau;
+    T eta = T(0);
+    bool ok = false;
+    if (j < k - 1) {  // psi ~ c1 + s1/(a - eta), phi ~ c2 + s2/(b - eta)
+      const T b = (dl[j + 1] - base) - tau;
+      const T s1 = dpsi * a * a, c1 = psi - dpsi * a, s2 = dphi * b * b, c2 = phi - dphi * b;
+      const T C = T(1) + c1 + c2;
+      const T Bq = C * (a + b) + s1 + s2;
+      const T sq = tb_sqrt(fmax(Bq * Bq - T(4) * C * a * b * f, T(0)));
+      const T q = Bq >= T(0) ? T(0.5) * (Bq + sq) : T(0.5) * (Bq - sq);
+      if (q != T(0)) { eta = a * b * f / q; ok = eta > a && eta < b; }
+      if (!ok && C != T(0)) { eta = q / C; ok = eta > a && eta < b; }
+    } else {
+      const T s1 = dpsi * a * a, C = T(1) + psi - dpsi * a;
+      if (C > T(0)) { eta = a + s1 / C; ok = true; }
+    }
+    T tn = tau + eta;
+    if (!ok || !(tn > lo && tn < hi)) tn = T(0.5) * (lo + hi);
+    tau = tn;
+  }
+  *o_out = o;
+  *tau_out = tau;
+}
+
+// Out[(r0 + j) ld + c0 + c] = sum_i gen(j, i) In[(srow ? srow[i] : i) ld + c0 + c]
+// for j < nrow, c < ncol, i < kdim: 64 x 64 output tiles, 4 x 4 per thread,
+// slabs of kDcK staged in shared memory (Wt: 64 x kDcK, Bt: kDcK x 64).
+template <typename T, typename Gen>
+__device__ void dc_gemm(int nrow, int kdim, int ncol, Gen gen, const T* In, const int* srow, T* Out, int r0, int c0,
+                        int ld, T* Wt, T* Bt) {
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  for (int j0 = 0; j0 < nrow; j0 += 64) {
+    for (int cb = 0; cb < ncol; cb += 64) {
+      T acc[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+      for (int i0 = 0; i0 < kdim; i0 += kDcK) {
+        for (int x = tid; x < 64 * kDcK; x += kEigThreads) {
+          const int jj = x / kDcK, kk = x - jj * kDcK, j = j0 + jj, i = i0 + kk;
+          Wt[x] = (j < nrow && i < kdim) ? gen(j, i) : T(0);
+          const int kb = x >> 6, cc = x & 63, ib = i0 + kb;
+          Bt[x] = (ib < kdim && cb + cc < ncol) ? In[(long long)(srow ? srow[ib] : ib) * ld + c0 + cb + cc] : T(0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kDcK; ++kk) {
+          T av[4], bv[4];
+#pragma unroll
+          for (int a = 0; a < 4; ++a) av[a] = Wt[(ty * 4 + a) * kDcK + kk];
+#pragma unroll
+          for (int b = 0; b < 4; ++b) bv[b] = Bt[kk * 64 + tx + 16 * b];
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+        }
+        __syncthreads();
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int j = j0 + ty * 4 + a;
+        if (j >= nrow) continue;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int c = cb + tx + 16 * b;
+          if (c < ncol) Out[(long long)(r0 + j) * ld + c0 + c] = acc[a][b];
+        }
+      }
+    }
+  }
+}
+
+// One merge of the node [lo, hi) torn at t: children's G blocks in Gi (the
+// node's diagonal block; Gi is overwritten), eigenvalues in d[lo, hi); result
+// in the same block of Go and in d[lo, hi).  ws: dc_ws_elems(hi - lo) T.
+template <typename T>
+__device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, T* Go, T* ws, T* red) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int m = hi - lo;
+  T* delta = ws;          // m: sorted eigenvalues (rotated pairs updated)
+  T* zs = delta + m;      // m: sorted z (unit norm)
+  T* dl = zs + m;         // k: non-deflated delta
+  T* zl = dl + m;         // k: their z, then the recomputed z
+  T* tv = zl + m;         // k: root offsets
+  T* inrm = tv + m;       // k: 1 / |w_j|
+  T* rc = inrm + m;       // rotations: cosine
+  T* rsn = rc + m;        //            sine
+  T* Wt = rsn + m;
+  T* Bt = Wt + 64 * kDcK;
+  int* rowof = reinterpret_cast<int*>(Bt + 64 * kDcK);  // m: row of sorted entry s
+  int* flg = rowof + m;   // m: deflated
+  int* ndl = flg + m;     // m: sorted index of the k non-deflated, then of the deflated
+  int* rp = ndl + m;      // rotations: rows
+  int* rq = rp + m;
+  int* ori = rq + m;      // k: root origin (index into dl)
+  int* srow = ori + m;    // k: row of non-deflated entry
+  __shared__ int s_k, s_nrot;
+  __shared__ T s_rho;
+  const T ev = e[t - 1];
+  const T rho = tb_abs(ev), sg = ev >= T(0) ? T(1) : T(-1);
+  // children's blocks are diagonal sub-blocks: clear the rest of the node's block
+  for (long long x = tid; x < (long long)m * m; x += nt) {
+    const int r = lo + (int)(x / m), c = lo + (int)(x % m);
+    if ((r < t) != (c < t)) Gi[(long long)r * n + c] = T(0);
+  }
+  // z and its norm
+  T part = T(0);
+  for (int r = lo + tid; r < hi; r += nt) {
+    const T z = r < t ? Gi[(long long)r * n + t - 1] : sg * Gi[(long long)r * n + t];
+    part += z * z;
+  }
+  const T zz = block_sum(part, red);  // synchronises
+  const T zsc = T(1) / tb_sqrt(zz), rhop = rho * zz;
+  // rank sort of the eigenvalues (ties by index)
+  for (int r = lo + tid; r < hi; r += nt) {
+    const T dr = d[r];
+    int rank = 0;
+    for (int q = lo; q < hi; ++q) {
+      const T dq = d[q];
+      rank += (dq < dr || (dq == dr && q < r)) ? 1 : 0;
+    }
+    rowof[rank] = r;
+    delta[rank] = dr;
+    zs[rank] = (r < t ? Gi[(long long)r * n + t - 1] : sg * Gi[(long long)r * n + t]) * zsc;
+  }
+  __syncthreads();
+  if (tid == 0) {  // deflation scan and compaction, in order
+    T dmax = T(0);
+    for (int s = 0; s < m; ++s) dmax = fmax(dmax, tb_abs(delta[s]));
+    const T tol = T(8) * Eps<T>::v * fmax(dmax, rhop);
+    int nrot = 0, prev = -1;
+    for (int s = 0; s < m; ++s) {
+      if (rhop * tb_abs(zs[s]) <= tol) { flg[s] = 1; continue; }
+      flg[s] = 0;
+      if (prev >= 0) {
+        const T za = zs[prev], zb = zs[s];
+        const T tau = tb_sqrt(za * za + zb * zb);
+        const T c = zb / tau, sn = -za / tau;
+        if (tb_abs((delta[s] - delta[prev]) * c * sn) <= tol) {
+          rp[nrot] = rowof[prev]; rq[nrot] = rowof[s]; rc[nrot] = c; rsn[nrot] = sn; ++nrot;
+          zs[s] = tau; zs[prev] = T(0);
+          const T dp = delta[prev], ds = delta[s];
+          delta[prev] = dp * c * c + ds * sn * sn;
+          delta[s] = dp * sn * sn + ds * c * c;
+          flg[prev] = 1;
+        }
+      }
+      prev = s;
+    }
+    int k = 0;
+    for (int s = 0; s < m; ++s)
+      if (!flg[s]) { ndl[k] = s; dl[k] = delta[s]; zl[k] = zs[s]; srow[k] = rowof[s]; ++k; }
+    int q = k;
+    for (int s = 0; s < m; ++s)
+      if (flg[s]) ndl[q++] = s;
+    s_k = k; s_nrot = nrot; s_rho = rhop;
+  }
+  __syncthreads();
+  const int k = s_k, nrot = s_nrot;
+  // close-pair rotations on the rows, one thread per column, in order
+  for (int c = lo + tid; c < hi; c += nt)
+    for (int q = 0; q < nrot; ++q) {
+      T* pa = Gi + (long long)rp[q] * n + c;
+      T* pb = Gi + (long long)rq[q] * n + c;
+      const T a = *pa, b = *pb;
+      *pa = rc[q] * a + rsn[q] * b;
+      *pb = rc[q] * b - rsn[q] * a;
+    }
+  for (int j = tid; j < k; j += nt) secular_root(j, k, dl, zl, s_rho, ori + j, tv + j);
+  __syncthreads();
+  for (int i = tid; i < k; i += nt) {  // Gu-Eisenstat: every ratio in (0, 1]
+    const T di = dl[i];
+    T prod = ((dl[ori[k - 1]] - di) + tv[k - 1]) / s_rho;
+    for (int j = 0; j < i; ++j) prod *= ((dl[ori[j]] - di) + tv[j]) / (dl[j] - di);
+    for (int j = i + 1; j < k; ++j) prod *= ((dl[ori[j - 1]] - di) + tv[j - 1]) / (dl[j] - di);
+    zl[i] = copysign(tb_sqrt(fmax(prod, T(0))), zl[i]);
+  }
+  __syncthreads();
+  for (int j = tid; j < k; j += nt) {
+    const T bj = dl[ori[j]], tj = tv[j];
+    T s = T(0);
+    for (int i = 0; i < k; ++i) {
+      const T w = zl[i] / ((dl[i] - bj) - tj);
+      s += w * w;
+    }
+    inrm[j] = T(1) / tb_sqrt(s);
+  }
+  __syncthreads();
+  // roots: Go rows lo .. lo+k-1; deflated: rows lo+k .. hi-1 copied
+  dc_gemm<T>(k, k, m,
+             [&](int j, int i) { return zl[i] / ((dl[i] - dl[ori[j]]) - tv[j]) * inrm[j]; },
+             Gi, srow, Go, lo, lo, n, Wt, Bt);
+  for (long long x = tid; x < (long long)(m - k) * m; x += nt) {
+    const int q = (int)(x / m), c = lo + (int)(x % m);
+    Go[(long long)(lo + k + q) * n + c] = Gi[(long long)rowof[ndl[k + q]] * n + c];
+  }
+  __syncthreads();
+  for (int j = tid; j < m; j += nt) d[lo + j] = j < k ? dl[ori[j]] + tv[j] : delta[ndl[j]];
+  __syncthreads();
+}
+
+// Eigenvalues (d) and eigenvector rows (Zc <- G Zc) of the tridiagonal
+// (d, e) by the merge tree; G0 and G1 are n x n buffers, ws dc_ws_elems(n).
+template <typename T>
+__device__ void dc_solve(T* d, T* e, T* Z, T* G0, T* G1, int n, T* ws, T* red) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  int depth = 0;
+  while ((1 << depth) < n) ++depth;
+  // tear every node (rho = |e[t-1]| off both neighbours) and place the leaves
+  for (int dep = 0; dep < depth; ++dep) {
+    for (int b = tid; b < (1 << dep); b += nt) {
+      int lo = 0, hi = n;
+      for (int l = 0; l < dep; ++l) {
+        const int mid = (lo + hi) >> 1;
+        if ((b >> (dep - 1 - l)) & 1) lo = mid; else hi = mid;
+      }
+      if (hi - lo < 2) continue;
+      const int t = (lo + hi) >> 1;
+      const T rho = tb_abs(e[t - 1]);
+      d[t - 1] -= rho;  // each index is the end of at most one tear on each side
+      d[t] -= rho;
+    }
+    __syncthreads();
+  }
+  for (int i = tid; i < n; i += nt) {
+    G0[(long long)i * n + i] = T(1);
+    G1[(long long)i * n + i] = T(1);
+  }
+  __syncthreads();
+  for (int dep = depth - 1; dep >= 0; --dep) {
+    T* Gi = ((depth - dep - 1) & 1) ? G1 : G0;
+    T* Go = ((depth - dep) & 1) ? G1 : G0;
+    for (int b = 0; b < (1 << dep); ++b) {
+      int lo = 0, hi = n;
+      for (int l = 0; l < dep; ++l) {
+        const int mid = (lo + hi) >> 1;
+        if ((b >> (dep - 1 - l)) & 1) lo = mid; else hi = mid;
+      }
+      if (hi - lo < 2) continue;
+      dc_merge<T>(d, e, n, lo, (lo + hi) >> 1, hi, Gi, Go, ws, red);
+    }
+  }
+  // Zc <- G Zc into the free buffer, then back
+  T* G = (depth & 1) ? G1 : G0;
+  T* F = (depth & 1) ? G0 : G1;
+  T* Wt = ws;
+  T* Bt = Wt + 64 * kDcK;
+  dc_gemm<T>(n, n, n, [&](int j, int i) { return G[(long long)j * n + i]; }, Z, nullptr, F, 0, 0, n, Wt, Bt);
+  __syncthreads();
+  for (long long x = tid; x < (long long)n * n; x += nt) Z[x] = F[x];
+  __syncthreads();
+}
+
 template <typename T>
 __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab, T* __restrict__ Zb,
-                                          double* __restrict__ wout, int* __restrict__ perm,
+                                          T* __restrict__ Sb, double* __restrict__ wout, int* __restrict__ perm,
                                           int* __restrict__ status, const int* __restrict__ active) {
   const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;  // largest structures first
   if (active && !active[m]) return;
@@ -604,7 +924,15 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
     }
   }
 
-  // ---- 3. implicit QL, producer (warp 0) / consumers (warps 1..)
+  // ---- 3a. divide and conquer when a scratch buffer is given (A is free now)
+  if (Sb && n >= kDcMin && dc_ws_elems<T>(n) <= (5 + 2 * kRing) * n) {
+    if (tid == 0) { q_fail = 0; e[n - 1] = T(0); }
+    __syncthreads();
+    dc_solve<T>(d, e, Z, A, Sb + mo, n, tau, red);
+    for (int i = tid; i < n; i += nt)
+      if (!(tb_abs(d[i]) < T(1e30))) q_fail = 1;  // non-finite input
+  } else {
+  // ---- 3b. implicit QL, producer (warp 0) / consumers (warps 1..)
   if (tid == 0) { q_full = 0; q_end = 0; q_fail = 0; e[n - 1] = T(0); }
   if (tid < kEigThreads / 32) q_done[tid] = 0;
   __syncthreads();
@@ -793,6 +1121,7 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
       }
     }
   }
+  }
   __syncthreads();
   if (q_fail) {
     if (tid == 0) status[m] = kStEigenFailed;  // k_fermi retires the structure
@@ -814,16 +1143,17 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
 }  // namespace
 
 __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __restrict__ Ab, double* __restrict__ Zb,
-                                                      double* __restrict__ wout, int* __restrict__ perm,
-                                                      int* __restrict__ status, const int* __restrict__ active) {
-  syev_body<double>(B, Ab, Zb, wout, perm, status, active);
+                                                      double* __restrict__ Sb, double* __restrict__ wout,
+                                                      int* __restrict__ perm, int* __restrict__ status,
+                                                      const int* __restrict__ active) {
+  syev_body<double>(B, Ab, Zb, Sb, wout, perm, status, active);
 }
 
 __global__ void __launch_bounds__(kEigThreads, 4) k_syev_f32(DevBatch B, float* __restrict__ Ab,
                                                           float* __restrict__ Zb, double* __restrict__ wout,
                                                           int* __restrict__ perm, int* __restrict__ status,
                                                           const int* __restrict__ active) {
-  syev_body<float>(B, Ab, Zb, wout, perm, status, active);
+  syev_body<float>(B, Ab, Zb, nullptr, wout, perm, status, active);
 }
 
 }  // namespace tb

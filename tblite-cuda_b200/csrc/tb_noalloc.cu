@@ -137,7 +137,7 @@ extern "C" tb_status tb_sygvd_noalloc(int32_t n, const double* H, const double* 
                                  v.active);
   k_gemm<<<ntiles, kGemmThreads, 0, st>>>(B, v.tiles, ntiles, v.X, 1, v.W, 0, nullptr, nullptr, nullptr, v.A, 1.0, 0.0,
                                  v.active);
-  k_syev<<<1, kEigThreads, syev_smem_bytes(n), st>>>(B, v.A, v.Z, w, v.perm, v.status, v.active);
+  k_syev<<<1, kEigThreads, syev_smem_bytes(n), st>>>(B, v.A, v.Z, v.W, w, v.perm, v.status, v.active);
   // C = X Z with the eigenvectors in ascending order
   k_gemm<<<ntiles, kGemmThreads, 0, st>>>(B, v.tiles, ntiles, v.X, 0, v.Z, 1, v.perm, nullptr, nullptr, C, 1.0, 0.0,
                                  v.active);

@@ -146,6 +146,34 @@ def test_sygvd_tridiagonal_panel_sizes(oracle):
         np.testing.assert_allclose(H @ C, C * w, atol=1e-11)
 
 
+def test_sygvd_divide_and_conquer():
+    # structures of 128 AOs and more take the divide-and-conquer tridiagonal
+    # solver: random spectra, 8-fold degenerate ones, nearly decoupled blocks
+    # (every merge deflates) and a multiple of the identity
+    rng = np.random.default_rng(9)
+    Hs = []
+    for n in (128, 129, 200, 256, 384):
+        M = rng.normal(size=(n, n))
+        Hs.append(0.5 * (M + M.T))
+    n = 256
+    Qm, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    Hs.append(Qm @ np.diag(np.repeat(np.arange(n // 8, dtype=float), 8)) @ Qm.T)
+    blocks = [rng.normal(size=(40, 40)) for _ in range(4)]
+    Bd = np.zeros((160, 160))
+    for i, b in enumerate(blocks):
+        Bd[40 * i:40 * i + 40, 40 * i:40 * i + 40] = b + b.T
+    Bd += 1e-13 * rng.normal(size=(160, 160))
+    Hs.append(0.5 * (Bd + Bd.T))
+    Hs.append(2.5 * np.eye(140))
+    st, out = capi.sygvd_batch(Hs, [np.eye(len(H)) for H in Hs])
+    assert st == capi.TB_OK
+    for H, (w, C) in zip(Hs, out):
+        scale = max(1.0, np.max(np.abs(H)))
+        np.testing.assert_allclose(w, np.linalg.eigvalsh(H), atol=1e-12 * scale * len(w) ** 0.5)
+        np.testing.assert_allclose(C.T @ C, np.eye(len(w)), atol=1e-12)
+        np.testing.assert_allclose(H @ C, C * w, atol=1e-12 * scale * len(w) ** 0.5)
+
+
 def test_sygvd_not_spd_status():
     st, _ = capi.sygvd_batch([np.eye(3)], [-np.eye(3)])
     assert st == capi.TB_NOT_SPD
