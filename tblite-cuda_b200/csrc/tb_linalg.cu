@@ -487,7 +487,9 @@ __device__ void secular_root(int j, int k, const T* dl, const T* z, T rho, int* 
 
 // Out[(r0 + j) ld + c0 + c] = sum_i gen(j, i) In[(srow ? srow[i] : i) ld + c0 + c]
 // for j < nrow, c < ncol, i < kdim: 64 x 64 output tiles, 4 x 4 per thread,
-// slabs of kDcK staged in shared memory (Wt: 64 x kDcK, Bt: kDcK x 64).
+// slabs of kDcK staged in shared memory (Wt: 64 x kDcK, Bt: kDcK x 64).  The
+// next slab (its loads and generated entries) is fetched into registers while
+// the current one is multiplied.
 template <typename T, typename Gen>
 __device__ void dc_gemm(int nrow, int kdim, int ncol, Gen gen, const T* In, const int* srow, T* Out, int r0, int c0,
                         int ld, T* Wt, T* Bt) {
@@ -499,14 +501,27 @@ __device__ void dc_gemm(int nrow, int kdim, int ncol, Gen gen, const T* In, cons
       for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
-      for (int i0 = 0; i0 < kdim; i0 += kDcK) {
-        for (int x = tid; x < 64 * kDcK; x += kEigThreads) {
+      constexpr int kPer = 64 * kDcK / kEigThreads;  // slab entries per thread
+      T wr[kPer], br[kPer];
+      auto fetch = [&](int i0) {
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+          const int x = tid + u * kEigThreads;
           const int jj = x / kDcK, kk = x - jj * kDcK, j = j0 + jj, i = i0 + kk;
-          Wt[x] = (j < nrow && i < kdim) ? gen(j, i) : T(0);
+          wr[u] = (j < nrow && i < kdim) ? gen(j, i) : T(0);
           const int kb = x >> 6, cc = x & 63, ib = i0 + kb;
-          Bt[x] = (ib < kdim && cb + cc < ncol) ? In[(long long)(srow ? srow[ib] : ib) * ld + c0 + cb + cc] : T(0);
+          br[u] = (ib < kdim && cb + cc < ncol) ? In[(long long)(srow ? srow[ib] : ib) * ld + c0 + cb + cc] : T(0);
+        }
+      };
+      fetch(0);
+      for (int i0 = 0; i0 < kdim; i0 += kDcK) {
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+          Wt[tid + u * kEigThreads] = wr[u];
+          Bt[tid + u * kEigThreads] = br[u];
         }
         __syncthreads();
+        if (i0 + kDcK < kdim) fetch(i0 + kDcK);
 #pragma unroll
         for (int kk = 0; kk < kDcK; ++kk) {
           T av[4], bv[4];
@@ -536,10 +551,14 @@ __device__ void dc_gemm(int nrow, int kdim, int ncol, Gen gen, const T* In, cons
 }
 
 // One merge of the node [lo, hi) torn at t: children's G blocks in Gi (the
-// node's diagonal block; Gi is overwritten), eigenvalues in d[lo, hi); result
-// in the same block of Go and in d[lo, hi).  ws: dc_ws_elems(hi - lo) T.
+// node's diagonal block), eigenvalues in d[lo, hi).  The rows lo..hi-1 of V
+// (columns vc0 .. vc0+vcols-1; V = Gi itself, or the children's eigenvectors
+// already applied to Zc) are combined into the same rows of Out and the
+// merged eigenvalues written to d[lo, hi).  V is overwritten.  ws:
+// dc_ws_elems(hi - lo) T.
 template <typename T>
-__device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, T* Go, T* ws, T* red) {
+__device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, T* V, int vc0, int vcols, T* Out,
+                         T* ws, T* red) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int m = hi - lo;
   T* delta = ws;          // m: sorted eigenvalues (rotated pairs updated)
@@ -564,10 +583,11 @@ __device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, 
   const T ev = e[t - 1];
   const T rho = tb_abs(ev), sg = ev >= T(0) ? T(1) : T(-1);
   // children's blocks are diagonal sub-blocks: clear the rest of the node's block
-  for (long long x = tid; x < (long long)m * m; x += nt) {
-    const int r = lo + (int)(x / m), c = lo + (int)(x % m);
-    if ((r < t) != (c < t)) Gi[(long long)r * n + c] = T(0);
-  }
+  if (V == Gi)
+    for (long long x = tid; x < (long long)m * m; x += nt) {
+      const int r = lo + (int)(x / m), c = lo + (int)(x % m);
+      if ((r < t) != (c < t)) Gi[(long long)r * n + c] = T(0);
+    }
   // z and its norm
   T part = T(0);
   for (int r = lo + tid; r < hi; r += nt) {
@@ -623,10 +643,10 @@ __device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, 
   __syncthreads();
   const int k = s_k, nrot = s_nrot;
   // close-pair rotations on the rows, one thread per column, in order
-  for (int c = lo + tid; c < hi; c += nt)
+  for (int c = vc0 + tid; c < vc0 + vcols; c += nt)
     for (int q = 0; q < nrot; ++q) {
-      T* pa = Gi + (long long)rp[q] * n + c;
-      T* pb = Gi + (long long)rq[q] * n + c;
+      T* pa = V + (long long)rp[q] * n + c;
+      T* pb = V + (long long)rq[q] * n + c;
       const T a = *pa, b = *pb;
       *pa = rc[q] * a + rsn[q] * b;
       *pb = rc[q] * b - rsn[q] * a;
@@ -651,69 +671,163 @@ __device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, 
     inrm[j] = T(1) / tb_sqrt(s);
   }
   __syncthreads();
-  // roots: Go rows lo .. lo+k-1; deflated: rows lo+k .. hi-1 copied
-  dc_gemm<T>(k, k, m,
+  // roots: Out rows lo .. lo+k-1; deflated: rows lo+k .. hi-1 copied
+  dc_gemm<T>(k, k, vcols,
              [&](int j, int i) { return zl[i] / ((dl[i] - dl[ori[j]]) - tv[j]) * inrm[j]; },
-             Gi, srow, Go, lo, lo, n, Wt, Bt);
-  for (long long x = tid; x < (long long)(m - k) * m; x += nt) {
-    const int q = (int)(x / m), c = lo + (int)(x % m);
-    Go[(long long)(lo + k + q) * n + c] = Gi[(long long)rowof[ndl[k + q]] * n + c];
+             V, srow, Out, lo, vc0, n, Wt, Bt);
+  for (long long x = tid; x < (long long)(m - k) * vcols; x += nt) {
+    const int q = (int)(x / vcols), c = vc0 + (int)(x % vcols);
+    Out[(long long)(lo + k + q) * n + c] = V[(long long)rowof[ndl[k + q]] * n + c];
   }
   __syncthreads();
   for (int j = tid; j < m; j += nt) d[lo + j] = j < k ? dl[ori[j]] + tv[j] : delta[ndl[j]];
   __syncthreads();
 }
 
+constexpr int kDcLeaf = 16;  // leaves of the merge tree: at most this many rows, solved by one warp
+
+// Leaf [lo, lo+s) of the tree (s <= kDcLeaf) by one warp: implicit QL with
+// Wilkinson shifts (the same sweep as the k_syev producer) on lane 0 over
+// d[lo..] and a private copy of the leaf's off-diagonal, each sweep's
+// rotations then applied by lanes (one per column) to the rows of the leaf's
+// eigenvector block U in shared memory; U is written to G's diagonal block.
+// Returns false if an eigenvalue took more than 60 sweeps.
+static_assert((kEigThreads / 32) * (kDcLeaf * kDcLeaf + 3 * kDcLeaf) <= (5 + 2 * kRing) * kDcMin,
+              "leaf workspace exceeds the free shared memory");
+
+template <typename T>
+__device__ bool dc_leaf(T* d, const T* e, int lo, int s, T* U, T* le, T* rcs, T* G, int n) {
+  const int lane = threadIdx.x & 31;
+  const T eps = Eps<T>::v;
+  for (int x = lane; x < s * s; x += 32) U[x] = (x / s == x % s) ? T(1) : T(0);
+  for (int i = lane; i < s; i += 32) le[i] = i < s - 1 ? e[lo + i] : T(0);
+  __syncwarp();
+  T* dd = d + lo;
+  bool ok = true;
+  for (int l = 0; l < s && ok; ++l) {
+    int iter = 0;
+    for (;;) {
+      int mq = s - 1;
+      for (int i = l; i < s - 1; ++i)
+        if (tb_abs(le[i]) <= eps * (tb_abs(dd[i]) + tb_abs(dd[i + 1]))) { mq = i; break; }
+      if (mq == l) break;
+      if (++iter > 60) { ok = false; break; }
+      int cnt = 0;
+      if (lane == 0) {
+        T g = (dd[l + 1] - dd[l]) / (T(2) * le[l]);
+        T r = tb_sqrt(g * g + T(1));
+        g = dd[mq] - dd[l] + le[l] / (g + (g >= T(0) ? r : -r));
+        T sn = T(1), c = T(1), pp = T(0);
+        bool underflow = false;
+        for (int i = mq - 1; i >= l; --i) {
+          const T f = sn * le[i], bb = c * le[i];
+          const T rr2 = f * f + g * g;
+          if (rr2 == T(0)) { dd[i + 1] -= pp; le[mq] = T(0); underflow = true; break; }
+          const T ri = chain_rsqrt(rr2);
+          r = rr2 * ri;
+          le[i + 1] = r;
+          sn = f * ri;
+          c = g * ri;
+          g = dd[i + 1] - pp;
+          r = (dd[i] - g) * sn + T(2) * c * bb;
+          pp = sn * r;
+          dd[i + 1] = g + pp;
+          g = c * r - bb;
+          rcs[2 * cnt] = c;
+          rcs[2 * cnt + 1] = sn;
+          ++cnt;
+        }
+        if (!underflow) { dd[l] -= pp; le[l] = g; le[mq] = T(0); }
+      }
+      cnt = __shfl_sync(0xffffffffu, cnt, 0);
+      __syncwarp();
+      if (lane < s) {  // rotation t acts on rows i = mq-1-t and i+1 of U
+        for (int t = 0; t < cnt; ++t) {
+          const int i = mq - 1 - t;
+          const T c = rcs[2 * t], sn = rcs[2 * t + 1];
+          const T x = U[i * s + lane], y = U[(i + 1) * s + lane];
+          U[(i + 1) * s + lane] = sn * x + c * y;
+          U[i * s + lane] = c * x - sn * y;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  for (int x = lane; x < s * s; x += 32) G[(long long)(lo + x / s) * n + lo + x % s] = U[x];
+  __syncwarp();
+  return ok;
+}
+
+// Node b of depth dep of the halving tree: [lo, hi); *plen = its parent's size.
+__device__ inline void dc_node(int n, int dep, int b, int* lo_out, int* hi_out, int* plen) {
+  int lo = 0, hi = n, pl = n + 1;
+  for (int l = 0; l < dep; ++l) {
+    const int mid = (lo + hi) >> 1;
+    pl = hi - lo;
+    if ((b >> (dep - 1 - l)) & 1) lo = mid; else hi = mid;
+  }
+  *lo_out = lo; *hi_out = hi; *plen = pl;
+}
+
 // Eigenvalues (d) and eigenvector rows (Zc <- G Zc) of the tridiagonal
 // (d, e) by the merge tree; G0 and G1 are n x n buffers, ws dc_ws_elems(n).
+// Returns false if a leaf failed to converge.
 template <typename T>
-__device__ void dc_solve(T* d, T* e, T* Z, T* G0, T* G1, int n, T* ws, T* red) {
-  const int tid = threadIdx.x, nt = blockDim.x;
-  int depth = 0;
-  while ((1 << depth) < n) ++depth;
-  // tear every node (rho = |e[t-1]| off both neighbours) and place the leaves
+__device__ bool dc_solve(T* d, T* e, T* Z, T* G0, T* G1, int n, T* ws, T* red) {
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+  __shared__ int s_fail;
+  int depth = 0;  // nodes at this depth have at most kDcLeaf rows
+  while (((n + (1 << depth) - 1) >> depth) > kDcLeaf) ++depth;
+  if (tid == 0) s_fail = 0;
+  // tear every internal node (rho = |e[t-1]| off both neighbours)
   for (int dep = 0; dep < depth; ++dep) {
     for (int b = tid; b < (1 << dep); b += nt) {
-      int lo = 0, hi = n;
-      for (int l = 0; l < dep; ++l) {
-        const int mid = (lo + hi) >> 1;
-        if ((b >> (dep - 1 - l)) & 1) lo = mid; else hi = mid;
-      }
-      if (hi - lo < 2) continue;
+      int lo, hi, pl;
+      dc_node(n, dep, b, &lo, &hi, &pl);
+      if (hi - lo <= kDcLeaf) continue;
       const int t = (lo + hi) >> 1;
       const T rho = tb_abs(e[t - 1]);
-      d[t - 1] -= rho;  // each index is the end of at most one tear on each side
+      d[t - 1] -= rho;  // nodes of one depth are disjoint
       d[t] -= rho;
     }
     __syncthreads();
   }
-  for (int i = tid; i < n; i += nt) {
-    G0[(long long)i * n + i] = T(1);
-    G1[(long long)i * n + i] = T(1);
-  }
-  __syncthreads();
-  for (int dep = depth - 1; dep >= 0; --dep) {
+  T* U = ws + wid * (kDcLeaf * kDcLeaf + 3 * kDcLeaf);  // per warp: U, off-diagonal, rotations
+  for (int dep = depth; dep >= 0; --dep) {
     T* Gi = ((depth - dep - 1) & 1) ? G1 : G0;
     T* Go = ((depth - dep) & 1) ? G1 : G0;
-    for (int b = 0; b < (1 << dep); ++b) {
-      int lo = 0, hi = n;
-      for (int l = 0; l < dep; ++l) {
-        const int mid = (lo + hi) >> 1;
-        if ((b >> (dep - 1 - l)) & 1) lo = mid; else hi = mid;
+    // leaves of this depth, one warp each
+    for (int b = wid; b < (1 << dep); b += nw) {
+      int lo, hi, pl;
+      dc_node(n, dep, b, &lo, &hi, &pl);
+      if (hi - lo < 1 || hi - lo > kDcLeaf || pl <= kDcLeaf) continue;
+      if (!dc_leaf<T>(d, e, lo, hi - lo, U, U + kDcLeaf * kDcLeaf, U + kDcLeaf * kDcLeaf + kDcLeaf, Go, n) && lane == 0)
+        s_fail = 1;
+    }
+    __syncthreads();
+    if (dep > 0) {
+      for (int b = 0; b < (1 << dep); ++b) {
+        int lo, hi, pl;
+        dc_node(n, dep, b, &lo, &hi, &pl);
+        if (hi - lo <= kDcLeaf) continue;
+        dc_merge<T>(d, e, n, lo, (lo + hi) >> 1, hi, Gi, Gi, lo, hi - lo, Go, ws, red);
       }
-      if (hi - lo < 2) continue;
-      dc_merge<T>(d, e, n, lo, (lo + hi) >> 1, hi, Gi, Go, ws, red);
+    } else {
+      // root: Y = diag(G_left, G_right) Zc into the free buffer, then the
+      // merge combines rows of Y straight into Zc
+      const int t = n >> 1;
+      T* Wt = ws;
+      T* Bt = Wt + 64 * kDcK;
+      for (int h = 0; h < 2; ++h) {
+        const int lc = h ? t : 0, sz = h ? n - t : t;
+        dc_gemm<T>(sz, sz, n, [&](int j, int i) { return Gi[(long long)(lc + j) * n + lc + i]; },
+                   Z + (long long)lc * n, nullptr, Go, lc, 0, n, Wt, Bt);
+      }
+      __syncthreads();
+      dc_merge<T>(d, e, n, 0, t, n, Gi, Go, 0, n, Z, ws, red);
     }
   }
-  // Zc <- G Zc into the free buffer, then back
-  T* G = (depth & 1) ? G1 : G0;
-  T* F = (depth & 1) ? G0 : G1;
-  T* Wt = ws;
-  T* Bt = Wt + 64 * kDcK;
-  dc_gemm<T>(n, n, n, [&](int j, int i) { return G[(long long)j * n + i]; }, Z, nullptr, F, 0, 0, n, Wt, Bt);
-  __syncthreads();
-  for (long long x = tid; x < (long long)n * n; x += nt) Z[x] = F[x];
-  __syncthreads();
+  return s_fail == 0;
 }
 
 template <typename T>
@@ -928,9 +1042,9 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
   if (Sb && n >= kDcMin && dc_ws_elems<T>(n) <= (5 + 2 * kRing) * n) {
     if (tid == 0) { q_fail = 0; e[n - 1] = T(0); }
     __syncthreads();
-    dc_solve<T>(d, e, Z, A, Sb + mo, n, tau, red);
+    const bool conv = dc_solve<T>(d, e, Z, A, Sb + mo, n, tau, red);
     for (int i = tid; i < n; i += nt)
-      if (!(tb_abs(d[i]) < T(1e30))) q_fail = 1;  // non-finite input
+      if (!conv || !(tb_abs(d[i]) < T(1e30))) q_fail = 1;  // a leaf did not converge, or non-finite input
   } else {
   // ---- 3b. implicit QL, producer (warp 0) / consumers (warps 1..)
   if (tid == 0) { q_full = 0; q_end = 0; q_fail = 0; e[n - 1] = T(0); }
