@@ -255,14 +255,15 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
 //  4. Ascending order by rank (ties by index).
 namespace {
 
-constexpr int kWalkBatch = 12;  // rows per load batch in the Householder column walk
 // Tridiagonalisation panel: reflectors per panel (2 panel n <= ring) and rows
 // per load batch of the panel-closing walk.  FP64 moves twice the bytes per
 // element, so the walk is traffic-bound and wide panels pay; in FP32 a panel
 // of one (each step's update fused with the next product) is as fast.
 template <typename T> struct PanelCfg;
-template <> struct PanelCfg<double> { static constexpr int width = 8, batch = 4; };
+template <> struct PanelCfg<double> { static constexpr int width = 8, batch = 12; };
 template <> struct PanelCfg<float> { static constexpr int width = 1, batch = 12; };
+// rows per load batch of the read-only Householder column walk
+template <typename T> struct WalkCfg { static constexpr int batch = sizeof(T) == 8 ? 24 : 12; };
 static_assert(PanelCfg<double>::width <= kRing && PanelCfg<float>::width <= kRing, "panel exceeds the ring");
 constexpr int kQBlock = 16;     // reflectors per compact-WY block of the Q accumulation
 constexpr int kWaveK = 4;            // QL sweeps applied per pass over Zc
@@ -326,11 +327,14 @@ __device__ void reflector(T* A, int n, int k, T* v, T* tau, T* e, T* red, T* sh)
 // Column walk over the block rows r0..r0+nr-1, columns c0..c0+nc-1 of a
 // row-major matrix M: optionally M[r][c] -= a_r b_c + b_r a_c (with a, b
 // indexed from the block's origin), and out_c = scale * sum_r M_new[r][c] x_r.
-// One thread per column; rows are loaded in batches of kWalkBatch before any
-// of them is written back, so a batch costs about one L2 round trip.
+// One thread per column; rows are loaded in batches of WalkCfg<T>::batch before any
+// of them is written back, so a batch costs about one L2 round trip.  Kept
+// out of line (as is panel_walk) so that its batch registers are allocated
+// apart from the rest of the eigensolver.
 template <typename T>
-__device__ void colwalk(T* M, int n, int r0, int nr, int c0, int nc, bool upd, const T* a,
+__device__ __noinline__ void colwalk(T* M, int n, int r0, int nr, int c0, int nc, bool upd, const T* a,
                         const T* b, int aoff, const T* x, T* out, T scale) {
+  constexpr int kWalkBatch = WalkCfg<T>::batch;
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int jj = tid; jj < nc; jj += nt) {
     const int c = c0 + jj;
@@ -363,7 +367,7 @@ __device__ void colwalk(T* M, int n, int r0, int nr, int c0, int nc, bool upd, c
 // index), and out_c = scale * sum_r M_new[r][c] x_{r-r0}.  One thread per
 // column keeps its column's pair entries in registers.
 template <typename T>
-__device__ void panel_walk(T* M, int n, int r0, int nm, const T* PV, const T* PW, const T* x, T* out, T scale) {
+__device__ __noinline__ void panel_walk(T* M, int n, int r0, int nm, const T* PV, const T* PW, const T* x, T* out, T scale) {
   constexpr int kPanel = PanelCfg<T>::width, kPanelBatch = PanelCfg<T>::batch;
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int jj = tid; jj < nm; jj += nt) {
