@@ -327,7 +327,7 @@ def main():
     ent = tr.get(name) if isinstance(tr, dict) else None
     roof["traffic"] = ent.get("bytes_per_launch") if isinstance(ent, dict) else None
     if roof["traffic"] is not None:
-        roof["traffic_source"] = "profiles/ncu_traffic.json (ncu dram bytes, small case scaled by sum N^2)"
+        roof["traffic_source"] = "profiles/ncu_traffic.json: " + str(ent.get("capture", "ncu dram bytes"))
     total_ms = sum(v[1] for v in prof_tot.values())
     kernels = {k: {"launches": v[0], "ms": round(v[1], 3), "share": round(v[1] / total_ms, 4)}
                for k, v in sorted(prof_tot.items(), key=lambda kv: -kv[1][1])}
