@@ -660,11 +660,13 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
   TB_K("gemm_tc", 2.0 * n3_lo, 1,
        k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, lo, S.status));
   TB_K("gemm", 2.0 * n3_hi, 1,
-       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi));
+       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi,
+                                                  kGemmKUpToJ));
   TB_K("gemm_tc", 2.0 * n3_lo, 1,
        k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, lo, S.status));
   TB_K("gemm", 2.0 * n3_hi, 1,
-       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, hi));
+       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, hi,
+                                                  kGemmKUpToI | kGemmSym));
   // FP32 eigensolve of every active structure
   TB_K("convert", 0, 0, k_to_f32<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, b->Af, S.active));
   TB_K("syev_f32", 4.0 * (n3_lo + n3_hi), 1,
@@ -708,12 +710,14 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
   TB_K("gemm_tc", 2.0 * n3_lo, 1,
        k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->X, 0, b->Vn, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, lo, S.status));
   TB_K("gemm", 2.0 * n3_hi, 1,
-       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 0, b->Z, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi));
+       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 0, b->Z, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi,
+                                                  kGemmKFromI));
   // P = C diag(f) C^T
   TB_K("gemm_tc", 2.0 * n2occ_lo, 1,
        k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.0, 0.0, lo, S.status));
   TB_K("gemm", 2.0 * n2occ_hi, 1,
-       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.0, 0.0, hi));
+       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.0, 0.0, hi,
+                                                  kGemmSym));
   return TB_OK;
 }
 
@@ -955,10 +959,10 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
     // F' = X^T F X  (T = F X in W, then F' into F): 2 x 2N^3
     TB_K("gemm", 2.0 * n3, 1,
          k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->F, 0, b->X, 0, nullptr, nullptr, nullptr,
-                                           b->W, 1.0, 0.0, S.active));
+                                           b->W, 1.0, 0.0, S.active, kGemmKUpToJ));
     TB_K("gemm", 2.0 * n3, 1,
          k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 1, b->W, 0, nullptr, nullptr, nullptr,
-                                           b->F, 1.0, 0.0, S.active));
+                                           b->F, 1.0, 0.0, S.active, kGemmKUpToI | kGemmSym));
     // symmetric eigensolve with vectors: canonical 4 N^3
     TB_K("syev", 4.0 * n3, 1,
          k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->W, b->w, b->perm, S.status, S.active));
@@ -978,10 +982,10 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
     // C = X Z (eigenvectors in ascending order through perm): 2N^3; P = C diag(f) C^T: 2 N^2 n_occ
     TB_K("gemm", 2.0 * n3, 1,
          k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr,
-                                           b->W, 1.0, 0.0, S.active));
+                                           b->W, 1.0, 0.0, S.active, kGemmKFromI));
     TB_K("gemm", 2.0 * n2occ, 1,
          k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim,
-                                           b->P, 1.0, 0.0, S.active));
+                                           b->P, 1.0, 0.0, S.active, kGemmSym));
   } else {
     const tb_status ms = mixed_core(b, st, n3_lo, n3_hi, n2occ_lo, n2occ_hi, gemm_grid, fermi_smem);
     if (ms != TB_OK) return ms;
@@ -1518,8 +1522,10 @@ tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const 
                                         mb.ms.status + m);
     if (!e.empty()) return fail(TB_CUDA_ERROR, "library Cholesky: " + e);
   }
-  k_gemm<<<grid, kGemmThreads>>>(B, mb.d_tiles, nt, mb.F, 0, mb.X, 0, nullptr, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);
-  k_gemm<<<grid, kGemmThreads>>>(B, mb.d_tiles, nt, mb.X, 1, mb.W, 0, nullptr, nullptr, nullptr, mb.F, 1.0, 0.0, mb.ms.active);
+  k_gemm<<<grid, kGemmThreads>>>(B, mb.d_tiles, nt, mb.F, 0, mb.X, 0, nullptr, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active,
+                                 kGemmKUpToJ);
+  k_gemm<<<grid, kGemmThreads>>>(B, mb.d_tiles, nt, mb.X, 1, mb.W, 0, nullptr, nullptr, nullptr, mb.F, 1.0, 0.0, mb.ms.active,
+                                 kGemmKUpToI | kGemmSym);
   const size_t smem = syev_smem_bytes(std::max(mb.nmax_in, 1));
   {
     const tb_status ss = raise_smem_limits();
@@ -1536,7 +1542,8 @@ tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const 
                                       mb.lib_bytes, mb.lib_info + 2 * k + 1, mb.ms.status + m);
     if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
   }
-  k_gemm<<<grid, kGemmThreads>>>(B, mb.d_tiles, nt, mb.X, 0, mb.Z, 1, mb.perm, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active);
+  k_gemm<<<grid, kGemmThreads>>>(B, mb.d_tiles, nt, mb.X, 0, mb.Z, 1, mb.perm, nullptr, nullptr, mb.W, 1.0, 0.0, mb.ms.active,
+                                 kGemmKFromI);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(TB_CUDA_ERROR, cudaGetErrorString(e));
   TB_CUDA(cudaMemcpy(w, mb.w, mb.no * 8, cudaMemcpyDeviceToHost));

@@ -79,9 +79,11 @@ cudaError_t launch_integrals(const DevParams& P, const DevBatch& B, const int* n
 // linear algebra
 __global__ void k_cholesky(DevBatch B, const double* S, double* W, int* status, const int* active);
 __global__ void k_trinv(DevBatch B, const double* W, double* X, const int* status);
+// k_gemm shapes (bit mask): zeros of a triangular factor and symmetric results
+constexpr int kGemmKUpToJ = 1, kGemmKUpToI = 2, kGemmKFromI = 4, kGemmSym = 8;
 __global__ void k_gemm(DevBatch B, const int4* tiles, int ntiles, const double* Ab, int ta, const double* Bb, int tb_,
                        const int* perm, const double* ks, const int* kdim, double* Cb, double alpha, double beta,
-                       const int* active);
+                       const int* active, int shape = 0);
 // Sb: optional n x n scratch per structure (same offsets as Ab); with it,
 // structures of at least 128 AOs take divide and conquer instead of QL
 __global__ void k_syev(DevBatch B, double* Ab, double* Zb, double* Sb, double* wout, int* perm, int* status,

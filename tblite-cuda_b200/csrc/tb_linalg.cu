@@ -86,6 +86,11 @@ __global__ void k_trinv(DevBatch B, const double* __restrict__ W, double* __rest
 // the list (structure, tile row, tile col).  Square n_m x n_m operands with
 // leading dimension n_m at offset moff[m]; K = kdim[m] if kdim != NULL.
 // op(B) may gather its columns through perm (eigenvector reordering).
+// `shape` skips known zeros and redundant tiles: kGemmKUpToJ (op(B) upper
+// triangular: only k < the tile's last column), kGemmKUpToI (op(A) lower
+// triangular: k < its last row), kGemmKFromI (op(A) upper triangular: k >=
+// its first row), kGemmSym (C symmetric: tiles below the diagonal are skipped
+// and every off-diagonal tile is also written transposed).
 // 64 x 64 tiles on the FP64 tensor instruction mma.sync.m8n8k4.f64: four warps,
 // each owning a 32 x 32 quarter as 4 x 4 fragments of 8 x 8 (32 accumulators
 // per lane).  K slabs of 16 are staged by cp.async in a two-stage ring (zero
@@ -117,7 +122,8 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
                                                        const double* __restrict__ Bb, int tb_,
                                                        const int* __restrict__ perm, const double* __restrict__ ks,
                                                        const int* __restrict__ kdim, double* __restrict__ Cb,
-                                                       double alpha, double beta, const int* __restrict__ active) {
+                                                       double alpha, double beta, const int* __restrict__ active,
+                                                       int shape) {
   __shared__ __align__(16) double As[2][GK][GP];
   __shared__ __align__(16) double Bs[2][GK][GP];
   __shared__ __align__(16) double Ks[2][GK];
@@ -129,6 +135,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
     const int4 tl = tiles[t];
     const int m = tl.x;
     if (active && !active[m]) continue;
+    if ((shape & kGemmSym) && tl.z < tl.y) continue;
     const int n = B.ooff[m + 1] - B.ooff[m];
     const int K = kdim ? kdim[m] : n;
     const long long mo = B.moff[m];
@@ -138,6 +145,10 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
     const int* pm = perm ? perm + vo : nullptr;
     const double* kv = ks ? ks + vo : nullptr;
     const int i0 = tl.y * GT, j0 = tl.z * GT;
+    int klo = 0, khi = K;
+    if (shape & kGemmKUpToJ) khi = min(khi, j0 + GT);
+    if (shape & kGemmKUpToI) khi = min(khi, i0 + GT);
+    if (shape & kGemmKFromI) klo = min(i0, K);
     double acc[4][4][2];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
@@ -189,12 +200,12 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
       if (kv && tid < GK) cp_async8(&Ks[buf][tid], k0 + tid < K ? kv + k0 + tid : kv, k0 + tid < K);
       cp_async_commit();
     };
-    const int nk = (K + GK - 1) / GK;
-    if (nk > 0) issue(0, 0);
+    const int nk = khi > klo ? (khi - klo + GK - 1) / GK : 0;
+    if (nk > 0) issue(0, klo);
     for (int kt = 0; kt < nk; ++kt) {
       const int cur = kt & 1;
       if (kt + 1 < nk) {
-        issue(cur ^ 1, (kt + 1) * GK);
+        issue(cur ^ 1, klo + (kt + 1) * GK);
         cp_async_wait<1>();
       } else {
         cp_async_wait<0>();
@@ -229,7 +240,9 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
           const int gj = j0 + wc + 8 * y + 2 * tg + h;
           if (gj >= n) continue;
           double* c = Cb + mo + (long long)gi * n + gj;
-          *c = beta == 0.0 ? alpha * acc[x][y][h] : alpha * acc[x][y][h] + beta * (*c);
+          const double r = beta == 0.0 ? alpha * acc[x][y][h] : alpha * acc[x][y][h] + beta * (*c);
+          *c = r;
+          if ((shape & kGemmSym) && i0 != j0) Cb[mo + (long long)gj * n + gi] = r;
         }
       }
     }

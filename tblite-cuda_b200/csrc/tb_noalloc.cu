@@ -134,13 +134,13 @@ extern "C" tb_status tb_sygvd_noalloc(int32_t n, const double* H, const double* 
   k_trinv<<<1, 256, 0, st>>>(B, v.W, v.X, v.status);
   // A = X^T H X (T = H X kept in W, whose Cholesky factor is no longer needed)
   k_gemm<<<ntiles, kGemmThreads, 0, st>>>(B, v.tiles, ntiles, H, 0, v.X, 0, nullptr, nullptr, nullptr, v.W, 1.0, 0.0,
-                                 v.active);
+                                 v.active, kGemmKUpToJ);
   k_gemm<<<ntiles, kGemmThreads, 0, st>>>(B, v.tiles, ntiles, v.X, 1, v.W, 0, nullptr, nullptr, nullptr, v.A, 1.0, 0.0,
-                                 v.active);
+                                 v.active, kGemmKUpToI | kGemmSym);
   k_syev<<<1, kEigThreads, syev_smem_bytes(n), st>>>(B, v.A, v.Z, v.W, w, v.perm, v.status, v.active);
   // C = X Z with the eigenvectors in ascending order
   k_gemm<<<ntiles, kGemmThreads, 0, st>>>(B, v.tiles, ntiles, v.X, 0, v.Z, 1, v.perm, nullptr, nullptr, C, 1.0, 0.0,
-                                 v.active);
+                                 v.active, kGemmKFromI);
   e = cudaGetLastError();
   if (e != cudaSuccess) return noalloc_fail(TB_CUDA_ERROR, cudaGetErrorString(e));
   int status = 0;
