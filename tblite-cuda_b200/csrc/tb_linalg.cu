@@ -12,10 +12,18 @@
 namespace tb {
 
 // ------------------------------------------------------------ Cholesky
-// Left-looking column Cholesky of the structure's overlap S (row-major),
-// result stored column-major in W (W[k][i] = L[i][k], i >= k).
+// Left-looking Cholesky of the structure's overlap S (row-major), result
+// stored column-major in W (W[k][i] = L[i][k], i >= k), kFactorGroup columns
+// at a time: every row i of the group's columns is first updated with all
+// finished columns k < j0 (each W[k][i] read once per group, the group's
+// entries W[k][j0..] broadcast), then the group is finished column by column
+// with the in-group terms.  Reads of the finished part drop by the group size
+// against a column-at-a-time walk.
+constexpr int kFactorGroup = 16;
+
 __global__ void k_cholesky(DevBatch B, const double* __restrict__ S, double* __restrict__ W,
                            int* __restrict__ status, const int* __restrict__ active) {
+  constexpr int G = kFactorGroup;
   const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;
   if (active && !active[m]) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
@@ -23,41 +31,63 @@ __global__ void k_cholesky(DevBatch B, const double* __restrict__ S, double* __r
   const long long mo = B.moff[m];
   const double* s = S + mo;
   double* w = W + mo;
-  __shared__ double red[32];
+  const int tid = threadIdx.x, nt = blockDim.x;
   __shared__ double ljj;
   __shared__ int bad;
-  if (threadIdx.x == 0) bad = 0;
+  if (tid == 0) bad = 0;
   __syncthreads();
-  for (int j = 0; j < n; ++j) {
-    double part = 0.0;
-    for (int k = threadIdx.x; k < j; k += blockDim.x) {
-      const double x = w[(long long)k * n + j];
-      part += x * x;
-    }
-    const double tot = block_sum(part, red);
-    if (threadIdx.x == 0) {
-      const double d = s[(long long)j * n + j] - tot;
-      if (!(d > 0.0)) { bad = 1; ljj = 1.0; } else ljj = sqrt(d);
-      w[(long long)j * n + j] = ljj;
+  for (int j0 = 0; j0 < n; j0 += G) {
+    const int gq = min(G, n - j0);
+    for (int i = j0 + tid; i < n; i += nt) {
+      double acc[G];
+#pragma unroll
+      for (int q = 0; q < G; ++q) acc[q] = q < gq ? s[(long long)(j0 + q) * n + i] : 0.0;
+      for (int k = 0; k < j0; ++k) {
+        const double a = w[(long long)k * n + i];
+        const double* wk = w + (long long)k * n + j0;
+#pragma unroll
+        for (int q = 0; q < G; ++q)
+          if (q < gq) acc[q] -= a * wk[q];
+      }
+#pragma unroll
+      for (int q = 0; q < G; ++q)
+        if (q < gq) w[(long long)(j0 + q) * n + i] = acc[q];
     }
     __syncthreads();
+    for (int q = 0; q < gq; ++q) {
+      const int j = j0 + q;
+      if (tid == 0) {
+        double d = w[(long long)j * n + j];
+        for (int p = 0; p < q; ++p) {
+          const double l = w[(long long)(j0 + p) * n + j];
+          d -= l * l;
+        }
+        if (!(d > 0.0)) { bad = 1; ljj = 1.0; } else ljj = sqrt(d);
+        w[(long long)j * n + j] = ljj;
+      }
+      __syncthreads();
+      if (bad) break;
+      const double inv = 1.0 / ljj;
+      for (int i = j + 1 + tid; i < n; i += nt) {
+        double t = w[(long long)j * n + i];
+        for (int p = 0; p < q; ++p) t -= w[(long long)(j0 + p) * n + i] * w[(long long)(j0 + p) * n + j];
+        w[(long long)j * n + i] = t * inv;
+      }
+      __syncthreads();
+    }
     if (bad) break;
-    const double inv = 1.0 / ljj;
-    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
-      double t = s[(long long)j * n + i];
-      for (int k = 0; k < j; ++k) t -= w[(long long)k * n + i] * w[(long long)k * n + j];
-      w[(long long)j * n + i] = t * inv;
-    }
-    __syncthreads();
   }
-  if (threadIdx.x == 0 && bad) status[m] = kStNotSpd;
+  if (tid == 0 && bad) status[m] = kStNotSpd;
 }
 
 // X = L^-T (upper triangular, row-major): column c solves L^T x = e_c by
-// backward substitution; all threads walk r = n-1 .. 0 in lock step so that
-// W[r][k] is a broadcast and X[k][c] a coalesced read.
+// backward substitution, kFactorGroup rows at a time from the bottom: the
+// group's rows are first reduced with every finished row below it (each
+// X[k][c] read once per group, the group's L entries broadcast), then solved
+// upwards inside the group.  Each thread owns its columns, so no barrier.
 __global__ void k_trinv(DevBatch B, const double* __restrict__ W, double* __restrict__ X,
                         const int* __restrict__ status) {
+  constexpr int G = kFactorGroup;
   const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;
   if (status[m] != kStOk) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
@@ -67,16 +97,30 @@ __global__ void k_trinv(DevBatch B, const double* __restrict__ W, double* __rest
   double* x = X + mo;
   for (int c0 = 0; c0 < n; c0 += blockDim.x) {
     const int c = c0 + threadIdx.x;
-    for (int r = n - 1; r >= 0; --r) {
-      if (c < n) {
-        if (r > c) {
-          x[(long long)r * n + c] = 0.0;
-        } else {
-          double t = (r == c) ? 1.0 : 0.0;
-          for (int k = r + 1; k <= c; ++k) t -= w[(long long)r * n + k] * x[(long long)k * n + c];
-          x[(long long)r * n + c] = t / w[(long long)r * n + r];
-        }
+    if (c >= n) continue;
+    for (int r1 = n - 1; r1 >= 0; r1 -= G) {
+      const int gq = min(G, r1 + 1);
+      double acc[G];
+#pragma unroll
+      for (int q = 0; q < G; ++q) acc[q] = (q < gq && r1 - q == c) ? 1.0 : 0.0;
+      for (int k = r1 + 1; k <= c; ++k) {  // X[k][c] = 0 for k > c
+        const double xk = x[(long long)k * n + c];
+#pragma unroll
+        for (int q = 0; q < G; ++q)
+          if (q < gq) acc[q] -= w[(long long)(r1 - q) * n + k] * xk;  // W[r][k] = L[k][r]
       }
+      double xg[G];
+#pragma unroll
+      for (int q = 0; q < G; ++q) {
+        if (q >= gq) break;
+        const int r = r1 - q;
+        double t = acc[q];
+        for (int p = 0; p < q; ++p) t -= w[(long long)r * n + (r1 - p)] * xg[p];
+        xg[q] = r > c ? 0.0 : t / w[(long long)r * n + r];
+      }
+#pragma unroll
+      for (int q = 0; q < G; ++q)
+        if (q < gq) x[(long long)(r1 - q) * n + c] = xg[q];
     }
   }
 }
