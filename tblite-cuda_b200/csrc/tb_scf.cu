@@ -154,19 +154,23 @@ __global__ void k_potential(DevParams P, DevBatch B, const double* __restrict__ 
 // ------------------------------------------------------------ Fock build
 // add_pot_to_h1 (src/scf/potential.cu:224-272 with the quoted add_vat_to_vsh,
 // add_vsh_to_vao, add_vao_to_h1 and add_vmp_to_h1): 32x32 tiles, the
-// transposed D/Q elements staged through shared memory.
+// transposed D/Q elements staged through shared memory.  F is symmetric (the
+// moment planes enter as M[mu][nu] v(nu) + M[nu][mu] v(mu)), so only tiles on
+// and above the diagonal are computed; an off-diagonal tile is also written
+// transposed (through the same shared tile), which halves the reads.
 __global__ void __launch_bounds__(256) k_fock(DevBatch B, const int4* __restrict__ tiles, int ntiles,
                                               const double* __restrict__ S, const double* __restrict__ H0,
                                               const double* __restrict__ D, const double* __restrict__ Q,
                                               const double* __restrict__ vsh, const double* __restrict__ vat,
                                               const double* __restrict__ vdp, const double* __restrict__ vqp,
                                               double* __restrict__ F, const int* __restrict__ active) {
-  __shared__ double T[32][33];
+  constexpr int kPl = 3;  // moment planes staged per round
+  __shared__ double T[kPl][32][33];
   const int t = blockIdx.x;
   if (t >= ntiles) return;
   const int4 tl = tiles[t];
   const int m = tl.x;
-  if (!active[m]) return;
+  if (!active[m] || tl.y > tl.z) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
   const long long mo = B.moff[m], nn = (long long)n * n;
   const int o0 = B.ooff[m], a0 = B.aoff[m], s0 = B.soff[m];
@@ -188,29 +192,49 @@ __global__ void __launch_bounds__(256) k_fock(DevBatch B, const int4* __restrict
       acc[r] = H0[e] - S[e] * 0.5 * (vao_mu + vao_nu);
     }
   }
-  // moment planes: -0.5 * (M[k][mu][nu] v[at(nu)][k] + M[k][nu][mu] v[at(mu)][k])
-  for (int plane = 0; plane < 9; ++plane) {
-    const double* M = plane < 3 ? D + 3 * mo + plane * nn : Q + 6 * mo + (plane - 3) * nn;
-    const double* V = plane < 3 ? vdp : vqp;
-    const int stride = plane < 3 ? 3 : 6, k = plane < 3 ? plane : plane - 3;
-    // stage the transposed tile M[c0.., r0..]
+  // moment planes: -0.5 * (M[k][mu][nu] v[at(nu)][k] + M[k][nu][mu] v[at(mu)][k]),
+  // kPl planes per round (their transposed tiles staged together, their
+  // direct elements loaded together) so a round costs one load round trip
+  for (int pl0 = 0; pl0 < 9; pl0 += kPl) {
+    double dir[kPl][4];
     __syncthreads();
-    for (int r = 0; r < 4; ++r) {
-      const int row = c0 + ty + 8 * r, col = r0 + tx;
-      T[ty + 8 * r][tx] = (row < n && col < n) ? M[(long long)row * n + col] : 0.0;
+#pragma unroll
+    for (int q = 0; q < kPl; ++q) {
+      const int plane = pl0 + q;
+      const double* M = plane < 3 ? D + 3 * mo + plane * nn : Q + 6 * mo + (plane - 3) * nn;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int row = c0 + ty + 8 * r, col = r0 + tx;
+        T[q][ty + 8 * r][tx] = (row < n && col < n) ? M[(long long)row * n + col] : 0.0;
+        dir[q][r] = (mu[r] < n && nu_ok) ? M[(long long)mu[r] * n + nu] : 0.0;
+      }
     }
     __syncthreads();
-    const double vnu = nu_ok ? V[stride * (a0 + at_nu) + k] : 0.0;
-    for (int r = 0; r < 4; ++r) {
-      if (mu[r] >= n || !nu_ok) continue;
-      const double vmu = V[stride * (a0 + B.ao_at[o0 + mu[r]]) + k];
-      const double direct = M[(long long)mu[r] * n + nu];
-      const double trans = T[tx][ty + 8 * r];  // M[nu][mu]
-      acc[r] -= 0.5 * (direct * vnu + trans * vmu);
+#pragma unroll
+    for (int q = 0; q < kPl; ++q) {
+      const int plane = pl0 + q;
+      const double* V = plane < 3 ? vdp : vqp;
+      const int stride = plane < 3 ? 3 : 6, k = plane < 3 ? plane : plane - 3;
+      const double vnu = nu_ok ? V[stride * (a0 + at_nu) + k] : 0.0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        if (mu[r] >= n || !nu_ok) continue;
+        const double vmu = V[stride * (a0 + B.ao_at[o0 + mu[r]]) + k];
+        acc[r] -= 0.5 * (dir[q][r] * vnu + T[q][tx][ty + 8 * r] * vmu);  // T: M[nu][mu]
+      }
     }
   }
   for (int r = 0; r < 4; ++r)
     if (mu[r] < n && nu_ok) F[mo + (long long)mu[r] * n + nu] = acc[r];
+  if (r0 != c0) {  // F[c0.., r0..] = this tile transposed
+    __syncthreads();
+    for (int r = 0; r < 4; ++r) T[0][ty + 8 * r][tx] = acc[r];
+    __syncthreads();
+    for (int r = 0; r < 4; ++r) {
+      const int row = c0 + ty + 8 * r, col = r0 + tx;
+      if (row < n && col < n) F[mo + (long long)row * n + col] = T[0][tx][ty + 8 * r];
+    }
+  }
 }
 
 // ------------------------------------------------------------ Fermi
@@ -334,7 +358,22 @@ __global__ void __launch_bounds__(256) k_mulliken_cols(DevBatch B, const int2* _
   double acc[11];
   for (int k = 0; k < 11; ++k) acc[k] = 0.0;
   if (nu < n) {
-    for (int mu = ty; mu < n; mu += 8) {
+    // two rows per step so that 22 independent loads are in flight
+    int mu = ty;
+    for (; mu + 8 < n; mu += 16) {
+      const long long e = (long long)mu * n + nu, e2 = e + 8LL * n;
+      const double p = P[mo + e], p2 = P[mo + e2];
+      double v[11], v2[11];
+      v[0] = S[mo + e]; v2[0] = S[mo + e2];
+      v[1] = H0[mo + e]; v2[1] = H0[mo + e2];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) { v[2 + k] = D[3 * mo + k * nn + e]; v2[2 + k] = D[3 * mo + k * nn + e2]; }
+#pragma unroll
+      for (int k = 0; k < 6; ++k) { v[5 + k] = Q[6 * mo + k * nn + e]; v2[5 + k] = Q[6 * mo + k * nn + e2]; }
+#pragma unroll
+      for (int k = 0; k < 11; ++k) acc[k] += p * v[k] + p2 * v2[k];
+    }
+    for (; mu < n; mu += 8) {
       const long long e = (long long)mu * n + nu;
       const double p = P[mo + e];
       acc[0] += p * S[mo + e];
