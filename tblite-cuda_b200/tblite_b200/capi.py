@@ -112,19 +112,45 @@ def default_options(**kw) -> Options:
     return o
 
 
+def _record_dtype(cls, kinds):
+    """numpy view of a ctypes record array: same offsets and itemsize; pointer
+    fields as unsigned integers (addresses)."""
+    names = [f[0] for f in cls._fields_]
+    return np.dtype({"names": names, "formats": [kinds[k] for k in names],
+                     "offsets": [getattr(cls, k).offset for k in names], "itemsize": C.sizeof(cls)})
+
+
+_STRUCT_DT = _record_dtype(Structure, {"nat": np.int32, "uhf": np.int32, "charge": np.float64,
+                                       "id": np.uintp, "xyz": np.uintp})
+_RESULT_DT = _record_dtype(Result, dict(
+    {k: np.float64 for k in ("energy", "e_rep", "e_elec", "e_band", "e_ts", "e_es2", "e_aes2", "e_es3",
+                             "scf_error")},
+    dipole=(np.float64, 3), iterations=np.int32, status=np.int32, nsh=np.int32, nao=np.int32,
+    qat=np.uintp, qsh=np.uintp, dpat=np.uintp, qpat=np.uintp))
+
+
 def _structs(mols):
-    """Pack Molecule-like objects (id, xyz, charge, uhf) into tb_structure records."""
-    keep, arr = [], (Structure * len(mols))()
-    for i, m in enumerate(mols):
-        ids = np.ascontiguousarray(m.id, np.int32)
-        xyz = np.ascontiguousarray(m.xyz, np.float64).reshape(-1, 3)
-        keep.append((ids, xyz))
-        arr[i].nat = ids.shape[0]
-        arr[i].uhf = int(getattr(m, "uhf", 0))
-        arr[i].charge = float(getattr(m, "charge", 0.0))
-        arr[i].id = ids.ctypes.data_as(_ip)
-        arr[i].xyz = xyz.ctypes.data_as(_dp)
-    return arr, keep
+    """Pack Molecule-like objects (id, xyz, charge, uhf) into tb_structure records.
+    All species ids and coordinates go into two contiguous arrays; the records
+    are filled through a numpy view of the ctypes array (pointer = base address
+    + offset), so the cost does not grow with a Python loop of ctypes calls."""
+    n = len(mols)
+    arr = (Structure * n)()
+    if n == 0:
+        return arr, ()
+    idl = [np.asarray(m.id, np.int32).ravel() for m in mols]
+    ids = np.ascontiguousarray(np.concatenate(idl))
+    xyz = np.ascontiguousarray(np.concatenate([np.asarray(m.xyz, np.float64).reshape(-1, 3) for m in mols]))
+    nat = np.fromiter((len(a) for a in idl), np.int64, n)
+    off = np.zeros(n, np.int64)
+    np.cumsum(nat[:-1], out=off[1:])
+    v = np.frombuffer(arr, dtype=_STRUCT_DT)
+    v["nat"] = nat
+    v["uhf"] = [int(getattr(m, "uhf", 0)) for m in mols]
+    v["charge"] = [float(getattr(m, "charge", 0.0)) for m in mols]
+    v["id"] = ids.ctypes.data + ids.itemsize * off
+    v["xyz"] = xyz.ctypes.data + 3 * xyz.itemsize * off
+    return arr, (ids, xyz, nat, off)
 
 
 class Calculator:
@@ -151,6 +177,13 @@ class Calculator:
               "tb_basis_size")
         return nsh.value, nao.value
 
+    def _species_basis(self):
+        """Shells and AOs per species (from one-atom structures, once)."""
+        if getattr(self, "_sp_basis", None) is None:
+            ns = load_library().tb_calculator_nspecies(self.h)
+            self._sp_basis = np.array([self.basis_size(_Atom(z)) for z in range(ns)], np.int64).reshape(-1, 2)
+        return self._sp_basis
+
     def cutoff(self, accuracy=1.0):
         return load_library().tb_get_cutoff(self.h, C.c_double(accuracy))
 
@@ -159,23 +192,54 @@ class Calculator:
         L = load_library()
         arr, keep = _structs(mols)
         o = default_options(**opts)
-        res = (Result * len(mols))()
-        bufs = []
-        for i, m in enumerate(mols):
-            nsh, nao = self.basis_size(m)
-            b = dict(qat=np.zeros(m.nat), qsh=np.zeros(nsh), dpat=np.zeros((m.nat, 3)),
-                     qpat=np.zeros((m.nat, 6)))
-            bufs.append(b)
-            res[i].qat = b["qat"].ctypes.data_as(_dp)
-            res[i].qsh = b["qsh"].ctypes.data_as(_dp)
-            res[i].dpat = b["dpat"].ctypes.data_as(_dp)
-            res[i].qpat = b["qpat"].ctypes.data_as(_dp)
-        st = L.tb_singlepoint_batch(self.h, arr, C.c_int32(len(mols)), C.byref(o), res,
-                                    C.c_void_p(stream or 0))
+        n = len(mols)
+        res = (Result * n)()
+        # output arrays for all structures at once; each structure gets views
+        tab = self._species_basis()
+        if n:
+            ids, _, nat, off = keep
+            if ids.size and (ids.min() < 0 or ids.max() >= len(tab)):
+                for m in mols:  # raises the library's own error for the bad species
+                    self.basis_size(m)
+            owner = np.repeat(np.arange(n), nat)
+            nsh = np.bincount(owner, weights=tab[ids, 0], minlength=n).astype(np.int64)
+        else:
+            nat = off = nsh = np.zeros(0, np.int64)
+        soff = np.zeros(n, np.int64)
+        if n:
+            np.cumsum(nsh[:-1], out=soff[1:])
+        na, ns = int(nat.sum()), int(nsh.sum())
+        qat, qsh, dpat, qpat = np.zeros(na), np.zeros(ns), np.zeros((na, 3)), np.zeros((na, 6))
+        v = np.frombuffer(res, dtype=_RESULT_DT) if n else None
+        if n:
+            v["qat"] = qat.ctypes.data + 8 * off
+            v["qsh"] = qsh.ctypes.data + 8 * soff
+            v["dpat"] = dpat.ctypes.data + 24 * off
+            v["qpat"] = qpat.ctypes.data + 48 * off
+        st = L.tb_singlepoint_batch(self.h, arr, C.c_int32(n), C.byref(o), res, C.c_void_p(stream or 0))
         if st not in (TB_OK,) and (raise_on_error or st in (TB_BAD_INPUT, TB_CUDA_ERROR,
                                                             TB_CAPACITY_EXCEEDED, TB_PARAM_ERROR)):
             check(st, "tb_singlepoint_batch")
-        return [_result_dict(r, b) for r, b in zip(res, bufs)]
+        out = []
+        for i in range(n):
+            a0, a1, s0 = int(off[i]), int(off[i] + nat[i]), int(soff[i])
+            r = v[i]
+            out.append(dict(energy=float(r["energy"]), e_rep=float(r["e_rep"]), e_elec=float(r["e_elec"]),
+                            e_band=float(r["e_band"]), e_ts=float(r["e_ts"]), e_es2=float(r["e_es2"]),
+                            e_aes2=float(r["e_aes2"]), e_es3=float(r["e_es3"]), dipole=np.array(r["dipole"]),
+                            scf_error=float(r["scf_error"]), iterations=int(r["iterations"]),
+                            status=int(r["status"]), nsh=int(r["nsh"]), nao=int(r["nao"]),
+                            qat=qat[a0:a1], qsh=qsh[s0:s0 + int(nsh[i])], dpat=dpat[a0:a1], qpat=qpat[a0:a1]))
+        return out
+
+
+class _Atom:
+    """One atom of species z at the origin (for per-species basis sizes)."""
+
+    def __init__(self, z):
+        self.id = np.array([z], np.int32)
+        self.xyz = np.zeros((1, 3))
+        self.nat = 1
 
 
 def _result_dict(r, b):
