@@ -216,7 +216,12 @@ struct tb_calculator {
     double c = 0, d = 0;  // one cuSOLVER call: c + d N^3 seconds
   } eig;
   std::mutex tune_mu;
+  // pinned staging buffer for the batch metadata upload, reused across batches
+  std::mutex stage_mu;
+  char* stage = nullptr;
+  size_t stage_bytes = 0;
   ~tb_calculator() {
+    if (stage) cudaFreeHost(stage);
     if (d_sp) cudaFree(d_sp);
     if (d_sh) cudaFree(d_sh);
     if (d_hscale) cudaFree(d_hscale);
@@ -351,6 +356,28 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   std::vector<int> id, at_mol, sh_type, sh_at, sh_iao, at_ish, ao_at, ao_sh;
   b->h_xyz.clear();
   b->h_nocc.clear();
+  {  // sizes first, so that the index maps are filled without reallocation
+    long long na = 0, ns = 0, no = 0, t64 = 0, t128 = 0, t32 = 0, c32 = 0;
+    for (int m = 0; m < nmol; ++m) {
+      const tb_structure& s = mols[m];
+      if (s.nat <= 0 || !s.id) continue;
+      long long sh = 0, ao = 0;
+      for (int a = 0; a < s.nat; ++a) {
+        const int z = s.id[a];
+        if (z < 0 || z >= (int)P.sp.size()) continue;
+        const SpeciesParam& sp = P.sp[z];
+        sh += sp.nsh;
+        for (int k = 0; k < sp.nsh; ++k) ao += msao(P.sh[sp.sh0 + k].ang);
+      }
+      na += s.nat; ns += sh; no += ao;
+      const long long a64 = (ao + 63) / 64, a128 = (ao + kTcTile - 1) / kTcTile, a32 = (ao + 31) / 32;
+      t64 += a64 * a64; t128 += a128 * a128; t32 += a32 * a32; c32 += a32;
+    }
+    id.reserve(na); at_mol.reserve(na); at_ish.reserve(na); b->h_xyz.reserve(3 * na);
+    sh_type.reserve(ns); sh_at.reserve(ns); sh_iao.reserve(ns); ao_at.reserve(no); ao_sh.reserve(no);
+    b->h_nocc.reserve(nmol);
+    b->tiles64.reserve(t64); b->tiles128.reserve(t128); b->tiles32.reserve(t32); b->chunks32.reserve(c32);
+  }
   for (int m = 0; m < nmol; ++m) {
     const tb_structure& s = mols[m];
     if (s.nat <= 0 || !s.id || !s.xyz) return fail(TB_BAD_INPUT, "structure " + std::to_string(m) + ": empty or null");
@@ -487,9 +514,18 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
       return fail(TB_CUDA_ERROR, "workspace of " + std::to_string(L.total >> 20) + " MiB: " + cudaGetErrorString(e));
   }
   char* base = arena->base;
-  // ---- metadata upload (one host blob, one copy)
-  std::vector<char> blob(meta_end, 0);
-  auto put = [&](size_t off, const void* src, size_t n) { if (n) std::memcpy(blob.data() + off, src, n); };
+  // ---- metadata upload (one host blob in the calculator's pinned staging
+  // buffer, one copy; the padding between fields is never read)
+  std::lock_guard<std::mutex> stage_lk(calc->stage_mu);
+  if (calc->stage_bytes < meta_end) {
+    if (calc->stage) cudaFreeHost(calc->stage);
+    calc->stage = nullptr;
+    calc->stage_bytes = 0;
+    TB_CUDA(cudaMallocHost(&calc->stage, meta_end + (meta_end >> 2)));
+    calc->stage_bytes = meta_end + (meta_end >> 2);
+  }
+  char* blob = calc->stage;
+  auto put = [&](size_t off, const void* src, size_t n) { if (n) std::memcpy(blob + off, src, n); };
   put(o_meta_aoff, b->h_aoff.data(), (NM + 1) * I4);
   put(o_meta_soff, b->h_soff.data(), (NM + 1) * I4);
   put(o_meta_ooff, b->h_ooff.data(), (NM + 1) * I4);
@@ -521,7 +557,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
     return b->h_ooff[a + 1] - b->h_ooff[a] > b->h_ooff[c + 1] - b->h_ooff[c];
   });
   put(o_order, order.data(), NM * I4);
-  TB_CUDA(cudaMemcpy(base, blob.data(), meta_end, cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMemcpy(base, blob, meta_end, cudaMemcpyHostToDevice));
 
   DevBatch& d = b->db;
   d.nmol = nmol; d.nat_tot = (int)NA; d.nsh_tot = (int)NS; d.nao_tot = (int)NO;

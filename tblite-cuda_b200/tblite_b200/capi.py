@@ -220,16 +220,21 @@ class Calculator:
         if st not in (TB_OK,) and (raise_on_error or st in (TB_BAD_INPUT, TB_CUDA_ERROR,
                                                             TB_CAPACITY_EXCEEDED, TB_PARAM_ERROR)):
             check(st, "tb_singlepoint_batch")
+        if not n:
+            return []
+        # each field converted once for all structures (numpy scalar access per field is slow)
+        keys = ("energy", "e_rep", "e_elec", "e_band", "e_ts", "e_es2", "e_aes2", "e_es3", "scf_error",
+                "iterations", "status", "nsh", "nao")
+        cols = [v[k].tolist() for k in keys]
+        dip = v["dipole"].copy()
+        a0s, a1s = off.tolist(), (off + nat).tolist()
+        s0s, s1s = soff.tolist(), (soff + nsh).tolist()
         out = []
         for i in range(n):
-            a0, a1, s0 = int(off[i]), int(off[i] + nat[i]), int(soff[i])
-            r = v[i]
-            out.append(dict(energy=float(r["energy"]), e_rep=float(r["e_rep"]), e_elec=float(r["e_elec"]),
-                            e_band=float(r["e_band"]), e_ts=float(r["e_ts"]), e_es2=float(r["e_es2"]),
-                            e_aes2=float(r["e_aes2"]), e_es3=float(r["e_es3"]), dipole=np.array(r["dipole"]),
-                            scf_error=float(r["scf_error"]), iterations=int(r["iterations"]),
-                            status=int(r["status"]), nsh=int(r["nsh"]), nao=int(r["nao"]),
-                            qat=qat[a0:a1], qsh=qsh[s0:s0 + int(nsh[i])], dpat=dpat[a0:a1], qpat=qpat[a0:a1]))
+            d = {k: c[i] for k, c in zip(keys, cols)}
+            a0, a1 = a0s[i], a1s[i]
+            d.update(dipole=dip[i], qat=qat[a0:a1], qsh=qsh[s0s[i]:s1s[i]], dpat=dpat[a0:a1], qpat=qpat[a0:a1])
+            out.append(d)
         return out
 
 
