@@ -54,6 +54,8 @@ struct DevBatch {
   const int* ao_at;      // [nao_tot] local atom index
   const int* ao_sh;      // [nao_tot] local shell index
   const int* order;      // [nmol] structures by decreasing N (one-CTA-per-structure kernels), may be null
+  const long long* s2off;  // shell-pair table offset (nsh^2 per structure), may be null
+  const long long* a2off;  // atom-pair table offset (nat^2 per structure), may be null
   int lib_above;         // 0: every structure on the in-house kernels; else structures with N > lib_above
                          // (all of them when -1) are factorised and diagonalised by the library path
 };

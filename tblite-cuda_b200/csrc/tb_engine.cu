@@ -237,7 +237,7 @@ struct tb_batch {
   Arena own;
   Arena* arena = nullptr;
   std::vector<int> h_aoff, h_soff, h_ooff, h_mixoff;
-  std::vector<long long> h_moff, h_poff;
+  std::vector<long long> h_moff, h_poff, h_s2off, h_a2off;
   std::vector<int4> tiles64, tiles32, tiles128;
   std::vector<int2> chunks32;
   std::vector<double> h_xyz;
@@ -248,6 +248,7 @@ struct tb_batch {
   int *cnt, *npair, *pair_i, *pair_j;
   long long* inl;
   double *S, *H0, *D, *Q, *X, *W, *F, *Z, *P;
+  double *gtab, *atab;  // Coulomb pair tables of the fixed geometry (k_pair_tables)
   double *w, *focc, *vsh, *vat, *vdp, *vqp, *colred, *qsh_out, *qat_out, *dpat_out, *qpat_out;
   int *perm, *kdim;
   double *q_in, *dq, *dqlast, *qlast, *df, *u, *amat, *omega;
@@ -353,6 +354,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   b->mixed = opt->precision == 1;
   b->h_aoff.assign(nmol + 1, 0); b->h_soff.assign(nmol + 1, 0); b->h_ooff.assign(nmol + 1, 0);
   b->h_mixoff.assign(nmol + 1, 0); b->h_moff.assign(nmol + 1, 0); b->h_poff.assign(nmol + 1, 0);
+  b->h_s2off.assign(nmol + 1, 0); b->h_a2off.assign(nmol + 1, 0);
   std::vector<int> id, at_mol, sh_type, sh_at, sh_iao, at_ish, ao_at, ao_sh;
   b->h_xyz.clear();
   b->h_nocc.clear();
@@ -418,6 +420,8 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
     b->h_mixoff[m + 1] = b->h_mixoff[m] + nsh + 9 * s.nat;
     b->h_moff[m + 1] = b->h_moff[m] + (long long)nao * nao;
     b->h_poff[m + 1] = b->h_poff[m] + (long long)s.nat * (s.nat - 1) / 2;
+    b->h_s2off[m + 1] = b->h_s2off[m] + (long long)nsh * nsh;
+    b->h_a2off[m + 1] = b->h_a2off[m] + (long long)s.nat * s.nat;
     b->nmax = std::max(b->nmax, nao);
     b->natmax = std::max(b->natmax, (int)s.nat);
     b->nshmax = std::max(b->nshmax, nsh);
@@ -474,6 +478,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   const long long NA = b->nat_tot, NS = b->nsh_tot, NO = b->nao_tot, N2 = b->n2_tot, NM = nmol, MX = b->mix_tot;
   size_t o_meta_aoff = L.add((NM + 1) * I4), o_meta_soff = L.add((NM + 1) * I4), o_meta_ooff = L.add((NM + 1) * I4),
          o_meta_mixoff = L.add((NM + 1) * I4), o_meta_moff = L.add((NM + 1) * 8), o_meta_poff = L.add((NM + 1) * 8),
+         o_meta_s2off = L.add((NM + 1) * 8), o_meta_a2off = L.add((NM + 1) * 8),
          o_xyz = L.add(3 * NA * D8), o_id = L.add(NA * I4), o_atmol = L.add(NA * I4), o_shtype = L.add(NS * I4),
          o_shat = L.add(NS * I4), o_shiao = L.add(NS * I4), o_atish = L.add(NA * I4), o_aoat = L.add(NO * I4),
          o_aosh = L.add(NO * I4), o_t64 = L.add(b->tiles64.size() * sizeof(int4)),
@@ -481,6 +486,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
          o_t32 = L.add(b->tiles32.size() * sizeof(int4)), o_c32 = L.add(b->chunks32.size() * sizeof(int2)),
          o_charge = L.add(NM * D8), o_uhf = L.add(NM * I4), o_order = L.add(NM * I4);
   const size_t meta_end = L.total;
+  size_t o_gtab = L.add((size_t)b->h_s2off[nmol] * D8), o_atab = L.add((size_t)b->h_a2off[nmol] * 3 * D8);
   size_t o_cn = L.add(NA * D8), o_mrad = L.add(NA * D8), o_erep = L.add(NA * D8), o_se = L.add(NS * D8),
          o_n0sh = L.add(NS * D8), o_cnt = L.add(NA * I4), o_inl = L.add(NA * 8), o_npair = L.add(NM * I4),
          o_pi = L.add(b->pair_cap * I4), o_pj = L.add(b->pair_cap * I4);
@@ -532,6 +538,8 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   put(o_meta_mixoff, b->h_mixoff.data(), (NM + 1) * I4);
   put(o_meta_moff, b->h_moff.data(), (NM + 1) * 8);
   put(o_meta_poff, b->h_poff.data(), (NM + 1) * 8);
+  put(o_meta_s2off, b->h_s2off.data(), (NM + 1) * 8);
+  put(o_meta_a2off, b->h_a2off.data(), (NM + 1) * 8);
   put(o_xyz, b->h_xyz.data(), 3 * NA * D8);
   put(o_id, id.data(), NA * I4);
   put(o_atmol, at_mol.data(), NA * I4);
@@ -563,7 +571,9 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   d.nmol = nmol; d.nat_tot = (int)NA; d.nsh_tot = (int)NS; d.nao_tot = (int)NO;
   d.aoff = at<int>(base, o_meta_aoff); d.soff = at<int>(base, o_meta_soff); d.ooff = at<int>(base, o_meta_ooff);
   d.mixoff = at<int>(base, o_meta_mixoff); d.moff = at<long long>(base, o_meta_moff);
-  d.poff = at<long long>(base, o_meta_poff); d.xyz = at<double>(base, o_xyz); d.id = at<int>(base, o_id);
+  d.poff = at<long long>(base, o_meta_poff);
+  d.s2off = at<long long>(base, o_meta_s2off); d.a2off = at<long long>(base, o_meta_a2off);
+  b->gtab = at<double>(base, o_gtab); b->atab = at<double>(base, o_atab); d.xyz = at<double>(base, o_xyz); d.id = at<int>(base, o_id);
   d.at_mol = at<int>(base, o_atmol); d.sh_type = at<int>(base, o_shtype); d.sh_at = at<int>(base, o_shat);
   d.sh_iao = at<int>(base, o_shiao); d.at_ish = at<int>(base, o_atish); d.ao_at = at<int>(base, o_aoat);
   d.ao_sh = at<int>(base, o_aosh);
@@ -907,6 +917,12 @@ tb_status batch_setup(tb_batch* b, cudaStream_t st) {
   TB_CUDA(cudaMemsetAsync(S.n_active, 0, sizeof(int), st));
   // ---- setup (once per structure)
   TB_K("atoms", 0, 0, k_atoms<<<nblk(B.nat_tot, 128), 128, 0, st>>>(Pc, B, b->cn, b->mrad, b->erep, b->se));
+  {
+    const long long mx = std::max((long long)b->nshmax * b->nshmax, (long long)b->natmax * b->natmax);
+    TB_K("pair_tables", 0, 0,
+         k_pair_tables<<<dim3(nmol, (unsigned)std::min<long long>(nblk(mx, 256), 64)), 256, 0, st>>>(
+             Pc, B, b->mrad, b->gtab, b->atab));
+  }
   TB_K("adjacency", 0, 0,
        k_adj_count<<<nblk((long long)B.nat_tot * 32, 256), 256, 0, st>>>(B, Pc.cutoff, b->cnt);
        TB_LAUNCH_CHECK();
@@ -986,7 +1002,8 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
          k_mix_next<<<nmol, 256, 0, st>>>(B, b->q_in, b->dq, b->dqlast, b->qlast, b->df, b->u, b->amat,
                                           b->omega, b->opt.max_iter, b->opt.mixer_damping, S));
   TB_K("potential", 0, 0,
-       k_potential<<<pot_grid, 256, 0, st>>>(Pc, B, b->q_in, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, S.active));
+       k_potential<<<pot_grid, 256, 0, st>>>(Pc, B, b->q_in, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, S.active,
+                                             b->gtab, b->atab));
   // Fock build: reads S, H0, D(3), Q(6), writes F -> 12 N^2 doubles
   TB_K("fock", 96.0 * n2, 2,
        k_fock<<<ntile32, 256, 0, st>>>(B, b->d_tiles32, ntile32, b->S, b->H0, b->D, b->Q, b->vsh, b->vat, b->vdp,
@@ -1034,7 +1051,7 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
        k_finalize<<<nmol, 256, 0, st>>>(Pc, B, b->colred, b->n0sh, b->mrad, b->q_in, b->dq, b->qsh_out, b->qat_out,
                                         b->dpat_out, b->qpat_out, econv, pconv, b->opt.max_iter, S,
                                         std::max(kMixedSwitchScale * econv, kMixedSwitchFloorE),
-                                        std::max(kMixedSwitchScale * pconv, kMixedSwitchFloorQ)));
+                                        std::max(kMixedSwitchScale * pconv, kMixedSwitchFloorQ), b->gtab, b->atab));
   return TB_OK;
 }
 
@@ -1418,7 +1435,7 @@ tb_status tb_coulomb_potential(const tb_calculator* calc, const tb_structure* mo
   TB_CUDA(cudaMemcpy(b->ms.active, &one, sizeof(int), cudaMemcpyHostToDevice));
   const DevParams P = params_for(calc, 1.0);
   k_potential<<<dim3(1, nblk(std::max(nat, nsh), 256)), 256>>>(P, b->db, b->q_in, b->mrad, b->vsh, b->vat, b->vdp,
-                                                               b->vqp, b->ms.active);
+                                                               b->vqp, b->ms.active, nullptr, nullptr);
   TB_LAUNCH_CHECK();
   if (vsh && d2h(vsh, b->vsh, nsh * 8)) return TB_CUDA_ERROR;
   if (vat && d2h(vat, b->vat, nat * 8)) return TB_CUDA_ERROR;

@@ -116,8 +116,11 @@ __global__ void k_oa_step(DevBatch B, double* G, double* Sm, double* V, double* 
 // SCF
 __global__ void k_scf_init(DevParams P, DevBatch B, const double* charge, const int* uhf, const double* erep,
                            double* n0sh, double* q_in, MolState S);
+// pair tables of the fixed geometry (gtab: gamma per shell pair, atab: 1/r, f3, f5 per atom pair)
+__global__ void k_pair_tables(DevParams P, DevBatch B, const double* mrad, double* gtab, double* atab);
+// gtab/atab may be null: the pair terms are then recomputed
 __global__ void k_potential(DevParams P, DevBatch B, const double* q_in, const double* mrad, double* vsh, double* vat,
-                            double* vdp, double* vqp, const int* active);
+                            double* vdp, double* vqp, const int* active, const double* gtab, const double* atab);
 __global__ void k_fock(DevBatch B, const int4* tiles, int ntiles, const double* S, const double* H0, const double* D,
                        const double* Q, const double* vsh, const double* vat, const double* vdp, const double* vqp,
                        double* F, const int* active);
@@ -128,7 +131,7 @@ __global__ void k_mulliken_cols(DevBatch B, const int2* chunks, int nchunks, con
 __global__ void k_finalize(DevParams P, DevBatch B, const double* colred, const double* n0sh, const double* mrad,
                            const double* q_in, double* dq, double* qsh_out, double* qat_out, double* dpat_out,
                            double* qpat_out, double econv, double pconv, int max_iter, MolState S,
-                           double econv_lo, double pconv_lo);
+                           double econv_lo, double pconv_lo, const double* gtab, const double* atab);
 __global__ void k_mix_next(DevBatch B, double* q_in, const double* dq, double* dqlast, double* qlast, double* df,
                            double* u, double* amat, double* omega, int memory, double damp, MolState S);
 

@@ -86,14 +86,56 @@ __global__ void k_scf_init(DevParams P, DevBatch B, const double* __restrict__ c
   }
 }
 
+// ------------------------------------------------------------ pair tables
+// The geometry is fixed during the SCF, so the shell-pair Coulomb kernel
+// gamma_ab (ES2) and the atom-pair 1/r and AES2 damping factors are
+// evaluated once per batch: gtab[s2off + a nsh + b] = gamma_ab(a, b);
+// atab[3 (a2off + A nat + B) + {0, 1, 2}] = {1/r, f3, f5} (zero for A = B).
+// Both tables are symmetric bit for bit (the terms only see squared
+// differences and symmetric sums), so the per-iteration kernels read column
+// t of them (coalesced) instead of recomputing log/exp/sqrt per pair.
+__global__ void k_pair_tables(DevParams P, DevBatch B, const double* __restrict__ mrad, double* __restrict__ gtab,
+                              double* __restrict__ atab) {
+  const int m = blockIdx.x;
+  const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0;
+  const int s0 = B.soff[m], nsh = B.soff[m + 1] - s0;
+  const double* xyz = B.xyz + 3 * a0;
+  double* g = gtab + B.s2off[m];
+  double* at = atab + 3 * B.a2off[m];
+  for (long long e = blockIdx.y * (long long)blockDim.x + threadIdx.x; e < (long long)nsh * nsh;
+       e += (long long)gridDim.y * blockDim.x) {
+    const int a = (int)(e / nsh), b = (int)(e - (long long)a * nsh);
+    const int A = B.sh_at[s0 + a], Bq = B.sh_at[s0 + b];
+    const double dx = xyz[3 * A] - xyz[3 * Bq], dy = xyz[3 * A + 1] - xyz[3 * Bq + 1], dz = xyz[3 * A + 2] - xyz[3 * Bq + 2];
+    g[e] = gamma_ab(P, B.sh_type[s0 + a], B.sh_type[s0 + b], A == Bq, dx * dx + dy * dy + dz * dz);
+  }
+  for (long long e = blockIdx.y * (long long)blockDim.x + threadIdx.x; e < (long long)nat * nat;
+       e += (long long)gridDim.y * blockDim.x) {
+    const int A = (int)(e / nat), Bq = (int)(e - (long long)A * nat);
+    double g1 = 0.0, f3 = 0.0, f5 = 0.0;
+    if (A != Bq) {
+      const double v[3] = {xyz[3 * Bq] - xyz[3 * A], xyz[3 * Bq + 1] - xyz[3 * A + 1], xyz[3 * Bq + 2] - xyz[3 * A + 2]};
+      const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+      g1 = 1.0 / sqrt(r2);
+      aes_damp(P, mrad[a0 + A], mrad[a0 + Bq], g1, f3, f5);
+    }
+    at[3 * e] = g1;
+    at[3 * e + 1] = f3;
+    at[3 * e + 2] = f5;
+  }
+}
+
 // ------------------------------------------------------------ potentials
 // tb_coulomb::get_potential for the mixed input moments q_in = [qsh, dpat,
 // qpat]: ES2 (vsh += gamma qsh), ES3 (vsh += qsh^2 dGamma), AES2 (the five
 // gemv of the quoted Fortran src/coulomb.cu:665-676) and the on-site kernels
-// (get_kernel_potential, :564-589).  grid = (structure, target chunk).
+// (get_kernel_potential, :564-589).  grid = (structure, target chunk).  With
+// the pair tables (gtab, atab non-null) the pair terms are read, not
+// recomputed; the arithmetic on them is unchanged.
 __global__ void k_potential(DevParams P, DevBatch B, const double* __restrict__ q_in,
                             const double* __restrict__ mrad, double* __restrict__ vsh, double* __restrict__ vat,
-                            double* __restrict__ vdp, double* __restrict__ vqp, const int* __restrict__ active) {
+                            double* __restrict__ vdp, double* __restrict__ vqp, const int* __restrict__ active,
+                            const double* __restrict__ gtab, const double* __restrict__ atab) {
   const int m = blockIdx.x;
   if (!active[m]) return;
   const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0;
@@ -107,10 +149,15 @@ __global__ void k_potential(DevParams P, DevBatch B, const double* __restrict__ 
   if (t < nsh) {
     const int ta = B.sh_type[s0 + t], A = B.sh_at[s0 + t];
     double v = 0.0;
-    for (int b = 0; b < nsh; ++b) {
-      const int Bq = B.sh_at[s0 + b];
-      const double dx = xyz[3 * A] - xyz[3 * Bq], dy = xyz[3 * A + 1] - xyz[3 * Bq + 1], dz = xyz[3 * A + 2] - xyz[3 * Bq + 2];
-      v += gamma_ab(P, ta, B.sh_type[s0 + b], A == Bq, dx * dx + dy * dy + dz * dz) * qsh[b];
+    if (gtab) {
+      const double* gc = gtab + B.s2off[m] + t;  // column t = row t
+      for (int b = 0; b < nsh; ++b) v += gc[(long long)b * nsh] * qsh[b];
+    } else {
+      for (int b = 0; b < nsh; ++b) {
+        const int Bq = B.sh_at[s0 + b];
+        const double dx = xyz[3 * A] - xyz[3 * Bq], dy = xyz[3 * A + 1] - xyz[3 * Bq + 1], dz = xyz[3 * A + 2] - xyz[3 * Bq + 2];
+        v += gamma_ab(P, ta, B.sh_type[s0 + b], A == Bq, dx * dx + dy * dy + dz * dz) * qsh[b];
+      }
     }
     v += qsh[t] * qsh[t] * P.sh[ta].hubbard_deriv;
     vsh[s0 + t] = v;
@@ -120,13 +167,20 @@ __global__ void k_potential(DevParams P, DevBatch B, const double* __restrict__ 
     const int A = t;
     double va = 0.0, vd[3] = {0, 0, 0}, vq[6] = {0, 0, 0, 0, 0, 0};
     const double rA = mrad[a0 + A];
+    const double* ac = atab ? atab + 3 * (B.a2off[m] + A) : nullptr;  // column A = row A
     for (int Bq = 0; Bq < nat; ++Bq) {
       if (Bq == A) continue;
       const double v[3] = {xyz[3 * Bq] - xyz[3 * A], xyz[3 * Bq + 1] - xyz[3 * A + 1], xyz[3 * Bq + 2] - xyz[3 * A + 2]};
-      const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-      const double g1 = 1.0 / sqrt(r2), g3 = g1 * g1 * g1, g5 = g3 * g1 * g1;
-      double f3, f5;
-      aes_damp(P, rA, mrad[a0 + Bq], g1, f3, f5);
+      double g1, f3, f5;
+      if (ac) {
+        const double* e = ac + 3LL * Bq * nat;
+        g1 = e[0]; f3 = e[1]; f5 = e[2];
+      } else {
+        const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        g1 = 1.0 / sqrt(r2);
+        aes_damp(P, rA, mrad[a0 + Bq], g1, f3, f5);
+      }
+      const double g3 = g1 * g1 * g1, g5 = g3 * g1 * g1;
       // qat of atom Bq from its shells
       const int isb = B.at_ish[a0 + Bq], nsb = P.sp[B.id[a0 + Bq]].nsh;
       double qb = 0.0;
@@ -404,7 +458,8 @@ __global__ void k_finalize(DevParams P, DevBatch B, const double* __restrict__ c
                            const double* __restrict__ mrad, const double* __restrict__ q_in, double* __restrict__ dq,
                            double* __restrict__ qsh_out, double* __restrict__ qat_out, double* __restrict__ dpat_out,
                            double* __restrict__ qpat_out, double econv, double pconv, int max_iter, MolState S,
-                           double econv_lo, double pconv_lo) {
+                           double econv_lo, double pconv_lo, const double* __restrict__ gtab,
+                           const double* __restrict__ atab) {
   const int m = blockIdx.x;
   if (!S.active[m]) return;
   __shared__ double red[32];
@@ -449,10 +504,15 @@ __global__ void k_finalize(DevParams P, DevBatch B, const double* __restrict__ c
   for (int a = tid; a < nsh; a += nt) {
     const int ta = B.sh_type[s0 + a], A = B.sh_at[s0 + a];
     double v = 0.0;
-    for (int b = 0; b < nsh; ++b) {
-      const int Bq = B.sh_at[s0 + b];
-      const double dx = xyz[3 * A] - xyz[3 * Bq], dy = xyz[3 * A + 1] - xyz[3 * Bq + 1], dz = xyz[3 * A + 2] - xyz[3 * Bq + 2];
-      v += gamma_ab(P, ta, B.sh_type[s0 + b], A == Bq, dx * dx + dy * dy + dz * dz) * qs[b];
+    if (gtab) {
+      const double* gc = gtab + B.s2off[m] + a;  // column a = row a
+      for (int b = 0; b < nsh; ++b) v += gc[(long long)b * nsh] * qs[b];
+    } else {
+      for (int b = 0; b < nsh; ++b) {
+        const int Bq = B.sh_at[s0 + b];
+        const double dx = xyz[3 * A] - xyz[3 * Bq], dy = xyz[3 * A + 1] - xyz[3 * Bq + 1], dz = xyz[3 * A + 2] - xyz[3 * Bq + 2];
+        v += gamma_ab(P, ta, B.sh_type[s0 + b], A == Bq, dx * dx + dy * dy + dz * dz) * qs[b];
+      }
     }
     e2 += 0.5 * v * qs[a];
     e3 += qs[a] * qs[a] * qs[a] * P.sh[ta].hubbard_deriv / 3.0;
@@ -464,13 +524,20 @@ __global__ void k_finalize(DevParams P, DevBatch B, const double* __restrict__ c
     const double* qA = qpat_out + 6 * (a0 + A);
     double vd[3] = {0, 0, 0}, vq[6] = {0, 0, 0, 0, 0, 0};
     const double rA = mrad[a0 + A];
+    const double* ac = atab ? atab + 3 * (B.a2off[m] + A) : nullptr;  // column A = row A
     for (int Bq = 0; Bq < nat; ++Bq) {
       if (Bq == A) continue;
       const double v[3] = {xyz[3 * Bq] - xyz[3 * A], xyz[3 * Bq + 1] - xyz[3 * A + 1], xyz[3 * Bq + 2] - xyz[3 * A + 2]};
-      const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-      const double g1 = 1.0 / sqrt(r2), g3 = g1 * g1 * g1, g5 = g3 * g1 * g1;
-      double f3, f5;
-      aes_damp(P, rA, mrad[a0 + Bq], g1, f3, f5);
+      double g1, f3, f5;
+      if (ac) {
+        const double* e = ac + 3LL * Bq * nat;
+        g1 = e[0]; f3 = e[1]; f5 = e[2];
+      } else {
+        const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        g1 = 1.0 / sqrt(r2);
+        aes_damp(P, rA, mrad[a0 + Bq], g1, f3, f5);
+      }
+      const double g3 = g1 * g1 * g1, g5 = g3 * g1 * g1;
       const double qb = qat_out[a0 + Bq];
       const double* db = dpat_out + 3 * (a0 + Bq);
       const double vdb = v[0] * db[0] + v[1] * db[1] + v[2] * db[2];
