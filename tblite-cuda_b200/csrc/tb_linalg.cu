@@ -745,7 +745,7 @@ __device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, 
   __syncthreads();
 }
 
-constexpr int kDcLeaf = 16;  // leaves of the merge tree: at most this many rows, solved by one warp
+constexpr int kDcLeaf = 24;  // leaves of the merge tree: at most this many rows, solved by one warp
 
 // Leaf [lo, lo+s) of the tree (s <= kDcLeaf) by one warp: implicit QL with
 // Wilkinson shifts (the same sweep as the k_syev producer) on lane 0 over
@@ -753,8 +753,8 @@ constexpr int kDcLeaf = 16;  // leaves of the merge tree: at most this many rows
 // rotations then applied by lanes (one per column) to the rows of the leaf's
 // eigenvector block U in shared memory; U is written to G's diagonal block.
 // Returns false if an eigenvalue took more than 60 sweeps.
-static_assert((kEigThreads / 32) * (kDcLeaf * kDcLeaf + 3 * kDcLeaf) <= (5 + 2 * kRing) * kDcMin,
-              "leaf workspace exceeds the free shared memory");
+constexpr int kDcLeafWs = kDcLeaf * kDcLeaf + 3 * kDcLeaf;  // per leaf warp: U, off-diagonal, rotations
+static_assert(kDcLeafWs <= (5 + 2 * kRing) * kDcMin, "leaf workspace exceeds the free shared memory");
 
 template <typename T>
 __device__ bool dc_leaf(T* d, const T* e, int lo, int s, T* U, T* le, T* rcs, T* G, int n) {
@@ -853,12 +853,14 @@ __device__ bool dc_solve(T* d, T* e, T* Z, T* G0, T* G1, int n, T* ws, T* red) {
     }
     __syncthreads();
   }
-  T* U = ws + wid * (kDcLeaf * kDcLeaf + 3 * kDcLeaf);  // per warp: U, off-diagonal, rotations
+  // as many leaf warps as the free shared memory holds blocks for
+  const int lw = min(nw, (int)((5 + 2 * kRing) * (long long)n / kDcLeafWs));
+  T* U = ws + wid * kDcLeafWs;
   for (int dep = depth; dep >= 0; --dep) {
     T* Gi = ((depth - dep - 1) & 1) ? G1 : G0;
     T* Go = ((depth - dep) & 1) ? G1 : G0;
     // leaves of this depth, one warp each
-    for (int b = wid; b < (1 << dep); b += nw) {
+    for (int b = wid; wid < lw && b < (1 << dep); b += lw) {
       int lo, hi, pl;
       dc_node(n, dep, b, &lo, &hi, &pl);
       if (hi - lo < 1 || hi - lo > kDcLeaf || pl <= kDcLeaf) continue;
