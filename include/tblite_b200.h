@@ -99,6 +99,8 @@ typedef struct tb_calculator tb_calculator;
  * one: new_hamiltonian is declared at src/h0.h:80-86 but not defined).  Reads a
  * tblite-b200 parameter file (.tbp). */
 tb_status tb_calculator_create(const char* param_file, tb_calculator** out);
+/* Destroy batches and servers made from the calculator before it: they share
+ * its workspace and pinned host buffers. */
 void tb_calculator_destroy(tb_calculator* calc);
 int32_t tb_calculator_nspecies(const tb_calculator* calc);
 void tb_default_options(tb_options* opt);

@@ -220,8 +220,33 @@ struct tb_calculator {
   std::mutex stage_mu;
   char* stage = nullptr;
   size_t stage_bytes = 0;
+  // pinned int slots for the batches' per-iteration active counts: pinning and
+  // unpinning host memory are operating-system calls whose cost varies with
+  // the host's load, so a batch takes a slot instead of allocating its own
+  static constexpr int kPinSlots = 1024;
+  std::mutex pin_mu;
+  int* pin = nullptr;
+  std::vector<int> pin_free;
+  int* take_pin_slot() {
+    std::lock_guard<std::mutex> lk(pin_mu);
+    if (!pin) {
+      if (cudaMallocHost(&pin, kPinSlots * sizeof(int)) != cudaSuccess) { pin = nullptr; return nullptr; }
+      for (int i = kPinSlots - 1; i >= 0; --i) pin_free.push_back(i);
+    }
+    if (pin_free.empty()) return nullptr;
+    const int i = pin_free.back();
+    pin_free.pop_back();
+    return pin + i;
+  }
+  bool give_pin_slot(int* p) {  // false: not from the pool
+    std::lock_guard<std::mutex> lk(pin_mu);
+    if (!pin || p < pin || p >= pin + kPinSlots) return false;
+    pin_free.push_back((int)(p - pin));
+    return true;
+  }
   ~tb_calculator() {
     if (stage) cudaFreeHost(stage);
+    if (pin) cudaFreeHost(pin);
     if (d_sp) cudaFree(d_sp);
     if (d_sh) cudaFree(d_sh);
     if (d_hscale) cudaFree(d_hscale);
@@ -293,7 +318,7 @@ struct tb_batch {
   ~tb_batch() {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (cap) cudaStreamDestroy(cap);
-    if (h_nactive) cudaFreeHost(h_nactive);
+    if (h_nactive && !(calc && calc->give_pin_slot(h_nactive))) cudaFreeHost(h_nactive);
     for (cudaEvent_t e : evpool) cudaEventDestroy(e);
   }
 };
@@ -613,7 +638,8 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   s.fermi_warn = at<int>(base, o_ms_fw); s.dipole = at<double>(base, o_ms_dip); s.n_active = at<int>(base, o_ms_nact);
   s.phase = b->mixed ? at<int>(base, o_phase) : nullptr;
   s.n64 = b->mixed ? at<int>(base, o_n64) : nullptr;
-  if (!b->h_nactive) TB_CUDA(cudaMallocHost(&b->h_nactive, sizeof(int)));
+  if (!b->h_nactive) b->h_nactive = calc->take_pin_slot();
+  if (!b->h_nactive) TB_CUDA(cudaMallocHost(&b->h_nactive, sizeof(int)));  // pool exhausted
   return TB_OK;
 }
 
