@@ -93,7 +93,10 @@ __global__ void k_scf_init(DevParams P, DevBatch B, const double* __restrict__ c
 // atab[3 (a2off + A nat + B) + {0, 1, 2}] = {1/r, f3, f5} (zero for A = B).
 // Both tables are symmetric bit for bit (the terms only see squared
 // differences and symmetric sums), so the per-iteration kernels read column
-// t of them (coalesced) instead of recomputing log/exp/sqrt per pair.
+// t of them (coalesced) instead of recomputing log/exp/sqrt per pair.  The
+// reference likewise fills its Coulomb cache once per geometry
+// (effective_coulomb::update, src/coulomb.cu:82-98; damped_multipole::update,
+// :153) and reuses it in every iteration.
 __global__ void k_pair_tables(DevParams P, DevBatch B, const double* __restrict__ mrad, double* __restrict__ gtab,
                               double* __restrict__ atab) {
   const int m = blockIdx.x;
