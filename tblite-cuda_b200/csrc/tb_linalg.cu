@@ -478,10 +478,15 @@ __device__ __noinline__ void panel_walk(T* M, int n, int r0, int nm, const T* PV
 constexpr int kDcMin = 128;  // smallest structure solved this way (shared memory, see dc_ws_ok)
 constexpr int kDcK = 8;      // reduction slab of the tiled products
 
+// slabs of the tiled products: Wt 64 x kDcK, Bt kDcK x kDcBs (row padded by 4 so
+// that the DMMA fragment loads of a warp hit distinct banks)
+constexpr int kDcBs = 64 + 4;
+constexpr int kDcTileElems = 64 * kDcK + kDcK * kDcBs;
+
 // workspace of one merge of m entries, in units of T (the ints after the T arrays)
 template <typename T>
 __host__ __device__ constexpr int dc_ws_elems(int m) {
-  return 8 * m + 2 * 64 * kDcK + (7 * m * (int)sizeof(int) + (int)sizeof(T) - 1) / (int)sizeof(T);
+  return 8 * m + kDcTileElems + (7 * m * (int)sizeof(int) + (int)sizeof(T) - 1) / (int)sizeof(T);
 }
 
 // the workspace starts at tau: 5 n vectors + the ring are free after Q is formed
@@ -547,21 +552,31 @@ __device__ void secular_root(int j, int k, const T* dl, const T* z, T rho, int* 
 }
 
 // Out[(r0 + j) ld + c0 + c] = sum_i gen(j, i) In[(srow ? srow[i] : i) ld + c0 + c]
-// for j < nrow, c < ncol, i < kdim: 64 x 64 output tiles, 4 x 4 per thread,
-// slabs of kDcK staged in shared memory (Wt: 64 x kDcK, Bt: kDcK x 64).  The
-// next slab (its loads and generated entries) is fetched into registers while
-// the current one is multiplied.
+// for j < nrow, c < ncol, i < kdim: 64 x 64 output tiles, slabs of kDcK
+// staged in shared memory (Wt: 64 x kDcK, Bt: kDcK x 64 with padded rows).
+// The next slab (its loads and generated entries) is fetched into registers
+// while the current one is multiplied.  FP64: on the FP64 tensor instruction
+// mma.sync.m8n8k4 (each warp a 16 x 32 block as 2 x 4 fragments of 8 x 8);
+// FP32: 4 x 4 outputs per thread.
 template <typename T, typename Gen>
 __device__ void dc_gemm(int nrow, int kdim, int ncol, Gen gen, const T* In, const int* srow, T* Out, int r0, int c0,
                         int ld, T* Wt, T* Bt) {
+  constexpr bool kTensor = sizeof(T) == 8;
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, tg = lane & 3;
+  const int wrow = (warp >> 1) * 16, wcol = (warp & 1) * 32;  // this warp's block of the tile (FP64)
   for (int j0 = 0; j0 < nrow; j0 += 64) {
     for (int cb = 0; cb < ncol; cb += 64) {
-      T acc[4][4];
+      T acc[4][4];  // FP32: outputs; FP64: acc[x][2y + h] of fragment (x, y) for x < 2, y < 4
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+      T acc2[2][4];  // FP64: second half of the fragments' outputs
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc2[a][b] = T(0);
       constexpr int kPer = 64 * kDcK / kEigThreads;  // slab entries per thread
       T wr[kPer], br[kPer];
       auto fetch = [&](int i0) {
@@ -578,33 +593,63 @@ __device__ void dc_gemm(int nrow, int kdim, int ncol, Gen gen, const T* In, cons
       for (int i0 = 0; i0 < kdim; i0 += kDcK) {
 #pragma unroll
         for (int u = 0; u < kPer; ++u) {
-          Wt[tid + u * kEigThreads] = wr[u];
-          Bt[tid + u * kEigThreads] = br[u];
+          const int x = tid + u * kEigThreads;
+          Wt[x] = wr[u];
+          Bt[(x >> 6) * kDcBs + (x & 63)] = br[u];
         }
         __syncthreads();
         if (i0 + kDcK < kdim) fetch(i0 + kDcK);
+        if constexpr (kTensor) {
 #pragma unroll
-        for (int kk = 0; kk < kDcK; ++kk) {
-          T av[4], bv[4];
+          for (int k4 = 0; k4 < kDcK; k4 += 4) {
+            double af[2], bf[4];
 #pragma unroll
-          for (int a = 0; a < 4; ++a) av[a] = Wt[(ty * 4 + a) * kDcK + kk];
+            for (int x = 0; x < 2; ++x) af[x] = Wt[(wrow + 8 * x + g) * kDcK + k4 + tg];
 #pragma unroll
-          for (int b = 0; b < 4; ++b) bv[b] = Bt[kk * 64 + tx + 16 * b];
+            for (int y = 0; y < 4; ++y) bf[y] = Bt[(k4 + tg) * kDcBs + wcol + 8 * y + g];
 #pragma unroll
-          for (int a = 0; a < 4; ++a)
+            for (int x = 0; x < 2; ++x)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+              for (int y = 0; y < 4; ++y) dmma(acc[x][y], acc2[x][y], af[x], bf[y]);
+          }
+        } else {
+#pragma unroll
+          for (int kk = 0; kk < kDcK; ++kk) {
+            T av[4], bv[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) av[a] = Wt[(ty * 4 + a) * kDcK + kk];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) bv[b] = Bt[kk * kDcBs + tx + 16 * b];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+              for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+          }
         }
         __syncthreads();
       }
+      if constexpr (kTensor) {  // fragment (x, y): rows wrow + 8x + g, columns wcol + 8y + 2 tg + {0, 1}
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int j = j0 + ty * 4 + a;
-        if (j >= nrow) continue;
+        for (int x = 0; x < 2; ++x) {
+          const int j = j0 + wrow + 8 * x + g;
+          if (j >= nrow) continue;
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int c = cb + tx + 16 * b;
-          if (c < ncol) Out[(long long)(r0 + j) * ld + c0 + c] = acc[a][b];
+          for (int y = 0; y < 4; ++y) {
+            const int c = cb + wcol + 8 * y + 2 * tg;
+            if (c < ncol) Out[(long long)(r0 + j) * ld + c0 + c] = acc[x][y];
+            if (c + 1 < ncol) Out[(long long)(r0 + j) * ld + c0 + c + 1] = acc2[x][y];
+          }
+        }
+      } else {
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          const int j = j0 + ty * 4 + a;
+          if (j >= nrow) continue;
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const int c = cb + tx + 16 * b;
+            if (c < ncol) Out[(long long)(r0 + j) * ld + c0 + c] = acc[a][b];
+          }
         }
       }
     }
@@ -632,7 +677,7 @@ __device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, 
   T* rsn = rc + m;        //            sine
   T* Wt = rsn + m;
   T* Bt = Wt + 64 * kDcK;
-  int* rowof = reinterpret_cast<int*>(Bt + 64 * kDcK);  // m: row of sorted entry s
+  int* rowof = reinterpret_cast<int*>(Wt + kDcTileElems);  // m: row of sorted entry s
   int* flg = rowof + m;   // m: deflated
   int* ndl = flg + m;     // m: sorted index of the k non-deflated, then of the deflated
   int* rp = ndl + m;      // rotations: rows
