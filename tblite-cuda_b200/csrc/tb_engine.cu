@@ -574,6 +574,11 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   put(o_atish, at_ish.data(), NA * I4);
   put(o_aoat, ao_at.data(), NO * I4);
   put(o_aosh, ao_sh.data(), NO * I4);
+  // GEMM tiles of the largest structures first: their tiles carry the longest
+  // K ranges, so the grid-stride waves end on short tiles (LPT order)
+  std::stable_sort(b->tiles64.begin(), b->tiles64.end(), [&](const int4& x, const int4& y) {
+    return b->h_ooff[x.x + 1] - b->h_ooff[x.x] > b->h_ooff[y.x + 1] - b->h_ooff[y.x];
+  });
   put(o_t64, b->tiles64.data(), b->tiles64.size() * sizeof(int4));
   put(o_t128, b->tiles128.data(), b->tiles128.size() * sizeof(int4));
   put(o_t32, b->tiles32.data(), b->tiles32.size() * sizeof(int4));
