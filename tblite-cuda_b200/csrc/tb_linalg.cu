@@ -381,38 +381,27 @@ __device__ void reflector(T* A, int n, int k, T* v, T* tau, T* e, T* red, T* sh)
   __syncthreads();
 }
 
-// Column walk over the block rows r0..r0+nr-1, columns c0..c0+nc-1 of a
-// row-major matrix M: optionally M[r][c] -= a_r b_c + b_r a_c (with a, b
-// indexed from the block's origin), and out_c = scale * sum_r M_new[r][c] x_r.
-// One thread per column; rows are loaded in batches of WalkCfg<T>::batch before any
-// of them is written back, so a batch costs about one L2 round trip.  Kept
-// out of line (as is panel_walk) so that its batch registers are allocated
-// apart from the rest of the eigensolver.
+// Read-only column walk over the square block r0..r0+nm-1 (rows and columns)
+// of a row-major matrix M: out_c = scale * sum_r M[r][c] x_{r-r0}.  One thread
+// per column; rows are loaded in batches of WalkCfg<T>::batch before any is
+// used, so a batch costs about one L2 round trip.  Kept out of line (as is
+// panel_walk) so that its batch registers are allocated apart from the rest
+// of the eigensolver.
 template <typename T>
-__device__ __noinline__ void colwalk(T* M, int n, int r0, int nr, int c0, int nc, bool upd, const T* a,
-                        const T* b, int aoff, const T* x, T* out, T scale) {
+__device__ __noinline__ void colwalk(const T* M, int n, int r0, int nm, const T* x, T* out, T scale) {
   constexpr int kWalkBatch = WalkCfg<T>::batch;
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int jj = tid; jj < nc; jj += nt) {
-    const int c = c0 + jj;
-    const T aj = upd ? a[aoff + c0 - r0 + jj] : T(0), bj = upd ? b[aoff + c0 - r0 + jj] : T(0);
+  for (int jj = tid; jj < nm; jj += nt) {
+    const int c = r0 + jj;
     T acc = T(0);
-    for (int i0 = 0; i0 < nr; i0 += kWalkBatch) {
+    for (int i0 = 0; i0 < nm; i0 += kWalkBatch) {
       T q[kWalkBatch];
 #pragma unroll
       for (int u = 0; u < kWalkBatch; ++u)
-        q[u] = (i0 + u < nr) ? M[(long long)(r0 + i0 + u) * n + c] : T(0);
+        q[u] = (i0 + u < nm) ? M[(long long)(r0 + i0 + u) * n + c] : T(0);
 #pragma unroll
-      for (int u = 0; u < kWalkBatch; ++u) {
-        if (i0 + u < nr) {
-          if (upd) {
-            const int ri = aoff + i0 + u;
-            q[u] -= a[ri] * bj + b[ri] * aj;
-            M[(long long)(r0 + i0 + u) * n + c] = q[u];
-          }
-          acc += q[u] * x[i0 + u];
-        }
-      }
+      for (int u = 0; u < kWalkBatch; ++u)
+        if (i0 + u < nm) acc += q[u] * x[i0 + u];
     }
     out[jj] = scale * acc;
   }
@@ -994,7 +983,7 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
     const int nref = n - 2;     // reflectors 0 .. n-3
     reflector(A, n, 0, v, tau, e, red, sh);
     // p0 = tau0 * A[1..][1..] v0
-    colwalk<T>(A, n, 1, n - 1, 1, n - 1, false, nullptr, nullptr, 0, v, p, tau[0]);
+    colwalk<T>(A, n, 1, n - 1, v, p, tau[0]);
     __syncthreads();
     int np = 0;  // pairs in the open panel
     for (int k = 0; k < nref; ++k) {
@@ -1047,7 +1036,7 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
           panel_walk<T>(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r]);
           np = 0;
         } else {  // p_r = tau_r A0 vn
-          colwalk<T>(A, n, r + 1, n - r - 1, r + 1, n - r - 1, false, nullptr, nullptr, 0, vn, p, tau[r]);
+          colwalk<T>(A, n, r + 1, n - r - 1, vn, p, tau[r]);
         }
         __syncthreads();
       }
