@@ -317,7 +317,7 @@ namespace {
 // element, so the walk is traffic-bound and wide panels pay; in FP32 a panel
 // of one (each step's update fused with the next product) is as fast.
 template <typename T> struct PanelCfg;
-template <> struct PanelCfg<double> { static constexpr int width = 8, batch = 12; };
+template <> struct PanelCfg<double> { static constexpr int width = 8, batch = 6; };
 template <> struct PanelCfg<float> { static constexpr int width = 1, batch = 12; };
 // rows per load batch of the read-only Householder column walk
 template <typename T> struct WalkCfg { static constexpr int batch = sizeof(T) == 8 ? 24 : 12; };
@@ -381,29 +381,45 @@ __device__ void reflector(T* A, int n, int k, T* v, T* tau, T* e, T* red, T* sh)
   __syncthreads();
 }
 
+// Rows of a walk over an nm-column block are split in two halves (separate
+// threads, partial sums added at the end) when that shortens the slowest
+// thread: nm <= half the threads (idle warps otherwise) or nm > the threads
+// (a second column per thread otherwise walks all rows again).
+__device__ inline bool walk_split(int nm, int nt) { return 2 * nm <= nt || nm > nt; }
+
 // Read-only column walk over the square block r0..r0+nm-1 (rows and columns)
 // of a row-major matrix M: out_c = scale * sum_r M[r][c] x_{r-r0}.  One thread
-// per column; rows are loaded in batches of WalkCfg<T>::batch before any is
-// used, so a batch costs about one L2 round trip.  Kept out of line (as is
-// panel_walk) so that its batch registers are allocated apart from the rest
-// of the eigensolver.
+// per column (or per column half, see walk_split; the second halves' sums go
+// through `part`, nm entries); rows are loaded in batches of WalkCfg<T>::batch
+// before any is used, so a batch costs about one L2 round trip.  Kept out of
+// line (as is panel_walk) so that its batch registers are allocated apart from
+// the rest of the eigensolver.
 template <typename T>
-__device__ __noinline__ void colwalk(const T* M, int n, int r0, int nm, const T* x, T* out, T scale) {
+__device__ __noinline__ void colwalk(const T* M, int n, int r0, int nm, const T* x, T* out, T scale, T* part) {
   constexpr int kWalkBatch = WalkCfg<T>::batch;
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int jj = tid; jj < nm; jj += nt) {
+  const bool split = walk_split(nm, nt);
+  const int half = split ? (nm + 1) >> 1 : nm, nunit = split ? 2 * nm : nm;
+  for (int un = tid; un < nunit; un += nt) {
+    const int h = un >= nm, jj = h ? un - nm : un;
+    const int rb = h ? half : 0, re = h ? nm : half;
     const int c = r0 + jj;
     T acc = T(0);
-    for (int i0 = 0; i0 < nm; i0 += kWalkBatch) {
+    for (int i0 = rb; i0 < re; i0 += kWalkBatch) {
       T q[kWalkBatch];
 #pragma unroll
       for (int u = 0; u < kWalkBatch; ++u)
-        q[u] = (i0 + u < nm) ? M[(long long)(r0 + i0 + u) * n + c] : T(0);
+        q[u] = (i0 + u < re) ? M[(long long)(r0 + i0 + u) * n + c] : T(0);
 #pragma unroll
       for (int u = 0; u < kWalkBatch; ++u)
-        if (i0 + u < nm) acc += q[u] * x[i0 + u];
+        if (i0 + u < re) acc += q[u] * x[i0 + u];
     }
-    out[jj] = scale * acc;
+    if (h) part[jj] = acc;
+    else out[jj] = split ? acc : scale * acc;
+  }
+  if (split) {
+    __syncthreads();
+    for (int jj = tid; jj < nm; jj += nt) out[jj] = scale * (out[jj] + part[jj]);
   }
 }
 
@@ -411,12 +427,18 @@ __device__ __noinline__ void colwalk(const T* M, int n, int r0, int nm, const T*
 // r0..r0+nm-1 (both relative to the matrix origin, the block is square):
 // M -= sum_i PV_i PW_i^T + PW_i PV_i^T over the panel's pairs (absolute
 // index), and out_c = scale * sum_r M_new[r][c] x_{r-r0}.  One thread per
-// column keeps its column's pair entries in registers.
+// column (or column half, as in colwalk) keeps its column's pair entries in
+// registers.
 template <typename T>
-__device__ __noinline__ void panel_walk(T* M, int n, int r0, int nm, const T* PV, const T* PW, const T* x, T* out, T scale) {
+__device__ __noinline__ void panel_walk(T* M, int n, int r0, int nm, const T* PV, const T* PW, const T* x, T* out,
+                                        T scale, T* part) {
   constexpr int kPanel = PanelCfg<T>::width, kPanelBatch = PanelCfg<T>::batch;
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int jj = tid; jj < nm; jj += nt) {
+  const bool split = walk_split(nm, nt);
+  const int half = split ? (nm + 1) >> 1 : nm, nunit = split ? 2 * nm : nm;
+  for (int un = tid; un < nunit; un += nt) {
+    const int h = un >= nm, jj = h ? un - nm : un;
+    const int rb = h ? half : 0, re = h ? nm : half;
     const int c = r0 + jj;
     T vc[kPanel], wc[kPanel];
 #pragma unroll
@@ -425,14 +447,14 @@ __device__ __noinline__ void panel_walk(T* M, int n, int r0, int nm, const T* PV
       wc[i] = PW[(long long)i * n + c];
     }
     T acc = T(0);
-    for (int i0 = 0; i0 < nm; i0 += kPanelBatch) {
+    for (int i0 = rb; i0 < re; i0 += kPanelBatch) {
       T q[kPanelBatch];
 #pragma unroll
       for (int u = 0; u < kPanelBatch; ++u)
-        q[u] = (i0 + u < nm) ? M[(long long)(r0 + i0 + u) * n + c] : T(0);
+        q[u] = (i0 + u < re) ? M[(long long)(r0 + i0 + u) * n + c] : T(0);
 #pragma unroll
       for (int u = 0; u < kPanelBatch; ++u) {
-        if (i0 + u < nm) {
+        if (i0 + u < re) {
           const int rr = r0 + i0 + u;
           T y = q[u];
 #pragma unroll
@@ -442,7 +464,12 @@ __device__ __noinline__ void panel_walk(T* M, int n, int r0, int nm, const T* PV
         }
       }
     }
-    out[jj] = scale * acc;
+    if (h) part[jj] = acc;
+    else out[jj] = split ? acc : scale * acc;
+  }
+  if (split) {
+    __syncthreads();
+    for (int jj = tid; jj < nm; jj += nt) out[jj] = scale * (out[jj] + part[jj]);
   }
 }
 
@@ -983,7 +1010,7 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
     const int nref = n - 2;     // reflectors 0 .. n-3
     reflector(A, n, 0, v, tau, e, red, sh);
     // p0 = tau0 * A[1..][1..] v0
-    colwalk<T>(A, n, 1, n - 1, v, p, tau[0]);
+    colwalk<T>(A, n, 1, n - 1, v, p, tau[0], w);
     __syncthreads();
     int np = 0;  // pairs in the open panel
     for (int k = 0; k < nref; ++k) {
@@ -1033,10 +1060,10 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
       if (r < nref) {
         reflector(A, n, r, vn, tau, e, red, sh);
         if (np == kPanel) {  // close the panel: A -= V W^T + W V^T on the block, fused with p_r = tau_r A vn
-          panel_walk<T>(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r]);
+          panel_walk<T>(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r], w);
           np = 0;
         } else {  // p_r = tau_r A0 vn
-          colwalk<T>(A, n, r + 1, n - r - 1, vn, p, tau[r]);
+          colwalk<T>(A, n, r + 1, n - r - 1, vn, p, tau[r], w);
         }
         __syncthreads();
       }
