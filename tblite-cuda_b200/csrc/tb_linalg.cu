@@ -383,9 +383,13 @@ __device__ void reflector(T* A, int n, int k, T* v, T* tau, T* e, T* red, T* sh)
 
 // Rows of a walk over an nm-column block are split in two halves (separate
 // threads, partial sums added at the end) when that shortens the slowest
-// thread: nm <= half the threads (idle warps otherwise) or nm > the threads
-// (a second column per thread otherwise walks all rows again).
-__device__ inline bool walk_split(int nm, int nt) { return 2 * nm <= nt || nm > nt; }
+// thread's walk by more than an eighth: it walks ceil(nm/nt) whole columns,
+// or ceil(2nm/nt) halves.  True for nm <= nt/2 (idle warps otherwise) and for
+// the ranges of nm where a last partial round of whole columns would run.
+__device__ inline bool walk_split(int nm, int nt) {
+  const int whole = (nm + nt - 1) / nt * nm, halves = (2 * nm + nt - 1) / nt * ((nm + 1) >> 1);
+  return 8 * halves < 7 * whole;
+}
 
 // Read-only column walk over the square block r0..r0+nm-1 (rows and columns)
 // of a row-major matrix M: out_c = scale * sum_r M[r][c] x_{r-r0}.  One thread
@@ -470,6 +474,117 @@ __device__ __noinline__ void panel_walk(T* M, int n, int r0, int nm, const T* PV
   if (split) {
     __syncthreads();
     for (int jj = tid; jj < nm; jj += nt) out[jj] = scale * (out[jj] + part[jj]);
+  }
+}
+
+// One compact-WY block of the Q accumulation on the FP64 tensor instruction
+// (mma.sync.m8n8k4): with Zb the rows and columns c0..n-1 of Z (m x m) and Vs
+// the block's reflectors (kQBlock x m, shared memory),
+//   Wm = Zb Vs^T   (m x kQBlock, global scratch; 64-row tiles, slabs of Zb
+//                   staged in shared memory and prefetched into registers),
+//   Vs <- T^T Vs  (in place, one thread per column),
+//   Zb -= Wm Vs    (64 x 64 tiles, each warp 16 x 32 as 2 x 4 fragments,
+//                   accumulators initialised with Zb).
+// Same arithmetic as Zc <- Zc - (Zc V) T^T V^T row by row, with the products
+// on the tensor pipe and one shared-memory load per fragment instead of one
+// per multiply-add.  stage: 512 elements of shared memory.
+template <typename T>
+__device__ __noinline__ void formq_block_tc(T* Z, int n, int c0, int m, T* Vs, const T (*Ts)[kQBlock], T* Wm, T* stage) {
+  if constexpr (sizeof(T) == 8) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, tg = lane & 3;
+    T* Zb = Z + (long long)c0 * n + c0;
+    // Wm = Zb Vs^T: warp w owns rows 8w..8w+7 of the tile, the kQBlock columns as two fragments
+    for (int rt = 0; rt < m; rt += 64) {
+      double a0[2] = {0.0, 0.0}, a1[2] = {0.0, 0.0};
+      double pf[2];
+      auto fetch = [&](int k0) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int x = tid + 256 * u, r = rt + (x >> 3), c = k0 + (x & 7);
+          pf[u] = (r < m && c < m) ? Zb[(long long)r * n + c] : 0.0;
+        }
+      };
+      fetch(0);
+      for (int k0 = 0; k0 < m; k0 += 8) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) stage[tid + 256 * u] = pf[u];
+        __syncthreads();
+        if (k0 + 8 < m) fetch(k0 + 8);
+#pragma unroll
+        for (int k4 = 0; k4 < 8; k4 += 4) {
+          const int kk = k0 + k4 + tg;
+          const double af = stage[(8 * warp + g) * 8 + k4 + tg];
+#pragma unroll
+          for (int y = 0; y < 2; ++y) {
+            const double bf = kk < m ? Vs[(8 * y + g) * m + kk] : 0.0;
+            dmma(a0[y], a1[y], af, bf);
+          }
+        }
+        __syncthreads();
+      }
+      const int r = rt + 8 * warp + g;
+      if (r < m)
+#pragma unroll
+        for (int y = 0; y < 2; ++y) {
+          Wm[(long long)r * kQBlock + 8 * y + 2 * tg] = a0[y];
+          Wm[(long long)r * kQBlock + 8 * y + 2 * tg + 1] = a1[y];
+        }
+    }
+    __syncthreads();
+    // Vs <- T^T Vs
+    for (int cc = tid; cc < m; cc += nt) {
+      double vq[kQBlock];
+#pragma unroll
+      for (int q = 0; q < kQBlock; ++q) vq[q] = Vs[q * m + cc];
+#pragma unroll 2
+      for (int i = 0; i < kQBlock; ++i) {
+        double sum = 0.0;
+#pragma unroll
+        for (int q = 0; q < kQBlock; ++q) sum += Ts[q][i] * vq[q];
+        Vs[i * m + cc] = sum;
+      }
+    }
+    __syncthreads();
+    // Zb -= Wm Vs
+    const int wrow = (warp >> 1) * 16, wcol = (warp & 1) * 32;
+    for (int rt = 0; rt < m; rt += 64)
+      for (int ct = 0; ct < m; ct += 64) {
+        double d0[2][4], d1[2][4];
+#pragma unroll
+        for (int x = 0; x < 2; ++x)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) {
+            const int r = rt + wrow + 8 * x + g, c = ct + wcol + 8 * y + 2 * tg;
+            d0[x][y] = (r < m && c < m) ? Zb[(long long)r * n + c] : 0.0;
+            d1[x][y] = (r < m && c + 1 < m) ? Zb[(long long)r * n + c + 1] : 0.0;
+          }
+#pragma unroll
+        for (int k4 = 0; k4 < kQBlock; k4 += 4) {
+          double af[2], bf[4];
+#pragma unroll
+          for (int x = 0; x < 2; ++x) {
+            const int r = rt + wrow + 8 * x + g;
+            af[x] = r < m ? -Wm[(long long)r * kQBlock + k4 + tg] : 0.0;
+          }
+#pragma unroll
+          for (int y = 0; y < 4; ++y) {
+            const int c = ct + wcol + 8 * y + g;
+            bf[y] = c < m ? Vs[(k4 + tg) * m + c] : 0.0;
+          }
+#pragma unroll
+          for (int x = 0; x < 2; ++x)
+#pragma unroll
+            for (int y = 0; y < 4; ++y) dmma(d0[x][y], d1[x][y], af[x], bf[y]);
+        }
+#pragma unroll
+        for (int x = 0; x < 2; ++x)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) {
+            const int r = rt + wrow + 8 * x + g, c = ct + wcol + 8 * y + 2 * tg;
+            if (r < m && c < m) Zb[(long long)r * n + c] = d0[x][y];
+            if (r < m && c + 1 < m) Zb[(long long)r * n + c + 1] = d1[x][y];
+          }
+      }
   }
 }
 
@@ -954,54 +1069,22 @@ __device__ bool dc_solve(T* d, T* e, T* Z, T* G0, T* G1, int n, T* ws, T* red) {
   return s_fail == 0;
 }
 
+// Phase 1 of syev_body: A (n x n, symmetric, row-major) is reduced to
+// tridiagonal form in place; reflector k is stored in row k of A from column
+// k+1 on (leading 1), its scale in tau[k], the off-diagonal in e.  Out of line
+// so that its registers are allocated apart from the later phases.
 template <typename T>
-__device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab, T* __restrict__ Zb,
-                                          T* __restrict__ Sb, double* __restrict__ wout, int* __restrict__ perm,
-                                          int* __restrict__ status, const int* __restrict__ active) {
-  const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;  // largest structures first
-  if (active && !active[m]) return;
-  if (status[m] != kStOk) return;
-  const int n = B.ooff[m + 1] - B.ooff[m];
-  if (on_library(B, n)) return;
-  const long long mo = B.moff[m];
-  const long long vo = B.ooff[m];
-  T* A = Ab + mo;
-  T* Z = Zb + mo;
-  extern __shared__ __align__(16) unsigned char syev_smem[];
-  T* sm = reinterpret_cast<T*>(syev_smem);
-  T* d = sm;          // n
-  T* e = d + n;       // n
-  T* tau = e + n;     // n
-  T* v = tau + n;     // n
-  T* vn = v + n;      // n
-  T* p = vn + n;      // n
-  T* w = p + n;       // n
-  T* ring = w + n;    // kRing slots x (n cosines + n sines)
-  __shared__ T red[kEigThreads / 32];
-  __shared__ T sh[4];
-  __shared__ int q_full, q_end, q_fail, sh_head[kRing][2];
-  __shared__ int q_done[kEigThreads / 32];  // sweeps finished, per consumer warp
+__device__ __noinline__ void tridiagonalise(T* A, int n, T* e, T* tau, T* v, T* vn, T* p, T* w, T* ring, T* red,
+                                            T* sh) {
   const int tid = threadIdx.x, nt = blockDim.x;
-
-  // symmetrise
-  for (long long x = tid; x < (long long)n * n; x += nt) {
-    const int i = (int)(x / n), j = (int)(x % n);
-    if (i < j) {
-      const T s = T(0.5) * (A[(long long)i * n + j] + A[(long long)j * n + i]);
-      A[(long long)i * n + j] = s;
-      A[(long long)j * n + i] = s;
-    }
-  }
-  for (int i = tid; i < n; i += nt) { e[i] = T(0); tau[i] = T(0); }
-  __syncthreads();
-
-  // ---- 1. tridiagonalisation in panels of PanelCfg<T>::width reflectors.  Within a
+  // tridiagonalisation in panels of PanelCfg<T>::width reflectors.  Within a
   // panel the trailing block keeps its value A0 from the panel start; step k
   // forms p = tau A0 v and corrects it with the open pairs (v_i, w_i):
   // A = A0 - sum_i (v_i w_i^T + w_i v_i^T).  Only the row that yields the next
   // reflector is brought up to date; the block itself is rewritten once, when
   // the panel closes, fused with the next step's product.
-  if (n >= 3) {
+  if (n < 3) return;
+  {
     const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
     constexpr int kPanel = PanelCfg<T>::width;
     T* PV = ring;               // kPanel x n: v_i of the open panel (absolute index)
@@ -1070,11 +1153,15 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
       T* t = v; v = vn; vn = t;
     }
   }
-  for (int i = tid; i < n; i += nt) d[i] = A[(long long)i * n + i];
-  if (tid == 0 && n >= 2) e[n - 2] = A[(long long)(n - 2) * n + n - 1];
-  __syncthreads();
+}
 
-  // ---- 2. Zc = Q^T (row c of Zc = column c of Q), Q = H_0 H_1 ... H_{n-3},
+// Phase 2 of syev_body: Z = Q^T from the reflectors left in A and tau by
+// tridiagonalise.  ring: kQBlock x n of shared memory; stage: 4n free shared
+// elements; Sq: an n x n global scratch (or null).  Out of line like phase 1.
+template <typename T>
+__device__ __noinline__ void form_q(const T* A, T* Z, int n, const T* tau, T* ring, T* stage, T* Sq) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  // Zc = Q^T (row c of Zc = column c of Q), Q = H_0 H_1 ... H_{n-3},
   // accumulated backwards in blocks of kQBlock reflectors in compact WY form:
   // H_k0 ... H_k1 = I - V T V^T (V = [v_k0 .. v_k1], T upper triangular), so
   // Zc <- Zc H_k1 ... H_k0 = Zc - (Zc V) T^T V^T on rows and columns >= k0+1.
@@ -1090,6 +1177,9 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
     __shared__ T yv[kQBlock][kQBlock];          // V^T V (upper part)
     __shared__ T wps[kEigThreads / 32][kQBlock];  // per warp: (row . V) T^T
     T* Vs = ring;                               // kQBlock x m, m <= n - 1
+    // FP64 with a scratch matrix: each block's products on the tensor pipe
+    // (formq_block_tc; Wm in Sq, slabs staged in stage, 4n >= 512)
+    const bool tcq = Sq && sizeof(T) == 8 && n >= kDcMin && nt == 256;
     const int nref = n - 2;
     for (int k1 = nref - 1; k1 >= 0; k1 -= kQBlock) {
       const int k0 = k1 - kQBlock + 1 > 0 ? k1 - kQBlock + 1 : 0, bb = k1 - k0 + 1;
@@ -1128,6 +1218,11 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
         }
       }
       __syncthreads();
+      if (tcq) {
+        formq_block_tc<T>(Z, n, c0, m, Vs, Ts, Sq, stage);
+        __syncthreads();
+        continue;
+      }
       for (int r = c0 + wid; r < n; r += nw) {
         T* zr = Z + (long long)r * n + c0;
         T acc[kQBlock];
@@ -1161,6 +1256,56 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
       __syncthreads();
     }
   }
+
+}
+
+template <typename T>
+__device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab, T* __restrict__ Zb,
+                                          T* __restrict__ Sb, double* __restrict__ wout, int* __restrict__ perm,
+                                          int* __restrict__ status, const int* __restrict__ active) {
+  const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;  // largest structures first
+  if (active && !active[m]) return;
+  if (status[m] != kStOk) return;
+  const int n = B.ooff[m + 1] - B.ooff[m];
+  if (on_library(B, n)) return;
+  const long long mo = B.moff[m];
+  const long long vo = B.ooff[m];
+  T* A = Ab + mo;
+  T* Z = Zb + mo;
+  extern __shared__ __align__(16) unsigned char syev_smem[];
+  T* sm = reinterpret_cast<T*>(syev_smem);
+  T* d = sm;          // n
+  T* e = d + n;       // n
+  T* tau = e + n;     // n
+  T* v = tau + n;     // n
+  T* vn = v + n;      // n
+  T* p = vn + n;      // n
+  T* w = p + n;       // n
+  T* ring = w + n;    // kRing slots x (n cosines + n sines)
+  __shared__ T red[kEigThreads / 32];
+  __shared__ T sh[4];
+  __shared__ int q_full, q_end, q_fail, sh_head[kRing][2];
+  __shared__ int q_done[kEigThreads / 32];  // sweeps finished, per consumer warp
+  const int tid = threadIdx.x, nt = blockDim.x;
+
+  // symmetrise
+  for (long long x = tid; x < (long long)n * n; x += nt) {
+    const int i = (int)(x / n), j = (int)(x % n);
+    if (i < j) {
+      const T s = T(0.5) * (A[(long long)i * n + j] + A[(long long)j * n + i]);
+      A[(long long)i * n + j] = s;
+      A[(long long)j * n + i] = s;
+    }
+  }
+  for (int i = tid; i < n; i += nt) { e[i] = T(0); tau[i] = T(0); }
+  __syncthreads();
+
+  tridiagonalise<T>(A, n, e, tau, v, vn, p, w, ring, red, sh);
+  for (int i = tid; i < n; i += nt) d[i] = A[(long long)i * n + i];
+  if (tid == 0 && n >= 2) e[n - 2] = A[(long long)(n - 2) * n + n - 1];
+  __syncthreads();
+
+  form_q<T>(A, Z, n, tau, ring, tau + n, Sb ? Sb + mo : nullptr);
 
   // ---- 3a. divide and conquer when a scratch buffer is given (A is free now)
   if (Sb && n >= kDcMin && dc_ws_elems<T>(n) <= (5 + 2 * kRing) * n) {
