@@ -319,8 +319,13 @@ namespace {
 template <typename T> struct PanelCfg;
 template <> struct PanelCfg<double> { static constexpr int width = 8, batch = 6; };
 template <> struct PanelCfg<float> { static constexpr int width = 1, batch = 12; };
-// rows per load batch of the read-only Householder column walk
-template <typename T> struct WalkCfg { static constexpr int batch = sizeof(T) == 8 ? 24 : 12; };
+// Read-only Householder walk (colwalk): the warps form kWalkRowGroups row
+// groups (interleaved rows) times nw / kWalkRowGroups column groups; a lane
+// holds `cols` columns (32 apart) of its group's strip and loads `rows` rows
+// of them before using any, so a warp reads whole row segments (contiguous
+// for DRAM) with cols * rows loads in flight per lane.
+constexpr int kWalkRowGroups = 4;
+template <typename T> struct WalkCfg { static constexpr int cols = 3, rows = 4; };
 static_assert(PanelCfg<double>::width <= kRing && PanelCfg<float>::width <= kRing, "panel exceeds the ring");
 constexpr int kQBlock = 16;     // reflectors per compact-WY block of the Q accumulation
 constexpr int kWaveK = 4;            // QL sweeps applied per pass over Zc
@@ -391,47 +396,60 @@ __device__ inline bool walk_split(int nm, int nt) {
   return 8 * halves < 7 * whole;
 }
 
-// Read-only column walk over the square block r0..r0+nm-1 (rows and columns)
-// of a row-major matrix M: out_c = scale * sum_r M[r][c] x_{r-r0}.  One thread
-// per column (or per column half, see walk_split; the second halves' sums go
-// through `part`, nm entries); rows are loaded in batches of WalkCfg<T>::batch
-// before any is used, so a batch costs about one L2 round trip.  Kept out of
-// line (as is panel_walk) so that its batch registers are allocated apart from
-// the rest of the eigensolver.
+// Read-only walk over the square block r0..r0+nm-1 (rows and columns) of a
+// row-major matrix M: out_c = scale * sum_r M[r][c] x_{r-r0}.  Row group g
+// (warps g, g + kWalkRowGroups, ...) sums rows g, g + kWalkRowGroups, ... into
+// its own partial vector (group 0: out, groups 1..3: p1, p2, p3, nm entries
+// each, distinct from x and out); the partials are added at the end in a fixed
+// order, so the result is deterministic.  Needs a multiple of kWalkRowGroups
+// warps.  Kept out of line (as is panel_walk) so that its load registers are
+// allocated apart from the rest of the eigensolver.
 template <typename T>
-__device__ __noinline__ void colwalk(const T* M, int n, int r0, int nm, const T* x, T* out, T scale, T* part) {
-  constexpr int kWalkBatch = WalkCfg<T>::batch;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const bool split = walk_split(nm, nt);
-  const int half = split ? (nm + 1) >> 1 : nm, nunit = split ? 2 * nm : nm;
-  for (int un = tid; un < nunit; un += nt) {
-    const int h = un >= nm, jj = h ? un - nm : un;
-    const int rb = h ? half : 0, re = h ? nm : half;
-    const int c = r0 + jj;
-    T acc = T(0);
-    for (int i0 = rb; i0 < re; i0 += kWalkBatch) {
-      T q[kWalkBatch];
+__device__ __noinline__ void colwalk(const T* M, int n, int r0, int nm, const T* x, T* out, T scale, T* p1, T* p2,
+                                     T* p3) {
+  constexpr int kJ = WalkCfg<T>::cols, kR = WalkCfg<T>::rows, kG = kWalkRowGroups;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int ncg = (nt >> 5) / kG, rg = warp % kG, cg = warp / kG;
+  const int strip = 32 * kJ * ncg;  // columns per pass
+  T* mine = rg == 0 ? out : (rg == 1 ? p1 : (rg == 2 ? p2 : p3));
+  const T* Mb = M + (long long)r0 * n + r0;
+  for (int c0 = 0; c0 < nm; c0 += strip) {
+    const int cb = c0 + cg * 32 * kJ + lane;
+    T acc[kJ];
 #pragma unroll
-      for (int u = 0; u < kWalkBatch; ++u)
-        q[u] = (i0 + u < re) ? M[(long long)(r0 + i0 + u) * n + c] : T(0);
+    for (int j = 0; j < kJ; ++j) acc[j] = T(0);
+    for (int rb = rg; rb < nm; rb += kG * kR) {
+      T q[kR][kJ];
 #pragma unroll
-      for (int u = 0; u < kWalkBatch; ++u)
-        if (i0 + u < re) acc += q[u] * x[i0 + u];
+      for (int u = 0; u < kR; ++u)
+#pragma unroll
+        for (int j = 0; j < kJ; ++j) {
+          const int r = rb + kG * u, c = cb + 32 * j;
+          q[u][j] = (r < nm && c < nm) ? Mb[(long long)r * n + c] : T(0);
+        }
+#pragma unroll
+      for (int u = 0; u < kR; ++u) {
+        const int r = rb + kG * u;
+        const T xr = r < nm ? x[r] : T(0);
+#pragma unroll
+        for (int j = 0; j < kJ; ++j) acc[j] += q[u][j] * xr;
+      }
     }
-    if (h) part[jj] = acc;
-    else out[jj] = split ? acc : scale * acc;
+#pragma unroll
+    for (int j = 0; j < kJ; ++j) {
+      const int c = cb + 32 * j;
+      if (c < nm) mine[c] = acc[j];
+    }
   }
-  if (split) {
-    __syncthreads();
-    for (int jj = tid; jj < nm; jj += nt) out[jj] = scale * (out[jj] + part[jj]);
-  }
+  __syncthreads();
+  for (int c = tid; c < nm; c += nt) out[c] = scale * (((out[c] + p1[c]) + p2[c]) + p3[c]);
 }
 
 // Closing walk of a tridiagonalisation panel over rows and columns
 // r0..r0+nm-1 (both relative to the matrix origin, the block is square):
 // M -= sum_i PV_i PW_i^T + PW_i PV_i^T over the panel's pairs (absolute
 // index), and out_c = scale * sum_r M_new[r][c] x_{r-r0}.  One thread per
-// column (or column half, as in colwalk) keeps its column's pair entries in
+// column (or column half, see walk_split) keeps its column's pair entries in
 // registers.
 template <typename T>
 __device__ __noinline__ void panel_walk(T* M, int n, int r0, int nm, const T* PV, const T* PW, const T* x, T* out,
@@ -1074,8 +1092,8 @@ __device__ bool dc_solve(T* d, T* e, T* Z, T* G0, T* G1, int n, T* ws, T* red) {
 // k+1 on (leading 1), its scale in tau[k], the off-diagonal in e.  Out of line
 // so that its registers are allocated apart from the later phases.
 template <typename T>
-__device__ __noinline__ void tridiagonalise(T* A, int n, T* e, T* tau, T* v, T* vn, T* p, T* w, T* ring, T* red,
-                                            T* sh) {
+__device__ __noinline__ void tridiagonalise(T* A, int n, T* e, T* tau, T* v, T* vn, T* p, T* w, T* d, T* ring,
+                                            T* red, T* sh) {
   const int tid = threadIdx.x, nt = blockDim.x;
   // tridiagonalisation in panels of PanelCfg<T>::width reflectors.  Within a
   // panel the trailing block keeps its value A0 from the panel start; step k
@@ -1093,7 +1111,7 @@ __device__ __noinline__ void tridiagonalise(T* A, int n, T* e, T* tau, T* v, T* 
     const int nref = n - 2;     // reflectors 0 .. n-3
     reflector(A, n, 0, v, tau, e, red, sh);
     // p0 = tau0 * A[1..][1..] v0
-    colwalk<T>(A, n, 1, n - 1, v, p, tau[0], w);
+    colwalk<T>(A, n, 1, n - 1, v, p, tau[0], w, d, vn);
     __syncthreads();
     int np = 0;  // pairs in the open panel
     for (int k = 0; k < nref; ++k) {
@@ -1146,7 +1164,7 @@ __device__ __noinline__ void tridiagonalise(T* A, int n, T* e, T* tau, T* v, T* 
           panel_walk<T>(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r], w);
           np = 0;
         } else {  // p_r = tau_r A0 vn
-          colwalk<T>(A, n, r + 1, n - r - 1, vn, p, tau[r], w);
+          colwalk<T>(A, n, r + 1, n - r - 1, vn, p, tau[r], w, d, v);  // v is in PV already
         }
         __syncthreads();
       }
@@ -1300,7 +1318,7 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
   for (int i = tid; i < n; i += nt) { e[i] = T(0); tau[i] = T(0); }
   __syncthreads();
 
-  tridiagonalise<T>(A, n, e, tau, v, vn, p, w, ring, red, sh);
+  tridiagonalise<T>(A, n, e, tau, v, vn, p, w, d, ring, red, sh);  // d: scratch until the end
   for (int i = tid; i < n; i += nt) d[i] = A[(long long)i * n + i];
   if (tid == 0 && n >= 2) e[n - 2] = A[(long long)(n - 2) * n + n - 1];
   __syncthreads();
