@@ -495,6 +495,88 @@ __device__ __noinline__ void panel_walk(T* M, int n, int r0, int nm, const T* PV
   }
 }
 
+// FP64 panel-closing walk on the tensor instruction (mma.sync m8n8k4), same
+// result as panel_walk up to rounding: with the panel's 8 pairs as
+// K = [PV; PW] (16 x n) and L = [PW; PV], the block is updated as
+// M -= K^T L over 16 x 32 tiles per warp (accumulators initialised from M,
+// stored back), and out_c = scale * sum_r M_new[r][c] x_{r-r0} is formed from
+// the same fragments.  Warps as in colwalk: kWalkRowGroups groups of
+// interleaved 16-row tiles times nw / kWalkRowGroups column groups; the row
+// groups' partial sums go through out, p1, p2, p3 (nm entries each).
+__device__ __noinline__ void panel_walk_tc(double* M, int n, int r0, int nm, const double* PV, const double* PW,
+                                           const double* x, double* out, double scale, double* p1, double* p2,
+                                           double* p3) {
+  static_assert(PanelCfg<double>::width == 8, "two panel halves of four k-steps");
+  constexpr int kG = kWalkRowGroups;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+  const int ncg = (nt >> 5) / kG, rg = warp % kG, cg = warp / kG;
+  double* mine = rg == 0 ? out : (rg == 1 ? p1 : (rg == 2 ? p2 : p3));
+  double* Mb = M + (long long)r0 * n + r0;
+  for (int c0 = 0; c0 < nm; c0 += 32 * ncg) {
+    const int cw = c0 + 32 * cg;  // this warp's first column (relative)
+    for (int rt = 16 * rg; rt < nm; rt += 16 * kG) {
+      double d[2][4][2];
+#pragma unroll
+      for (int xx = 0; xx < 2; ++xx)
+#pragma unroll
+        for (int y = 0; y < 4; ++y)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int r = rt + 8 * xx + g, c = cw + 8 * y + 2 * t + h;
+            d[xx][y][h] = (r < nm && c < nm) ? Mb[(long long)r * n + c] : 0.0;
+          }
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        const int k = 4 * (ks & 1) + t;                                 // pair index
+        const double* Kr = (ks < 2 ? PV : PW) + (long long)k * n + r0;  // row side
+        const double* Lc = (ks < 2 ? PW : PV) + (long long)k * n + r0;  // column side
+        double a[2], b[4];
+#pragma unroll
+        for (int xx = 0; xx < 2; ++xx) {
+          const int r = rt + 8 * xx + g;
+          a[xx] = r < nm ? -Kr[r] : 0.0;
+        }
+#pragma unroll
+        for (int y = 0; y < 4; ++y) {
+          const int c = cw + 8 * y + g;
+          b[y] = c < nm ? Lc[c] : 0.0;
+        }
+#pragma unroll
+        for (int xx = 0; xx < 2; ++xx)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) dmma(d[xx][y][0], d[xx][y][1], a[xx], b[y]);
+      }
+      const double x0 = rt + g < nm ? x[rt + g] : 0.0, x1 = rt + 8 + g < nm ? x[rt + 8 + g] : 0.0;
+#pragma unroll
+      for (int xx = 0; xx < 2; ++xx)
+#pragma unroll
+        for (int y = 0; y < 4; ++y)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int r = rt + 8 * xx + g, c = cw + 8 * y + 2 * t + h;
+            if (r < nm && c < nm) Mb[(long long)r * n + c] = d[xx][y][h];
+          }
+      // this tile's column sums over its 16 rows (the eight row lanes g are
+      // lanes t, t + 4, ..., t + 28), added to the warp's own entries of `mine`
+#pragma unroll
+      for (int y = 0; y < 4; ++y)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          double v = d[0][y][h] * x0 + d[1][y][h] * x1;
+          v += __shfl_xor_sync(0xffffffffu, v, 4);
+          v += __shfl_xor_sync(0xffffffffu, v, 8);
+          v += __shfl_xor_sync(0xffffffffu, v, 16);
+          const int c = cw + 8 * y + 2 * t + h;
+          if (g == 0 && c < nm) mine[c] = rt == 16 * rg ? v : mine[c] + v;
+        }
+    }
+    if (16 * rg >= nm)  // a row group without rows still owns its partial entries
+      for (int c = cw + lane; c < cw + 32 && c < nm; c += 32) mine[c] = 0.0;
+  }
+  __syncthreads();
+  for (int c = tid; c < nm; c += nt) out[c] = scale * (((out[c] + p1[c]) + p2[c]) + p3[c]);
+}
+
 // One compact-WY block of the Q accumulation on the FP64 tensor instruction
 // (mma.sync.m8n8k4): with Zb the rows and columns c0..n-1 of Z (m x m) and Vs
 // the block's reflectors (kQBlock x m, shared memory),
@@ -1161,7 +1243,10 @@ __device__ __noinline__ void tridiagonalise(T* A, int n, T* e, T* tau, T* v, T* 
       if (r < nref) {
         reflector(A, n, r, vn, tau, e, red, sh);
         if (np == kPanel) {  // close the panel: A -= V W^T + W V^T on the block, fused with p_r = tau_r A vn
-          panel_walk<T>(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r], w);
+          if constexpr (sizeof(T) == 8)
+            panel_walk_tc(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r], w, d, v);  // v is in PV already
+          else
+            panel_walk<T>(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r], w);
           np = 0;
         } else {  // p_r = tau_r A0 vn
           colwalk<T>(A, n, r + 1, n - r - 1, vn, p, tau[r], w, d, v);  // v is in PV already
