@@ -445,6 +445,85 @@ __device__ __noinline__ void colwalk(const T* M, int n, int r0, int nm, const T*
   for (int c = tid; c < nm; c += nt) out[c] = scale * (((out[c] + p1[c]) + p2[c]) + p3[c]);
 }
 
+// The same product as colwalk from the upper triangle of the block only
+// (half the bytes): with U the upper triangle including the diagonal,
+// out = scale (U^T x + (U - diag) x).  Warp w takes rows w, w + 8, ...: for
+// each strip of 32 kSymCols columns a lane loads the upper part of kSymRows
+// of its rows at a time; the column products go to the warp's own vector
+// gp[w][.] (global scratch, 8 nm entries), the row products are reduced
+// across the warp and added to out[r] (the row's owner warp only), then
+// out_c = scale (out_c + sum_w gp[w][c]) in a fixed order.  FP64, 8 warps.
+constexpr int kSymCols = 3, kSymRows = 4, kSymMin = 96;  // kSymMin: smallest block that takes symwalk
+__device__ __noinline__ void symwalk(const double* M, int n, int r0, int nm, const double* x, double* out, double scale,
+                                     double* gp) {
+  static_assert(kSymRows == 4, "the row reduction below pairs four rows");
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const double* Mb = M + (long long)r0 * n + r0;
+  for (int c = tid; c < nm; c += nt) out[c] = 0.0;
+  __syncthreads();
+  for (int cs = 0; cs < nm; cs += 32 * kSymCols) {
+    const int ce = min(cs + 32 * kSymCols, nm);
+    double xs[kSymCols], acc[kSymCols];
+#pragma unroll
+    for (int j = 0; j < kSymCols; ++j) {
+      const int c = cs + lane + 32 * j;
+      xs[j] = c < nm ? x[c] : 0.0;
+      acc[j] = 0.0;
+    }
+    for (int rb = warp; rb < ce; rb += 8 * kSymRows) {
+      double a[kSymRows][kSymCols];
+#pragma unroll
+      for (int u = 0; u < kSymRows; ++u)
+#pragma unroll
+        for (int j = 0; j < kSymCols; ++j) {
+          const int r = rb + 8 * u, c = cs + lane + 32 * j;
+          a[u][j] = (r < ce && c >= r && c < nm) ? Mb[(long long)r * n + c] : 0.0;
+        }
+      double v[kSymRows];
+#pragma unroll
+      for (int u = 0; u < kSymRows; ++u) {
+        const int r = rb + 8 * u;
+        const double xr = r < nm ? x[r] : 0.0;
+        v[u] = 0.0;
+#pragma unroll
+        for (int j = 0; j < kSymCols; ++j) {
+          const int c = cs + lane + 32 * j;
+          acc[j] += a[u][j] * xr;
+          if (c > r) v[u] += a[u][j] * xs[j];
+        }
+      }
+      // the four row sums across the warp: halves exchange pairs (xor 16),
+      // quarters exchange one (xor 8), then a butterfly over the last 3 bits;
+      // lane 8u ends with the total of row u
+      const bool h16 = lane & 16, h8 = lane & 8;
+      double k0 = h16 ? v[2] : v[0], k1 = h16 ? v[3] : v[1];
+      k0 += __shfl_xor_sync(0xffffffffu, h16 ? v[0] : v[2], 16);
+      k1 += __shfl_xor_sync(0xffffffffu, h16 ? v[1] : v[3], 16);
+      double k = h8 ? k1 : k0;
+      k += __shfl_xor_sync(0xffffffffu, h8 ? k0 : k1, 8);
+      k += __shfl_xor_sync(0xffffffffu, k, 4);
+      k += __shfl_xor_sync(0xffffffffu, k, 2);
+      k += __shfl_xor_sync(0xffffffffu, k, 1);
+      if ((lane & 7) == 0) {
+        const int r = rb + 8 * (lane >> 3);
+        if (r < ce) out[r] += k;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kSymCols; ++j) {
+      const int c = cs + lane + 32 * j;
+      if (c < nm) gp[(long long)warp * nm + c] = acc[j];
+    }
+  }
+  __syncthreads();
+  for (int c = tid; c < nm; c += nt) {
+    double t = out[c];
+#pragma unroll
+    for (int w = 0; w < 8; ++w) t += gp[(long long)w * nm + c];
+    out[c] = scale * t;
+  }
+}
+
 // Closing walk of a tridiagonalisation panel over rows and columns
 // r0..r0+nm-1 (both relative to the matrix origin, the block is square):
 // M -= sum_i PV_i PW_i^T + PW_i PV_i^T over the panel's pairs (absolute
@@ -1175,7 +1254,7 @@ __device__ bool dc_solve(T* d, T* e, T* Z, T* G0, T* G1, int n, T* ws, T* red) {
 // so that its registers are allocated apart from the later phases.
 template <typename T>
 __device__ __noinline__ void tridiagonalise(T* A, int n, T* e, T* tau, T* v, T* vn, T* p, T* w, T* d, T* ring,
-                                            T* red, T* sh) {
+                                            T* red, T* sh, T* gs) {
   const int tid = threadIdx.x, nt = blockDim.x;
   // tridiagonalisation in panels of PanelCfg<T>::width reflectors.  Within a
   // panel the trailing block keeps its value A0 from the panel start; step k
@@ -1249,7 +1328,14 @@ __device__ __noinline__ void tridiagonalise(T* A, int n, T* e, T* tau, T* v, T* 
             panel_walk<T>(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r], w);
           np = 0;
         } else {  // p_r = tau_r A0 vn
-          colwalk<T>(A, n, r + 1, n - r - 1, vn, p, tau[r], w, d, v);  // v is in PV already
+          if constexpr (sizeof(T) == 8) {
+            if (gs && n - r - 1 >= kSymMin)
+              symwalk(A, n, r + 1, n - r - 1, vn, p, tau[r], gs);
+            else
+              colwalk<T>(A, n, r + 1, n - r - 1, vn, p, tau[r], w, d, v);  // v is in PV already
+          } else {
+            colwalk<T>(A, n, r + 1, n - r - 1, vn, p, tau[r], w, d, v);
+          }
         }
         __syncthreads();
       }
@@ -1403,7 +1489,9 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
   for (int i = tid; i < n; i += nt) { e[i] = T(0); tau[i] = T(0); }
   __syncthreads();
 
-  tridiagonalise<T>(A, n, e, tau, v, vn, p, w, d, ring, red, sh);  // d: scratch until the end
+  // d: scratch until the end; the global scratch (8n entries) takes the partial products of symwalk
+  const bool symw = sizeof(T) == 8 && Sb && nt == 256 && n >= kSymMin + 1;
+  tridiagonalise<T>(A, n, e, tau, v, vn, p, w, d, ring, red, sh, symw ? Sb + mo : nullptr);
   for (int i = tid; i < n; i += nt) d[i] = A[(long long)i * n + i];
   if (tid == 0 && n >= 2) e[n - 2] = A[(long long)(n - 2) * n + n - 1];
   __syncthreads();
