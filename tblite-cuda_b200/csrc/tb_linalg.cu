@@ -453,7 +453,8 @@ __device__ __noinline__ void colwalk(const T* M, int n, int r0, int nm, const T*
 // gp[w][.] (global scratch, 8 nm entries), the row products are reduced
 // across the warp and added to out[r] (the row's owner warp only), then
 // out_c = scale (out_c + sum_w gp[w][c]) in a fixed order.  FP64, 8 warps.
-constexpr int kSymCols = 3, kSymRows = 4, kSymMin = 96;  // kSymMin: smallest block that takes symwalk
+constexpr int kSymCols = 3, kSymRows = 4;
+constexpr int kSymMin = 96;  // structures of more AOs take the upper-triangle walks (scratch of 8n <= n^2)
 __device__ __noinline__ void symwalk(const double* M, int n, int r0, int nm, const double* x, double* out, double scale,
                                      double* gp) {
   static_assert(kSymRows == 4, "the row reduction below pairs four rows");
@@ -654,6 +655,111 @@ __device__ __noinline__ void panel_walk_tc(double* M, int n, int r0, int nm, con
   }
   __syncthreads();
   for (int c = tid; c < nm; c += nt) out[c] = scale * (((out[c] + p1[c]) + p2[c]) + p3[c]);
+}
+
+// panel_walk_tc on the upper triangle of the block only (as symwalk for
+// colwalk): tiles wholly below the diagonal are skipped, entries below it are
+// neither read nor written.  Column products (entries on and above the
+// diagonal) and row products (above it) of warp w accumulate in gp[w][.]
+// (global scratch, 8 nm entries); out_c = scale sum_w gp[w][c].
+__device__ __noinline__ void panel_walk_tc_sym(double* M, int n, int r0, int nm, const double* PV, const double* PW,
+                                               const double* x, double* out, double scale, double* gp) {
+  constexpr int kG = kWalkRowGroups;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+  const int ncg = (nt >> 5) / kG, rg = warp % kG, cg = warp / kG;
+  double* mine = gp + (long long)warp * nm;
+  for (int c = lane; c < nm; c += 32) mine[c] = 0.0;
+  __syncwarp();
+  double* Mb = M + (long long)r0 * n + r0;
+  for (int c0 = 0; c0 < nm; c0 += 32 * ncg) {
+    const int cw = c0 + 32 * cg;  // this warp's first column (relative)
+    if (cw >= nm) continue;
+    const int rend = min(nm, cw + 32);  // rows with an entry on or above the diagonal in these columns
+    for (int rt = 16 * rg; rt < rend; rt += 16 * kG) {
+      double d[2][4][2];
+#pragma unroll
+      for (int xx = 0; xx < 2; ++xx)
+#pragma unroll
+        for (int y = 0; y < 4; ++y)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int r = rt + 8 * xx + g, c = cw + 8 * y + 2 * t + h;
+            d[xx][y][h] = (r < nm && c < nm && c >= r) ? Mb[(long long)r * n + c] : 0.0;
+          }
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        const int k = 4 * (ks & 1) + t;
+        const double* Kr = (ks < 2 ? PV : PW) + (long long)k * n + r0;
+        const double* Lc = (ks < 2 ? PW : PV) + (long long)k * n + r0;
+        double a[2], b[4];
+#pragma unroll
+        for (int xx = 0; xx < 2; ++xx) {
+          const int r = rt + 8 * xx + g;
+          a[xx] = r < nm ? -Kr[r] : 0.0;
+        }
+#pragma unroll
+        for (int y = 0; y < 4; ++y) {
+          const int c = cw + 8 * y + g;
+          b[y] = c < nm ? Lc[c] : 0.0;
+        }
+#pragma unroll
+        for (int xx = 0; xx < 2; ++xx)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) dmma(d[xx][y][0], d[xx][y][1], a[xx], b[y]);
+      }
+      // store the upper entries and drop the others from the products below
+#pragma unroll
+      for (int xx = 0; xx < 2; ++xx)
+#pragma unroll
+        for (int y = 0; y < 4; ++y)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int r = rt + 8 * xx + g, c = cw + 8 * y + 2 * t + h;
+            if (r < nm && c < nm && c >= r) Mb[(long long)r * n + c] = d[xx][y][h];
+            else d[xx][y][h] = 0.0;
+          }
+      const double x0 = rt + g < nm ? x[rt + g] : 0.0, x1 = rt + 8 + g < nm ? x[rt + 8 + g] : 0.0;
+      // row products (strictly above the diagonal) over this tile's columns
+      double rp0 = 0.0, rp1 = 0.0;
+#pragma unroll
+      for (int y = 0; y < 4; ++y)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int c = cw + 8 * y + 2 * t + h;
+          const double xc = c < nm ? x[c] : 0.0;
+          if (c > rt + g) rp0 += d[0][y][h] * xc;
+          if (c > rt + 8 + g) rp1 += d[1][y][h] * xc;
+        }
+      // column products over the tile's 16 rows (row lanes g: lanes t + 4g)
+#pragma unroll
+      for (int y = 0; y < 4; ++y)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          double v = d[0][y][h] * x0 + d[1][y][h] * x1;
+          v += __shfl_xor_sync(0xffffffffu, v, 4);
+          v += __shfl_xor_sync(0xffffffffu, v, 8);
+          v += __shfl_xor_sync(0xffffffffu, v, 16);
+          const int c = cw + 8 * y + 2 * t + h;
+          if (g == 0 && c < nm) mine[c] += v;
+        }
+      __syncwarp();
+      rp0 += __shfl_xor_sync(0xffffffffu, rp0, 1);
+      rp0 += __shfl_xor_sync(0xffffffffu, rp0, 2);
+      rp1 += __shfl_xor_sync(0xffffffffu, rp1, 1);
+      rp1 += __shfl_xor_sync(0xffffffffu, rp1, 2);
+      if (t == 0) {
+        if (rt + g < nm) mine[rt + g] += rp0;
+        if (rt + 8 + g < nm) mine[rt + 8 + g] += rp1;
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int c = tid; c < nm; c += nt) {
+    double v = 0.0;
+    for (int w = 0; w < (nt >> 5); ++w) v += gp[(long long)w * nm + c];
+    out[c] = scale * v;
+  }
 }
 
 // One compact-WY block of the Q accumulation on the FP64 tensor instruction
@@ -1322,14 +1428,17 @@ __device__ __noinline__ void tridiagonalise(T* A, int n, T* e, T* tau, T* v, T* 
       if (r < nref) {
         reflector(A, n, r, vn, tau, e, red, sh);
         if (np == kPanel) {  // close the panel: A -= V W^T + W V^T on the block, fused with p_r = tau_r A vn
-          if constexpr (sizeof(T) == 8)
-            panel_walk_tc(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r], w, d, v);  // v is in PV already
-          else
+          if constexpr (sizeof(T) == 8) {
+            if (gs)  // the lower triangle is stale from the first upper-only walk on
+              panel_walk_tc_sym(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r], gs);
+            else
+              panel_walk_tc(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r], w, d, v);  // v is in PV already
+          } else
             panel_walk<T>(A, n, r + 1, n - r - 1, PV, PW, vn, p, tau[r], w);
           np = 0;
         } else {  // p_r = tau_r A0 vn
           if constexpr (sizeof(T) == 8) {
-            if (gs && n - r - 1 >= kSymMin)
+            if (gs)
               symwalk(A, n, r + 1, n - r - 1, vn, p, tau[r], gs);
             else
               colwalk<T>(A, n, r + 1, n - r - 1, vn, p, tau[r], w, d, v);  // v is in PV already
