@@ -764,37 +764,45 @@ __device__ __noinline__ void panel_walk_tc_sym(double* M, int n, int r0, int nm,
 
 // One compact-WY block of the Q accumulation on the FP64 tensor instruction
 // (mma.sync.m8n8k4): with Zb the rows and columns c0..n-1 of Z (m x m) and Vs
-// the block's reflectors (kQBlock x m, shared memory),
-//   Wm = Zb Vs^T   (m x kQBlock, global scratch; 64-row tiles, slabs of Zb
-//                   staged in shared memory and prefetched into registers),
-//   Vs <- T^T Vs  (in place, one thread per column),
-//   Zb -= Wm Vs    (64 x 64 tiles, each warp 16 x 32 as 2 x 4 fragments,
-//                   accumulators initialised with Zb).
-// Same arithmetic as Zc <- Zc - (Zc V) T^T V^T row by row, with the products
-// on the tensor pipe and one shared-memory load per fragment instead of one
-// per multiply-add.  stage: 512 elements of shared memory.
+// the block's reflectors (kQBlock x m, shared memory), for each tile of 64
+// rows of Zb in turn
+//   Wm = Zt Vs^T    (64 x kQBlock; warp w rows 8w..8w+7, slabs of 64 x 8
+//                    staged in shared memory and prefetched into registers),
+//   Wt = Wm T^T     (64 x kQBlock, four entries per thread),
+//   Zt -= Wt Vs     (64 x 64 tiles, each warp 16 x 32 as 2 x 4 fragments,
+//                    accumulators initialised with Zt),
+// so that a tile is read again by the update while it is still in L2.  Same
+// arithmetic as Zc <- Zc - (Zc V) T^T V^T row by row.  Wm and Wt go through
+// the global scratch Wq (2 x 64 x kQBlock); stage: 512 elements of shared
+// memory.  256 threads.
 template <typename T>
-__device__ __noinline__ void formq_block_tc(T* Z, int n, int c0, int m, T* Vs, const T (*Ts)[kQBlock], T* Wm, T* stage) {
+__device__ __noinline__ void formq_block_tc(T* Z, int n, int c0, int m, const T* Vs, const T (*Ts)[kQBlock], T* Wq,
+                                            T* stage) {
   if constexpr (sizeof(T) == 8) {
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, tg = lane & 3;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, tg = lane & 3;
     T* Zb = Z + (long long)c0 * n + c0;
-    // Wm = Zb Vs^T: warp w owns rows 8w..8w+7 of the tile, the kQBlock columns as two fragments
+    T* Wm = Wq;                   // 64 x kQBlock
+    T* Wt = Wq + 64 * kQBlock;    // 64 x kQBlock
+    const int wrow = (warp >> 1) * 16, wcol = (warp & 1) * 32;
     for (int rt = 0; rt < m; rt += 64) {
+      // Wm = Zt Vs^T
       double a0[2] = {0.0, 0.0}, a1[2] = {0.0, 0.0};
       double pf[2];
-      auto fetch = [&](int k0) {
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int x = tid + 256 * u, r = rt + (x >> 3), c = k0 + (x & 7);
-          pf[u] = (r < m && c < m) ? Zb[(long long)r * n + c] : 0.0;
-        }
-      };
-      fetch(0);
+      for (int u = 0; u < 2; ++u) {
+        const int x = tid + 256 * u, r = rt + (x >> 3), c = x & 7;
+        pf[u] = (r < m && c < m) ? Zb[(long long)r * n + c] : 0.0;
+      }
       for (int k0 = 0; k0 < m; k0 += 8) {
 #pragma unroll
         for (int u = 0; u < 2; ++u) stage[tid + 256 * u] = pf[u];
         __syncthreads();
-        if (k0 + 8 < m) fetch(k0 + 8);
+        if (k0 + 8 < m)
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const int x = tid + 256 * u, r = rt + (x >> 3), c = k0 + 8 + (x & 7);
+            pf[u] = (r < m && c < m) ? Zb[(long long)r * n + c] : 0.0;
+          }
 #pragma unroll
         for (int k4 = 0; k4 < 8; k4 += 4) {
           const int kk = k0 + k4 + tg;
@@ -807,32 +815,23 @@ __device__ __noinline__ void formq_block_tc(T* Z, int n, int c0, int m, T* Vs, c
         }
         __syncthreads();
       }
-      const int r = rt + 8 * warp + g;
-      if (r < m)
 #pragma unroll
-        for (int y = 0; y < 2; ++y) {
-          Wm[(long long)r * kQBlock + 8 * y + 2 * tg] = a0[y];
-          Wm[(long long)r * kQBlock + 8 * y + 2 * tg + 1] = a1[y];
-        }
-    }
-    __syncthreads();
-    // Vs <- T^T Vs
-    for (int cc = tid; cc < m; cc += nt) {
-      double vq[kQBlock];
+      for (int y = 0; y < 2; ++y) {
+        Wm[(8 * warp + g) * kQBlock + 8 * y + 2 * tg] = a0[y];
+        Wm[(8 * warp + g) * kQBlock + 8 * y + 2 * tg + 1] = a1[y];
+      }
+      __syncthreads();
+      // Wt = Wm T^T: entry (r, i) = sum_q Wm[r][q] T[i][q]
 #pragma unroll
-      for (int q = 0; q < kQBlock; ++q) vq[q] = Vs[q * m + cc];
-#pragma unroll 2
-      for (int i = 0; i < kQBlock; ++i) {
+      for (int u = 0; u < 4; ++u) {
+        const int x = tid + 256 * u, r = x >> 4, i = x & (kQBlock - 1);
         double sum = 0.0;
 #pragma unroll
-        for (int q = 0; q < kQBlock; ++q) sum += Ts[q][i] * vq[q];
-        Vs[i * m + cc] = sum;
+        for (int q = 0; q < kQBlock; ++q) sum += Wm[r * kQBlock + q] * Ts[i][q];
+        Wt[x] = sum;
       }
-    }
-    __syncthreads();
-    // Zb -= Wm Vs
-    const int wrow = (warp >> 1) * 16, wcol = (warp & 1) * 32;
-    for (int rt = 0; rt < m; rt += 64)
+      __syncthreads();
+      // Zt -= Wt Vs
       for (int ct = 0; ct < m; ct += 64) {
         double d0[2][4], d1[2][4];
 #pragma unroll
@@ -847,10 +846,7 @@ __device__ __noinline__ void formq_block_tc(T* Z, int n, int c0, int m, T* Vs, c
         for (int k4 = 0; k4 < kQBlock; k4 += 4) {
           double af[2], bf[4];
 #pragma unroll
-          for (int x = 0; x < 2; ++x) {
-            const int r = rt + wrow + 8 * x + g;
-            af[x] = r < m ? -Wm[(long long)r * kQBlock + k4 + tg] : 0.0;
-          }
+          for (int x = 0; x < 2; ++x) af[x] = -Wt[(wrow + 8 * x + g) * kQBlock + k4 + tg];
 #pragma unroll
           for (int y = 0; y < 4; ++y) {
             const int c = ct + wcol + 8 * y + g;
@@ -870,6 +866,8 @@ __device__ __noinline__ void formq_block_tc(T* Z, int n, int c0, int m, T* Vs, c
             if (r < m && c + 1 < m) Zb[(long long)r * n + c + 1] = d1[x][y];
           }
       }
+      __syncthreads();  // Wm and Wt are rewritten by the next tile
+    }
   }
 }
 
@@ -1497,22 +1495,22 @@ __device__ __noinline__ void form_q(const T* A, T* Z, int n, const T* tau, T* ri
         if (lane == 0) yv[j][i] = acc;
       }
       __syncthreads();
-      if (tid == 0) {  // T column by column: T[i][i] = tau, T[0:i][i] = -tau T[0:i][0:i] (V^T v_i)[0:i]
+      if (tid < kQBlock) {  // T column by column, lane r: T[i][i] = tau, T[0:i][i] = -tau T[0:i][0:i] (V^T v_i)[0:i]
+        const int r = tid;
         for (int i = 0; i < kQBlock; ++i) {
           const T ti = i < bb ? tau[k0 + i] : T(0);
-          for (int r = 0; r < kQBlock; ++r) {
-            T x = T(0);
-            if (i < bb) {
-              if (r == i) {
-                x = ti;
-              } else if (r < i) {
-                T sacc = T(0);
-                for (int q = r; q < i; ++q) sacc += Ts[r][q] * yv[q][i];
-                x = -ti * sacc;
-              }
+          T x = T(0);
+          if (i < bb) {
+            if (r == i) {
+              x = ti;
+            } else if (r < i) {
+              T sacc = T(0);
+              for (int q = r; q < i; ++q) sacc += Ts[r][q] * yv[q][i];
+              x = -ti * sacc;
             }
-            Ts[r][i] = x;
           }
+          Ts[r][i] = x;
+          __syncwarp(0xffffu);
         }
       }
       __syncthreads();
