@@ -347,6 +347,22 @@ __device__ inline float tb_rsqrt(float x) {
 
 // reciprocal square root on the QL rotation chain (FP32: one Newton step on the estimate)
 __device__ inline double chain_rsqrt(double x) { return rsqrt(x); }
+
+// 1/x for the divide-and-conquer inner loops: the hardware reciprocal
+// estimate (rcp.approx.ftz.f64) refined by two Newton-Raphson steps for
+// f(r) = 1/r - x, r <- r + r (1 - x r), each squaring the relative error;
+// within a few units in the last place, not correctly rounded.  x = 0 gives
+// inf and |x| = inf gives 0, as 1/x does.  FP32 keeps the division.
+__device__ inline double dc_rcp(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  if (r == 0.0 || isinf(r)) return r;
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
+__device__ inline float dc_rcp(float x) { return 1.0f / x; }
 __device__ inline float chain_rsqrt(float x) { return tb_rsqrt(x); }
 
 template <typename T>
@@ -917,7 +933,7 @@ __device__ void secular_root(int j, int k, const T* dl, const T* z, T rho, int* 
   if (j < k - 1) {
     const T mid = T(0.5) * (dl[j + 1] - dl[j]);
     T f = T(1);
-    for (int i = 0; i < k; ++i) f += rho * z[i] * z[i] / ((dl[i] - dl[j]) - mid);
+    for (int i = 0; i < k; ++i) f += rho * z[i] * z[i] * dc_rcp((dl[i] - dl[j]) - mid);
     if (f >= T(0)) { o = j; lo = T(0); hi = mid; }
     else { o = j + 1; lo = -mid; hi = T(0); }
   } else {
@@ -930,7 +946,7 @@ __device__ void secular_root(int j, int k, const T* dl, const T* z, T rho, int* 
   for (int it = 0; it < 100; ++it) {
     T psi = T(0), phi = T(0), dpsi = T(0), dphi = T(0);
     for (int i = 0; i < k; ++i) {
-      const T r = T(1) / ((dl[i] - base) - tau);
+      const T r = dc_rcp((dl[i] - base) - tau);
       const T q = z[i] * z[i] * r;
       if (i <= j) { psi += q; dpsi += q * r; }
       else { phi += q; dphi += q * r; }
@@ -1104,10 +1120,8 @@ __device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, 
   const T rho = tb_abs(ev), sg = ev >= T(0) ? T(1) : T(-1);
   // children's blocks are diagonal sub-blocks: clear the rest of the node's block
   if (V == Gi)
-    for (long long x = tid; x < (long long)m * m; x += nt) {
-      const int r = lo + (int)(x / m), c = lo + (int)(x % m);
-      if ((r < t) != (c < t)) Gi[(long long)r * n + c] = T(0);
-    }
+    for (int r = lo + (tid >> 5); r < hi; r += nt >> 5)
+      for (int c = (r < t ? t : lo) + (tid & 31); c < (r < t ? hi : t); c += 32) Gi[(long long)r * n + c] = T(0);
   // z and its norm
   T part = T(0);
   for (int r = lo + tid; r < hi; r += nt) {
@@ -1176,8 +1190,8 @@ __device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, 
   for (int i = tid; i < k; i += nt) {  // Gu-Eisenstat: every ratio in (0, 1]
     const T di = dl[i];
     T prod = ((dl[ori[k - 1]] - di) + tv[k - 1]) / s_rho;
-    for (int j = 0; j < i; ++j) prod *= ((dl[ori[j]] - di) + tv[j]) / (dl[j] - di);
-    for (int j = i + 1; j < k; ++j) prod *= ((dl[ori[j - 1]] - di) + tv[j - 1]) / (dl[j] - di);
+    for (int j = 0; j < i; ++j) prod *= ((dl[ori[j]] - di) + tv[j]) * dc_rcp(dl[j] - di);
+    for (int j = i + 1; j < k; ++j) prod *= ((dl[ori[j - 1]] - di) + tv[j - 1]) * dc_rcp(dl[j] - di);
     zl[i] = copysign(tb_sqrt(fmax(prod, T(0))), zl[i]);
   }
   __syncthreads();
@@ -1185,7 +1199,7 @@ __device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, 
     const T bj = dl[ori[j]], tj = tv[j];
     T s = T(0);
     for (int i = 0; i < k; ++i) {
-      const T w = zl[i] / ((dl[i] - bj) - tj);
+      const T w = zl[i] * dc_rcp((dl[i] - bj) - tj);
       s += w * w;
     }
     inrm[j] = T(1) / tb_sqrt(s);
@@ -1193,11 +1207,12 @@ __device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, 
   __syncthreads();
   // roots: Out rows lo .. lo+k-1; deflated: rows lo+k .. hi-1 copied
   dc_gemm<T>(k, k, vcols,
-             [&](int j, int i) { return zl[i] / ((dl[i] - dl[ori[j]]) - tv[j]) * inrm[j]; },
+             [&](int j, int i) { return zl[i] * dc_rcp((dl[i] - dl[ori[j]]) - tv[j]) * inrm[j]; },
              V, srow, Out, lo, vc0, n, Wt, Bt);
-  for (long long x = tid; x < (long long)(m - k) * vcols; x += nt) {
-    const int q = (int)(x / vcols), c = vc0 + (int)(x % vcols);
-    Out[(long long)(lo + k + q) * n + c] = V[(long long)rowof[ndl[k + q]] * n + c];
+  for (int q = tid >> 5; q < m - k; q += nt >> 5) {
+    const T* src = V + (long long)rowof[ndl[k + q]] * n;
+    T* dst = Out + (long long)(lo + k + q) * n;
+    for (int c = vc0 + (tid & 31); c < vc0 + vcols; c += 32) dst[c] = src[c];
   }
   __syncthreads();
   for (int j = tid; j < m; j += nt) d[lo + j] = j < k ? dl[ori[j]] + tv[j] : delta[ndl[j]];
@@ -1465,7 +1480,8 @@ __device__ __noinline__ void form_q(const T* A, T* Z, int n, const T* tau, T* ri
   // once per reflector.  V is staged in shared memory (the rotation ring is not
   // in use yet); one warp per row: partial dots of the row with the kQBlock
   // reflectors, a warp reduction, T^T applied by kQBlock lanes, then the update.
-  for (long long x = tid; x < (long long)n * n; x += nt) Z[x] = ((x / n) == (x % n)) ? T(1) : T(0);
+  for (int i = tid >> 5; i < n; i += nt >> 5)
+    for (int j = tid & 31; j < n; j += 32) Z[(long long)i * n + j] = i == j ? T(1) : T(0);
   __syncthreads();
   {
     const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
@@ -1585,14 +1601,12 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
   const int tid = threadIdx.x, nt = blockDim.x;
 
   // symmetrise
-  for (long long x = tid; x < (long long)n * n; x += nt) {
-    const int i = (int)(x / n), j = (int)(x % n);
-    if (i < j) {
+  for (int i = tid >> 5; i < n; i += nt >> 5)
+    for (int j = i + 1 + (tid & 31); j < n; j += 32) {
       const T s = T(0.5) * (A[(long long)i * n + j] + A[(long long)j * n + i]);
       A[(long long)i * n + j] = s;
       A[(long long)j * n + i] = s;
     }
-  }
   for (int i = tid; i < n; i += nt) { e[i] = T(0); tau[i] = T(0); }
   __syncthreads();
 
