@@ -1143,36 +1143,61 @@ __device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, 
     zs[rank] = (r < t ? Gi[(long long)r * n + t - 1] : sg * Gi[(long long)r * n + t]) * zsc;
   }
   __syncthreads();
-  if (tid == 0) {  // deflation scan and compaction, in order
+  if (tid < 32) {  // deflation scan (lane 0, in order) and compaction (warp ballots), warp 0
+    const int lane = tid;
     T dmax = T(0);
-    for (int s = 0; s < m; ++s) dmax = fmax(dmax, tb_abs(delta[s]));
+    for (int s = lane; s < m; s += 32) dmax = fmax(dmax, tb_abs(delta[s]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
     const T tol = T(8) * Eps<T>::v * fmax(dmax, rhop);
-    int nrot = 0, prev = -1;
-    for (int s = 0; s < m; ++s) {
-      if (rhop * tb_abs(zs[s]) <= tol) { flg[s] = 1; continue; }
-      flg[s] = 0;
-      if (prev >= 0) {
-        const T za = zs[prev], zb = zs[s];
-        const T tau = tb_sqrt(za * za + zb * zb);
-        const T c = zb / tau, sn = -za / tau;
-        if (tb_abs((delta[s] - delta[prev]) * c * sn) <= tol) {
-          rp[nrot] = rowof[prev]; rq[nrot] = rowof[s]; rc[nrot] = c; rsn[nrot] = sn; ++nrot;
-          zs[s] = tau; zs[prev] = T(0);
-          const T dp = delta[prev], ds = delta[s];
-          delta[prev] = dp * c * c + ds * sn * sn;
-          delta[s] = dp * sn * sn + ds * c * c;
-          flg[prev] = 1;
+    for (int s = lane; s < m; s += 32) flg[s] = rhop * tb_abs(zs[s]) <= tol ? 1 : 0;
+    __syncwarp();
+    if (lane == 0) {
+      // close pair (prev, s): the rotation zeroing z_prev (c = z_s / tau, sn = -z_prev / tau,
+      // tau = |(z_prev, z_s)|) deflates when |(d_s - d_prev) c sn| <= tol, tested as
+      // |d_s - d_prev| |z_prev z_s| <= tol tau^2 without the square root
+      int nrot = 0, prev = -1;
+      for (int s = 0; s < m; ++s) {
+        if (flg[s]) continue;
+        if (prev >= 0) {
+          const T za = zs[prev], zb = zs[s], t2 = za * za + zb * zb;
+          if (tb_abs(delta[s] - delta[prev]) * tb_abs(za * zb) <= tol * t2) {
+            const T tau = tb_sqrt(t2);
+            const T c = zb / tau, sn = -za / tau;
+            rp[nrot] = rowof[prev]; rq[nrot] = rowof[s]; rc[nrot] = c; rsn[nrot] = sn; ++nrot;
+            zs[s] = tau; zs[prev] = T(0);
+            const T dp = delta[prev], ds = delta[s];
+            delta[prev] = dp * c * c + ds * sn * sn;
+            delta[s] = dp * sn * sn + ds * c * c;
+            flg[prev] = 1;
+          }
         }
+        prev = s;
       }
-      prev = s;
+      s_nrot = nrot;
     }
+    __syncwarp();
+    // non-deflated entries first, then the deflated ones, each in order
     int k = 0;
-    for (int s = 0; s < m; ++s)
-      if (!flg[s]) { ndl[k] = s; dl[k] = delta[s]; zl[k] = zs[s]; srow[k] = rowof[s]; ++k; }
+    for (int s0 = 0; s0 < m; s0 += 32) {
+      const int s = s0 + lane;
+      const bool keep = s < m && !flg[s];
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int pos = k + __popc(bal & ((1u << lane) - 1u));
+        ndl[pos] = s; dl[pos] = delta[s]; zl[pos] = zs[s]; srow[pos] = rowof[s];
+      }
+      k += __popc(bal);
+    }
     int q = k;
-    for (int s = 0; s < m; ++s)
-      if (flg[s]) ndl[q++] = s;
-    s_k = k; s_nrot = nrot; s_rho = rhop;
+    for (int s0 = 0; s0 < m; s0 += 32) {
+      const int s = s0 + lane;
+      const bool defl = s < m && flg[s];
+      const unsigned bal = __ballot_sync(0xffffffffu, defl);
+      if (defl) ndl[q + __popc(bal & ((1u << lane) - 1u))] = s;
+      q += __popc(bal);
+    }
+    if (lane == 0) { s_k = k; s_rho = rhop; }
   }
   __syncthreads();
   const int k = s_k, nrot = s_nrot;
