@@ -1451,20 +1451,64 @@ __device__ __noinline__ void tridiagonalise(T* A, int n, T* e, T* tau, T* v, T* 
       __syncthreads();
       // row r = k+1 (columns r..n-1) brought up to date; the last step also row n-1's diagonal
       const int r = k + 1;
-      for (int c = r + tid; c < n; c += nt) {
-        T x = A[(long long)r * n + c];
-        for (int i = 0; i < np; ++i)
-          x -= PV[(long long)i * n + r] * PW[(long long)i * n + c] + PW[(long long)i * n + r] * PV[(long long)i * n + c];
-        A[(long long)r * n + c] = x;
+      if (r == nref) {
+        for (int c = r + tid; c < n; c += nt) {
+          T x = A[(long long)r * n + c];
+          for (int i = 0; i < np; ++i)
+            x -= PV[(long long)i * n + r] * PW[(long long)i * n + c] + PW[(long long)i * n + r] * PV[(long long)i * n + c];
+          A[(long long)r * n + c] = x;
+        }
+        if (tid == 0) {
+          T x = A[(long long)(n - 1) * n + n - 1];
+          for (int i = 0; i < np; ++i) x -= T(2) * PV[(long long)i * n + n - 1] * PW[(long long)i * n + n - 1];
+          A[(long long)(n - 1) * n + n - 1] = x;
+        }
+        __syncthreads();
       }
-      if (r == nref && tid == 0) {
-        T x = A[(long long)(n - 1) * n + n - 1];
-        for (int i = 0; i < np; ++i) x -= T(2) * PV[(long long)i * n + n - 1] * PW[(long long)i * n + n - 1];
-        A[(long long)(n - 1) * n + n - 1] = x;
-      }
-      __syncthreads();
       if (r < nref) {
-        reflector(A, n, r, vn, tau, e, red, sh);
+        // the updated row goes straight into reflector r (as `reflector` does from A): the
+        // diagonal back to A, the rest through vn, then the reflector (or, for a zero tail,
+        // the row itself) back into row r
+        const int mr = n - r - 1;
+        T part2 = T(0);
+        for (int c = r + tid; c < n; c += nt) {
+          T x = A[(long long)r * n + c];
+          for (int i = 0; i < np; ++i)
+            x -= PV[(long long)i * n + r] * PW[(long long)i * n + c] + PW[(long long)i * n + r] * PV[(long long)i * n + c];
+          if (c == r) {
+            A[(long long)r * n + r] = x;
+          } else {
+            vn[c - r - 1] = x;
+            if (c > r + 1) part2 += x * x;
+          }
+        }
+        const T sigma = block_sum_syev(part2, red);  // synchronises
+        if (tid == 0) {
+          const T alpha = vn[0];
+          if (sigma == T(0)) {
+            tau[r] = T(0); e[r] = alpha; sh[0] = T(0); sh[1] = T(0);
+          } else {
+            const T rr = tb_sqrt(alpha * alpha + sigma);
+            const T beta = alpha <= T(0) ? rr : -rr;
+            tau[r] = (beta - alpha) / beta;
+            e[r] = beta;
+            sh[0] = tau[r];
+            sh[1] = T(1) / (alpha - beta);
+          }
+        }
+        __syncthreads();
+        {
+          const T scal = sh[1];
+          const bool refl = sh[0] != T(0);
+          T* rowr = A + (long long)r * n + r + 1;
+          for (int i = tid; i < mr; i += nt) {
+            const T u = vn[i];
+            const T x = i == 0 ? T(1) : (refl ? u * scal : T(0));
+            vn[i] = x;
+            rowr[i] = refl ? x : u;
+          }
+          __syncthreads();
+        }
         if (np == kPanel) {  // close the panel: A -= V W^T + W V^T on the block, fused with p_r = tau_r A vn
           if constexpr (sizeof(T) == 8) {
             if (gs)  // the lower triangle is stale from the first upper-only walk on
