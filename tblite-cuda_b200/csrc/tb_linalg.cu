@@ -789,9 +789,11 @@ __device__ __noinline__ void panel_walk_tc_sym(double* M, int n, int r0, int nm,
 //                    accumulators initialised with Zt),
 // so that a tile is read again by the update while it is still in L2.  Same
 // arithmetic as Zc <- Zc - (Zc V) T^T V^T row by row.  Wm and Wt go through
-// the global scratch Wq (2 x 64 x kQBlock); stage: 512 elements of shared
-// memory.  256 threads.
-template <typename T>
+// the global scratch Wq (2 x 64 x kQBlock); stage: 512 nsub elements of
+// shared memory (nsub <= kFqSubMax sub-slabs of 8 columns per barrier pair).
+// 256 threads.
+constexpr int kFqSubMax = 4;  // 8-column sub-slabs staged per barrier pair (at most)
+template <typename T, int nsub>
 __device__ __noinline__ void formq_block_tc(T* Z, int n, int c0, int m, const T* Vs, const T (*Ts)[kQBlock], T* Wq,
                                             T* stage) {
   if constexpr (sizeof(T) == 8) {
@@ -802,31 +804,35 @@ __device__ __noinline__ void formq_block_tc(T* Z, int n, int c0, int m, const T*
     const int wrow = (warp >> 1) * 16, wcol = (warp & 1) * 32;
     for (int rt = 0; rt < m; rt += 64) {
       // Wm = Zt Vs^T
+      // slabs of nsub x 8 columns per barrier pair (sub-slab j: 64 x 8 at stage + 512 j)
       double a0[2] = {0.0, 0.0}, a1[2] = {0.0, 0.0};
-      double pf[2];
+      double pf[2 * nsub];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int x = tid + 256 * u, r = rt + (x >> 3), c = x & 7;
+      for (int u = 0; u < 2 * nsub; ++u) {
+        const int x = tid + 256 * u, r = rt + ((x & 511) >> 3), c = 8 * (x >> 9) + (x & 7);
         pf[u] = (r < m && c < m) ? Zb[(long long)r * n + c] : 0.0;
       }
-      for (int k0 = 0; k0 < m; k0 += 8) {
+      for (int k0 = 0; k0 < m; k0 += 8 * nsub) {
 #pragma unroll
-        for (int u = 0; u < 2; ++u) stage[tid + 256 * u] = pf[u];
+        for (int u = 0; u < 2 * nsub; ++u) stage[tid + 256 * u] = pf[u];
         __syncthreads();
-        if (k0 + 8 < m)
+        if (k0 + 8 * nsub < m)
 #pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            const int x = tid + 256 * u, r = rt + (x >> 3), c = k0 + 8 + (x & 7);
+          for (int u = 0; u < 2 * nsub; ++u) {
+            const int x = tid + 256 * u, r = rt + ((x & 511) >> 3), c = k0 + 8 * nsub + 8 * (x >> 9) + (x & 7);
             pf[u] = (r < m && c < m) ? Zb[(long long)r * n + c] : 0.0;
           }
 #pragma unroll
-        for (int k4 = 0; k4 < 8; k4 += 4) {
-          const int kk = k0 + k4 + tg;
-          const double af = stage[(8 * warp + g) * 8 + k4 + tg];
+        for (int j = 0; j < nsub; ++j) {
 #pragma unroll
-          for (int y = 0; y < 2; ++y) {
-            const double bf = kk < m ? Vs[(8 * y + g) * m + kk] : 0.0;
-            dmma(a0[y], a1[y], af, bf);
+          for (int k4 = 0; k4 < 8; k4 += 4) {
+            const int kk = k0 + 8 * j + k4 + tg;
+            const double af = stage[512 * j + (8 * warp + g) * 8 + k4 + tg];
+#pragma unroll
+            for (int y = 0; y < 2; ++y) {
+              const double bf = kk < m ? Vs[(8 * y + g) * m + kk] : 0.0;
+              dmma(a0[y], a1[y], af, bf);
+            }
           }
         }
         __syncthreads();
@@ -1600,7 +1606,12 @@ __device__ __noinline__ void form_q(const T* A, T* Z, int n, const T* tau, T* ri
       }
       __syncthreads();
       if (tcq) {
-        formq_block_tc<T>(Z, n, c0, m, Vs, Ts, Sq, stage);
+        switch (min(kFqSubMax, n / 128)) {  // stage (4n elements) holds 512 per sub-slab
+          case 1: formq_block_tc<T, 1>(Z, n, c0, m, Vs, Ts, Sq, stage); break;
+          case 2: formq_block_tc<T, 2>(Z, n, c0, m, Vs, Ts, Sq, stage); break;
+          case 3: formq_block_tc<T, 3>(Z, n, c0, m, Vs, Ts, Sq, stage); break;
+          default: formq_block_tc<T, 4>(Z, n, c0, m, Vs, Ts, Sq, stage); break;
+        }
         __syncthreads();
         continue;
       }
