@@ -911,7 +911,7 @@ __device__ __noinline__ void formq_block_tc(T* Z, int n, int c0, int m, const T*
 //    w_j = z_i / (delta_i - lambda_j) are orthogonal to working accuracy;
 //  * G_node = W G_children as a tiled product with W generated on the fly.
 // Finally Zc <- G Zc (Zc = Q^T), and the eigenvalues are left in d.
-constexpr int kDcMin = 128;  // smallest structure solved this way (shared memory, see dc_ws_ok)
+constexpr int kDcMin = 112;  // smallest structure solved this way (its workspace fits from 112 rows on)
 constexpr int kDcK = 8;      // reduction slab of the tiled products
 
 // slabs of the tiled products: Wt 64 x kDcK, Bt kDcK x kDcBs (row padded by 4 so
@@ -1566,7 +1566,7 @@ __device__ __noinline__ void form_q(const T* A, T* Z, int n, const T* tau, T* ri
     T* Vs = ring;                               // kQBlock x m, m <= n - 1
     // FP64 with a scratch matrix: each block's products on the tensor pipe
     // (formq_block_tc; Wm in Sq, slabs staged in stage, 4n >= 512)
-    const bool tcq = Sq && sizeof(T) == 8 && n >= kDcMin && nt == 256;
+    const bool tcq = Sq && sizeof(T) == 8 && n >= 128 && nt == 256;  // stage: 4n >= 512
     const int nref = n - 2;
     for (int k1 = nref - 1; k1 >= 0; k1 -= kQBlock) {
       const int k0 = k1 - kQBlock + 1 > 0 ? k1 - kQBlock + 1 : 0, bb = k1 - k0 + 1;
