@@ -10,8 +10,29 @@ namespace tb {
 
 constexpr int kEigThreads = 256;
 constexpr int kRing = 8;  // QL sweeps buffered between the k_syev producer and consumers
-// shared memory of k_syev: d, e, tau, v, vn, p, w (7n) + the rotation ring (2 n kRing)
-inline size_t syev_smem_bytes(int n, size_t elem = sizeof(double)) { return (7 + 2 * (size_t)kRing) * (size_t)n * elem; }
+// k_syev's divide and conquer: structures of kDcMin+ rows (more than two leaves of
+// 24), merge products in 64 x 64 tiles with reduction slabs of kDcK (Wt 64 x kDcK,
+// Bt kDcK x kDcBs, rows padded by 4 against bank conflicts)
+constexpr int kDcMin = 64;
+constexpr int kDcK = 8;
+constexpr int kDcBs = 64 + 4;
+constexpr int kDcTileElems = 64 * kDcK + kDcK * kDcBs;
+// workspace of one merge of m entries, in units of T (the ints after the T arrays)
+template <typename T>
+__host__ __device__ constexpr int dc_ws_elems(int m) {
+  return 8 * m + kDcTileElems + (7 * m * (int)sizeof(int) + (int)sizeof(T) - 1) / (int)sizeof(T);
+}
+// shared memory of k_syev: d, e, tau, v, vn, p, w (7n) + the rotation ring (2 n kRing);
+// in FP64 at least d, e and the divide-and-conquer workspace (from tau on) for
+// kDcMin+ rows, so that the solver chosen for a structure depends on its size only
+inline size_t syev_smem_bytes(int n, size_t elem = sizeof(double)) {
+  size_t v = (7 + 2 * (size_t)kRing) * (size_t)n;
+  if (elem == sizeof(double) && n >= kDcMin) {
+    const size_t dc = 2 * (size_t)n + (size_t)dc_ws_elems<double>(n);
+    if (dc > v) v = dc;
+  }
+  return v * elem;
+}
 constexpr int kSyevMaxN = 1216;
 constexpr int kGemmThreads = 128;  // block size of k_gemm
 

@@ -911,23 +911,9 @@ __device__ __noinline__ void formq_block_tc(T* Z, int n, int c0, int m, const T*
 //    w_j = z_i / (delta_i - lambda_j) are orthogonal to working accuracy;
 //  * G_node = W G_children as a tiled product with W generated on the fly.
 // Finally Zc <- G Zc (Zc = Q^T), and the eigenvalues are left in d.
-constexpr int kDcMin = 112;  // smallest structure solved this way (its workspace fits from 112 rows on)
-constexpr int kDcK = 8;      // reduction slab of the tiled products
-
-// slabs of the tiled products: Wt 64 x kDcK, Bt kDcK x kDcBs (row padded by 4 so
-// that the DMMA fragment loads of a warp hit distinct banks)
-constexpr int kDcBs = 64 + 4;
-constexpr int kDcTileElems = 64 * kDcK + kDcK * kDcBs;
-
-// workspace of one merge of m entries, in units of T (the ints after the T arrays)
-template <typename T>
-__host__ __device__ constexpr int dc_ws_elems(int m) {
-  return 8 * m + kDcTileElems + (7 * m * (int)sizeof(int) + (int)sizeof(T) - 1) / (int)sizeof(T);
-}
-
-// the workspace starts at tau: 5 n vectors + the ring are free after Q is formed
-static_assert(dc_ws_elems<double>(kDcMin) <= (5 + 2 * kRing) * kDcMin,
-              "divide-and-conquer workspace exceeds the free shared memory");
+// kDcMin, kDcK, kDcBs, kDcTileElems and dc_ws_elems (tb_kernels.h): the
+// workspace starts at tau and runs to the end of the dynamic shared memory,
+// which syev_smem_bytes sizes so that every structure of kDcMin+ rows has it.
 
 // Root j of 1 + rho sum_i z_i^2 / (dl_i - lambda) = 0 (dl strictly ascending,
 // rho > 0): lambda = dl[*o] + *tau.
@@ -1259,7 +1245,7 @@ constexpr int kDcLeaf = 24;  // leaves of the merge tree: at most this many rows
 // eigenvector block U in shared memory; U is written to G's diagonal block.
 // Returns false if an eigenvalue took more than 60 sweeps.
 constexpr int kDcLeafWs = kDcLeaf * kDcLeaf + 3 * kDcLeaf;  // per leaf warp: U, off-diagonal, rotations
-static_assert(kDcLeafWs <= (5 + 2 * kRing) * kDcMin, "leaf workspace exceeds the free shared memory");
+static_assert(kDcLeafWs <= dc_ws_elems<double>(kDcMin), "leaf workspace exceeds the divide-and-conquer workspace");
 
 template <typename T>
 __device__ bool dc_leaf(T* d, const T* e, int lo, int s, T* U, T* le, T* rcs, T* G, int n) {
@@ -1339,7 +1325,7 @@ __device__ inline void dc_node(int n, int dep, int b, int* lo_out, int* hi_out, 
 // (d, e) by the merge tree; G0 and G1 are n x n buffers, ws dc_ws_elems(n).
 // Returns false if a leaf failed to converge.
 template <typename T>
-__device__ bool dc_solve(T* d, T* e, T* Z, T* G0, T* G1, int n, T* ws, T* red) {
+__device__ bool dc_solve(T* d, T* e, T* Z, T* G0, T* G1, int n, T* ws, T* red, long long ws_cap) {
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
   __shared__ int s_fail;
   int depth = 0;  // nodes at this depth have at most kDcLeaf rows
@@ -1359,7 +1345,7 @@ __device__ bool dc_solve(T* d, T* e, T* Z, T* G0, T* G1, int n, T* ws, T* red) {
     __syncthreads();
   }
   // as many leaf warps as the free shared memory holds blocks for
-  const int lw = min(nw, (int)((5 + 2 * kRing) * (long long)n / kDcLeafWs));
+  const int lw = (int)min((long long)nw, ws_cap / kDcLeafWs);
   T* U = ws + wid * kDcLeafWs;
   for (int dep = depth; dep >= 0; --dep) {
     T* Gi = ((depth - dep - 1) & 1) ? G1 : G0;
@@ -1699,11 +1685,15 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
 
   form_q<T>(A, Z, n, tau, ring, tau + n, Sb ? Sb + mo : nullptr);
 
-  // ---- 3a. divide and conquer when a scratch buffer is given (A is free now)
-  if (Sb && n >= kDcMin && dc_ws_elems<T>(n) <= (5 + 2 * kRing) * n) {
+  // ---- 3a. divide and conquer when a scratch buffer is given (A is free now); the
+  // workspace runs from tau to the end of the dynamic shared memory
+  unsigned dyn_bytes;
+  asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_bytes));
+  const long long ws_cap = (long long)(dyn_bytes / sizeof(T)) - 2LL * n;
+  if (Sb && n >= kDcMin && dc_ws_elems<T>(n) <= ws_cap) {
     if (tid == 0) { q_fail = 0; e[n - 1] = T(0); }
     __syncthreads();
-    const bool conv = dc_solve<T>(d, e, Z, A, Sb + mo, n, tau, red);
+    const bool conv = dc_solve<T>(d, e, Z, A, Sb + mo, n, tau, red, ws_cap);
     for (int i = tid; i < n; i += nt)
       if (!conv || !(tb_abs(d[i]) < T(1e30))) q_fail = 1;  // a leaf did not converge, or non-finite input
   } else {

@@ -147,13 +147,13 @@ def test_sygvd_tridiagonal_panel_sizes(oracle):
 
 
 def test_sygvd_divide_and_conquer():
-    # structures of 112 AOs and more take the divide-and-conquer tridiagonal
+    # structures of 64 AOs and more take the divide-and-conquer tridiagonal
     # solver (from 128 on with the tensor-core Q formation): random spectra,
     # 8-fold degenerate ones, nearly decoupled blocks (every merge deflates)
     # and a multiple of the identity
     rng = np.random.default_rng(9)
     Hs = []
-    for n in (112, 113, 127, 128, 129, 200, 256, 384):
+    for n in (64, 65, 97, 111, 127, 128, 129, 200, 256, 384):
         M = rng.normal(size=(n, n))
         Hs.append(0.5 * (M + M.T))
     n = 256
