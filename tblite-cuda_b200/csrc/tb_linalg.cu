@@ -312,12 +312,13 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
 //  4. Ascending order by rank (ties by index).
 namespace {
 
-// Tridiagonalisation panel: reflectors per panel (2 panel n <= ring) and rows
-// per load batch of the panel-closing walk.  FP64 moves twice the bytes per
-// element, so the walk is traffic-bound and wide panels pay; in FP32 a panel
-// of one (each step's update fused with the next product) is as fast.
+// Tridiagonalisation panel: reflectors per panel (2 panel n <= ring) and, for
+// the FP32 column form of the panel-closing walk, rows per load batch.  FP64
+// moves twice the bytes per element, so its walks are traffic-bound and wide
+// panels pay (its panel-closing walk is panel_walk_tc / panel_walk_tc_sym); in
+// FP32 a panel of one (each step's update fused with the next product) is as fast.
 template <typename T> struct PanelCfg;
-template <> struct PanelCfg<double> { static constexpr int width = 8, batch = 6; };
+template <> struct PanelCfg<double> { static constexpr int width = 8; };
 template <> struct PanelCfg<float> { static constexpr int width = 1, batch = 12; };
 // Read-only Householder walk (colwalk): the warps form kWalkRowGroups row
 // groups (interleaved rows) times nw / kWalkRowGroups column groups; a lane
@@ -1223,9 +1224,17 @@ __device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, 
   }
   __syncthreads();
   // roots: Out rows lo .. lo+k-1; deflated: rows lo+k .. hi-1 copied
-  dc_gemm<T>(k, k, vcols,
-             [&](int j, int i) { return zl[i] * dc_rcp((dl[i] - dl[ori[j]]) - tv[j]) * inrm[j]; },
-             V, srow, Out, lo, vc0, n, Wt, Bt);
+  auto wgen = [&](int j, int i) { return zl[i] * dc_rcp((dl[i] - dl[ori[j]]) - tv[j]) * inrm[j]; };
+  if (V != Gi) {
+    // the root: Gi is free once z has been read, so W is formed there once
+    // (row stride n) instead of once per 64-column tile of the product
+    for (int j = tid >> 5; j < k; j += nt >> 5)
+      for (int i = tid & 31; i < k; i += 32) Gi[(long long)j * n + i] = wgen(j, i);
+    __syncthreads();
+    dc_gemm<T>(k, k, vcols, [&](int j, int i) { return Gi[(long long)j * n + i]; }, V, srow, Out, lo, vc0, n, Wt, Bt);
+  } else {
+    dc_gemm<T>(k, k, vcols, wgen, V, srow, Out, lo, vc0, n, Wt, Bt);
+  }
   for (int q = tid >> 5; q < m - k; q += nt >> 5) {
     const T* src = V + (long long)rowof[ndl[k + q]] * n;
     T* dst = Out + (long long)(lo + k + q) * n;
