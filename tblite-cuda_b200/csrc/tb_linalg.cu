@@ -1225,13 +1225,19 @@ __device__ void dc_merge(T* d, const T* e, int n, int lo, int t, int hi, T* Gi, 
   __syncthreads();
   // roots: Out rows lo .. lo+k-1; deflated: rows lo+k .. hi-1 copied
   auto wgen = [&](int j, int i) { return zl[i] * dc_rcp((dl[i] - dl[ori[j]]) - tv[j]) * inrm[j]; };
-  if (V != Gi) {
-    // the root: Gi is free once z has been read, so W is formed there once
-    // (row stride n) instead of once per 64-column tile of the product
+  // W formed once (row stride n) instead of once per 64-column tile of the
+  // product, where Gi has a free k x k block: at the root all of Gi is free
+  // once z has been read; below it, rows lo.. of Gi beside the node's block
+  // (columns hi.. or ..lo) belong to no node of this level
+  T* Wb = nullptr;
+  if (V != Gi) Wb = Gi;
+  else if (hi + k <= n) Wb = Gi + (long long)lo * n + hi;
+  else if (lo >= k) Wb = Gi + (long long)lo * n + (lo - k);
+  if (Wb) {
     for (int j = tid >> 5; j < k; j += nt >> 5)
-      for (int i = tid & 31; i < k; i += 32) Gi[(long long)j * n + i] = wgen(j, i);
+      for (int i = tid & 31; i < k; i += 32) Wb[(long long)j * n + i] = wgen(j, i);
     __syncthreads();
-    dc_gemm<T>(k, k, vcols, [&](int j, int i) { return Gi[(long long)j * n + i]; }, V, srow, Out, lo, vc0, n, Wt, Bt);
+    dc_gemm<T>(k, k, vcols, [&](int j, int i) { return Wb[(long long)j * n + i]; }, V, srow, Out, lo, vc0, n, Wt, Bt);
   } else {
     dc_gemm<T>(k, k, vcols, wgen, V, srow, Out, lo, vc0, n, Wt, Bt);
   }
