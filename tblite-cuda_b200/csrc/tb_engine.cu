@@ -1152,21 +1152,36 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
 tb_status batch_results(tb_batch* b, tb_result* out, cudaStream_t st) {
   const int nmol = b->nmol;
   const int NA = b->nat_tot, NS = b->nsh_tot;
-  std::vector<double> erep(nmol), eelec(nmol), eband(nmol), ets(nmol), e2(nmol), ea(nmol), e3(nmol), err(nmol),
-      dip(3 * nmol), qat(NA), qsh(NS), dp(3 * NA), qp(6 * NA);
-  std::vector<int> iscf(nmol), status(nmol), fw(nmol);
+  // the device results land in the calculator's pinned staging buffer (one
+  // copy each at full link speed; pageable destinations would be copied
+  // through driver bounce buffers), then go to the caller's records
+  const size_t nd = 11 * (size_t)nmol + 10 * (size_t)NA + (size_t)NS, bytes = 8 * nd + 12 * (size_t)nmol;
+  std::lock_guard<std::mutex> stage_lk(b->calc->stage_mu);
+  if (b->calc->stage_bytes < bytes) {
+    if (b->calc->stage) cudaFreeHost(b->calc->stage);
+    b->calc->stage = nullptr;
+    b->calc->stage_bytes = 0;
+    TB_CUDA(cudaMallocHost(&b->calc->stage, bytes + (bytes >> 2)));
+    b->calc->stage_bytes = bytes + (bytes >> 2);
+  }
+  double* hd = reinterpret_cast<double*>(b->calc->stage);
+  double *erep = hd, *eelec = erep + nmol, *eband = eelec + nmol, *ets = eband + nmol, *e2 = ets + nmol,
+         *ea = e2 + nmol, *e3 = ea + nmol, *err = e3 + nmol, *dip = err + nmol, *qat = dip + 3 * nmol,
+         *qsh = qat + NA, *dp = qsh + NS, *qp = dp + 3 * NA;
+  int* hi = reinterpret_cast<int*>(hd + nd);
+  int *iscf = hi, *status = iscf + nmol, *fw = status + nmol;
   const MolState& S = b->ms;
   auto cp = [&](void* dst, const void* src, size_t n) {
     return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, st);
   };
-  TB_CUDA(cp(erep.data(), S.e_rep, nmol * 8)); TB_CUDA(cp(eelec.data(), S.eelec, nmol * 8));
-  TB_CUDA(cp(eband.data(), S.e_band, nmol * 8)); TB_CUDA(cp(ets.data(), S.e_ts, nmol * 8));
-  TB_CUDA(cp(e2.data(), S.e_es2, nmol * 8)); TB_CUDA(cp(ea.data(), S.e_aes2, nmol * 8));
-  TB_CUDA(cp(e3.data(), S.e_es3, nmol * 8)); TB_CUDA(cp(err.data(), S.scf_error, nmol * 8));
-  TB_CUDA(cp(dip.data(), S.dipole, 3 * nmol * 8)); TB_CUDA(cp(iscf.data(), S.iscf, nmol * 4));
-  TB_CUDA(cp(status.data(), S.status, nmol * 4)); TB_CUDA(cp(fw.data(), S.fermi_warn, nmol * 4));
-  TB_CUDA(cp(qat.data(), b->qat_out, NA * 8)); TB_CUDA(cp(qsh.data(), b->qsh_out, NS * 8));
-  TB_CUDA(cp(dp.data(), b->dpat_out, 3 * NA * 8)); TB_CUDA(cp(qp.data(), b->qpat_out, 6 * NA * 8));
+  TB_CUDA(cp(erep, S.e_rep, nmol * 8)); TB_CUDA(cp(eelec, S.eelec, nmol * 8));
+  TB_CUDA(cp(eband, S.e_band, nmol * 8)); TB_CUDA(cp(ets, S.e_ts, nmol * 8));
+  TB_CUDA(cp(e2, S.e_es2, nmol * 8)); TB_CUDA(cp(ea, S.e_aes2, nmol * 8));
+  TB_CUDA(cp(e3, S.e_es3, nmol * 8)); TB_CUDA(cp(err, S.scf_error, nmol * 8));
+  TB_CUDA(cp(dip, S.dipole, 3 * nmol * 8)); TB_CUDA(cp(iscf, S.iscf, nmol * 4));
+  TB_CUDA(cp(status, S.status, nmol * 4)); TB_CUDA(cp(fw, S.fermi_warn, nmol * 4));
+  TB_CUDA(cp(qat, b->qat_out, NA * 8)); TB_CUDA(cp(qsh, b->qsh_out, NS * 8));
+  TB_CUDA(cp(dp, b->dpat_out, 3 * NA * 8)); TB_CUDA(cp(qp, b->qpat_out, 6 * NA * 8));
   TB_CUDA(cudaStreamSynchronize(st));
   tb_status first = TB_OK;
   for (int m = 0; m < nmol; ++m) {
@@ -1181,10 +1196,10 @@ tb_status batch_results(tb_batch* b, tb_result* out, cudaStream_t st) {
     r.nsh = b->h_soff[m + 1] - b->h_soff[m];
     r.nao = b->h_ooff[m + 1] - b->h_ooff[m];
     const int a0 = b->h_aoff[m], na = b->h_aoff[m + 1] - a0, s0 = b->h_soff[m];
-    if (r.qat) std::memcpy(r.qat, qat.data() + a0, na * 8);
-    if (r.qsh) std::memcpy(r.qsh, qsh.data() + s0, r.nsh * 8);
-    if (r.dpat) std::memcpy(r.dpat, dp.data() + 3 * a0, 3 * na * 8);
-    if (r.qpat) std::memcpy(r.qpat, qp.data() + 6 * a0, 6 * na * 8);
+    if (r.qat) std::memcpy(r.qat, qat + a0, na * 8);
+    if (r.qsh) std::memcpy(r.qsh, qsh + s0, r.nsh * 8);
+    if (r.dpat) std::memcpy(r.dpat, dp + 3 * a0, 3 * na * 8);
+    if (r.qpat) std::memcpy(r.qpat, qp + 6 * a0, 6 * na * 8);
     if (stt != kStOk && first == TB_OK) first = (tb_status)stt;
   }
   if (first != TB_OK) g_err = "at least one structure did not finish with TB_OK (see tb_result.status)";
