@@ -166,6 +166,11 @@ def test_sygvd_divide_and_conquer():
     Bd += 1e-13 * rng.normal(size=(160, 160))
     Hs.append(0.5 * (Bd + Bd.T))
     Hs.append(2.5 * np.eye(140))
+    Hs.append(-1.5 * np.eye(64))  # smallest divide-and-conquer size, fully degenerate
+    b2 = [rng.normal(size=(40, 40)) for _ in range(2)]
+    Bs = np.zeros((80, 80))
+    Bs[:40, :40], Bs[40:, 40:] = b2[0] + b2[0].T, b2[1] + b2[1].T
+    Hs.append(Bs)  # decoupled halves: the root merge deflates every entry
     st, out = capi.sygvd_batch(Hs, [np.eye(len(H)) for H in Hs])
     assert st == capi.TB_OK
     for H, (w, C) in zip(Hs, out):
