@@ -106,7 +106,7 @@ __global__ void k_gemm(DevBatch B, const int4* tiles, int ntiles, const double* 
                        const int* perm, const double* ks, const int* kdim, double* Cb, double alpha, double beta,
                        const int* active, int shape = 0);
 // Sb: optional n x n scratch per structure (same offsets as Ab); with it,
-// structures of at least 112 AOs take divide and conquer instead of QL
+// structures of at least kDcMin (64) AOs take divide and conquer instead of QL
 __global__ void k_syev(DevBatch B, double* Ab, double* Zb, double* Sb, double* wout, int* perm, int* status,
                        const int* active);
 // the same eigensolver in FP32 (A and Z float, eigenvalues written as double)
