@@ -295,20 +295,25 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
 
 // ------------------------------------------------------------ eigensolver
 // Symmetric eigenproblem of A (n x n, row-major, overwritten) for every
-// active structure, one CTA per structure: w ascending, eigenvector j =
-// row perm[j] of Zc (n x n, one eigenvector per row).
+// active structure, one CTA of 256 threads per structure: w ascending,
+// eigenvector j = row perm[j] of Zc (n x n, one eigenvector per row).
 //
-//  1. Householder tridiagonalisation.  Step k's rank-2 update of the trailing
-//     block and step k+1's product A22 v are done in ONE read+write pass over
-//     the block (thread per column, rows in groups of 8), so each step moves
-//     16 mm^2 bytes instead of 24 mm^2.  Reflector k is kept in row k of A.
-//  2. Q = H_0 ... H_{n-3} accumulated backwards as Zc = Q^T, again with the
-//     update of step k and the dot products of step k-1 in one pass.
-//  3. Implicit QL with Wilkinson shift.  Warp 0 (lane 0) runs the scalar
-//     rotation chain of sweep q+1 while warps 1.. apply sweep q to rows (i,i+1)
-//     of Zc, coalesced across columns; sweeps are handed over through a 2-slot shared-memory ring guarded by
-//     counters.  Every wait is bounded: on timeout the structure is marked
-//     failed and all warps leave.
+//  1. Householder tridiagonalisation in panels (tridiagonalise): within a
+//     panel the trailing block keeps its value from the panel start, each
+//     step forms its product with one read-only walk and corrects it with the
+//     panel's pairs; the panel-closing walk applies the rank-2 width update
+//     fused with the next product.  Walks read row segments (colwalk); with
+//     a scratch matrix (FP64) they read only the upper triangle (symwalk,
+//     panel_walk_tc_sym, the latter on the FP64 tensor instruction).
+//     Reflector k is kept in row k of A.
+//  2. Zc = Q^T accumulated backwards in compact-WY blocks of kQBlock
+//     reflectors (form_q; FP64 with a scratch matrix: formq_block_tc, 64-row
+//     tiles on the FP64 tensor instruction).
+//  3. Tridiagonal eigenproblem: divide and conquer (dc_solve) for FP64
+//     structures of kDcMin+ rows with a scratch matrix, else implicit QL
+//     with Wilkinson shift (warp 0 runs the rotation chain, warps 1.. apply
+//     sweeps to Zc through a kRing-slot shared-memory ring; every wait is
+//     bounded, on timeout the structure is marked failed).
 //  4. Ascending order by rank (ties by index).
 namespace {
 
