@@ -18,6 +18,7 @@
 #include <mutex>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/tblite_b200.h"
@@ -383,80 +384,111 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   std::vector<int> id, at_mol, sh_type, sh_at, sh_iao, at_ish, ao_at, ao_sh;
   b->h_xyz.clear();
   b->h_nocc.clear();
-  {  // sizes first, so that the index maps are filled without reallocation
-    long long na = 0, ns = 0, no = 0, t64 = 0, t128 = 0, t32 = 0, c32 = 0;
-    for (int m = 0; m < nmol; ++m) {
-      const tb_structure& s = mols[m];
-      if (s.nat <= 0 || !s.id) continue;
-      long long sh = 0, ao = 0;
-      for (int a = 0; a < s.nat; ++a) {
-        const int z = s.id[a];
-        if (z < 0 || z >= (int)P.sp.size()) continue;
-        const SpeciesParam& sp = P.sp[z];
-        sh += sp.nsh;
-        for (int k = 0; k < sp.nsh; ++k) ao += msao(P.sh[sp.sh0 + k].ang);
-      }
-      na += s.nat; ns += sh; no += ao;
-      const long long a64 = (ao + 63) / 64, a128 = (ao + kTcTile - 1) / kTcTile, a32 = (ao + 31) / 32;
-      t64 += a64 * a64; t128 += a128 * a128; t32 += a32 * a32; c32 += a32;
-    }
-    id.reserve(na); at_mol.reserve(na); at_ish.reserve(na); b->h_xyz.reserve(3 * na);
-    sh_type.reserve(ns); sh_at.reserve(ns); sh_iao.reserve(ns); ao_at.reserve(no); ao_sh.reserve(no);
-    b->h_nocc.reserve(nmol);
-    b->tiles64.reserve(t64); b->tiles128.reserve(t128); b->tiles32.reserve(t32); b->chunks32.reserve(c32);
-  }
+  // validation and sizes per structure, in order (the first bad structure is
+  // the one reported), then offsets, then the index maps filled in parallel
+  // over structures, each at its own offsets
+  std::vector<int> nsh_m(nmol), nao_m(nmol);
   for (int m = 0; m < nmol; ++m) {
     const tb_structure& s = mols[m];
     if (s.nat <= 0 || !s.id || !s.xyz) return fail(TB_BAD_INPUT, "structure " + std::to_string(m) + ": empty or null");
-    int nsh = 0, nao = 0;
+    int sh = 0, ao = 0;
     for (int a = 0; a < s.nat; ++a) {
       const int z = s.id[a];
       if (z < 0 || z >= (int)P.sp.size()) return fail(TB_BAD_INPUT, "structure " + std::to_string(m) + ": bad species");
-      id.push_back(z);
-      at_mol.push_back(m);
-      at_ish.push_back(nsh);
-      for (int k = 0; k < 3; ++k) {
-        const double x = s.xyz[3 * a + k];
-        if (!std::isfinite(x)) return fail(TB_BAD_INPUT, "structure " + std::to_string(m) + ": non-finite coordinate");
-        b->h_xyz.push_back(x);
-      }
+      for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(s.xyz[3 * a + k]))
+          return fail(TB_BAD_INPUT, "structure " + std::to_string(m) + ": non-finite coordinate");
+      const SpeciesParam& sp = P.sp[z];
+      sh += sp.nsh;
+      for (int k = 0; k < sp.nsh; ++k) ao += msao(P.sh[sp.sh0 + k].ang);
+    }
+    nsh_m[m] = sh;
+    nao_m[m] = ao;
+  }
+  std::vector<long long> t64o(nmol + 1, 0), t128o(nmol + 1, 0), t32o(nmol + 1, 0), c32o(nmol + 1, 0);
+  for (int m = 0; m < nmol; ++m) {
+    const int nat = mols[m].nat, nsh = nsh_m[m], nao = nao_m[m];
+    b->h_aoff[m + 1] = b->h_aoff[m] + nat;
+    b->h_soff[m + 1] = b->h_soff[m] + nsh;
+    b->h_ooff[m + 1] = b->h_ooff[m] + nao;
+    b->h_mixoff[m + 1] = b->h_mixoff[m] + nsh + 9 * nat;
+    b->h_moff[m + 1] = b->h_moff[m] + (long long)nao * nao;
+    b->h_poff[m + 1] = b->h_poff[m] + (long long)nat * (nat - 1) / 2;
+    b->h_s2off[m + 1] = b->h_s2off[m] + (long long)nsh * nsh;
+    b->h_a2off[m + 1] = b->h_a2off[m] + (long long)nat * nat;
+    b->nmax = std::max(b->nmax, nao);
+    b->natmax = std::max(b->natmax, nat);
+    b->nshmax = std::max(b->nshmax, nsh);
+    const long long a64 = (nao + 63) / 64, a128 = (nao + kTcTile - 1) / kTcTile, a32 = (nao + 31) / 32;
+    t64o[m + 1] = t64o[m] + a64 * a64;
+    t128o[m + 1] = t128o[m] + a128 * a128;
+    t32o[m + 1] = t32o[m] + a32 * a32;
+    c32o[m + 1] = c32o[m] + a32;
+  }
+  {
+    const long long na = b->h_aoff[nmol], ns = b->h_soff[nmol], no = b->h_ooff[nmol];
+    id.resize(na); at_mol.resize(na); at_ish.resize(na); b->h_xyz.resize(3 * na);
+    sh_type.resize(ns); sh_at.resize(ns); sh_iao.resize(ns); ao_at.resize(no); ao_sh.resize(no);
+    b->h_nocc.resize(nmol);
+    b->tiles64.resize(t64o[nmol]); b->tiles128.resize(t128o[nmol]); b->tiles32.resize(t32o[nmol]);
+    b->chunks32.resize(c32o[nmol]);
+  }
+  auto fill = [&](int m) {
+    const tb_structure& s = mols[m];
+    const int a0 = b->h_aoff[m], s0 = b->h_soff[m], o0 = b->h_ooff[m];
+    int nsh = 0, nao = 0;
+    double nref = -s.charge;
+    for (int a = 0; a < s.nat; ++a) {
+      const int z = s.id[a];
+      id[a0 + a] = z;
+      at_mol[a0 + a] = m;
+      at_ish[a0 + a] = nsh;
+      for (int k = 0; k < 3; ++k) b->h_xyz[3 * (long long)(a0 + a) + k] = s.xyz[3 * a + k];
       const SpeciesParam& sp = P.sp[z];
       for (int k = 0; k < sp.nsh; ++k) {
         const ShellParam& sh = P.sh[sp.sh0 + k];
-        sh_type.push_back(sp.sh0 + k);
-        sh_at.push_back(a);
-        sh_iao.push_back(nao);
-        for (int x = 0; x < msao(sh.ang); ++x) { ao_at.push_back(a); ao_sh.push_back(nsh); }
+        sh_type[s0 + nsh] = sp.sh0 + k;
+        sh_at[s0 + nsh] = a;
+        sh_iao[s0 + nsh] = nao;
+        for (int x = 0; x < msao(sh.ang); ++x) { ao_at[o0 + nao + x] = a; ao_sh[o0 + nao + x] = nsh; }
         nao += msao(sh.ang);
         nsh += 1;
+        nref += sh.refocc;
       }
     }
-    {
-      double nref = -s.charge;
-      for (int a = 0; a < s.nat; ++a) {
-        const SpeciesParam& sp = P.sp[s.id[a]];
-        for (int k = 0; k < sp.nsh; ++k) nref += P.sh[sp.sh0 + k].refocc;
-      }
-      b->h_nocc.push_back(std::ceil(0.5 * nref));
-    }
-    b->h_aoff[m + 1] = b->h_aoff[m] + s.nat;
-    b->h_soff[m + 1] = b->h_soff[m] + nsh;
-    b->h_ooff[m + 1] = b->h_ooff[m] + nao;
-    b->h_mixoff[m + 1] = b->h_mixoff[m] + nsh + 9 * s.nat;
-    b->h_moff[m + 1] = b->h_moff[m] + (long long)nao * nao;
-    b->h_poff[m + 1] = b->h_poff[m] + (long long)s.nat * (s.nat - 1) / 2;
-    b->h_s2off[m + 1] = b->h_s2off[m] + (long long)nsh * nsh;
-    b->h_a2off[m + 1] = b->h_a2off[m] + (long long)s.nat * s.nat;
-    b->nmax = std::max(b->nmax, nao);
-    b->natmax = std::max(b->natmax, (int)s.nat);
-    b->nshmax = std::max(b->nshmax, nsh);
+    b->h_nocc[m] = std::ceil(0.5 * nref);
+    long long i64 = t64o[m], i128 = t128o[m], i32 = t32o[m], ic = c32o[m];
     for (int t = 0; t < (nao + 63) / 64; ++t)
-      for (int u = 0; u < (nao + 63) / 64; ++u) b->tiles64.push_back(make_int4(m, t, u, 0));
+      for (int u = 0; u < (nao + 63) / 64; ++u) b->tiles64[i64++] = make_int4(m, t, u, 0);
     for (int t = 0; t < (nao + kTcTile - 1) / kTcTile; ++t)
-      for (int u = 0; u < (nao + kTcTile - 1) / kTcTile; ++u) b->tiles128.push_back(make_int4(m, t, u, 0));
+      for (int u = 0; u < (nao + kTcTile - 1) / kTcTile; ++u) b->tiles128[i128++] = make_int4(m, t, u, 0);
     for (int t = 0; t < (nao + 31) / 32; ++t) {
-      b->chunks32.push_back(make_int2(m, t));
-      for (int u = 0; u < (nao + 31) / 32; ++u) b->tiles32.push_back(make_int4(m, t, u, 0));
+      b->chunks32[ic++] = make_int2(m, t);
+      for (int u = 0; u < (nao + 31) / 32; ++u) b->tiles32[i32++] = make_int4(m, t, u, 0);
+    }
+  };
+  {
+    const long long na = b->h_aoff[nmol];
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nth = (int)std::min<long long>(std::min(hw, 8), std::max<long long>(1, na / 8192));
+    if (nth <= 1) {
+      for (int m = 0; m < nmol; ++m) fill(m);
+    } else {  // contiguous ranges of about na / nth atoms
+      std::vector<std::thread> pool;
+      int lo = 0;
+      try {
+        for (int t = 0; t < nth && lo < nmol; ++t) {
+          const long long target = na * (t + 1) / nth;
+          int hi = lo;
+          while (hi < nmol && (t == nth - 1 || b->h_aoff[hi] < target)) ++hi;
+          if (hi == lo) hi = lo + 1;
+          pool.emplace_back([&fill, lo, hi]() { for (int m = lo; m < hi; ++m) fill(m); });
+          lo = hi;
+        }
+      } catch (...) {  // no thread: the ranges not handed out are filled here
+      }
+      for (int m = lo; m < nmol; ++m) fill(m);
+      for (auto& th : pool) th.join();
     }
   }
   // solver choice: 0 auto (in-house up to kSyevMaxN AOs, library above), 1 in-house only, 2 library only
