@@ -64,6 +64,27 @@ def dist_setup(args):
     return ws, rank, local
 
 
+def rank_seed(rank):
+    """Seed of a rank's own batch (replicas: every rank its own structures)."""
+    return 1001 + rank
+
+
+def max_over_ranks(x, ws, device=None):
+    """The largest of x over the ranks of the default process group (x on one rank)."""
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(ws, steps, per_rank_units, elapsed):
+    """Whole-job throughput: the units every rank processed over the slowest rank's time."""
+    return ws * steps * per_rank_units / elapsed
+
+
 class ClockSampler:
     """nvidia-smi clocks/throttle sampling during the timed region."""
 
@@ -248,7 +269,7 @@ def main():
                                device_id=torch.device("cuda", local))
     from tblite_b200 import Calculator, capi, geometry
     calc = Calculator()
-    mols = geometry.water_clusters(args.count, seed=1001 + rank)
+    mols = geometry.water_clusters(args.count, seed=rank_seed(rank))
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
     nat = sum(m.nat for m in mols)
@@ -266,12 +287,8 @@ def main():
         dist.barrier()
     clocks = sampler.stop()
     for name, f in forms.items():
-        el = f["elapsed"]
-        if ws > 1:
-            tt = torch.tensor([el], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            el = float(tt.item())
-        f["value"] = ws * args.steps * len(mols) / el
+        el = max_over_ranks(f["elapsed"], ws, device="cuda")
+        f["value"] = job_rate(ws, args.steps, len(mols), el)
         f["ms_per_step"] = el / args.steps * 1e3
     e_fp = np.array([r["energy"] for r in forms["fp64"]["res"]])
     e_mx = np.array([r["energy"] for r in forms["mixed"]["res"]])
@@ -295,12 +312,8 @@ def main():
     for _ in range(args.steps):
         calc.singlepoint_batch(mols, stream=sh, precision=head_prec, use_graphs=1)
     torch.cuda.synchronize()
-    e2e_t = time.perf_counter() - te
-    if ws > 1:
-        tt = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_t = float(tt.item())
-    e2e = {"value": ws * args.steps * len(mols) / e2e_t, "unit": UNIT, "h2d_bytes_per_step": ids_bytes,
+    e2e_t = max_over_ranks(time.perf_counter() - te, ws, device="cuda")
+    e2e = {"value": job_rate(ws, args.steps, len(mols), e2e_t), "unit": UNIT, "h2d_bytes_per_step": ids_bytes,
            "d2h_bytes_per_step": out_bytes}
 
     # ---------------- roofline of the dominant kernel class (live CUDA-event times, headline form)
