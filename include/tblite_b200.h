@@ -39,7 +39,9 @@ typedef enum tb_status {
   TB_NOT_SPD = 2,              /* overlap matrix not positive definite          */
   TB_SCF_NOT_CONVERGED = 3,    /* max_iter reached                              */
   TB_FERMI_NOT_CONVERGED = 4,  /* Fermi level solve hit its iteration cap       */
-  TB_EIGEN_FAILED = 5,         /* QL iteration cap reached                      */
+  TB_EIGEN_FAILED = 5,         /* tridiagonal solve failed: QL (or a divide-and-
+                                  conquer leaf) hit its sweep cap, or the matrix
+                                  was not finite                                */
   TB_CAPACITY_EXCEEDED = 6,    /* request larger than a stated maximum          */
   TB_CUDA_ERROR = 7,           /* CUDA runtime error (see tb_last_error)        */
   TB_PARAM_ERROR = 8           /* parameter file could not be read              */
