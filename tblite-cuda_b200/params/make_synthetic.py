@@ -46,6 +46,9 @@ from scipy.optimize import minimize
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "synthetic_hco.tbp")
+# test file with one more element whose shell set includes a d shell, so that
+# the d-shell integral, transformation and Fock paths are exercised
+OUT_D = os.path.join(HERE, "synthetic_hcos.tbp")
 
 # radial grid for the fits
 _R = np.linspace(1e-6, 40.0, 40001)
@@ -153,19 +156,32 @@ ELEMENTS = [
 ]
 
 
-def main():
+# S-like element with an s+p+d valence shell set (d empty in the reference
+# occupation, as for the heavier main-group elements of GFN2)
+ELEMENT_S = ("S", 16,
+             dict(rad=1.80, rcov=2.00, en=2.58, rep_alpha=1.80, rep_zeff=8.00,
+                  mp_rad=3.20, mp_vcn=2.0, dkernel=0.0060, qkernel=0.0015),
+             [(3, 0, 2.10, 4, dict(selfenergy=-0.6200, kcn=0.0040, shpoly=-0.010, refocc=2.0,
+                                   hubbard=0.4400, hubbard_deriv=0.0900)),
+              (3, 1, 1.85, 4, dict(selfenergy=-0.4200, kcn=0.0020, shpoly=0.030, refocc=4.0,
+                                   hubbard=0.3900, hubbard_deriv=0.0500)),
+              (3, 2, 1.20, 3, dict(selfenergy=-0.1200, kcn=0.0010, shpoly=0.060, refocc=0.0,
+                                   hubbard=0.3000, hubbard_deriv=0.0300))])
+
+
+def write(path, name, title, elements):
     lines = [
-        "# SYNTHETIC GFN2-shaped parameters for H, C, O.",
+        f"# SYNTHETIC GFN2-shaped parameters for {title}.",
         "# These are NOT the GFN2-xTB parameters; they only have the same fields and",
         "# plausible magnitudes. Generated by make_synthetic.py (deterministic).",
         "format tblite-b200-params 1",
-        "name synthetic-gfn2-shaped-HCO",
+        f"name {name}",
     ]
     for k, v in GLOBALS.items():
         lines.append(f"global {k} {v!r}")
     for (li, lj), v in sorted(KSHELL.items()):
         lines.append(f"kshell {li} {lj} {v!r}")
-    for sym, z, escal, shells in ELEMENTS:
+    for sym, z, escal, shells in elements:
         lines.append(f"element {sym} {z}")
         for k, v in escal.items():
             lines.append(f"  {k} {v!r}")
@@ -181,9 +197,15 @@ def main():
             lines.append("    coeff " + " ".join(f"{x:.17g}" for x in coeff))
             lines.append("  end")
         lines.append("end")
-    with open(OUT, "w") as fh:
+    with open(path, "w") as fh:
         fh.write("\n".join(lines) + "\n")
-    print("wrote", OUT)
+    print("wrote", path)
+
+
+def main():
+    write(OUT, "synthetic-gfn2-shaped-HCO", "H, C, O", ELEMENTS)
+    write(OUT_D, "synthetic-gfn2-shaped-HCOS", "H, C, O, S (test file: S has a d shell)",
+          ELEMENTS + [ELEMENT_S])
 
 
 if __name__ == "__main__":
