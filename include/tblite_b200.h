@@ -95,6 +95,40 @@ typedef struct tb_result {
   double* qpat;           /* [nat][6] atomic quadrupoles                       */
 } tb_result;
 
+/* wavefunction_type (src/wavefunction/type.h:81-99) of one structure, as the
+ * in/out argument `wfn` of xtb_singlepoint (src/xtb.cu:188-197).  One density
+ * for both spin channels (nspin = 1, as the reference's SCF; uhf only splits
+ * the electrons, get_alpha_beta_occupation, src/wavefunction/type.cu:3-14).
+ * The arrays are caller-owned host buffers sized from tb_basis_size; a NULL
+ * array is neither read nor written.
+ *   in:  guess = 1 starts the SCF from qsh, dpat and qpat as given (for
+ *        example the result of an earlier singlepoint of the same or a nearby
+ *        geometry, the reference's wfn carried from call to call); guess = 0
+ *        uses the default start (the charge spread over the shells by their
+ *        reference occupations, no multipoles).
+ *   out: everything else, from the last SCF iteration of the structure. */
+typedef struct tb_wavefunction {
+  int32_t guess;          /* in                                                */
+  int32_t nspin;          /* 1                                                 */
+  int32_t nat, nsh, nao;
+  int32_t homo[2];        /* highest orbital of the aufbau filling per channel
+                             (1-based count, floor(nel[s]))                    */
+  double kt;              /* electronic temperature (Eh)                       */
+  double nocc;            /* electrons                                         */
+  double nuhf;            /* unpaired electrons                                */
+  double nel[2];          /* alpha, beta electrons                             */
+  double* n0at;           /* [nat]   reference occupation per atom             */
+  double* n0sh;           /* [nsh]   reference occupation per shell            */
+  double* emo;            /* [nao]   orbital energies, ascending               */
+  double* focc;           /* [nao]   occupations, alpha + beta                 */
+  double* density;        /* [nao][nao] P = C diag(focc) C^T                   */
+  double* coeff;          /* [nao][nao] coeff[mu * nao + i]: AO mu of orbital i */
+  double* qat;            /* [nat]   atomic charges                            */
+  double* qsh;            /* [nsh]   shell charges        (in with guess = 1)  */
+  double* dpat;           /* [nat][3] atomic dipoles      (in with guess = 1)  */
+  double* qpat;           /* [nat][6] atomic quadrupoles  (in with guess = 1)  */
+} tb_wavefunction;
+
 typedef struct tb_calculator tb_calculator;
 
 /* xtb_calculator construction (src/xtb.h:105-126; the reference never builds
@@ -113,10 +147,13 @@ const char* tb_last_error(void);
 tb_status tb_basis_size(const tb_calculator* calc, const tb_structure* mol, int32_t* nsh, int32_t* nao);
 
 /* xtb_singlepoint (src/xtb.cu:188-434) for nmol structures at once, host
- * buffers in and out.  Returns TB_OK when every structure succeeded, else the
- * first failing structure's status; per-structure status is in out[i].status. */
+ * buffers in and out.  wfn_inout is NULL or nmol records (the reference's
+ * wavefunction_type& wfn, in and out).  Returns TB_OK when every structure
+ * succeeded, else the first failing structure's status; per-structure status
+ * is in out[i].status. */
 tb_status tb_singlepoint_batch(tb_calculator* calc, const tb_structure* mols, int32_t nmol,
-                               const tb_options* opt, tb_result* out, void* stream);
+                               const tb_options* opt, tb_wavefunction* wfn_inout, tb_result* out,
+                               void* stream);
 
 /* Device-resident batches (for serving and for timing without host copies):
  * create uploads geometry and sizes workspaces, run executes the full
@@ -126,6 +163,11 @@ tb_status tb_batch_create(tb_calculator* calc, const tb_structure* mols, int32_t
                           const tb_options* opt, tb_batch** out);
 tb_status tb_batch_run(tb_batch* batch, void* stream);
 tb_status tb_batch_results(tb_batch* batch, tb_result* out, void* stream);
+/* Starting guesses for the next tb_batch_run from nmol wavefunction records
+ * (records with guess = 0 keep the default start), and the wavefunctions of
+ * the last run (the same records as tb_singlepoint_batch's wfn_inout). */
+tb_status tb_batch_set_guess(tb_batch* batch, const tb_wavefunction* wfn);
+tb_status tb_batch_wavefunction(tb_batch* batch, tb_wavefunction* wfn, void* stream);
 /* kernels launched by the last tb_batch_run (device work items, not host calls) */
 int64_t tb_batch_launches(const tb_batch* batch);
 /* Instrumentation (no counterpart in the reference, which only times its one
@@ -217,8 +259,10 @@ tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const 
  * static ~2 MiB device array of the library (held by each GPU that loads the
  * library until exit).  n <= 256, else TB_CAPACITY_EXCEEDED.  All calls on a
  * device share that array: calls whose GPU work overlaps race, so serialise
- * them.  The first call on a device looks up the array's address; make it
- * before any stream capture.  Synchronous on `stream`. */
+ * them.  The first call on a device does a one-time set-up (it looks up the
+ * array's address and raises the eigensolver's shared memory limit, neither of
+ * which allocates); make it before any stream capture.  Synchronous on
+ * `stream`. */
 tb_status tb_sygvd_noalloc(int32_t n, const double* H, const double* S, double* w, double* C, void* stream);
 
 /* get_fermi_filling (src/wavefunction/fermi.cu:100-124) for one spin channel. */

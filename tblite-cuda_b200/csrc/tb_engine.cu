@@ -280,6 +280,13 @@ struct tb_batch {
   double *q_in, *dq, *dqlast, *qlast, *df, *u, *amat, *omega;
   double* charge;
   int* uhf;
+  // caller's starting moments (tb_wavefunction.guess): host copy in the q_in
+  // layout, per-structure flags, and their device buffers
+  std::vector<double> h_guess;
+  std::vector<int> h_guess_flag;
+  bool any_guess = false;
+  double* d_guess = nullptr;
+  int* d_guess_flag = nullptr;
   int4 *d_tiles64, *d_tiles32, *d_tiles128;
   int2* d_chunks32;
   int* h_nactive = nullptr;  // pinned
@@ -291,6 +298,7 @@ struct tb_batch {
   size_t lib_bytes = 0;
   int* lib_info = nullptr;   // 2 per library structure
   std::vector<int> h_active, h_status;
+  std::vector<int> h_species;  // species index per atom of the batch
   // mixed-precision form (tb_options.precision = 1)
   bool mixed = false;
   float *Af = nullptr, *Zf = nullptr, *wf = nullptr;
@@ -563,6 +571,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
          o_ms_ees2 = L.add(NM * D8), o_ms_eaes2 = L.add(NM * D8), o_ms_ees3 = L.add(NM * D8),
          o_ms_err = L.add(NM * D8), o_ms_fw = L.add(NM * I4), o_ms_dip = L.add(3 * NM * D8),
          o_ms_nact = L.add(I4);
+  size_t o_guess = L.add(MX * D8), o_gflag = L.add(NM * I4);
   size_t o_lwork = L.add(std::max<size_t>(b->lib_bytes, 16)), o_linfo = L.add((2 * b->big.size() + 2) * I4);
   // mixed-precision form: FP32 eigensolver input/output, refinement buffers, phase state
   const long long MXN2 = b->mixed ? N2 : 0, MXNO = b->mixed ? NO : 0, MXNM = b->mixed ? NM : 0;
@@ -599,6 +608,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   put(o_meta_a2off, b->h_a2off.data(), (NM + 1) * 8);
   put(o_xyz, b->h_xyz.data(), 3 * NA * D8);
   put(o_id, id.data(), NA * I4);
+  b->h_species.swap(id);
   put(o_atmol, at_mol.data(), NA * I4);
   put(o_shtype, sh_type.data(), NS * I4);
   put(o_shat, sh_at.data(), NS * I4);
@@ -650,6 +660,10 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   }
   b->d_tiles64 = at<int4>(base, o_t64); b->d_tiles128 = at<int4>(base, o_t128); b->d_tiles32 = at<int4>(base, o_t32); b->d_chunks32 = at<int2>(base, o_c32);
   b->charge = at<double>(base, o_charge); b->uhf = at<int>(base, o_uhf);
+  b->d_guess = at<double>(base, o_guess); b->d_guess_flag = at<int>(base, o_gflag);
+  b->h_guess.clear();
+  b->h_guess_flag.clear();
+  b->any_guess = false;
   b->cn = at<double>(base, o_cn); b->mrad = at<double>(base, o_mrad); b->erep = at<double>(base, o_erep);
   b->se = at<double>(base, o_se); b->n0sh = at<double>(base, o_n0sh); b->cnt = at<int>(base, o_cnt);
   b->inl = at<long long>(base, o_inl); b->npair = at<int>(base, o_npair); b->pair_i = at<int>(base, o_pi);
@@ -1018,6 +1032,13 @@ tb_status batch_setup(tb_batch* b, cudaStream_t st) {
     prof_stop(b, st, "factor_lib", e0, 0, 0);
   }
   TB_K("scf_init", 0, 0, k_scf_init<<<nmol, 256, 0, st>>>(Pc, B, b->charge, b->uhf, b->erep, b->n0sh, b->q_in, S));
+  if (b->any_guess) {
+    TB_CUDA(cudaMemcpyAsync(b->d_guess, b->h_guess.data(), b->h_guess.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, st));
+    TB_CUDA(cudaMemcpyAsync(b->d_guess_flag, b->h_guess_flag.data(), nmol * sizeof(int), cudaMemcpyHostToDevice,
+                            st));
+    TB_K("scf_init", 0, 0, k_apply_guess<<<nmol, 256, 0, st>>>(B, b->d_guess, b->d_guess_flag, b->q_in));
+  }
   {
     const tb_status ss = raise_smem_limits();
     if (ss != TB_OK) return ss;
@@ -1238,6 +1259,95 @@ tb_status batch_results(tb_batch* b, tb_result* out, cudaStream_t st) {
   return first;
 }
 
+// Starting moments of the next run from the caller's wavefunctions: records
+// with guess = 1 provide qsh, dpat and qpat, written into the mixer layout
+// [qsh, dpat, qpat] of their structure (k_apply_guess copies them over the
+// default guess after k_scf_init).
+tb_status batch_set_guess(tb_batch* b, const tb_wavefunction* wfn) {
+  const int nmol = b->nmol;
+  b->h_guess.assign((size_t)b->mix_tot, 0.0);
+  b->h_guess_flag.assign(nmol, 0);
+  b->any_guess = false;
+  if (!wfn) return TB_OK;
+  for (int m = 0; m < nmol; ++m) {
+    const tb_wavefunction& w = wfn[m];
+    if (!w.guess) continue;
+    if (!w.qsh || !w.dpat || !w.qpat)
+      return fail(TB_BAD_INPUT, "wavefunction " + std::to_string(m) + ": guess = 1 needs qsh, dpat and qpat");
+    const int nat = b->h_aoff[m + 1] - b->h_aoff[m], nsh = b->h_soff[m + 1] - b->h_soff[m];
+    double* g = b->h_guess.data() + b->h_mixoff[m];
+    for (int i = 0; i < nsh; ++i) g[i] = w.qsh[i];
+    for (int i = 0; i < 3 * nat; ++i) g[nsh + i] = w.dpat[i];
+    for (int i = 0; i < 6 * nat; ++i) g[nsh + 3 * nat + i] = w.qpat[i];
+    for (int i = 0; i < nsh + 9 * nat; ++i)
+      if (!std::isfinite(g[i])) return fail(TB_BAD_INPUT, "wavefunction " + std::to_string(m) + ": non-finite guess");
+    b->h_guess_flag[m] = 1;
+    b->any_guess = true;
+  }
+  return TB_OK;
+}
+
+// wavefunction_type of every structure after a run (tb_wavefunction): the
+// scalars, the per-structure vectors gathered in one copy per field, and the
+// density and coefficient matrices copied straight into the caller's arrays.
+// W holds C = X Z of the structure's last iteration (the density GEMM reads
+// it; nothing later overwrites it), P its density, w and focc its orbital
+// energies (ascending) and occupations.
+tb_status batch_wavefunction(tb_batch* b, tb_wavefunction* wfn, cudaStream_t st) {
+  const int nmol = b->nmol;
+  const int NA = b->nat_tot, NS = b->nsh_tot, NO = b->nao_tot;
+  std::vector<double> emo(NO), focc(NO), n0sh(NS), nel(2 * (size_t)nmol), qat(NA), qsh(NS), dp(3 * (size_t)NA),
+      qp(6 * (size_t)NA);
+  auto cp = [&](void* dst, const void* src, size_t n) { return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, st); };
+  TB_CUDA(cp(emo.data(), b->w, NO * 8));
+  TB_CUDA(cp(focc.data(), b->focc, NO * 8));
+  TB_CUDA(cp(n0sh.data(), b->n0sh, NS * 8));
+  TB_CUDA(cp(nel.data(), b->ms.nel, 2 * (size_t)nmol * 8));
+  TB_CUDA(cp(qat.data(), b->qat_out, NA * 8));
+  TB_CUDA(cp(qsh.data(), b->qsh_out, NS * 8));
+  TB_CUDA(cp(dp.data(), b->dpat_out, 3 * (size_t)NA * 8));
+  TB_CUDA(cp(qp.data(), b->qpat_out, 6 * (size_t)NA * 8));
+  for (int m = 0; m < nmol; ++m) {
+    tb_wavefunction& w = wfn[m];
+    const long long nn = b->h_moff[m + 1] - b->h_moff[m];
+    if (w.density) TB_CUDA(cp(w.density, b->P + b->h_moff[m], nn * 8));
+    if (w.coeff) TB_CUDA(cp(w.coeff, b->W + b->h_moff[m], nn * 8));
+  }
+  TB_CUDA(cudaStreamSynchronize(st));
+  const HostParams& P = b->calc->hp;
+  for (int m = 0; m < nmol; ++m) {
+    tb_wavefunction& w = wfn[m];
+    const int a0 = b->h_aoff[m], s0 = b->h_soff[m], o0 = b->h_ooff[m];
+    w.nspin = 1;
+    w.nat = b->h_aoff[m + 1] - a0;
+    w.nsh = b->h_soff[m + 1] - s0;
+    w.nao = b->h_ooff[m + 1] - o0;
+    w.kt = b->opt.kt;
+    w.nel[0] = nel[2 * m];
+    w.nel[1] = nel[2 * m + 1];
+    w.nocc = w.nel[0] + w.nel[1];
+    w.nuhf = w.nel[0] - w.nel[1];
+    for (int s = 0; s < 2; ++s) w.homo[s] = (int32_t)std::floor(w.nel[s]);
+    if (w.emo) std::memcpy(w.emo, emo.data() + o0, w.nao * 8);
+    if (w.focc) std::memcpy(w.focc, focc.data() + o0, w.nao * 8);
+    if (w.n0sh) std::memcpy(w.n0sh, n0sh.data() + s0, w.nsh * 8);
+    if (w.n0at) {  // the shells of an atom are consecutive
+      int s = s0;
+      for (int a = 0; a < w.nat; ++a) {
+        const int nsh_a = P.sp[b->h_species[a0 + a]].nsh;
+        double t = 0.0;
+        for (int k = 0; k < nsh_a; ++k) t += n0sh[s++];
+        w.n0at[a] = t;
+      }
+    }
+    if (w.qat) std::memcpy(w.qat, qat.data() + a0, w.nat * 8);
+    if (w.qsh) std::memcpy(w.qsh, qsh.data() + s0, w.nsh * 8);
+    if (w.dpat) std::memcpy(w.dpat, dp.data() + 3 * (size_t)a0, 3 * (size_t)w.nat * 8);
+    if (w.qpat) std::memcpy(w.qpat, qp.data() + 6 * (size_t)a0, 6 * (size_t)w.nat * 8);
+  }
+  return TB_OK;
+}
+
 }  // namespace
 
 // error text for the allocation-free entry point (tb_noalloc.cu)
@@ -1344,6 +1454,16 @@ tb_status tb_batch_results(tb_batch* b, tb_result* out, void* stream) {
   return batch_results(b, out, (cudaStream_t)stream);
 }
 
+tb_status tb_batch_set_guess(tb_batch* b, const tb_wavefunction* wfn) {
+  if (!b) return fail(TB_BAD_INPUT, "null batch");
+  return batch_set_guess(b, wfn);
+}
+
+tb_status tb_batch_wavefunction(tb_batch* b, tb_wavefunction* wfn, void* stream) {
+  if (!b || !wfn) return fail(TB_BAD_INPUT, "null argument");
+  return batch_wavefunction(b, wfn, (cudaStream_t)stream);
+}
+
 int64_t tb_batch_launches(const tb_batch* b) { return b ? b->launches : 0; }
 
 int32_t tb_batch_profile(const tb_batch* b, int32_t max, char* names, int64_t* launches, double* ms, double* work,
@@ -1363,7 +1483,7 @@ int32_t tb_batch_profile(const tb_batch* b, int32_t max, char* names, int64_t* l
 void tb_batch_destroy(tb_batch* b) { delete b; }
 
 tb_status tb_singlepoint_batch(tb_calculator* calc, const tb_structure* mols, int32_t nmol, const tb_options* opt,
-                               tb_result* out, void* stream) {
+                               tb_wavefunction* wfn_inout, tb_result* out, void* stream) {
   if (!calc || !mols || !out) return fail(TB_BAD_INPUT, "null argument");
   tb_options o;
   if (opt) o = *opt; else tb_default_options(&o);
@@ -1371,9 +1491,19 @@ tb_status tb_singlepoint_batch(tb_calculator* calc, const tb_structure* mols, in
   tb_batch b;
   tb_status st = batch_build(calc, mols, nmol, &o, &b, &calc->arena);
   if (st != TB_OK) return st;
+  if (wfn_inout) {
+    st = batch_set_guess(&b, wfn_inout);
+    if (st != TB_OK) return st;
+  }
   st = batch_run(&b, (cudaStream_t)stream);
   if (st != TB_OK) return st;
-  return batch_results(&b, out, (cudaStream_t)stream);
+  const tb_status rs = batch_results(&b, out, (cudaStream_t)stream);
+  if (rs == TB_CUDA_ERROR) return rs;
+  if (wfn_inout) {  // also for structures that failed: their records hold their last state
+    st = batch_wavefunction(&b, wfn_inout, (cudaStream_t)stream);
+    if (st != TB_OK) return st;
+  }
+  return rs;
 }
 
 }  // extern "C"

@@ -86,6 +86,19 @@ __global__ void k_scf_init(DevParams P, DevBatch B, const double* __restrict__ c
   }
 }
 
+// Starting point of the SCF taken from the caller's wavefunction (the
+// reference's xtb_singlepoint takes wfn in and out, src/xtb.cu:188-197, and
+// its first iteration builds the potential from the charges it holds): the
+// moments [qsh, dpat, qpat] of flagged structures replace the default guess
+// that k_scf_init wrote.
+__global__ void k_apply_guess(DevBatch B, const double* __restrict__ guess, const int* __restrict__ flag,
+                              double* __restrict__ q_in) {
+  const int m = blockIdx.x;
+  if (!flag[m]) return;
+  const int mo = B.mixoff[m], ndim = B.mixoff[m + 1] - mo;
+  for (int i = threadIdx.x; i < ndim; i += blockDim.x) q_in[mo + i] = guess[mo + i];
+}
+
 // ------------------------------------------------------------ pair tables
 // The geometry is fixed during the SCF, so the shell-pair Coulomb kernel
 // gamma_ab (ES2) and the atom-pair 1/r and AES2 damping factors are

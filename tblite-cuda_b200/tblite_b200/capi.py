@@ -49,6 +49,15 @@ class Result(C.Structure):
                 ("qpat", _dp)]
 
 
+class Wavefunction(C.Structure):
+    """tb_wavefunction: wavefunction_type (reference src/wavefunction/type.h:81-99)."""
+    _fields_ = [("guess", C.c_int32), ("nspin", C.c_int32), ("nat", C.c_int32), ("nsh", C.c_int32),
+                ("nao", C.c_int32), ("homo", C.c_int32 * 2), ("kt", C.c_double), ("nocc", C.c_double),
+                ("nuhf", C.c_double), ("nel", C.c_double * 2), ("n0at", _dp), ("n0sh", _dp), ("emo", _dp),
+                ("focc", _dp), ("density", _dp), ("coeff", _dp), ("qat", _dp), ("qsh", _dp), ("dpat", _dp),
+                ("qpat", _dp)]
+
+
 EXPORTS = [
     "tb_calculator_create", "tb_calculator_destroy", "tb_calculator_nspecies", "tb_default_options",
     "tb_last_error", "tb_basis_size", "tb_singlepoint_batch", "tb_batch_create", "tb_batch_run",
@@ -56,6 +65,7 @@ EXPORTS = [
     "tb_atomic_properties", "tb_repulsion", "tb_get_hamiltonian", "tb_coulomb_potential",
     "tb_add_pot_to_h1", "tb_sygvd_batch", "tb_fermi_filling", "tb_batch_profile",
     "tb_server_create", "tb_server_submit", "tb_server_step", "tb_server_poll", "tb_server_destroy",
+    "tb_batch_set_guess", "tb_batch_wavefunction", "tb_sygvd_noalloc",
 ]
 
 _lib = None
@@ -187,8 +197,13 @@ class Calculator:
     def cutoff(self, accuracy=1.0):
         return load_library().tb_get_cutoff(self.h, C.c_double(accuracy))
 
-    def singlepoint_batch(self, mols, stream=None, raise_on_error=False, **opts):
-        """Run xtb_singlepoint for every structure; returns a list of result dicts."""
+    def singlepoint_batch(self, mols, stream=None, raise_on_error=False, wavefunction=False, guess=None, **opts):
+        """Run xtb_singlepoint for every structure; returns a list of result dicts.
+
+        wavefunction=True adds r["wfn"] (the tb_wavefunction record as a dict:
+        emo, focc, density, coeff, n0at, n0sh, nel, homo, ...).  guess is None or
+        a list (one entry per structure, None for the default start) of dicts
+        with qsh, dpat and qpat to start the SCF from, e.g. an earlier result."""
         L = load_library()
         arr, keep = _structs(mols)
         o = default_options(**opts)
@@ -216,7 +231,10 @@ class Calculator:
             v["qsh"] = qsh.ctypes.data + 8 * soff
             v["dpat"] = dpat.ctypes.data + 24 * off
             v["qpat"] = qpat.ctypes.data + 48 * off
-        st = L.tb_singlepoint_batch(self.h, arr, C.c_int32(n), C.byref(o), res, C.c_void_p(stream or 0))
+        wfn, wbufs = None, None
+        if n and (wavefunction or guess is not None):
+            wfn, wbufs = _wavefunction_records(self, mols, guess, wavefunction)
+        st = L.tb_singlepoint_batch(self.h, arr, C.c_int32(n), C.byref(o), wfn, res, C.c_void_p(stream or 0))
         if st not in (TB_OK,) and (raise_on_error or st in (TB_BAD_INPUT, TB_CUDA_ERROR,
                                                             TB_CAPACITY_EXCEEDED, TB_PARAM_ERROR)):
             check(st, "tb_singlepoint_batch")
@@ -234,6 +252,10 @@ class Calculator:
             d = {k: c[i] for k, c in zip(keys, cols)}
             a0, a1 = a0s[i], a1s[i]
             d.update(dipole=dip[i], qat=qat[a0:a1], qsh=qsh[s0s[i]:s1s[i]], dpat=dpat[a0:a1], qpat=qpat[a0:a1])
+            if wavefunction:
+                w = wfn[i]
+                d["wfn"] = dict(wbufs[i], nspin=w.nspin, nat=w.nat, nsh=w.nsh, nao=w.nao, homo=list(w.homo),
+                                kt=w.kt, nocc=w.nocc, nuhf=w.nuhf, nel=list(w.nel))
             out.append(d)
         return out
 
@@ -253,6 +275,34 @@ def _result_dict(r, b):
              scf_error=r.scf_error, iterations=r.iterations, status=r.status, nsh=r.nsh, nao=r.nao)
     d.update(b)
     return d
+
+
+def _wavefunction_records(calc, mols, guess, outputs):
+    """tb_wavefunction records for mols: output arrays when `outputs`, the
+    caller's starting moments where guess[i] is given."""
+    n = len(mols)
+    rec = (Wavefunction * n)()
+    bufs = []
+    for i, m in enumerate(mols):
+        nsh, nao = calc.basis_size(m)
+        b = {}
+        if outputs:
+            b = dict(n0at=np.zeros(m.nat), n0sh=np.zeros(nsh), emo=np.zeros(nao), focc=np.zeros(nao),
+                     density=np.zeros((nao, nao)), coeff=np.zeros((nao, nao)), qat=np.zeros(m.nat),
+                     qsh=np.zeros(nsh), dpat=np.zeros((m.nat, 3)), qpat=np.zeros((m.nat, 6)))
+        g = guess[i] if guess is not None else None
+        if g is not None:
+            for k, shape in (("qsh", (nsh,)), ("dpat", (m.nat, 3)), ("qpat", (m.nat, 6))):
+                a = np.ascontiguousarray(np.array(g[k], np.float64).reshape(shape))
+                if k in b:
+                    b[k][...] = a
+                else:
+                    b[k] = a
+            rec[i].guess = 1
+        for k, a in b.items():
+            setattr(rec[i], k, a.ctypes.data_as(_dp))
+        bufs.append(b)
+    return rec, bufs
 
 
 class Batch:
