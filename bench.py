@@ -48,12 +48,15 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--count", type=int, default=1024, help="structures per batch")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "water_box_1000", "serving"],
-                    help="water_box_1000: one 3000-atom / 6000-AO structure, time per SCF iteration; "
+    ap.add_argument("--workload", default=WORKLOAD,
+                    choices=[WORKLOAD, "alkanes_256", "water_box_1000", "serving"],
+                    help="alkanes_256: 256 alkanes C20-C199, both forms with per-structure errors; "
+                         "water_box_1000: one 3000-atom / 6000-AO structure, time per SCF iteration; "
                          "serving: the request stream through tb_server, both forms")
-    ap.add_argument("--serving-requests", type=int, default=300,
-                    help="requests of the bounded serving sample (0: skip)")
-    ap.add_argument("--serving-rate", type=float, default=30.0, help="Poisson arrival rate per second")
+    ap.add_argument("--serving-requests", type=int, default=400,
+                    help="requests of the bounded serving sample per form (0: skip)")
+    ap.add_argument("--serving-rate", type=float, default=1000.0,
+                    help="Poisson arrival rate per second (default above capacity: latency measures the GPU)")
     return ap.parse_args()
 
 
@@ -164,24 +167,49 @@ def ncu_traffic():
     return None
 
 
-def cpu_baseline(mols, nthreads, target_s=12.0):
-    """FP64 oracle (CPU restatement) on a bounded sample of the workload."""
+def oracle_for_timing():
+    """The FP64 oracle built on this host with -march=native (rebuilt here, so
+    the instruction set is this CPU's), else the portable build."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
+    build = "portable build (-O3)"
+    try:
+        r = subprocess.run(["make", "-B", "-s", "-C", os.path.join(ROOT, "oracle"), "liboracle_native.so"],
+                           capture_output=True, text=True, timeout=300)
+        so = os.path.join(ROOT, "oracle", "liboracle_native.so")
+        if r.returncode == 0 and os.path.exists(so):
+            pyoracle.use_library(so)
+            build = "built on this host with -O3 -march=native"
+    except Exception:
+        pass
     orc = pyoracle.Oracle(os.path.join(ROOT, "tblite-cuda_b200", "params", "synthetic_hco.tbp"))
-    # calibrate on a small sample, then size the sample to about target_s seconds
-    probe = mols[:max(1, min(len(mols), nthreads))]
+    return orc, build
+
+
+def lpt_sample(mols, start, count):
+    """`count` consecutive structures of the workload from `start` (wrapping),
+    as indices ordered largest first, so that a dynamic one-structure-per-thread
+    schedule ends with small structures (balanced threads)."""
+    idx = [(start + k) % len(mols) for k in range(count)]
+    return sorted(idx, key=lambda i: -mols[i].nat)
+
+
+def cpu_baseline(orc, build, mols, nthreads, target_s=12.0):
+    """FP64 oracle (CPU restatement) on a bounded, load-balanced sample of the workload:
+    at least 8 structures per thread, largest first, sized to about target_s seconds."""
+    probe = lpt_sample(mols, 0, max(1, min(len(mols), nthreads)))
     t = time.perf_counter()
-    orc.singlepoint_batch(probe, nthreads=nthreads)
+    orc.singlepoint_batch([mols[i] for i in probe], nthreads=nthreads)
     dt = max(time.perf_counter() - t, 1e-3)
     per = dt / len(probe) * nthreads  # seconds per structure per thread
-    count = int(min(len(mols), max(len(probe), target_s * nthreads / max(per, 1e-6))))
-    sample = mols[:count]
+    count = int(min(len(mols), max(8 * nthreads, target_s * nthreads / max(per, 1e-6))))
+    sample = lpt_sample(mols, 0, count)
     t = time.perf_counter()
-    res = orc.singlepoint_batch(sample, nthreads=nthreads)
+    res = orc.singlepoint_batch([mols[i] for i in sample], nthreads=nthreads)
     dt = time.perf_counter() - t
     return {"value": count / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
-            "sample": f"first {count} of the {len(mols)} water clusters, one structure per thread, {dt:.1f} s"}, res, count
+            "sample": f"first {count} of the {len(mols)} structures of the workload, largest first, one "
+                      f"structure per thread, {dt:.1f} s; oracle {build}"}, res, sample
 
 
 def time_form(capi, torch, calc, mols, args, stream, precision):
@@ -263,6 +291,8 @@ def main():
         return run_water_box(args, torch)
     if args.workload == "serving":
         return run_serving(args, torch)
+    if args.workload == "alkanes_256":
+        return run_alkanes(args, torch)
     if ws > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
@@ -345,11 +375,18 @@ def main():
     kernels = {k: {"launches": v[0], "ms": round(v[1], 3), "share": round(v[1] / total_ms, 4)}
                for k, v in sorted(prof_tot.items(), key=lambda kv: -kv[1][1])}
 
-    # ---------------- serving latency (bounded sample of the request stream), headline form
+    # ---------------- serving latency (bounded sample of the request stream), both forms
     serving = None
     if rank == 0 and args.serving_requests > 0:
         free, _ = torch.cuda.mem_get_info()
-        serving = serving_run(capi, calc, args.serving_requests, args.serving_rate, head_prec, int(0.5 * free))
+        serving = {}
+        for sname, sprec in (("fp64", 0), ("mixed", 1)):
+            serving_run(capi, calc, min(32, args.serving_requests), args.serving_rate, sprec, int(0.5 * free))
+            serving[sname] = serving_run(capi, calc, args.serving_requests, args.serving_rate, sprec,
+                                         int(0.5 * free))
+
+    # ---------------- the plain form one structure per call (no batching), for the batching gain
+    one = one_per_call(calc, mols, torch, sh) if rank == 0 else None
 
     res = head["res"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -370,17 +407,21 @@ def main():
             "mixed_vs_fp64": forms["mixed"]["value"] / forms["fp64"]["value"]}
     if serving is not None:
         line["serving"] = serving
+    if one is not None:
+        line["forms"]["fp64_one_structure_per_call"] = one
+        line["batched_vs_one_per_call"] = value / one["value"]
     iters = [r["iterations"] for r in res]
     line["scf_iterations"] = {"mean": float(np.mean(iters)), "max": int(max(iters))}
     line["status_ok"] = int(sum(r["status"] == 0 for r in res))
 
     if rank == 0 and not args.no_cpu_baseline:
         nthreads = os.cpu_count() or 1
-        cb, ores, count = cpu_baseline(mols, nthreads)
+        orc, build = oracle_for_timing()
+        cb, ores, sample = cpu_baseline(orc, build, mols, nthreads)
         line["cpu_baseline"] = cb
-        de = [abs(r["energy"] - o["energy"]) for r, o in zip(res[:count], ores)]
+        de = [abs(res[i]["energy"] - o["energy"]) for i, o in zip(sample, ores)]
         line["max_abs_dE_vs_oracle"] = max(de)
-        line["structures_checked_vs_oracle"] = count
+        line["structures_checked_vs_oracle"] = len(sample)
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -390,6 +431,79 @@ def main():
 
 def launches_of(forms, name):
     return int(forms[name]["launches"])
+
+
+def one_per_call(calc, mols, torch, sh, count=48):
+    """The plain FP64 form without batching: tb_singlepoint_batch called once per
+    structure on an evenly spaced sample of the workload (host buffers)."""
+    sample = [mols[int(i)] for i in range(0, len(mols), max(1, len(mols) // count))][:count]
+    for m in sample[:4]:
+        calc.singlepoint_batch([m], stream=sh, precision=0)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for m in sample:
+        calc.singlepoint_batch([m], stream=sh, precision=0)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t
+    return {"value": len(sample) / dt, "unit": UNIT, "structures": len(sample),
+            "sample": "evenly spaced structures of the batch, one tb_singlepoint_batch call each"}
+
+
+def run_alkanes(args, torch):
+    """The 256-alkane workload (C20-C199, 62-599 atoms, 122-1196 AOs): both forms
+    timed as for the water clusters; per-structure |dE|, max |dq| and |dmu| of the
+    mixed form against the FP64 form on every structure, and the energies of both
+    forms against the FP64 oracle on the smallest structures (a bounded CPU sample)."""
+    import numpy as np
+    from tblite_b200 import Calculator, capi, geometry
+    calc = Calculator()
+    mols = geometry.alkanes(256, seed=1002)
+    stream = torch.cuda.Stream()
+    sampler = ClockSampler(0)
+    sampler.start()
+    forms = {name: time_form(capi, torch, calc, mols, args, stream, prec)
+             for name, prec in (("fp64", 0), ("mixed", 1))}
+    clocks = sampler.stop()
+    for f in forms.values():
+        f["value"] = len(mols) * args.steps / f["elapsed"]
+        f["ms_per_step"] = f["elapsed"] / args.steps * 1e3
+
+    def errs(a, b):
+        return {"dE": [abs(x["energy"] - y["energy"]) for x, y in zip(a, b)],
+                "dq": [float(np.max(np.abs(np.asarray(x["qat"]) - np.asarray(y["qat"])))) for x, y in zip(a, b)],
+                "dmu": [float(np.max(np.abs(np.asarray(x["dipole"]) - np.asarray(y["dipole"]))))
+                        for x, y in zip(a, b)]}
+
+    fp, mx = forms["fp64"]["res"], forms["mixed"]["res"]
+    e = errs(mx, fp)
+    line = {"metric": METRIC, "value": max(f["value"] for f in forms.values()), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic", "clocks": clocks,
+            "config": {"workload": "alkanes_256", "structures": len(mols), "n": "U{20..200} (drawn 20-199)",
+                       "seed": 1002, "aos": "122-1196", "accuracy": 1.0},
+            "forms": {k: {"value": f["value"], "ms_per_step": f["ms_per_step"],
+                          "status_ok": int(sum(r["status"] == 0 for r in f["res"])),
+                          "scf_iterations_mean": float(np.mean([r["iterations"] for r in f["res"]]))}
+                      for k, f in forms.items()},
+            "mixed_vs_fp64": forms["mixed"]["value"] / forms["fp64"]["value"],
+            "mixed_vs_fp64_errors": {k: {"max": float(np.max(v)), "median": float(np.median(v))}
+                                     for k, v in e.items()},
+            "mixed_vs_fp64_errors_per_structure": e}
+    if not args.no_cpu_baseline:
+        nthreads = os.cpu_count() or 1
+        orc, build = oracle_for_timing()
+        small = sorted(range(len(mols)), key=lambda i: mols[i].nat)[:2 * nthreads]
+        t = time.perf_counter()
+        ores = orc.singlepoint_batch([mols[i] for i in small[::-1]], nthreads=nthreads)[::-1]
+        dt = time.perf_counter() - t
+        line["vs_oracle"] = {
+            "structures": len(small), "oracle": build,
+            "aos": f"{calc.basis_size(mols[small[0]])[1]}-{calc.basis_size(mols[small[-1]])[1]}",
+            "fp64_dE_max": max(abs(fp[i]["energy"] - o["energy"]) for i, o in zip(small, ores)),
+            "mixed_dE_max": max(abs(mx[i]["energy"] - o["energy"]) for i, o in zip(small, ores))}
+        line["cpu_baseline"] = {"value": len(small) / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
+                                "sample": f"the {len(small)} smallest alkanes, one structure per thread, {dt:.1f} s"}
+    print(json.dumps(line))
 
 
 def run_serving(args, torch):
@@ -460,19 +574,20 @@ def run_reference(args, ws, rank):
     if rank != 0:
         return
     from tblite_b200 import geometry
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle
-    orc = pyoracle.Oracle(os.path.join(ROOT, "tblite-cuda_b200", "params", "synthetic_hco.tbp"))
+    orc, build = oracle_for_timing()
     mols = geometry.water_clusters(args.count, seed=1001)
     nthreads = os.cpu_count() or 1
-    per_step = min(len(mols), 2 * nthreads)
+    # each timed step: 8 structures per thread of the workload, consecutive
+    # through the batch and run largest first, so that no thread idles while
+    # another finishes a large cluster (the whole run stays within minutes)
+    per_step = min(len(mols), 8 * nthreads)
     for w in range(args.warmup):
-        orc.singlepoint_batch(mols[:nthreads], nthreads=nthreads)
+        orc.singlepoint_batch([mols[i] for i in lpt_sample(mols, w * nthreads, nthreads)], nthreads=nthreads)
     t = time.perf_counter()
     done = 0
     for s in range(args.steps):
-        sample = mols[(s * per_step) % len(mols):][:per_step]
-        orc.singlepoint_batch(sample, nthreads=nthreads)
+        sample = lpt_sample(mols, s * per_step, per_step)
+        orc.singlepoint_batch([mols[i] for i in sample], nthreads=nthreads)
         done += len(sample)
     dt = time.perf_counter() - t
     value = done / dt
@@ -481,7 +596,8 @@ def run_reference(args, ws, rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "structures_per_step": per_step, "waters": "U{8..64}", "seed": 1001},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
-                             "sample": f"{per_step} water clusters per step, one structure per thread"},
+                             "sample": f"{per_step} consecutive water clusters per step ({args.steps} steps), "
+                                       f"largest first, one structure per thread; oracle {build}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference (tornikeo/tblite-cuda) does not compile or converge; this times its FP64 CPU "
                     "restatement (oracle/) on the same workload"}

@@ -40,6 +40,15 @@ def _i(a):
 _lib = None
 
 
+def use_library(path: str):
+    """Load the oracle from another build of the same source (e.g. the
+    -march=native one the CPU baseline times); call before the first use."""
+    global LIB
+    if _lib is not None:
+        raise RuntimeError("oracle library already loaded")
+    LIB = path
+
+
 def lib():
     global _lib
     if _lib is None:
