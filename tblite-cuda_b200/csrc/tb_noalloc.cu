@@ -17,9 +17,12 @@
 //    contents; each call rewrites everything it reads before reading it.
 //    Calls whose GPU work overlaps (different streams, different host threads
 //    without ordering) race on the array: serialise them.
-//  * The first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress, cached per device); make that first call before
-//    any stream capture begins.
+//  * The first call on a device does its set-up: it raises the eigensolver
+//    kernel's dynamic shared memory limit to what n = 256 needs (above the
+//    48 KiB default from n = 237 on; setting a kernel attribute allocates
+//    nothing) and looks up the array's device address (cudaGetSymbolAddress,
+//    cached per device).  Make that first call before any stream capture
+//    begins.
 //  * The call is synchronous: it waits for its stream to read the status.
 #include <cuda_runtime.h>
 
@@ -114,11 +117,20 @@ extern "C" tb_status tb_sygvd_noalloc(int32_t n, const double* H, const double* 
   {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_addr[dev]) {
-      e = cudaGetSymbolAddress(reinterpret_cast<void**>(&g_noalloc_addr[dev]), g_noalloc_scratch);
-      if (e != cudaSuccess) {
-        g_noalloc_addr[dev] = nullptr;
-        return noalloc_fail(TB_CUDA_ERROR, cudaGetErrorString(e));
-      }
+      // per-device set-up, with this device current: the eigensolver's shared
+      // memory opt-in for the largest accepted n (raised only: the batched
+      // paths may already have set a higher limit), then the scratch address
+      // (cached last, so that a failed set-up is retried by the next call)
+      cudaFuncAttributes fa;
+      e = cudaFuncGetAttributes(&fa, (const void*)k_syev);
+      const int need = (int)syev_smem_bytes(kNoAllocMaxN);
+      if (e == cudaSuccess && fa.maxDynamicSharedSizeBytes < need)
+        e = cudaFuncSetAttribute((const void*)k_syev, cudaFuncAttributeMaxDynamicSharedMemorySize, need);
+      if (e != cudaSuccess) return noalloc_fail(TB_CUDA_ERROR, cudaGetErrorString(e));
+      double* addr = nullptr;
+      e = cudaGetSymbolAddress(reinterpret_cast<void**>(&addr), g_noalloc_scratch);
+      if (e != cudaSuccess) return noalloc_fail(TB_CUDA_ERROR, cudaGetErrorString(e));
+      g_noalloc_addr[dev] = addr;
     }
     base = g_noalloc_addr[dev];
   }
