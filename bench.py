@@ -5,8 +5,8 @@ Workload (default): 1024 water clusters of U{8..64} rigid waters (24-192 atoms,
 48-384 AOs), seeded synthetic inputs built by the cluster rules (no dataset).
 One step = the full singlepoint (setup + SCF to convergence) of the whole
 batch.  Both forms are timed (tb_options.precision 0 and 1) with the geometry
-already resident on the device and one captured SCF iteration replayed as a
-CUDA graph; `value` is the faster form whose energies agree with the FP64 form
+already resident on the device and the whole SCF loop launched as one CUDA graph
+(a conditional WHILE node over one captured iteration); `value` is the faster form whose energies agree with the FP64 form
 to 1e-6 Eh (config.form names it, `forms` lists both).  `e2e` times the public
 tb_singlepoint_batch of that form with host buffers (the upload of the inputs
 and the download of every result inside the timed region).  The working set
@@ -396,7 +396,8 @@ def main():
             "config": {"workload": WORKLOAD, "form": head_name, "structures_per_gpu": len(mols),
                        "waters": "U{8..64}", "atoms": nat, "aos": nao, "seed": 1001,
                        "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (no flush needed)",
-                       "accuracy": 1.0, "graphs": "one captured SCF iteration replayed"},
+                       "accuracy": 1.0,
+                       "graphs": "whole SCF loop as one graph launch (conditional WHILE node)"},
             "e2e": e2e, "gpu_launches": launches_of(forms, head_name), "roofline": roof, "kernels": kernels,
             "clocks": clocks,
             "forms": {k: {"value": f["value"], "ms_per_step": f["ms_per_step"],

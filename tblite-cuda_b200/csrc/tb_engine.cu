@@ -308,7 +308,9 @@ struct tb_batch {
   DevParams Pc{};
   int it = 0;
   cudaStream_t cap = nullptr;       // capture stream of the iteration graph
-  cudaGraphExec_t gexec = nullptr;  // one SCF iteration (tb_options.use_graphs)
+  cudaGraphExec_t gexec = nullptr;  // one SCF iteration (tb_options.use_graphs, serving)
+  cudaGraphExec_t gloop = nullptr;  // the whole SCF loop as a conditional WHILE node (use_graphs)
+  int* it_dev = nullptr;            // SCF iterations run by the loop graph
   int64_t launches_per_iter = 0;
   int64_t launches = 0;
   size_t bytes = 0;
@@ -326,6 +328,7 @@ struct tb_batch {
   size_t evused = 0;
   ~tb_batch() {
     if (gexec) cudaGraphExecDestroy(gexec);
+    if (gloop) cudaGraphExecDestroy(gloop);
     if (cap) cudaStreamDestroy(cap);
     if (h_nactive && !(calc && calc->give_pin_slot(h_nactive))) cudaFreeHost(h_nactive);
     for (cudaEvent_t e : evpool) cudaEventDestroy(e);
@@ -570,7 +573,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
          o_ms_status = L.add(NM * I4), o_ms_ets = L.add(NM * D8), o_ms_eband = L.add(NM * D8),
          o_ms_ees2 = L.add(NM * D8), o_ms_eaes2 = L.add(NM * D8), o_ms_ees3 = L.add(NM * D8),
          o_ms_err = L.add(NM * D8), o_ms_fw = L.add(NM * I4), o_ms_dip = L.add(3 * NM * D8),
-         o_ms_nact = L.add(I4);
+         o_ms_nact = L.add(I4), o_itdev = L.add(I4);
   size_t o_guess = L.add(MX * D8), o_gflag = L.add(NM * I4);
   size_t o_lwork = L.add(std::max<size_t>(b->lib_bytes, 16)), o_linfo = L.add((2 * b->big.size() + 2) * I4);
   // mixed-precision form: FP32 eigensolver input/output, refinement buffers, phase state
@@ -687,6 +690,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   s.e_es2 = at<double>(base, o_ms_ees2); s.e_aes2 = at<double>(base, o_ms_eaes2);
   s.e_es3 = at<double>(base, o_ms_ees3); s.scf_error = at<double>(base, o_ms_err);
   s.fermi_warn = at<int>(base, o_ms_fw); s.dipole = at<double>(base, o_ms_dip); s.n_active = at<int>(base, o_ms_nact);
+  b->it_dev = at<int>(base, o_itdev);
   s.phase = b->mixed ? at<int>(base, o_phase) : nullptr;
   s.n64 = b->mixed ? at<int>(base, o_n64) : nullptr;
   if (!b->h_nactive) b->h_nactive = calc->take_pin_slot();
@@ -1190,9 +1194,66 @@ tb_status batch_iterate(tb_batch* b, cudaStream_t st, int* n_active) {
   return finish_iteration(b, st, n_active);
 }
 
+// The whole SCF loop as one graph launch: a conditional WHILE node whose body
+// is one captured iteration (iterate_body) followed by k_loop_control, which
+// counts the iteration on the device and sets the loop condition to "some
+// structure still iterating and fewer than max_iter iterations", the same
+// test the host loop of batch_run makes after each iteration.  No host
+// synchronisation inside the loop; one read of the iteration count after it.
+tb_status run_loop_graph(tb_batch* b, cudaStream_t st) {
+  if (!b->gloop) {
+    if (!b->cap) TB_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    TB_CUDA(cudaGraphCreate(&g, 0));
+    auto fail_graph = [&](cudaError_t e) {
+      cudaGraphDestroy(g);
+      return fail(TB_CUDA_ERROR, std::string("SCF loop graph: ") + cudaGetErrorString(e));
+    };
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return fail_graph(e);
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+    if (e != cudaSuccess) return fail_graph(e);
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(b->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return fail_graph(e);
+    const int64_t l0 = b->launches;
+    tb_status bs = iterate_body(b, b->cap);
+    if (bs == TB_OK) {
+      k_loop_control<<<1, 1, 0, b->cap>>>(h, b->ms.n_active, b->it_dev, b->opt.max_iter);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) ++b->launches;
+    }
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(b->cap, &captured);
+    if (bs != TB_OK) { cudaGraphDestroy(g); return bs; }
+    if (e != cudaSuccess) return fail_graph(e);
+    if (ce != cudaSuccess) return fail_graph(ce);
+    e = cudaGraphInstantiate(&b->gloop, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { b->gloop = nullptr; return fail(TB_CUDA_ERROR, std::string("SCF loop graph: ") + cudaGetErrorString(e)); }
+    b->launches_per_iter = b->launches - l0;
+    b->launches = l0;
+  }
+  TB_CUDA(cudaMemsetAsync(b->it_dev, 0, sizeof(int), st));
+  TB_CUDA(cudaGraphLaunch(b->gloop, st));
+  TB_CUDA(cudaMemcpyAsync(b->h_nactive, b->it_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+  TB_CUDA(cudaStreamSynchronize(st));
+  b->it = *b->h_nactive;
+  b->launches += b->launches_per_iter * b->it;
+  return TB_OK;
+}
+
 tb_status batch_run(tb_batch* b, cudaStream_t st) {
   tb_status s = batch_setup(b, st);
   if (s != TB_OK) return s;
+  if (b->opt.use_graphs && !b->opt.profile && b->big.empty()) return run_loop_graph(b, st);
   for (int it = 0; it < b->opt.max_iter; ++it) {
     int na = 0;
     s = batch_iterate(b, st, &na);

@@ -137,6 +137,8 @@ __global__ void k_oa_step(DevBatch B, double* G, double* Sm, double* V, double* 
 // SCF
 __global__ void k_scf_init(DevParams P, DevBatch B, const double* charge, const int* uhf, const double* erep,
                            double* n0sh, double* q_in, MolState S);
+// end of one iteration of the SCF loop graph: counts it and sets the loop condition
+__global__ void k_loop_control(cudaGraphConditionalHandle h, const int* n_active, int* it, int max_iter);
 // caller's starting moments (wavefunction guess) into q_in for flagged structures
 __global__ void k_apply_guess(DevBatch B, const double* guess, const int* flag, double* q_in);
 // pair tables of the fixed geometry (gtab: gamma per shell pair, atab: 1/r, f3, f5 per atom pair)

@@ -86,6 +86,17 @@ __global__ void k_scf_init(DevParams P, DevBatch B, const double* __restrict__ c
   }
 }
 
+// Last node of the body of the SCF loop graph (one graph launch runs the whole
+// loop): counts the iteration and keeps the WHILE node looping while a
+// structure is still active and the iteration budget is not spent (the
+// convergence test itself is made per structure by k_finalize).
+__global__ void k_loop_control(cudaGraphConditionalHandle h, const int* __restrict__ n_active, int* __restrict__ it,
+                               int max_iter) {
+  const int done = *it + 1;
+  *it = done;
+  cudaGraphSetConditional(h, (*n_active > 0 && done < max_iter) ? 1u : 0u);
+}
+
 // Starting point of the SCF taken from the caller's wavefunction (the
 // reference's xtb_singlepoint takes wfn in and out, src/xtb.cu:188-197, and
 // its first iteration builds the potential from the charges it holds): the

@@ -280,14 +280,28 @@ def test_device_batch_api(gpu_calc, oracle):
 
 @pytest.mark.parametrize("precision", [0, 1])
 def test_graph_replay_equals_eager(gpu_calc, precision):
-    # use_graphs captures one SCF iteration per batch and replays it
+    # use_graphs runs the whole SCF loop as one graph launch (a conditional
+    # WHILE node over one captured iteration plus the loop-control kernel)
     mols = g.water_clusters(6, seed=13, nmin=2, nmax=20)
     eager = capi.Batch(gpu_calc, mols, precision=precision)
     eager.run()
     graph = capi.Batch(gpu_calc, mols, precision=precision, use_graphs=1)
     graph.run()
     graph.run()  # second run replays the instantiated graph
-    assert graph.launches() == eager.launches()
-    for a, b in zip(eager.results(), graph.results()):
+    res = graph.results()
+    iters = max(r["iterations"] for r in res)
+    assert graph.launches() == eager.launches() + iters  # one loop-control kernel per iteration
+    for a, b in zip(eager.results(), res):
         assert a["energy"] == b["energy"] and a["iterations"] == b["iterations"]
         np.testing.assert_array_equal(a["qat"], b["qat"])
+
+
+def test_graph_loop_stops_at_max_iter(gpu_calc):
+    m = g.octane()
+    r = gpu_calc.singlepoint_batch([m], max_iter=2, use_graphs=1)[0]
+    assert r["status"] == capi.TB_SCF_NOT_CONVERGED and r["iterations"] == 2
+    b = capi.Batch(gpu_calc, [m], max_iter=2, use_graphs=1)
+    b.run()
+    e = capi.Batch(gpu_calc, [m], max_iter=2)
+    e.run()
+    assert b.launches() == e.launches() + 2
