@@ -264,7 +264,7 @@ struct tb_batch {
   Arena* arena = nullptr;
   std::vector<int> h_aoff, h_soff, h_ooff, h_mixoff;
   std::vector<long long> h_moff, h_poff, h_s2off, h_a2off;
-  std::vector<int4> tiles64, tiles32, tiles128;
+  std::vector<int4> tiles64, tiles32, tiles128;  // tiles32: upper 32x32 tiles (t <= u), Fock build
   std::vector<int2> chunks32;
   std::vector<double> h_xyz;
   // device views
@@ -287,6 +287,9 @@ struct tb_batch {
   bool any_guess = false;
   double* d_guess = nullptr;
   int* d_guess_flag = nullptr;
+  // nspin = 2 read-out: per-channel occupations (3 x nao_tot) and structure flags
+  double* d_fspin = nullptr;
+  int* d_wflag = nullptr;
   int4 *d_tiles64, *d_tiles32, *d_tiles128;
   int2* d_chunks32;
   int* h_nactive = nullptr;  // pinned
@@ -433,7 +436,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
     const long long a64 = (nao + 63) / 64, a128 = (nao + kTcTile - 1) / kTcTile, a32 = (nao + 31) / 32;
     t64o[m + 1] = t64o[m] + a64 * a64;
     t128o[m + 1] = t128o[m] + a128 * a128;
-    t32o[m + 1] = t32o[m] + a32 * a32;
+    t32o[m + 1] = t32o[m] + a32 * (a32 + 1) / 2;
     c32o[m + 1] = c32o[m] + a32;
   }
   {
@@ -475,7 +478,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
       for (int u = 0; u < (nao + kTcTile - 1) / kTcTile; ++u) b->tiles128[i128++] = make_int4(m, t, u, 0);
     for (int t = 0; t < (nao + 31) / 32; ++t) {
       b->chunks32[ic++] = make_int2(m, t);
-      for (int u = 0; u < (nao + 31) / 32; ++u) b->tiles32[i32++] = make_int4(m, t, u, 0);
+      for (int u = t; u < (nao + 31) / 32; ++u) b->tiles32[i32++] = make_int4(m, t, u, 0);
     }
   };
   {
@@ -574,7 +577,8 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
          o_ms_ees2 = L.add(NM * D8), o_ms_eaes2 = L.add(NM * D8), o_ms_ees3 = L.add(NM * D8),
          o_ms_err = L.add(NM * D8), o_ms_fw = L.add(NM * I4), o_ms_dip = L.add(3 * NM * D8),
          o_ms_nact = L.add(I4), o_itdev = L.add(I4);
-  size_t o_guess = L.add(MX * D8), o_gflag = L.add(NM * I4);
+  size_t o_guess = L.add(MX * D8), o_gflag = L.add(NM * I4), o_fspin = L.add(3 * NO * D8),
+         o_wflag = L.add(NM * I4);
   size_t o_lwork = L.add(std::max<size_t>(b->lib_bytes, 16)), o_linfo = L.add((2 * b->big.size() + 2) * I4);
   // mixed-precision form: FP32 eigensolver input/output, refinement buffers, phase state
   const long long MXN2 = b->mixed ? N2 : 0, MXNO = b->mixed ? NO : 0, MXNM = b->mixed ? NM : 0;
@@ -664,6 +668,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   b->d_tiles64 = at<int4>(base, o_t64); b->d_tiles128 = at<int4>(base, o_t128); b->d_tiles32 = at<int4>(base, o_t32); b->d_chunks32 = at<int2>(base, o_c32);
   b->charge = at<double>(base, o_charge); b->uhf = at<int>(base, o_uhf);
   b->d_guess = at<double>(base, o_guess); b->d_guess_flag = at<int>(base, o_gflag);
+  b->d_fspin = at<double>(base, o_fspin); b->d_wflag = at<int>(base, o_wflag);
   b->h_guess.clear();
   b->h_guess_flag.clear();
   b->any_guess = false;
@@ -857,7 +862,7 @@ tb_status raise_smem_limits() {
   TB_CUDA(cudaGetDevice(&dev));
   TB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   const void* ks[] = {(const void*)k_syev, (const void*)k_syev_f32, (const void*)k_fermi, (const void*)k_oa_step,
-                      (const void*)k_gemm_tc};
+                      (const void*)k_gemm_tc, (const void*)k_fock};
   for (const void* k : ks) {
     cudaFuncAttributes a;
     TB_CUDA(cudaFuncGetAttributes(&a, k));
@@ -1094,7 +1099,7 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
                                              b->gtab, b->atab));
   // Fock build: reads S, H0, D(3), Q(6), writes F -> 12 N^2 doubles
   TB_K("fock", 96.0 * n2, 2,
-       k_fock<<<ntile32, 256, 0, st>>>(B, b->d_tiles32, ntile32, b->S, b->H0, b->D, b->Q, b->vsh, b->vat, b->vdp,
+       k_fock<<<ntile32, 256, fock_smem_bytes(), st>>>(B, b->d_tiles32, ntile32, b->S, b->H0, b->D, b->Q, b->vsh, b->vat, b->vdp,
                                        b->vqp, b->F, S.active));
   if (!b->mixed) {
     // F' = X^T F X  (T = F X in W, then F' into F): 2 x 2N^3
@@ -1354,9 +1359,59 @@ tb_status batch_set_guess(tb_batch* b, const tb_wavefunction* wfn) {
 // W holds C = X Z of the structure's last iteration (the density GEMM reads
 // it; nothing later overwrites it), P its density, w and focc its orbital
 // energies (ascending) and occupations.
+// Records with nspin = 2 get tblite's open-shell representation: both spin
+// channels share the orbital energies and coefficients (GFN2 has no
+// spin-dependent potential); per channel the Fermi filling of its electrons
+// (k_spin_occupations), the densities P_alpha = C f_a C^T and P_beta = C f_b
+// C^T (into X and F, free after a run: the next run's setup rewrites them),
+// and the moments as (total, up - down), the latter from the Mulliken sums of
+// P_alpha - P_beta = C (f_a - f_b) C^T (into Z; k_spin_moments, into the
+// potential buffers, also free after a run).
+tb_status spin_readout(tb_batch* b, const std::vector<int>& flag, cudaStream_t st) {
+  const DevBatch& B = b->db;
+  const int nmol = b->nmol, nt = (int)b->tiles64.size(), nchunk = (int)b->chunks32.size();
+  const int gemm_grid = std::min(nt, 148 * 8);
+  const long long NO = b->nao_tot;
+  TB_CUDA(cudaMemcpyAsync(b->d_wflag, flag.data(), nmol * sizeof(int), cudaMemcpyHostToDevice, st));
+  k_spin_occupations<<<nmol, 128, (size_t)b->nmax * sizeof(double), st>>>(B, b->w, b->opt.kt, b->ms.nel, b->d_wflag,
+                                                                          b->d_fspin);
+  TB_LAUNCH_CHECK();
+  double* out[3] = {b->X, b->F, b->Z};  // P_alpha, P_beta, P_alpha - P_beta
+  for (int c = 0; c < 3; ++c) {
+    k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, nt, b->W, 0, b->W, 1, nullptr, b->d_fspin + c * NO,
+                                               b->kdim, out[c], 1.0, 0.0, b->d_wflag, kGemmSym);
+    TB_LAUNCH_CHECK();
+  }
+  k_mulliken_cols<<<nchunk, 256, 0, st>>>(B, b->d_chunks32, nchunk, b->Z, b->S, b->H0, b->D, b->Q, b->colred,
+                                          b->d_wflag);
+  TB_LAUNCH_CHECK();
+  k_spin_moments<<<nmol, 256, 0, st>>>(b->Pc, B, b->colred, b->d_wflag, b->vsh, b->vat, b->vdp, b->vqp);
+  TB_LAUNCH_CHECK();
+  return TB_OK;
+}
+
 tb_status batch_wavefunction(tb_batch* b, tb_wavefunction* wfn, cudaStream_t st) {
   const int nmol = b->nmol;
   const int NA = b->nat_tot, NS = b->nsh_tot, NO = b->nao_tot;
+  std::vector<int> spin2(nmol, 0);
+  bool any2 = false;
+  for (int m = 0; m < nmol; ++m) {
+    if (wfn[m].nspin != 0 && wfn[m].nspin != 1 && wfn[m].nspin != 2)
+      return fail(TB_BAD_INPUT, "wavefunction " + std::to_string(m) + ": nspin must be 1 or 2");
+    spin2[m] = wfn[m].nspin == 2;
+    any2 |= spin2[m] != 0;
+  }
+  std::vector<double> fsp, msh, mat, mdp, mqp;
+  if (any2) {
+    const tb_status ss = spin_readout(b, spin2, st);
+    if (ss != TB_OK) return ss;
+    fsp.resize(3 * (size_t)NO); msh.resize(NS); mat.resize(NA); mdp.resize(3 * (size_t)NA); mqp.resize(6 * (size_t)NA);
+    TB_CUDA(cudaMemcpyAsync(fsp.data(), b->d_fspin, 2 * (size_t)NO * 8, cudaMemcpyDeviceToHost, st));
+    TB_CUDA(cudaMemcpyAsync(msh.data(), b->vsh, NS * 8, cudaMemcpyDeviceToHost, st));
+    TB_CUDA(cudaMemcpyAsync(mat.data(), b->vat, NA * 8, cudaMemcpyDeviceToHost, st));
+    TB_CUDA(cudaMemcpyAsync(mdp.data(), b->vdp, 3 * (size_t)NA * 8, cudaMemcpyDeviceToHost, st));
+    TB_CUDA(cudaMemcpyAsync(mqp.data(), b->vqp, 6 * (size_t)NA * 8, cudaMemcpyDeviceToHost, st));
+  }
   std::vector<double> emo(NO), focc(NO), n0sh(NS), nel(2 * (size_t)nmol), qat(NA), qsh(NS), dp(3 * (size_t)NA),
       qp(6 * (size_t)NA);
   auto cp = [&](void* dst, const void* src, size_t n) { return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, st); };
@@ -1370,16 +1425,27 @@ tb_status batch_wavefunction(tb_batch* b, tb_wavefunction* wfn, cudaStream_t st)
   TB_CUDA(cp(qp.data(), b->qpat_out, 6 * (size_t)NA * 8));
   for (int m = 0; m < nmol; ++m) {
     tb_wavefunction& w = wfn[m];
-    const long long nn = b->h_moff[m + 1] - b->h_moff[m];
-    if (w.density) TB_CUDA(cp(w.density, b->P + b->h_moff[m], nn * 8));
-    if (w.coeff) TB_CUDA(cp(w.coeff, b->W + b->h_moff[m], nn * 8));
+    const long long mo = b->h_moff[m], nn = b->h_moff[m + 1] - mo;
+    if (spin2[m]) {  // [2][nao][nao]: alpha, beta
+      if (w.density) {
+        TB_CUDA(cp(w.density, b->X + mo, nn * 8));
+        TB_CUDA(cp(w.density + nn, b->F + mo, nn * 8));
+      }
+      if (w.coeff) {
+        TB_CUDA(cp(w.coeff, b->W + mo, nn * 8));
+        TB_CUDA(cp(w.coeff + nn, b->W + mo, nn * 8));
+      }
+    } else {
+      if (w.density) TB_CUDA(cp(w.density, b->P + mo, nn * 8));
+      if (w.coeff) TB_CUDA(cp(w.coeff, b->W + mo, nn * 8));
+    }
   }
   TB_CUDA(cudaStreamSynchronize(st));
   const HostParams& P = b->calc->hp;
   for (int m = 0; m < nmol; ++m) {
     tb_wavefunction& w = wfn[m];
     const int a0 = b->h_aoff[m], s0 = b->h_soff[m], o0 = b->h_ooff[m];
-    w.nspin = 1;
+    w.nspin = spin2[m] ? 2 : 1;
     w.nat = b->h_aoff[m + 1] - a0;
     w.nsh = b->h_soff[m + 1] - s0;
     w.nao = b->h_ooff[m + 1] - o0;
@@ -1390,7 +1456,12 @@ tb_status batch_wavefunction(tb_batch* b, tb_wavefunction* wfn, cudaStream_t st)
     w.nuhf = w.nel[0] - w.nel[1];
     for (int s = 0; s < 2; ++s) w.homo[s] = (int32_t)std::floor(w.nel[s]);
     if (w.emo) std::memcpy(w.emo, emo.data() + o0, w.nao * 8);
-    if (w.focc) std::memcpy(w.focc, focc.data() + o0, w.nao * 8);
+    if (w.emo && spin2[m]) std::memcpy(w.emo + w.nao, emo.data() + o0, w.nao * 8);
+    if (w.focc && !spin2[m]) std::memcpy(w.focc, focc.data() + o0, w.nao * 8);
+    if (w.focc && spin2[m]) {
+      std::memcpy(w.focc, fsp.data() + o0, w.nao * 8);
+      std::memcpy(w.focc + w.nao, fsp.data() + NO + o0, w.nao * 8);
+    }
     if (w.n0sh) std::memcpy(w.n0sh, n0sh.data() + s0, w.nsh * 8);
     if (w.n0at) {  // the shells of an atom are consecutive
       int s = s0;
@@ -1405,6 +1476,12 @@ tb_status batch_wavefunction(tb_batch* b, tb_wavefunction* wfn, cudaStream_t st)
     if (w.qsh) std::memcpy(w.qsh, qsh.data() + s0, w.nsh * 8);
     if (w.dpat) std::memcpy(w.dpat, dp.data() + 3 * (size_t)a0, 3 * (size_t)w.nat * 8);
     if (w.qpat) std::memcpy(w.qpat, qp.data() + 6 * (size_t)a0, 6 * (size_t)w.nat * 8);
+    if (spin2[m]) {  // channel 1: up - down
+      if (w.qat) std::memcpy(w.qat + w.nat, mat.data() + a0, w.nat * 8);
+      if (w.qsh) std::memcpy(w.qsh + w.nsh, msh.data() + s0, w.nsh * 8);
+      if (w.dpat) std::memcpy(w.dpat + 3 * w.nat, mdp.data() + 3 * (size_t)a0, 3 * (size_t)w.nat * 8);
+      if (w.qpat) std::memcpy(w.qpat + 6 * w.nat, mqp.data() + 6 * (size_t)a0, 6 * (size_t)w.nat * 8);
+    }
   }
   return TB_OK;
 }
@@ -1733,8 +1810,12 @@ tb_status tb_add_pot_to_h1(const tb_calculator* calc, const tb_structure* mol, c
   TB_CUDA(cudaMemcpy(b->vqp, vqp, 6 * nat * 8, cudaMemcpyHostToDevice));
   const int one = 1;
   TB_CUDA(cudaMemcpy(b->ms.active, &one, sizeof(int), cudaMemcpyHostToDevice));
+  {
+    const tb_status ss = raise_smem_limits();
+    if (ss != TB_OK) return ss;
+  }
   const int nt = (int)b->tiles32.size();
-  k_fock<<<nt, 256>>>(b->db, b->d_tiles32, nt, b->S, b->H0, b->D, b->Q, b->vsh, b->vat, b->vdp, b->vqp, b->F,
+  k_fock<<<nt, 256, fock_smem_bytes()>>>(b->db, b->d_tiles32, nt, b->S, b->H0, b->D, b->Q, b->vsh, b->vat, b->vdp, b->vqp, b->F,
                       b->ms.active);
   TB_LAUNCH_CHECK();
   return d2h(F, b->F, nn);

@@ -146,10 +146,18 @@ __global__ void k_pair_tables(DevParams P, DevBatch B, const double* mrad, doubl
 // gtab/atab may be null: the pair terms are then recomputed
 __global__ void k_potential(DevParams P, DevBatch B, const double* q_in, const double* mrad, double* vsh, double* vat,
                             double* vdp, double* vqp, const int* active, const double* gtab, const double* atab);
+// dynamic shared memory of k_fock (the nine staged transposed tiles)
+size_t fock_smem_bytes();
 __global__ void k_fock(DevBatch B, const int4* tiles, int ntiles, const double* S, const double* H0, const double* D,
                        const double* Q, const double* vsh, const double* vat, const double* vdp, const double* vqp,
                        double* F, const int* active);
 __global__ void k_fermi(DevBatch B, const double* w, double kt, double* focc, int* kdim, MolState S);
+// nspin = 2 read-out: per-channel occupations f[0] alpha, f[1] beta, f[2] alpha - beta (f: 3 x nao_tot)
+__global__ void k_spin_occupations(DevBatch B, const double* w, double kt, const double* nel, const int* flag,
+                                   double* f);
+// moments of the magnetization density from its Mulliken column sums (colred)
+__global__ void k_spin_moments(DevParams P, DevBatch B, const double* colred, const int* flag, double* qsh,
+                               double* qat, double* dpat, double* qpat);
 __global__ void k_mulliken_cols(DevBatch B, const int2* chunks, int nchunks, const double* P, const double* S,
                                 const double* H0, const double* D, const double* Q, double* colred,
                                 const int* active);

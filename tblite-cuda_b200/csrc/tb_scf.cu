@@ -234,19 +234,30 @@ __global__ void k_potential(DevParams P, DevBatch B, const double* __restrict__ 
 
 // ------------------------------------------------------------ Fock build
 // add_pot_to_h1 (src/scf/potential.cu:224-272 with the quoted add_vat_to_vsh,
-// add_vsh_to_vao, add_vao_to_h1 and add_vmp_to_h1): 32x32 tiles, the
-// transposed D/Q elements staged through shared memory.  F is symmetric (the
-// moment planes enter as M[mu][nu] v(nu) + M[nu][mu] v(mu)), so only tiles on
-// and above the diagonal are computed; an off-diagonal tile is also written
-// transposed (through the same shared tile), which halves the reads.
-__global__ void __launch_bounds__(256) k_fock(DevBatch B, const int4* __restrict__ tiles, int ntiles,
-                                              const double* __restrict__ S, const double* __restrict__ H0,
-                                              const double* __restrict__ D, const double* __restrict__ Q,
-                                              const double* __restrict__ vsh, const double* __restrict__ vat,
-                                              const double* __restrict__ vdp, const double* __restrict__ vqp,
-                                              double* __restrict__ F, const int* __restrict__ active) {
-  constexpr int kPl = 3;  // moment planes staged per round
-  __shared__ double T[kPl][32][33];
+// add_vsh_to_vao, add_vao_to_h1 and add_vmp_to_h1): 32x32 tiles.  F is
+// symmetric (the moment planes enter as M[mu][nu] v(nu) + M[nu][mu] v(mu)), so
+// the tile list holds only tiles on and above the diagonal; an off-diagonal
+// tile is also written transposed (through shared memory), which halves the
+// reads.  The kernel is bound by how many bytes are in flight: every CTA
+// issues all of its loads in one round -- the nine transposed moment tiles
+// (M[nu][mu]) as cp.async copies into shared memory (74 KiB, no registers
+// held), the nine direct tiles and S, H0 into registers -- and waits once.
+constexpr int kFockPitch = 33;  // padded rows: the transposed reads are conflict-free
+size_t fock_smem_bytes() { return (size_t)9 * 32 * kFockPitch * sizeof(double); }
+
+__device__ __forceinline__ void fock_cp_async8(double* smem, const double* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int nb = valid ? 8 : 0;  // bytes read; the rest of the 8 is zero-filled
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(nb) : "memory");
+}
+
+__global__ void __launch_bounds__(256, 2) k_fock(DevBatch B, const int4* __restrict__ tiles, int ntiles,
+                                                 const double* __restrict__ S, const double* __restrict__ H0,
+                                                 const double* __restrict__ D, const double* __restrict__ Q,
+                                                 const double* __restrict__ vsh, const double* __restrict__ vat,
+                                                 const double* __restrict__ vdp, const double* __restrict__ vqp,
+                                                 double* __restrict__ F, const int* __restrict__ active) {
+  extern __shared__ double fock_T[];  // [9][32][kFockPitch]: T[q][row][col] = M_q[c0 + row][r0 + col]
   const int t = blockIdx.x;
   if (t >= ntiles) return;
   const int4 tl = tiles[t];
@@ -257,63 +268,77 @@ __global__ void __launch_bounds__(256) k_fock(DevBatch B, const int4* __restrict
   const int o0 = B.ooff[m], a0 = B.aoff[m], s0 = B.soff[m];
   const int r0 = tl.y * 32, c0 = tl.z * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 rows of 32
-  double acc[4];
-  int mu[4];
-  const int nu = c0 + tx;
-  const bool nu_ok = nu < n;
-  const int at_nu = nu_ok ? B.ao_at[o0 + nu] : 0;
-  const double vao_nu = nu_ok ? vsh[s0 + B.ao_sh[o0 + nu]] + vat[a0 + at_nu] : 0.0;
-  for (int r = 0; r < 4; ++r) {
-    mu[r] = r0 + ty + 8 * r;
-    acc[r] = 0.0;
-    if (mu[r] < n && nu_ok) {
-      const int at_mu = B.ao_at[o0 + mu[r]];
-      const double vao_mu = vsh[s0 + B.ao_sh[o0 + mu[r]]] + vat[a0 + at_mu];
-      const long long e = mo + (long long)mu[r] * n + nu;
-      acc[r] = H0[e] - S[e] * 0.5 * (vao_mu + vao_nu);
-    }
-  }
-  // moment planes: -0.5 * (M[k][mu][nu] v[at(nu)][k] + M[k][nu][mu] v[at(mu)][k]),
-  // kPl planes per round (their transposed tiles staged together, their
-  // direct elements loaded together) so a round costs one load round trip
-  for (int pl0 = 0; pl0 < 9; pl0 += kPl) {
-    double dir[kPl][4];
-    __syncthreads();
+  // 1. the transposed tiles of the nine moment planes, asynchronously
 #pragma unroll
-    for (int q = 0; q < kPl; ++q) {
-      const int plane = pl0 + q;
-      const double* M = plane < 3 ? D + 3 * mo + plane * nn : Q + 6 * mo + (plane - 3) * nn;
+  for (int q = 0; q < 9; ++q) {
+    const double* M = q < 3 ? D + 3 * mo + q * nn : Q + 6 * mo + (q - 3) * nn;
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int row = c0 + ty + 8 * r, col = r0 + tx;
-        T[q][ty + 8 * r][tx] = (row < n && col < n) ? M[(long long)row * n + col] : 0.0;
-        dir[q][r] = (mu[r] < n && nu_ok) ? M[(long long)mu[r] * n + nu] : 0.0;
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < kPl; ++q) {
-      const int plane = pl0 + q;
-      const double* V = plane < 3 ? vdp : vqp;
-      const int stride = plane < 3 ? 3 : 6, k = plane < 3 ? plane : plane - 3;
-      const double vnu = nu_ok ? V[stride * (a0 + at_nu) + k] : 0.0;
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        if (mu[r] >= n || !nu_ok) continue;
-        const double vmu = V[stride * (a0 + B.ao_at[o0 + mu[r]]) + k];
-        acc[r] -= 0.5 * (dir[q][r] * vnu + T[q][tx][ty + 8 * r] * vmu);  // T: M[nu][mu]
-      }
-    }
-  }
-  for (int r = 0; r < 4; ++r)
-    if (mu[r] < n && nu_ok) F[mo + (long long)mu[r] * n + nu] = acc[r];
-  if (r0 != c0) {  // F[c0.., r0..] = this tile transposed
-    __syncthreads();
-    for (int r = 0; r < 4; ++r) T[0][ty + 8 * r][tx] = acc[r];
-    __syncthreads();
     for (int r = 0; r < 4; ++r) {
       const int row = c0 + ty + 8 * r, col = r0 + tx;
-      if (row < n && col < n) F[mo + (long long)row * n + col] = T[0][tx][ty + 8 * r];
+      const bool ok = row < n && col < n;
+      fock_cp_async8(&fock_T[(q * 32 + ty + 8 * r) * kFockPitch + tx], ok ? M + (long long)row * n + col : M, ok);
+    }
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  // 2. the direct elements of S, H0 and the nine planes, into registers
+  int mu[4];
+  bool ok[4];
+  const int nu = c0 + tx;
+  const bool nu_ok = nu < n;
+  double s_[4], h_[4], dir[9][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    mu[r] = r0 + ty + 8 * r;
+    ok[r] = mu[r] < n && nu_ok;
+    const long long e = mo + (long long)mu[r] * n + nu;
+    s_[r] = ok[r] ? S[e] : 0.0;
+    h_[r] = ok[r] ? H0[e] : 0.0;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const double* M = q < 3 ? D + 3 * mo + q * nn : Q + 6 * mo + (q - 3) * nn;
+      dir[q][r] = ok[r] ? M[(long long)mu[r] * n + nu] : 0.0;
+    }
+  }
+  // 3. potentials of the column's AO and of the rows' AOs
+  const int at_nu = nu_ok ? B.ao_at[o0 + nu] : 0;
+  const double vao_nu = nu_ok ? vsh[s0 + B.ao_sh[o0 + nu]] + vat[a0 + at_nu] : 0.0;
+  double vm_nu[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) vm_nu[q] = nu_ok ? (q < 3 ? vdp[3 * (a0 + at_nu) + q] : vqp[6 * (a0 + at_nu) + q - 3]) : 0.0;
+  double acc[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    acc[r] = 0.0;
+    if (!ok[r]) continue;
+    const int at_mu = B.ao_at[o0 + mu[r]];
+    const double vao_mu = vsh[s0 + B.ao_sh[o0 + mu[r]]] + vat[a0 + at_mu];
+    acc[r] = h_[r] - s_[r] * 0.5 * (vao_mu + vao_nu);
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+  // 4. -0.5 * (M[q][mu][nu] v[at(nu)][q] + M[q][nu][mu] v[at(mu)][q]), planes in order
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    if (!ok[r]) continue;
+    const int at_mu = a0 + B.ao_at[o0 + mu[r]];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const double vmu = q < 3 ? vdp[3 * at_mu + q] : vqp[6 * at_mu + q - 3];
+      acc[r] -= 0.5 * (dir[q][r] * vm_nu[q] + fock_T[(q * 32 + tx) * kFockPitch + ty + 8 * r] * vmu);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+    if (ok[r]) F[mo + (long long)mu[r] * n + nu] = acc[r];
+  if (r0 != c0) {  // F[c0.., r0..] = this tile transposed
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 4; ++r) fock_T[(ty + 8 * r) * kFockPitch + tx] = acc[r];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int row = c0 + ty + 8 * r, col = r0 + tx;
+      if (row < n && col < n) F[mo + (long long)row * n + col] = fock_T[tx * kFockPitch + ty + 8 * r];
     }
   }
 }
@@ -412,6 +437,71 @@ __global__ void k_fermi(DevBatch B, const double* __restrict__ w, double kt, dou
     kdim[m] = last;
     S.e_ts[m] = ts;
     if (!ok_all) S.fermi_warn[m] = 1;
+  }
+}
+
+// nspin = 2 (tblite's open-shell representation; the reference stops at
+// "Unimplemented", src/scf/iterators.cu:247-248).  GFN2 has no spin-dependent
+// potential, so both channels share the Fock matrix, its orbital energies and
+// coefficients, and the SCF is the one above; the channels differ only in
+// their Fermi filling (nel(spin) electrons, the spin loop of get_density,
+// src/scf/iterators.cu:223-239).  Recomputed here for the read-out with the
+// same fermi_channel as k_fermi, so the channels add up to its occupations.
+__global__ void k_spin_occupations(DevBatch B, const double* __restrict__ w, double kt,
+                                   const double* __restrict__ nel, const int* __restrict__ flag,
+                                   double* __restrict__ f) {
+  const int m = blockIdx.x;
+  if (!flag[m]) return;
+  const int n = B.ooff[m + 1] - B.ooff[m], o0 = B.ooff[m], no = B.nao_tot;
+  extern __shared__ double occ[];  // n
+  __shared__ double red[32];
+  for (int spin = 0; spin < 2; ++spin) {
+    int ok;
+    double ef;
+    __syncthreads();
+    fermi_channel(n, nel[2 * m + spin], kt, w + o0, occ, red, ok, ef);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) f[spin * no + o0 + i] = occ[i];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) f[2 * no + o0 + i] = f[o0 + i] - f[no + o0 + i];
+}
+
+// Channel 1 of the charge/magnetization representation (updown_to_magnet,
+// src/wavefunction/spin.h:4-16: (up, down) -> (up + down, up - down)): with
+// q(spin) = n0/2 - population(P_spin), up - down is minus the population of
+// P_alpha - P_beta, whose Mulliken column sums colred holds; dipoles and
+// quadrupoles likewise (same reduction as k_finalize with no reference
+// occupation).
+__global__ void k_spin_moments(DevParams P, DevBatch B, const double* __restrict__ colred,
+                               const int* __restrict__ flag, double* __restrict__ qsh, double* __restrict__ qat,
+                               double* __restrict__ dpat, double* __restrict__ qpat) {
+  const int m = blockIdx.x;
+  if (!flag[m]) return;
+  const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0, s0 = B.soff[m], nsh = B.soff[m + 1] - s0, o0 = B.ooff[m];
+  for (int s = threadIdx.x; s < nsh; s += blockDim.x) {
+    const int i0 = B.sh_iao[s0 + s], na = msao(P.sh[B.sh_type[s0 + s]].ang);
+    double v = 0.0;
+    for (int x = 0; x < na; ++x) v += colred[12 * (long long)(o0 + i0 + x)];
+    qsh[s0 + s] = -v;
+  }
+  __syncthreads();
+  for (int a = threadIdx.x; a < nat; a += blockDim.x) {
+    const int is = B.at_ish[a0 + a];
+    const SpeciesParam& sp = P.sp[B.id[a0 + a]];
+    double q = 0.0, d[3] = {0, 0, 0}, qq[6] = {0, 0, 0, 0, 0, 0};
+    for (int s = 0; s < sp.nsh; ++s) {
+      q += qsh[s0 + is + s];
+      const int i0 = B.sh_iao[s0 + is + s], na = msao(P.sh[sp.sh0 + s].ang);
+      for (int x = 0; x < na; ++x) {
+        const double* c = colred + 12 * (long long)(o0 + i0 + x);
+        for (int k = 0; k < 3; ++k) d[k] -= c[2 + k];
+        for (int k = 0; k < 6; ++k) qq[k] -= c[5 + k];
+      }
+    }
+    qat[a0 + a] = q;
+    for (int k = 0; k < 3; ++k) dpat[3 * (a0 + a) + k] = d[k];
+    for (int k = 0; k < 6; ++k) qpat[6 * (a0 + a) + k] = qq[k];
   }
 }
 
