@@ -96,20 +96,29 @@ typedef struct tb_result {
 } tb_result;
 
 /* wavefunction_type (src/wavefunction/type.h:81-99) of one structure, as the
- * in/out argument `wfn` of xtb_singlepoint (src/xtb.cu:188-197).  One density
- * for both spin channels (nspin = 1, as the reference's SCF; uhf only splits
- * the electrons, get_alpha_beta_occupation, src/wavefunction/type.cu:3-14).
- * The arrays are caller-owned host buffers sized from tb_basis_size; a NULL
- * array is neither read nor written.
+ * in/out argument `wfn` of xtb_singlepoint (src/xtb.cu:188-197).  The arrays
+ * are caller-owned host buffers sized from tb_basis_size; a NULL array is
+ * neither read nor written.
  *   in:  guess = 1 starts the SCF from qsh, dpat and qpat as given (for
  *        example the result of an earlier singlepoint of the same or a nearby
  *        geometry, the reference's wfn carried from call to call); guess = 0
  *        uses the default start (the charge spread over the shells by their
- *        reference occupations, no multipoles).
+ *        reference occupations, no multipoles).  With nspin = 2 channel 0 of
+ *        the moments is read.
+ *        nspin = 1 (or 0): one density for both spin channels, uhf only
+ *        splitting the electrons (get_alpha_beta_occupation,
+ *        src/wavefunction/type.cu:3-14).  nspin = 2: tblite's open-shell
+ *        representation, every array with a leading channel index (the
+ *        reference's [MAX_NSPIN] dimension): emo and coeff per channel (the
+ *        same in both: GFN2 has no spin-dependent potential), focc and
+ *        density per channel (alpha, beta: each channel's own Fermi
+ *        filling), and qat, qsh, dpat, qpat as (total, up - down)
+ *        (updown_to_magnet, src/wavefunction/spin.h:4-16).  The SCF and the
+ *        energy are the same for both.
  *   out: everything else, from the last SCF iteration of the structure. */
 typedef struct tb_wavefunction {
   int32_t guess;          /* in                                                */
-  int32_t nspin;          /* 1                                                 */
+  int32_t nspin;          /* in/out: 1 or 2 (see above)                        */
   int32_t nat, nsh, nao;
   int32_t homo[2];        /* highest orbital of the aufbau filling per channel
                              (1-based count, floor(nel[s]))                    */

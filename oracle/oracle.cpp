@@ -1237,6 +1237,363 @@ int singlepoint(const orc_params& P, int nat, const int* id, const double* xyz, 
   return status;
 }
 
+// ------------------------------------------------------------------ gradient
+// Analytic nuclear gradient of the singlepoint energy (the gradient/sigma
+// outputs of xtb_singlepoint, src/xtb.cu:195-196).  The reference computes
+// only the repulsion part (get_repulsion_derivs, src/xtb.cu:62-91, quoted);
+// the rest is the derivative of the energy expression restated above, with
+// the published structure of an SCC tight-binding gradient:
+//   dE/dR = dE_rep/dR + sum_mu,nu P dH0/dR - W dS/dR
+//         + sum over Mulliken moments (dE/dmoment) d(moment)/dR at fixed P
+//         + explicit geometric derivatives of E_ES2 and E_AES2 at fixed moments
+//         + (dE/dCN) dCN/dR  (self-energies and multipole damping radii),
+// W = C diag(f e) C^T the energy-weighted density (the free energy -TS is
+// variational with Fermi smearing).  Integral derivatives: the blocks depend
+// on vec = R_i - R_j only; with the moment operator on centre i,
+// d/dvec <phi_j|O_i|phi_i> = <d_r phi_j|O_i|phi_i>, the spatial derivative
+// of the j function (x^l exp(-a x^2) -> l x^(l-1) - 2 a x^(l+1)) -- the same
+// construction as the quoted multipole_grad_3d (src/multipole.cu:326-421),
+// which differentiates the i function with the operator on j.
+
+// 1-D moments of order 0..2 about centre i for Cartesian powers li (on i) and
+// lj (on j, up to kMaxL + 1), as in multipole_3d.
+void moments_1d_ext(int li, int lj, double rpi, double rpj, const double* s1d, double* v) {
+  double vi[kMaxL + 2] = {0}, vj[kMaxL + 2] = {0}, vv[2 * kMaxL + 3] = {0};
+  vi[li] = 1.0;
+  vj[lj] = 1.0;
+  horizontal_shift(rpi, li, vi);
+  if (lj == 3) { vj[0] += rpj * rpj * rpj; vj[1] += 3 * rpj * rpj; vj[2] += 3 * rpj; }
+  else horizontal_shift(rpj, lj, vj);
+  form_product(vi, vj, li, lj, vv);
+  v[0] = v[1] = v[2] = 0.0;
+  for (int l = 0; l <= li + lj; ++l) {
+    v[0] += s1d[l] * vv[l];
+    v[1] += (s1d[l + 1] + rpi * s1d[l]) * vv[l];
+    v[2] += (s1d[l + 2] + 2 * rpi * s1d[l + 1] + rpi * rpi * s1d[l]) * vv[l];
+  }
+}
+
+// Blocks of multipole_cgto and their derivatives with respect to vec:
+// ds[x][ij], dd[x][ij*3+k], dq[x][ij*6+c] (spherical, quadrupole traceless).
+void multipole_cgto_grad(const Shell& cj, const Shell& ci, double r2, const double* vec, double intcut,
+                         double* ovl, double* dpint, double* qpint, double (*ds)[25], double (*dd)[75],
+                         double (*dq)[150]) {
+  const int li = ci.ang, lj = cj.ang, mi = mlao(li), mj = mlao(lj), si = msao(li), sj = msao(lj);
+  // [0] the value, [1..3] the derivative along x, y, z
+  double s3d[4][36] = {{0}}, d3d[4][3][36] = {{{0}}}, q3d[4][6][36] = {{{0}}};
+  double s1d[2 * kMaxL + 5];
+  for (int ip = 0; ip < ci.nprim; ++ip) {
+    for (int jp = 0; jp < cj.nprim; ++jp) {
+      const double ai = ci.alpha[ip], aj = cj.alpha[jp];
+      const double eab = ai + aj, oab = 1.0 / eab;
+      const double est = ai * aj * r2 * oab;
+      if (est > intcut) continue;
+      const double pre = std::exp(-est) * kSqrtPi3 * std::pow(std::sqrt(oab), 3);
+      double rpi[3], rpj[3];
+      for (int k = 0; k < 3; ++k) { rpi[k] = -vec[k] * aj * oab; rpj[k] = vec[k] * ai * oab; }
+      for (int l = 0; l <= li + lj + 3; ++l) s1d[l] = overlap_1d(l, eab);
+      const double cc = ci.coeff[ip] * cj.coeff[jp] * pre;
+      for (int a = 0; a < mi; ++a)
+        for (int b = 0; b < mj; ++b) {
+          const int* la = kLx[a + lmap(li)];
+          const int* lb = kLx[b + lmap(lj)];
+          double v[3][3], g[3][3];
+          for (int k = 0; k < 3; ++k) {
+            moments_1d_ext(la[k], lb[k], rpi[k], rpj[k], s1d, v[k]);
+            double up[3], dn[3] = {0, 0, 0};
+            moments_1d_ext(la[k], lb[k] + 1, rpi[k], rpj[k], s1d, up);
+            if (lb[k] > 0) moments_1d_ext(la[k], lb[k] - 1, rpi[k], rpj[k], s1d, dn);
+            for (int o = 0; o < 3; ++o) g[k][o] = lb[k] * dn[o] - 2.0 * aj * up[o];
+          }
+          const int x = a * mj + b;
+          for (int t = 0; t < 4; ++t) {
+            // factor of direction k: the derivative table in direction t-1, the value elsewhere
+            auto f = [&](int k, int o) { return (t > 0 && k == t - 1) ? g[k][o] : v[k][o]; };
+            s3d[t][x] += cc * f(0, 0) * f(1, 0) * f(2, 0);
+            d3d[t][0][x] += cc * f(0, 1) * f(1, 0) * f(2, 0);
+            d3d[t][1][x] += cc * f(0, 0) * f(1, 1) * f(2, 0);
+            d3d[t][2][x] += cc * f(0, 0) * f(1, 0) * f(2, 1);
+            q3d[t][0][x] += cc * f(0, 2) * f(1, 0) * f(2, 0);
+            q3d[t][1][x] += cc * f(0, 1) * f(1, 1) * f(2, 0);
+            q3d[t][2][x] += cc * f(0, 0) * f(1, 2) * f(2, 0);
+            q3d[t][3][x] += cc * f(0, 1) * f(1, 0) * f(2, 1);
+            q3d[t][4][x] += cc * f(0, 0) * f(1, 1) * f(2, 1);
+            q3d[t][5][x] += cc * f(0, 0) * f(1, 0) * f(2, 2);
+          }
+        }
+    }
+  }
+  for (int t = 0; t < 4; ++t) {
+    double* so = t == 0 ? ovl : ds[t - 1];
+    double* dout = t == 0 ? dpint : dd[t - 1];
+    double* qout = t == 0 ? qpint : dq[t - 1];
+    double tmp[25];
+    transform0(lj, li, s3d[t], so);
+    for (int k = 0; k < 3; ++k) {
+      transform0(lj, li, d3d[t][k], tmp);
+      for (int x = 0; x < si * sj; ++x) dout[x * 3 + k] = tmp[x];
+    }
+    for (int k = 0; k < 6; ++k) {
+      transform0(lj, li, q3d[t][k], tmp);
+      for (int x = 0; x < si * sj; ++x) qout[x * 6 + k] = tmp[x];
+    }
+    for (int x = 0; x < si * sj; ++x) {
+      double* q = qout + 6 * x;
+      const double tr = 0.5 * (q[0] + q[2] + q[5]);
+      q[0] = 1.5 * q[0] - tr; q[1] = 1.5 * q[1]; q[2] = 1.5 * q[2] - tr;
+      q[3] = 1.5 * q[3]; q[4] = 1.5 * q[4]; q[5] = 1.5 * q[5] - tr;
+    }
+  }
+}
+
+// Derivative along vec_x of shift_operator's output (dj, qj) given the
+// derivatives of its inputs: ds, ddi[3], dqi[6] along x (x = 0, 1, 2).
+void shift_operator_grad(const double* vec, int x, double s, const double* di, double ds, const double* ddi,
+                         const double* dqi, double* ddj, double* dqj) {
+  double e[3] = {0, 0, 0};
+  e[x] = 1.0;
+  for (int k = 0; k < 3; ++k) ddj[k] = ddi[k] + e[k] * s + vec[k] * ds;
+  // t = the operator-shift terms before the trace removal, and their derivatives
+  const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 1, 2, 2, 2};
+  double dt[6];
+  for (int c = 0; c < 6; ++c) {
+    const int a = pa[c], b = pb[c];
+    if (a == b)
+      dt[c] = 2 * e[a] * di[a] + 2 * vec[a] * ddi[a] + 2 * vec[a] * e[a] * s + vec[a] * vec[a] * ds;
+    else
+      dt[c] = e[a] * di[b] + vec[a] * ddi[b] + e[b] * di[a] + vec[b] * ddi[a] +
+              (e[a] * vec[b] + vec[a] * e[b]) * s + vec[a] * vec[b] * ds;
+  }
+  const double tr = 0.5 * (dt[0] + dt[2] + dt[5]);
+  dqj[0] = dqi[0] + 1.5 * dt[0] - tr;
+  dqj[1] = dqi[1] + 1.5 * dt[1];
+  dqj[2] = dqi[2] + 1.5 * dt[2] - tr;
+  dqj[3] = dqi[3] + 1.5 * dt[3];
+  dqj[4] = dqi[4] + 1.5 * dt[4];
+  dqj[5] = dqi[5] + 1.5 * dt[5] - tr;
+}
+
+// Gradient (grad[nat][3]) and virial (sigma[3][3] = sum_A g_A R_A^T) of the
+// converged singlepoint held by wfn.
+void singlepoint_gradient(const orc_params& P, int nat, const int* id, const double* xyz, const Wavefunction& wfn,
+                          double* grad, double* sigma) {
+  Basis B;
+  make_basis(P, nat, id, B);
+  const int n = B.nao, nsh = B.nsh;
+  const size_t nn = (size_t)n * n;
+  for (int i = 0; i < 3 * nat; ++i) grad[i] = 0.0;
+  std::vector<double> cn(nat), se(nsh);
+  coordination_number(P, nat, id, xyz, cn.data());
+  get_selfenergy(P, B, id, cn.data(), se.data());
+  Coulomb C;
+  coulomb_update(P, B, id, xyz, cn.data(), C);
+  // potentials of the final moments: dE/dq_sh, dE/dq_at, dE/dmu, dE/dTheta
+  std::vector<double> vsh(nsh, 0.0), vat(nat, 0.0), vdp(3 * nat, 0.0), vqp(6 * nat, 0.0);
+  coulomb_potential(P, B, id, C, wfn.qsh.data(), wfn.qat.data(), wfn.dpat.data(), wfn.qpat.data(), vsh.data(),
+                    vat.data(), vdp.data(), vqp.data());
+  // energy-weighted density
+  std::vector<double> fe(n), W(nn);
+  for (int i = 0; i < n; ++i) fe[i] = wfn.focc[i] * wfn.emo[i];
+  density_matrix(n, wfn.C.data(), fe.data(), W.data());
+  const std::vector<double>& Pm = wfn.P;
+  std::vector<double> dEdse(nsh, 0.0), dEdcn(nat, 0.0), dEdrad(nat, 0.0);
+  // ---- off-site shell pairs: H0, overlap, Mulliken moments, W
+  const double intcut = integral_cutoff(1.0);
+  const double cutoff = get_cutoff(P, 1.0);
+  std::vector<int> inl, nnl, nlat, nltr;
+  adjacency(nat, xyz, cutoff, inl, nnl, nlat, nltr);
+  double stmp[25], dtmp[75], qtmp[150], ds[3][25], dd[3][75], dq[3][150];
+  for (int iat = 0; iat < nat; ++iat) {
+    const int izp = id[iat], is = B.ish_at[iat];
+    for (int img = 0; img < nnl[iat]; ++img) {
+      const int jat = nlat[inl[iat] + img];
+      const int jzp = id[jat], js = B.ish_at[jat];
+      const double vec[3] = {xyz[3 * iat] - xyz[3 * jat], xyz[3 * iat + 1] - xyz[3 * jat + 1],
+                             xyz[3 * iat + 2] - xyz[3 * jat + 2]};
+      const double r2 = vec[0] * vec[0] + vec[1] * vec[1] + vec[2] * vec[2];
+      const double r1 = std::sqrt(r2);
+      const double radsum = P.el[jzp].rad + P.el[izp].rad;
+      const double rr = std::sqrt(r1 / radsum);
+      double drr[3];  // d rr / d vec
+      for (int k = 0; k < 3; ++k) drr[k] = 0.5 / rr / radsum * vec[k] / r1;
+      double g[3] = {0, 0, 0};
+      for (int ish = 0; ish < B.nsh_at[iat]; ++ish) {
+        const int ii = B.iao_sh[is + ish];
+        const Shell& ci = P.el[izp].sh[ish];
+        for (int jsh = 0; jsh < B.nsh_at[jat]; ++jsh) {
+          const int jj = B.iao_sh[js + jsh];
+          const Shell& cj = P.el[jzp].sh[jsh];
+          multipole_cgto_grad(cj, ci, r2, vec, intcut, stmp, dtmp, qtmp, ds, dd, dq);
+          const double shpoly = (1.0 + ci.shpoly * rr) * (1.0 + cj.shpoly * rr);
+          const double dshpoly = ci.shpoly * (1.0 + cj.shpoly * rr) + cj.shpoly * (1.0 + ci.shpoly * rr);
+          const double hs = hscale(P, izp, ish, jzp, jsh);
+          const double hij = 0.5 * (se[is + ish] + se[js + jsh]) * hs * shpoly;
+          const int ni = msao(ci.ang), nj = msao(cj.ang);
+          double ese = 0.0;
+          for (int iao = 0; iao < ni; ++iao)
+            for (int jao = 0; jao < nj; ++jao) {
+              const int ij = iao * nj + jao;
+              const size_t mu = jj + jao, nu = ii + iao;
+              const double pij = Pm[mu * n + nu], wij = W[mu * n + nu];
+              const double vmu = vsh[B.ao2sh[mu]] + vat[B.ao2at[mu]], vnu = vsh[B.ao2sh[nu]] + vat[B.ao2at[nu]];
+              ese += pij * stmp[ij] * hs * shpoly;
+              for (int x = 0; x < 3; ++x) {
+                double gx = 2.0 * pij * (hij - 0.5 * (vmu + vnu)) * ds[x][ij] - 2.0 * wij * ds[x][ij];
+                gx += 2.0 * pij * stmp[ij] * 0.5 * (se[is + ish] + se[js + jsh]) * hs * dshpoly * drr[x];
+                double ddj[3], dqj[6];
+                shift_operator_grad(vec, x, stmp[ij], dtmp + 3 * ij, ds[x][ij], dd[x] + 3 * ij, dq[x] + 6 * ij, ddj,
+                                    dqj);
+                for (int k = 0; k < 3; ++k)
+                  gx -= pij * (vdp[3 * iat + k] * dd[x][3 * ij + k] + vdp[3 * jat + k] * ddj[k]);
+                for (int c = 0; c < 6; ++c)
+                  gx -= pij * (vqp[6 * iat + c] * dq[x][6 * ij + c] + vqp[6 * jat + c] * dqj[c]);
+                g[x] += gx;
+              }
+            }
+          dEdse[is + ish] += ese;
+          dEdse[js + jsh] += ese;
+        }
+      }
+      for (int k = 0; k < 3; ++k) { grad[3 * iat + k] += g[k]; grad[3 * jat + k] -= g[k]; }
+    }
+  }
+  // on-site diagonal of H0 = self-energies
+  for (int mu = 0; mu < n; ++mu) dEdse[B.ao2sh[mu]] += Pm[(size_t)mu * n + mu];
+  // ---- repulsion (get_repulsion_derivs, src/xtb.cu:62-91, quoted)
+  {
+    const double cut2 = P.glob("rep_cutoff") * P.glob("rep_cutoff");
+    for (int iat = 0; iat < nat; ++iat) {
+      const Element& ei = P.el[id[iat]];
+      for (int jat = 0; jat < iat; ++jat) {
+        const Element& ej = P.el[id[jat]];
+        const double r[3] = {xyz[3 * iat] - xyz[3 * jat], xyz[3 * iat + 1] - xyz[3 * jat + 1],
+                             xyz[3 * iat + 2] - xyz[3 * jat + 2]};
+        const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+        if (r2 > cut2 || r2 < 1.0e-12) continue;
+        const double r1 = std::sqrt(r2);
+        const double alpha = std::sqrt(ei.rep_alpha * ej.rep_alpha), zeff = ei.rep_zeff * ej.rep_zeff;
+        const double kexp = (ei.z <= 2 && ej.z <= 2) ? P.glob("rep_kexp_light") : P.glob("rep_kexp");
+        const double rexp = P.glob("rep_rexp");
+        const double r1k = std::pow(r1, kexp), exa = std::exp(-alpha * r1k), r1r = std::pow(r1, rexp);
+        const double dE = zeff * exa / r1r;
+        for (int k = 0; k < 3; ++k) {
+          const double dG = -(alpha * r1k * kexp + rexp) * dE * r[k] / r2;
+          grad[3 * iat + k] += dG;
+          grad[3 * jat + k] -= dG;
+        }
+      }
+    }
+  }
+  // ---- ES2 at fixed charges: E = 1/2 q^T gamma q, off-site gamma(r)
+  {
+    const double gexp = P.glob("gexp");
+    for (int iat = 0; iat < nat; ++iat)
+      for (int jat = 0; jat < iat; ++jat) {
+        const double v[3] = {xyz[3 * iat] - xyz[3 * jat], xyz[3 * iat + 1] - xyz[3 * jat + 1],
+                             xyz[3 * iat + 2] - xyz[3 * jat + 2]};
+        const double r1 = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        const double r1g = std::pow(r1, gexp);
+        double de = 0.0;
+        for (int ish = 0; ish < B.nsh_at[iat]; ++ish)
+          for (int jsh = 0; jsh < B.nsh_at[jat]; ++jsh) {
+            const double gam = 0.5 * (P.el[id[iat]].sh[ish].hubbard + P.el[id[jat]].sh[jsh].hubbard);
+            const double base = r1g + std::pow(gam, -gexp);
+            const double dg = -std::pow(r1, gexp - 1.0) * std::pow(base, -1.0 / gexp - 1.0);
+            de += wfn.qsh[B.ish_at[iat] + ish] * wfn.qsh[B.ish_at[jat] + jsh] * dg;
+          }
+        for (int k = 0; k < 3; ++k) {
+          grad[3 * iat + k] += de * v[k] / r1;
+          grad[3 * jat + k] -= de * v[k] / r1;
+        }
+      }
+  }
+  // ---- AES2 at fixed moments (get_multipole_matrix_0d kernels; v = R_i - R_j for
+  // source atom i and multipole atom j), and dE/d(damping radius)
+  {
+    const double k3 = P.glob("kdmp3"), k5 = P.glob("kdmp5");
+    const double* q = wfn.qat.data();
+    const double* mu = wfn.dpat.data();
+    const double* th = wfn.qpat.data();
+    for (int i = 0; i < nat; ++i)
+      for (int j = 0; j < nat; ++j) {
+        if (i == j) continue;
+        const double v[3] = {xyz[3 * i] - xyz[3 * j], xyz[3 * i + 1] - xyz[3 * j + 1], xyz[3 * i + 2] - xyz[3 * j + 2]};
+        const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2], r1 = std::sqrt(r2);
+        const double g1 = 1.0 / r1, g3 = g1 * g1 * g1, g5 = g3 * g1 * g1, g7 = g5 * g1 * g1;
+        const double R0 = 0.5 * (C.mrad[i] + C.mrad[j]), rr = R0 * g1;
+        const double t3 = 6.0 * std::pow(rr, k3), t5 = 6.0 * std::pow(rr, k5);
+        const double f3 = 1.0 / (1.0 + t3), f5 = 1.0 / (1.0 + t5);
+        const double df3 = -k3 * t3 / rr * f3 * f3, df5 = -k5 * t5 / rr * f5 * f5;  // d f / d rr
+        // e = q_i (mu_j.v) g3 f3 + 1/2 [(mu_j.mu_i) g3 f5 - 3 (mu_j.v)(mu_i.v) g5 f5] + q_i (Th_j : tc(v)) g5 f5
+        const double* mj = mu + 3 * j;
+        const double* mi = mu + 3 * i;
+        const double* tj = th + 6 * j;
+        const double mjv = mj[0] * v[0] + mj[1] * v[1] + mj[2] * v[2];
+        const double miv = mi[0] * v[0] + mi[1] * v[1] + mi[2] * v[2];
+        const double mm = mj[0] * mi[0] + mj[1] * mi[1] + mj[2] * mi[2];
+        const double tv = tj[0] * v[0] * v[0] + 2 * tj[1] * v[0] * v[1] + tj[2] * v[1] * v[1] +
+                          2 * tj[3] * v[0] * v[2] + 2 * tj[4] * v[1] * v[2] + tj[5] * v[2] * v[2];
+        double dtv[3];  // d tv / d v
+        dtv[0] = 2 * tj[0] * v[0] + 2 * tj[1] * v[1] + 2 * tj[3] * v[2];
+        dtv[1] = 2 * tj[1] * v[0] + 2 * tj[2] * v[1] + 2 * tj[4] * v[2];
+        dtv[2] = 2 * tj[3] * v[0] + 2 * tj[4] * v[1] + 2 * tj[5] * v[2];
+        // parts: A = q_i mjv g3 f3, Bp = 1/2 (mm g3 - 3 mjv miv g5) f5, Cp = q_i tv g5 f5
+        const double a_nof = q[i] * mjv * g3, b_nof = 0.5 * (mm * g3 - 3.0 * mjv * miv * g5), c_nof = q[i] * tv * g5;
+        for (int k = 0; k < 3; ++k) {
+          const double drr = -rr * v[k] / r2;  // d rr / d v_k
+          const double dg3 = -3.0 * g5 * v[k], dg5 = -5.0 * g7 * v[k];
+          const double da = q[i] * (mj[k] * g3 + mjv * dg3);
+          const double db = 0.5 * (mm * dg3 - 3.0 * (mj[k] * miv + mjv * mi[k]) * g5 - 3.0 * mjv * miv * dg5);
+          const double dc = q[i] * (dtv[k] * g5 + tv * dg5);
+          const double de = da * f3 + a_nof * df3 * drr + db * f5 + b_nof * df5 * drr + dc * f5 + c_nof * df5 * drr;
+          grad[3 * i + k] += de;
+          grad[3 * j + k] -= de;
+        }
+        // d e / d mrad_i = d e / d mrad_j = (a_nof df3 + (b_nof + c_nof) df5) * d rr / d R0 * 1/2
+        const double der = (a_nof * df3 + (b_nof + c_nof) * df5) * g1 * 0.5;
+        dEdrad[i] += der;
+        dEdrad[j] += der;
+      }
+  }
+  // ---- dE/dCN: self-energies (se = se0 - kcn CN) and damping radii (get_mrad)
+  {
+    const double shift = P.glob("mp_shift"), kexp = P.glob("mp_kexp"), rmax = P.glob("mp_rmax");
+    for (int iat = 0; iat < nat; ++iat) {
+      const Element& e = P.el[id[iat]];
+      double d = 0.0;
+      for (int s = 0; s < B.nsh_at[iat]; ++s) d -= e.sh[s].kcn * dEdse[B.ish_at[iat] + s];
+      const double t1 = std::exp(-kexp * (cn[iat] - e.mp_vcn - shift));
+      d += dEdrad[iat] * (rmax - e.mp_rad) * kexp * t1 / ((1.0 + t1) * (1.0 + t1));
+      dEdcn[iat] = d;
+    }
+    // dCN/dR of the counting function exp_count(ka, r, rc) exp_count(kb, r, rc + 2)
+    const double ka = 10.0, kb = 20.0, rshift = 2.0;
+    const double cut2 = P.glob("cn_cutoff") * P.glob("cn_cutoff");
+    for (int iat = 0; iat < nat; ++iat)
+      for (int jat = 0; jat < iat; ++jat) {
+        const double v[3] = {xyz[3 * iat] - xyz[3 * jat], xyz[3 * iat + 1] - xyz[3 * jat + 1],
+                             xyz[3 * iat + 2] - xyz[3 * jat + 2]};
+        const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        if (r2 > cut2 || r2 < 1.0e-12) continue;
+        const double r1 = std::sqrt(r2);
+        const double rc = P.el[id[iat]].rcov + P.el[id[jat]].rcov;
+        const double ea = exp_count(ka, r1, rc), eb = exp_count(kb, r1, rc + rshift);
+        const double dea = -ea * (1.0 - ea) * ka * rc / r2, deb = -eb * (1.0 - eb) * kb * (rc + rshift) / r2;
+        const double dc = (dea * eb + ea * deb) * (dEdcn[iat] + dEdcn[jat]);
+        for (int k = 0; k < 3; ++k) {
+          grad[3 * iat + k] += dc * v[k] / r1;
+          grad[3 * jat + k] -= dc * v[k] / r1;
+        }
+      }
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      double s = 0.0;
+      for (int i = 0; i < nat; ++i) s += grad[3 * i + a] * xyz[3 * i + b];
+      sigma[3 * a + b] = s;
+    }
+}
+
 void set_err(char* err, int len, const std::string& m) {
   if (err && len > 0) { std::snprintf(err, len, "%s", m.c_str()); }
 }
@@ -1410,6 +1767,63 @@ int orc_singlepoint(const orc_params* p, int nat, const int* id, const double* x
   if (qpat && !wfn.qpat.empty()) std::copy(wfn.qpat.begin(), wfn.qpat.end(), qpat);
   if (emo && !wfn.emo.empty()) std::copy(wfn.emo.begin(), wfn.emo.end(), emo);
   if (Pout && !wfn.P.empty()) std::copy(wfn.P.begin(), wfn.P.end(), Pout);
+  return st;
+}
+
+// nspin = 2 (tblite's open-shell representation; the reference stops at
+// "Unimplemented", src/scf/iterators.cu:247-248).  GFN2 has no spin-dependent
+// potential, so both channels share the Fock matrix, its orbital energies and
+// coefficients; each channel has its own Fermi filling with nel(spin)
+// electrons (the spin loop of get_density, src/scf/iterators.cu:223-239) and
+// its own density C f_spin C^T.  The Mulliken moments per channel are
+// n0/2 - population(P_spin) (charges) and -population(P_spin) (multipoles);
+// updown_to_magnet (src/wavefunction/spin.h:4-16, quoted) turns (up, down)
+// into (up + down, up - down): channel 0 is the closed-shell result and
+// channel 1 the moments of P_alpha - P_beta with no reference occupation.
+int orc_singlepoint_spin(const orc_params* p, int nat, const int* id, const double* xyz, double charge, int uhf,
+                         const orc_options* opt, orc_result* res, double* focc2, double* P2, double* qsh2,
+                         double* qat2, double* dpat2, double* qpat2) {
+  Wavefunction wfn;
+  int st = singlepoint(*p, nat, id, xyz, charge, uhf, *opt, *res, wfn);
+  if (res->status == ORC_BAD_INPUT) return st;
+  Basis B;
+  make_basis(*p, nat, id, B);
+  const int n = B.nao, nsh = B.nsh;
+  const size_t nn = (size_t)n * n;
+  std::vector<double> occ(2 * (size_t)n), Ps(2 * nn), Pm(nn);
+  for (int s = 0; s < 2; ++s) {
+    double ef = 0.0, ts = 0.0;
+    fermi_filling(n, wfn.nel[s], wfn.kt, wfn.emo.data(), occ.data() + (size_t)s * n, ef, ts);
+    density_matrix(n, wfn.C.data(), occ.data() + (size_t)s * n, Ps.data() + s * nn);
+  }
+  for (size_t k = 0; k < nn; ++k) Pm[k] = Ps[k] - Ps[nn + k];
+  // integrals of the structure for the magnetization moments
+  std::vector<double> cn(nat), se(nsh), S(nn), H0(nn), D(3 * nn), Q(6 * nn), zero(nsh, 0.0);
+  std::vector<double> qsh_m(nsh), qat_m(nat), dpat_m(3 * (size_t)nat), qpat_m(6 * (size_t)nat);
+  orc_hamiltonian(p, nat, id, xyz, S.data(), H0.data(), D.data(), Q.data());
+  mulliken(B, S.data(), D.data(), Q.data(), Pm.data(), zero.data(), qsh_m.data(), qat_m.data(), dpat_m.data(),
+           qpat_m.data());
+  if (focc2) std::copy(occ.begin(), occ.end(), focc2);
+  if (P2) std::copy(Ps.begin(), Ps.end(), P2);
+  auto two = [](double* out, const std::vector<double>& a, const std::vector<double>& b) {
+    if (!out) return;
+    std::copy(a.begin(), a.end(), out);
+    std::copy(b.begin(), b.end(), out + a.size());
+  };
+  two(qsh2, wfn.qsh, qsh_m);
+  two(qat2, wfn.qat, qat_m);
+  two(dpat2, wfn.dpat, dpat_m);
+  two(qpat2, wfn.qpat, qpat_m);
+  return st;
+}
+
+// Singlepoint plus its analytic gradient grad[nat][3] and virial sigma[3][3].
+int orc_singlepoint_gradient(const orc_params* p, int nat, const int* id, const double* xyz, double charge, int uhf,
+                             const orc_options* opt, orc_result* res, double* grad, double* sigma) {
+  Wavefunction wfn;
+  int st = singlepoint(*p, nat, id, xyz, charge, uhf, *opt, *res, wfn);
+  if (res->status == ORC_BAD_INPUT || res->status == ORC_NOT_SPD) return st;
+  singlepoint_gradient(*p, nat, id, xyz, wfn, grad, sigma);
   return st;
 }
 

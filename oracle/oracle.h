@@ -92,6 +92,18 @@ int orc_mulliken(const orc_params* p, int nat, const int* id, const double* S, c
 int orc_singlepoint(const orc_params* p, int nat, const int* id, const double* xyz, double charge,
                     int uhf, const orc_options* opt, orc_result* res, double* qat, double* qsh,
                     double* dpat, double* qpat, double* emo, double* P);
+/* The same singlepoint in tblite's nspin = 2 representation: per channel
+ * (alpha, beta) occupations focc2[2][nao] and densities P2[2][nao][nao]; the
+ * moments in the charge/magnetization representation (channel 0 = total,
+ * channel 1 = up - down): qsh2[2][nsh], qat2[2][nat], dpat2[2][nat][3],
+ * qpat2[2][nat][6].  Any output may be NULL. */
+int orc_singlepoint_spin(const orc_params* p, int nat, const int* id, const double* xyz, double charge,
+                         int uhf, const orc_options* opt, orc_result* res, double* focc2, double* P2,
+                         double* qsh2, double* qat2, double* dpat2, double* qpat2);
+/* The singlepoint and its analytic nuclear gradient grad[nat][3] (Eh/Bohr) and
+ * virial sigma[3][3] = sum_A grad_A R_A^T. */
+int orc_singlepoint_gradient(const orc_params* p, int nat, const int* id, const double* xyz, double charge,
+                             int uhf, const orc_options* opt, orc_result* res, double* grad, double* sigma);
 /* nmol structures packed back to back (atom offsets in aoff[nmol+1]), nthreads std::threads */
 int orc_singlepoint_batch(const orc_params* p, int nmol, const int* aoff, const int* id,
                           const double* xyz, const double* charge, const int* uhf,

@@ -63,7 +63,7 @@ def lib():
         for name in ("orc_basis_size", "orc_basis_maps", "orc_coordination_number", "orc_mrad",
                      "orc_selfenergy", "orc_hamiltonian", "orc_repulsion", "orc_coulomb_matrices",
                      "orc_coulomb_potential", "orc_coulomb_energy", "orc_fock", "orc_mulliken",
-                     "orc_singlepoint", "orc_singlepoint_batch", "orc_multipole_cgto", "orc_nspecies"):
+                     "orc_singlepoint", "orc_singlepoint_batch", "orc_singlepoint_spin", "orc_singlepoint_gradient", "orc_multipole_cgto", "orc_nspecies"):
             getattr(L, name).argtypes = None
             getattr(L, name).restype = C.c_int
         L.orc_default_options.argtypes = [C.POINTER(Options)]
@@ -245,6 +245,30 @@ class Oracle:
         out.update(energy=r.energy, e_rep=r.e_rep, e_elec=r.e_elec, e_band=r.e_band, e_ts=r.e_ts,
                    e_es2=r.e_es2, e_aes2=r.e_aes2, e_es3=r.e_es3, dipole=np.array(r.dipole[:]),
                    iterations=r.iterations, status=r.status)
+        return out
+
+    def singlepoint_gradient(self, mol, **opts):
+        """Energy, analytic gradient [nat][3] and virial [3][3] (orc_singlepoint_gradient)."""
+        ids = np.ascontiguousarray(mol.id, np.int32); xyz = np.ascontiguousarray(mol.xyz, np.float64)
+        o = default_options(**opts)
+        r = Result()
+        grad, sigma = np.zeros((len(ids), 3)), np.zeros((3, 3))
+        lib().orc_singlepoint_gradient(self.h, C.c_int(len(ids)), _i(ids), _d(xyz), C.c_double(mol.charge),
+                                       C.c_int(mol.uhf), C.byref(o), C.byref(r), _d(grad), _d(sigma))
+        return dict(energy=r.energy, gradient=grad, sigma=sigma, iterations=r.iterations, status=r.status)
+
+    def singlepoint_spin(self, mol, **opts):
+        """The singlepoint in the nspin = 2 representation (orc_singlepoint_spin)."""
+        ids = np.ascontiguousarray(mol.id, np.int32); xyz = np.ascontiguousarray(mol.xyz, np.float64)
+        nat = len(ids); nsh, nao = self.basis_size(ids)
+        o = default_options(**opts)
+        r = Result()
+        out = dict(focc=np.zeros((2, nao)), density=np.zeros((2, nao, nao)), qsh=np.zeros((2, nsh)),
+                   qat=np.zeros((2, nat)), dpat=np.zeros((2, nat, 3)), qpat=np.zeros((2, nat, 6)))
+        lib().orc_singlepoint_spin(self.h, C.c_int(nat), _i(ids), _d(xyz), C.c_double(mol.charge),
+                                   C.c_int(mol.uhf), C.byref(o), C.byref(r),
+                                   *[_d(out[k]) for k in ("focc", "density", "qsh", "qat", "dpat", "qpat")])
+        out.update(energy=r.energy, iterations=r.iterations, status=r.status)
         return out
 
     def singlepoint_batch(self, mols, nthreads=1, **opts):

@@ -5,6 +5,7 @@
 // host: it only builds index maps (the basis_type bookkeeping of
 // src/basis/type.h:56-73) and launches kernels.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <chrono>
@@ -26,6 +27,16 @@
 #include "tb_kernels.h"
 
 using namespace tb;
+
+// NVTX ranges per phase of a run (setup, SCF loop, read-outs, serving steps):
+// named spans on the host timeline for Nsight tools; without a tool attached
+// a push/pop is a no-op call.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 namespace {
 
@@ -384,6 +395,7 @@ int choose_lib_above(tb_calculator* c, std::vector<int> sizes) {
 // Build index maps, lay out the workspace, allocate, upload.
 tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, const tb_options* opt,
                       tb_batch* b, Arena* arena) {
+  NvtxRange nv("tb.batch_build");
   const HostParams& P = calc->hp;
   b->calc = calc;
   b->opt = *opt;
@@ -985,6 +997,7 @@ tb_status read_flags(tb_batch* b, cudaStream_t st) {
 // Setup of a run: status reset, per-structure setup kernels (CN, neighbour
 // list, integrals, S = L L^T and X = L^-T) and the SCF start (k_scf_init).
 tb_status batch_setup(tb_batch* b, cudaStream_t st) {
+  NvtxRange nv("tb.setup");
   tb_calculator* c = b->calc;
   const DevBatch& B = b->db;
   MolState& S = b->ms;
@@ -1059,6 +1072,7 @@ tb_status batch_setup(tb_batch* b, cudaStream_t st) {
 // active structure: launches only, no host synchronisation, so that the same
 // sequence can be captured once as a CUDA graph.
 tb_status iterate_body(tb_batch* b, cudaStream_t st) {
+  NvtxRange nv("tb.scf_iteration");
   const DevBatch& B = b->db;
   MolState& S = b->ms;
   const DevParams& Pc = b->Pc;
@@ -1206,6 +1220,7 @@ tb_status batch_iterate(tb_batch* b, cudaStream_t st, int* n_active) {
 // test the host loop of batch_run makes after each iteration.  No host
 // synchronisation inside the loop; one read of the iteration count after it.
 tb_status run_loop_graph(tb_batch* b, cudaStream_t st) {
+  NvtxRange nv("tb.scf_loop_graph");
   if (!b->gloop) {
     if (!b->cap) TB_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
     cudaGraph_t g = nullptr;
@@ -1269,6 +1284,7 @@ tb_status batch_run(tb_batch* b, cudaStream_t st) {
 }
 
 tb_status batch_results(tb_batch* b, tb_result* out, cudaStream_t st) {
+  NvtxRange nv("tb.results");
   const int nmol = b->nmol;
   const int NA = b->nat_tot, NS = b->nsh_tot;
   // the device results land in the calculator's pinned staging buffer (one
@@ -1391,6 +1407,7 @@ tb_status spin_readout(tb_batch* b, const std::vector<int>& flag, cudaStream_t s
 }
 
 tb_status batch_wavefunction(tb_batch* b, tb_wavefunction* wfn, cudaStream_t st) {
+  NvtxRange nv("tb.wavefunction");
   const int nmol = b->nmol;
   const int NA = b->nat_tot, NS = b->nsh_tot, NO = b->nao_tot;
   std::vector<int> spin2(nmol, 0);
@@ -2003,6 +2020,8 @@ struct tb_server {
     int64_t bytes = 0;
     bool inflight = false;  // an SCF iteration of this micro-batch is queued on st
     std::unique_ptr<Arena> ar;  // its workspace (from the pool)
+    int* h_act = nullptr;       // pinned: active flags, copied after each iteration on st
+    int h_cap = 0;
   };
   struct Done {
     int64_t ticket = 0;
@@ -2021,6 +2040,9 @@ struct tb_server {
   std::vector<std::unique_ptr<Arena>> pool;
   int64_t pooled = 0;
   std::vector<cudaStream_t> streams;
+  // pinned host buffers for the micro-batches' active flags, reused like the
+  // streams (pinning host memory is an operating-system call)
+  std::vector<std::pair<int*, int>> pinned;
   // arrivals are collected this long (or until max_batch are queued, or while
   // nothing is resident) so that micro-batches hold more than one request
   double window_s = 0.002;
@@ -2030,6 +2052,9 @@ struct tb_server {
       if (L.st) cudaStreamDestroy(L.st);
     }
     for (cudaStream_t st : streams) cudaStreamDestroy(st);
+    for (Live& L : live)
+      if (L.h_act) cudaFreeHost(L.h_act);
+    for (auto& p : pinned) cudaFreeHost(p.first);
   }
 };
 
@@ -2051,6 +2076,7 @@ int64_t workspace_estimate(const tb_options& o, int nat, int nsh, int nao) {
 }
 
 tb_status server_admit(tb_server* s) {
+  NvtxRange nv("tb.server_admit");
   if (s->queue.empty()) return TB_OK;
   const double waited =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - s->queue.front().t_submit).count();
@@ -2115,10 +2141,36 @@ tb_status server_admit(tb_server* s) {
 }
 
 // Results of the structures of L that finished since the last call.
+// Next SCF iteration of a micro-batch on its stream, followed on the same
+// stream by the copy of its active flags into the micro-batch's pinned buffer
+// (taken from the server's pool on first use).
+tb_status server_launch(tb_server* s, tb_server::Live& L) {
+  const int nmol = L.b->nmol;
+  if (!L.h_act) {
+    for (size_t i = 0; i < s->pinned.size(); ++i)
+      if (s->pinned[i].second >= nmol) {
+        L.h_act = s->pinned[i].first;
+        L.h_cap = s->pinned[i].second;
+        s->pinned.erase(s->pinned.begin() + i);
+        break;
+      }
+    if (!L.h_act) {
+      const int cap = std::max(nmol, 64);
+      TB_CUDA(cudaMallocHost(&L.h_act, cap * sizeof(int)));
+      L.h_cap = cap;
+    }
+  }
+  const tb_status st = launch_iteration(L.b, L.st);
+  if (st != TB_OK) return st;
+  TB_CUDA(cudaMemcpyAsync(L.h_act, L.b->ms.active, nmol * sizeof(int), cudaMemcpyDeviceToHost, L.st));
+  return TB_OK;
+}
+
 tb_status server_collect(tb_server* s, tb_server::Live& L) {
   const int nmol = L.b->nmol;
-  std::vector<int> act(nmol);
-  TB_CUDA(cudaMemcpy(act.data(), L.b->ms.active, nmol * sizeof(int), cudaMemcpyDeviceToHost));
+  // the active flags were copied on L.st after the iteration (server_launch),
+  // which has finished: no device round trip here
+  const std::vector<int> act(L.h_act, L.h_act + nmol);
   bool any = false;
   for (int m = 0; m < nmol; ++m) any |= !act[m] && !L.done[m];
   if (!any) return TB_OK;
@@ -2183,6 +2235,7 @@ tb_status tb_server_submit(tb_server* s, const tb_structure* mol, int64_t* ticke
 }
 
 tb_status tb_server_step(tb_server* s, int32_t* n_resident, int32_t* n_queued, int64_t* bytes_resident) {
+  NvtxRange nv("tb.server_step");
   if (!s) return fail(TB_BAD_INPUT, "null server");
   tb_status st = server_admit(s);
   if (st != TB_OK) return st;
@@ -2204,6 +2257,7 @@ tb_status tb_server_step(tb_server* s, int32_t* n_resident, int32_t* n_queued, i
       if (na <= 0 || L.b->it >= L.b->opt.max_iter) {
         delete L.b;
         s->streams.push_back(L.st);
+        if (L.h_act) s->pinned.push_back({L.h_act, L.h_cap});
         s->resident -= L.bytes;
         s->pooled += (int64_t)L.ar->cap;
         s->pool.push_back(std::move(L.ar));
@@ -2211,7 +2265,7 @@ tb_status tb_server_step(tb_server* s, int32_t* n_resident, int32_t* n_queued, i
         continue;
       }
     }
-    st = launch_iteration(L.b, L.st);
+    st = server_launch(s, L);
     if (st != TB_OK) return st;
     L.inflight = true;
     ++i;

@@ -197,13 +197,16 @@ class Calculator:
     def cutoff(self, accuracy=1.0):
         return load_library().tb_get_cutoff(self.h, C.c_double(accuracy))
 
-    def singlepoint_batch(self, mols, stream=None, raise_on_error=False, wavefunction=False, guess=None, **opts):
+    def singlepoint_batch(self, mols, stream=None, raise_on_error=False, wavefunction=False, guess=None, nspin=1,
+                          **opts):
         """Run xtb_singlepoint for every structure; returns a list of result dicts.
 
         wavefunction=True adds r["wfn"] (the tb_wavefunction record as a dict:
         emo, focc, density, coeff, n0at, n0sh, nel, homo, ...).  guess is None or
         a list (one entry per structure, None for the default start) of dicts
-        with qsh, dpat and qpat to start the SCF from, e.g. an earlier result."""
+        with qsh, dpat and qpat to start the SCF from, e.g. an earlier result.
+        nspin=2 returns the wavefunction in the open-shell representation
+        (leading channel index on every array, see tb_wavefunction)."""
         L = load_library()
         arr, keep = _structs(mols)
         o = default_options(**opts)
@@ -233,7 +236,7 @@ class Calculator:
             v["qpat"] = qpat.ctypes.data + 48 * off
         wfn, wbufs = None, None
         if n and (wavefunction or guess is not None):
-            wfn, wbufs = _wavefunction_records(self, mols, guess, wavefunction)
+            wfn, wbufs = _wavefunction_records(self, mols, guess, wavefunction, nspin)
         st = L.tb_singlepoint_batch(self.h, arr, C.c_int32(n), C.byref(o), wfn, res, C.c_void_p(stream or 0))
         if st not in (TB_OK,) and (raise_on_error or st in (TB_BAD_INPUT, TB_CUDA_ERROR,
                                                             TB_CAPACITY_EXCEEDED, TB_PARAM_ERROR)):
@@ -277,25 +280,28 @@ def _result_dict(r, b):
     return d
 
 
-def _wavefunction_records(calc, mols, guess, outputs):
-    """tb_wavefunction records for mols: output arrays when `outputs`, the
-    caller's starting moments where guess[i] is given."""
+def _wavefunction_records(calc, mols, guess, outputs, nspin=1):
+    """tb_wavefunction records for mols: output arrays when `outputs` (with a
+    leading channel index for nspin = 2), the caller's starting moments where
+    guess[i] is given."""
     n = len(mols)
     rec = (Wavefunction * n)()
     bufs = []
+    ch = (2,) if nspin == 2 else ()
     for i, m in enumerate(mols):
         nsh, nao = calc.basis_size(m)
         b = {}
+        rec[i].nspin = nspin
         if outputs:
-            b = dict(n0at=np.zeros(m.nat), n0sh=np.zeros(nsh), emo=np.zeros(nao), focc=np.zeros(nao),
-                     density=np.zeros((nao, nao)), coeff=np.zeros((nao, nao)), qat=np.zeros(m.nat),
-                     qsh=np.zeros(nsh), dpat=np.zeros((m.nat, 3)), qpat=np.zeros((m.nat, 6)))
+            b = dict(n0at=np.zeros(m.nat), n0sh=np.zeros(nsh), emo=np.zeros(ch + (nao,)), focc=np.zeros(ch + (nao,)),
+                     density=np.zeros(ch + (nao, nao)), coeff=np.zeros(ch + (nao, nao)), qat=np.zeros(ch + (m.nat,)),
+                     qsh=np.zeros(ch + (nsh,)), dpat=np.zeros(ch + (m.nat, 3)), qpat=np.zeros(ch + (m.nat, 6)))
         g = guess[i] if guess is not None else None
         if g is not None:
             for k, shape in (("qsh", (nsh,)), ("dpat", (m.nat, 3)), ("qpat", (m.nat, 6))):
                 a = np.ascontiguousarray(np.array(g[k], np.float64).reshape(shape))
                 if k in b:
-                    b[k][...] = a
+                    b[k].reshape((-1,) + shape)[0][...] = a  # channel 0 (total) is the guess
                 else:
                     b[k] = a
             rec[i].guess = 1

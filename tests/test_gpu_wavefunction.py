@@ -93,3 +93,28 @@ def test_bad_guess_rejected(gpu_calc):
     with pytest.raises(capi.TBError) as e:
         gpu_calc.singlepoint_batch([m], guess=[bad])
     assert e.value.status == capi.TB_BAD_INPUT
+
+
+@pytest.mark.parametrize("idx", [0, 2])
+def test_open_shell_representation_matches_oracle(gpu_calc, oracle, idx):
+    """nspin = 2 (tblite's open-shell representation; the reference stops at
+    "Unimplemented", src/scf/iterators.cu:247-248): per-channel occupations and
+    densities within 1e-9 and the (total, up - down) moments within 1e-7 of the
+    oracle; the total channel is the nspin = 1 result."""
+    m = _mols()[idx]
+    r = gpu_calc.singlepoint_batch([m], accuracy=1e-4, wavefunction=True, nspin=2)[0]
+    o = oracle.singlepoint_spin(m, accuracy=1e-4)
+    w = r["wfn"]
+    assert r["status"] == 0 and w["nspin"] == 2
+    np.testing.assert_allclose(w["focc"], o["focc"], atol=TOL)
+    np.testing.assert_allclose(w["density"], o["density"], atol=TOL)
+    for k in ("qat", "qsh", "dpat", "qpat"):
+        np.testing.assert_allclose(w[k], o[k], atol=1e-7)
+    np.testing.assert_array_equal(w["emo"][0], w["emo"][1])
+    r1 = gpu_calc.singlepoint_batch([m], accuracy=1e-4, wavefunction=True)[0]
+    assert r1["energy"] == r["energy"]
+    np.testing.assert_allclose(w["density"].sum(0), r1["wfn"]["density"], atol=1e-12)
+    np.testing.assert_array_equal(w["qat"][0], r1["qat"])
+    for s in range(2):
+        assert abs(w["focc"][s].sum() - w["nel"][s]) < 1e-9
+    assert abs(w["qat"][1].sum() + (w["nel"][0] - w["nel"][1])) < 1e-9  # up - down = -(N_up - N_down)

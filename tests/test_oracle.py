@@ -212,3 +212,38 @@ def test_parity_fixtures_reproduce():
         assert abs(o["energy"] - ref["energy"]) < 1e-10, name
         np.testing.assert_allclose(o["qat"], ref["qat"], atol=1e-10)
         np.testing.assert_allclose(o["dipole"], ref["dipole"], atol=1e-10)
+
+
+# ------------------------------------------------------------ analytic gradient
+def _fd_gradient(orc, mol, h=1e-4, acc=1e-7):
+    G = np.zeros((mol.nat, 3))
+    for a in range(mol.nat):
+        for k in range(3):
+            xp, xm = mol.xyz.copy(), mol.xyz.copy()
+            xp[a, k] += h
+            xm[a, k] -= h
+            ep = orc.singlepoint(g.Molecule(mol.id, xp, mol.charge, mol.uhf), accuracy=acc)["energy"]
+            em = orc.singlepoint(g.Molecule(mol.id, xm, mol.charge, mol.uhf), accuracy=acc)["energy"]
+            G[a, k] = (ep - em) / (2 * h)
+    return G
+
+
+def test_gradient_matches_finite_differences(oracle):
+    """The oracle's analytic gradient (every term of the energy: repulsion,
+    H0 and overlap with the energy-weighted density, Mulliken moments through
+    S, D, Q, ES2 and AES2 at fixed moments, coordination-number chains)
+    against central differences of the oracle energy, h = 1e-4 Bohr, SCF at
+    accuracy 1e-7; also translational and rotational invariance."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import make_parity_fixtures as fx
+    rng = np.random.default_rng(5)
+    o = g.octane()
+    cases = [(oracle, g.water_cluster(2, rng)), (oracle, g.Molecule(o.id[:8], o.xyz[:8], charge=1.0, uhf=1)),
+             (po.Oracle(fx.PARAMS["hcos"]), fx.rebuild(fx.load()["dimethyl_sulfide"]))]
+    for orc, m in cases:
+        r = orc.singlepoint_gradient(m, accuracy=1e-7)
+        assert r["status"] == 0
+        np.testing.assert_allclose(r["gradient"], _fd_gradient(orc, m), atol=1e-7)
+        np.testing.assert_allclose(r["gradient"].sum(0), 0.0, atol=1e-12)
+        np.testing.assert_allclose(r["sigma"], r["sigma"].T, atol=1e-11)
