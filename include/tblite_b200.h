@@ -93,6 +93,11 @@ typedef struct tb_result {
   double* qsh;            /* [nsh]    shell partial charges                    */
   double* dpat;           /* [nat][3] atomic dipoles                           */
   double* qpat;           /* [nat][6] atomic quadrupoles                       */
+  /* the gradient and sigma arguments of xtb_singlepoint (src/xtb.cu:195-196):
+   * gradient [nat][3] dE/dR in Eh/Bohr, computed when not NULL; sigma the
+   * virial sum_A gradient_A R_A^T (row-major 3x3), written with gradient */
+  double* gradient;
+  double sigma[9];
 } tb_result;
 
 /* wavefunction_type (src/wavefunction/type.h:81-99) of one structure, as the
@@ -176,6 +181,9 @@ tb_status tb_batch_results(tb_batch* batch, tb_result* out, void* stream);
  * (records with guess = 0 keep the default start), and the wavefunctions of
  * the last run (the same records as tb_singlepoint_batch's wfn_inout). */
 tb_status tb_batch_set_guess(tb_batch* batch, const tb_wavefunction* wfn);
+/* Analytic nuclear gradient of the last run: grad [nat_tot][3] (the batch's
+ * atoms in order), sigma [nmol][9]; either may be NULL. */
+tb_status tb_batch_gradient(tb_batch* batch, double* grad, double* sigma, void* stream);
 tb_status tb_batch_wavefunction(tb_batch* batch, tb_wavefunction* wfn, void* stream);
 /* kernels launched by the last tb_batch_run (device work items, not host calls) */
 int64_t tb_batch_launches(const tb_batch* batch);

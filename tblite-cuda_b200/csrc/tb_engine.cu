@@ -298,6 +298,11 @@ struct tb_batch {
   bool any_guess = false;
   double* d_guess = nullptr;
   int* d_guess_flag = nullptr;
+  // gradient read-out: its own workspace (allocated on first use), the
+  // gradient [nat_tot][3] and sigma [nmol][9] of the structures computed
+  Arena grad_ws;
+  double *d_grad = nullptr, *d_sigma = nullptr;
+  std::vector<int> h_grad_done;
   // nspin = 2 read-out: per-channel occupations (3 x nao_tot) and structure flags
   double* d_fspin = nullptr;
   int* d_wflag = nullptr;
@@ -311,7 +316,7 @@ struct tb_batch {
   void* lib_work = nullptr;
   size_t lib_bytes = 0;
   int* lib_info = nullptr;   // 2 per library structure
-  std::vector<int> h_active, h_status;
+  std::vector<int> h_active, h_status, h_phase;
   std::vector<int> h_species;  // species index per atom of the batch
   // mixed-precision form (tb_options.precision = 1)
   bool mixed = false;
@@ -783,11 +788,13 @@ tb_status prof_collect(tb_batch* b, cudaStream_t st) {
 constexpr double kMixedSwitchScale = 10.0, kMixedSwitchFloorE = 1e-5, kMixedSwitchFloorQ = 2e-4;
 
 // Eigen-decomposition and density of one SCF iteration in the mixed-precision
-// form (tb_mixed.cu).  Every matrix is stored in FP64.  F', C and P are
-// TF32x3 tensor-core GEMMs (k_gemm_tc, tcgen05) for structures in the mixed
-// phase and FP64 GEMMs in the FP64 phase; the eigenpairs come from the FP32 eigensolver and
-// FP64 refinement (one step in the mixed phase, two in the FP64 phase).
-// Leaves w, focc, kdim and P as the plain form does.
+// form (tb_mixed.cu).  Every matrix is stored in FP64.  Structures in the
+// mixed phase: F', C and P as TF32x3 tensor-core GEMMs (k_gemm_tc, tcgen05),
+// eigenpairs from the FP32 eigensolver and one FP64 Ogita-Aishima refinement
+// step.  Structures in the FP64 phase (the final iterations) run the plain
+// form's FP64 iteration: FP64 GEMMs and the FP64 eigensolver, so the
+// converged result carries no FP32 error.  Leaves w, focc, kdim and P as the
+// plain form does.
 tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, double n2occ_lo, double n2occ_hi,
                      int gemm_grid, size_t fermi_smem) {
   const DevBatch& B = b->db;
@@ -795,6 +802,7 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
   const int nmol = b->nmol, nt = (int)b->tiles64.size();
   const int4* T = b->d_tiles64;
   const size_t smem32 = syev_smem_bytes(std::max(b->nmax_in, 1), sizeof(float));
+  const size_t eig_smem = syev_smem_bytes(std::max(b->nmax_in, 1));
   int *lo = b->act_lo, *hi = b->act_hi;
   const int nt128 = (int)b->tiles128.size(), tc_grid = std::min(nt128, 148);
   const int4* T128 = b->d_tiles128;
@@ -811,50 +819,56 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
   TB_K("gemm", 2.0 * n3_hi, 1,
        k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, hi,
                                                   kGemmKUpToI | kGemmSym));
-  // FP32 eigensolve of every active structure
-  TB_K("convert", 0, 0, k_to_f32<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, b->Af, S.active));
-  TB_K("syev_f32", 4.0 * (n3_lo + n3_hi), 1,
-       k_syev_f32<<<nmol, kEigThreads, smem32, st>>>(B, b->Af, b->Zf, b->w, b->perm, S.status, S.active));
+  // mixed phase: FP32 eigensolve
+  TB_K("convert", 0, 0, k_to_f32<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, b->Af, lo));
+  TB_K("syev_f32", 4.0 * n3_lo, 1,
+       k_syev_f32<<<nmol, kEigThreads, smem32, st>>>(B, b->Af, b->Zf, b->w, b->perm, S.status, lo));
+  // FP64 phase: the FP64 eigensolver (eigenvectors as rows of Z, W as its scratch)
+  TB_K("syev", 4.0 * n3_hi, 1,
+       k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->W, b->w, b->perm, S.status, hi));
   for (size_t k = 0; k < b->big.size(); ++k) {
     const int m = b->big[k], n = b->h_ooff[m + 1] - b->h_ooff[m];
     if (!b->h_active[m] || b->h_status[m] != kStOk) continue;
     const long long mo = b->h_moff[m], vo = b->h_ooff[m];
     cudaEvent_t e0 = nullptr;
     prof_start(b, st, &e0);
-    const std::string e = b->lib.syev32(st, b->Af + mo, b->Zf + mo, b->wf + vo, b->w + vo, b->perm + vo, n,
-                                        b->lib_work, b->lib_bytes, b->lib_info + 2 * k, S.status + m);
+    std::string e;
+    if (b->h_phase[m] == 0)
+      e = b->lib.syev32(st, b->Af + mo, b->Zf + mo, b->wf + vo, b->w + vo, b->perm + vo, n, b->lib_work,
+                        b->lib_bytes, b->lib_info + 2 * k, S.status + m);
+    else
+      e = b->lib.syev(st, b->F + mo, b->Z + mo, b->w + vo, b->perm + vo, n, b->lib_work, b->lib_bytes,
+                      b->lib_info + 2 * k, S.status + m);
     if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
     ++b->launches;
-    prof_stop(b, st, "syev_lib_f32", e0, 4.0 * n * n * n, 1);
+    prof_stop(b, st, b->h_phase[m] == 0 ? "syev_lib_f32" : "syev_lib", e0, 4.0 * n * n * n, 1);
   }
-  // refinement in FP64 (GEMMs included): V = eigenvectors as columns in
-  // ascending order.  Step 1 (every active structure) Z -> Vn; step 2 (FP64
-  // phase only) Vn -> Z.
+  // mixed phase: one FP64 refinement step (GEMMs included) of the FP32
+  // eigenvectors, gathered into FP64 columns in ascending order (Z -> Vn)
   const size_t oa_smem = oa_smem_bytes(b->nmax);
-  TB_K("refine", 0, 0, k_gather_vectors<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->Zf, b->perm, b->Z, S.active));
-  for (int r = 0; r < 2; ++r) {
-    double* V = r == 0 ? b->Z : b->Vn;
-    double* Vo = r == 0 ? b->Vn : b->Z;
-    int* mk = r == 0 ? S.active : hi;
-    const double wk = 2.0 * (r == 0 ? n3_lo + n3_hi : n3_hi);
+  TB_K("refine", 0, 0, k_gather_vectors<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->Zf, b->perm, b->Z, lo));
+  {
+    double* V = b->Z;
+    double* Vo = b->Vn;
+    const double wk = 2.0 * n3_lo;
     TB_K("gemm", wk, 1,  // G = V^T V
-         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, V, 1, V, 0, nullptr, nullptr, nullptr, b->G, 1.0, 0.0, mk));
+         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, V, 1, V, 0, nullptr, nullptr, nullptr, b->G, 1.0, 0.0, lo));
     TB_K("gemm", wk, 1,  // W = F' V
-         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->F, 0, V, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, mk));
+         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->F, 0, V, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, lo));
     TB_K("gemm", wk, 1,  // Sm = V^T W (in P)
-         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, V, 1, b->W, 0, nullptr, nullptr, nullptr, b->P, 1.0, 0.0, mk));
-    // Rayleigh-Ritz in clusters only in the first of the FP64 phase's two steps
-    TB_K("refine", 0, 0, k_oa_step<<<nmol, 256, oa_smem, st>>>(B, b->G, b->P, V, b->w, mk, r == 0 ? hi : nullptr));
+         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, V, 1, b->W, 0, nullptr, nullptr, nullptr, b->P, 1.0, 0.0, lo));
+    TB_K("refine", 0, 0, k_oa_step<<<nmol, 256, oa_smem, st>>>(B, b->G, b->P, V, b->w, lo, nullptr));
     TB_CUDA(cudaMemcpyAsync(Vo, V, (size_t)b->n2_tot * sizeof(double), cudaMemcpyDeviceToDevice, st));
     TB_K("gemm", wk, 1,  // Vo = V + V E
-         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, V, 0, b->G, 0, nullptr, nullptr, nullptr, Vo, 1.0, 1.0, mk));
+         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, V, 0, b->G, 0, nullptr, nullptr, nullptr, Vo, 1.0, 1.0, lo));
   }
   TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
-  // C = X V into W (mixed phase: V after one step, in Vn; FP64 phase: after two, in Z)
+  // C = X V into W (mixed phase: V after the refinement step, in Vn; FP64
+  // phase: the eigenvector rows of Z in ascending order through perm)
   TB_K("gemm_tc", 2.0 * n3_lo, 1,
        k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->X, 0, b->Vn, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, lo, S.status));
   TB_K("gemm", 2.0 * n3_hi, 1,
-       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 0, b->Z, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi,
+       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr, b->W, 1.0, 0.0, hi,
                                                   kGemmKFromI));
   // P = C diag(f) C^T
   TB_K("gemm_tc", 2.0 * n2occ_lo, 1,
@@ -990,6 +1004,9 @@ tb_status read_flags(tb_batch* b, cudaStream_t st) {
   b->h_status.resize(nmol);
   TB_CUDA(cudaMemcpyAsync(b->h_active.data(), b->ms.active, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
   TB_CUDA(cudaMemcpyAsync(b->h_status.data(), b->ms.status, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
+  b->h_phase.assign(nmol, 0);
+  if (b->mixed)
+    TB_CUDA(cudaMemcpyAsync(b->h_phase.data(), b->ms.phase, nmol * sizeof(int), cudaMemcpyDeviceToHost, st));
   TB_CUDA(cudaStreamSynchronize(st));
   return TB_OK;
 }
@@ -1375,6 +1392,93 @@ tb_status batch_set_guess(tb_batch* b, const tb_wavefunction* wfn) {
 // W holds C = X Z of the structure's last iteration (the density GEMM reads
 // it; nothing later overwrites it), P its density, w and focc its orbital
 // energies (ascending) and occupations.
+// Analytic nuclear gradient and virial of the structures with flag[m] set,
+// after a run (the gradient/sigma outputs of xtb_singlepoint,
+// src/xtb.cu:195-196): the potentials of the final moments (k_potential on
+// [qsh, dpat, qpat] into the potential buffers, free after a run), the
+// energy-weighted density W = C diag(f e) C^T (into F, free after a run), the
+// shell-pair terms (k_grad_pairs_t, one item per neighbour shell pair, summed
+// per atom pair by k_grad_pair_reduce), dE/dCN per atom (k_grad_cn), every
+// atom's pair sum (k_grad_atoms) and sigma.  The workspace is the batch's own
+// (allocated on first use, reused by later calls).
+tb_status batch_gradient(tb_batch* b, const std::vector<int>& flag, cudaStream_t st) {
+  NvtxRange nv("tb.gradient");
+  tb_calculator* c = b->calc;
+  const DevBatch& B = b->db;
+  const int nmol = b->nmol, nt = (int)b->tiles64.size();
+  const long long NA = b->nat_tot, NO = b->nao_tot, NM = nmol, MX = b->mix_tot;
+  const int maxsp = c->maxsh * c->maxsh;
+  const long long items = b->pair_cap * maxsp;
+  Layout L;
+  const size_t o_item = L.add((size_t)items * 3 * 8), o_ese = L.add((size_t)b->h_s2off[nmol] * 8),
+               o_G = L.add((size_t)b->h_a2off[nmol] * 3 * 8), o_cn = L.add(NA * 8), o_fe = L.add(NO * 8),
+               o_qv = L.add(MX * 8), o_grad = L.add(3 * NA * 8), o_sig = L.add(9 * NM * 8), o_flag = L.add(NM * 4);
+  {
+    const cudaError_t e = b->grad_ws.reserve(L.total);
+    if (e != cudaSuccess)
+      return fail(TB_CUDA_ERROR, "gradient workspace of " + std::to_string(L.total >> 20) + " MiB: " +
+                                     cudaGetErrorString(e));
+  }
+  char* base = b->grad_ws.base;
+  double *item = at<double>(base, o_item), *ese = at<double>(base, o_ese), *G = at<double>(base, o_G),
+         *dcn = at<double>(base, o_cn), *fe = at<double>(base, o_fe), *qv = at<double>(base, o_qv);
+  int* dflag = at<int>(base, o_flag);
+  b->d_grad = at<double>(base, o_grad);
+  b->d_sigma = at<double>(base, o_sig);
+  TB_CUDA(cudaMemcpyAsync(dflag, flag.data(), nmol * sizeof(int), cudaMemcpyHostToDevice, st));
+  TB_CUDA(cudaMemsetAsync(item, 0, (size_t)items * 3 * 8, st));
+  TB_CUDA(cudaMemsetAsync(ese, 0, (size_t)b->h_s2off[nmol] * 8, st));
+  TB_CUDA(cudaMemsetAsync(G, 0, (size_t)b->h_a2off[nmol] * 3 * 8, st));
+  k_grad_prep<<<nmol, 256, 0, st>>>(B, dflag, b->focc, b->w, b->qsh_out, b->dpat_out, b->qpat_out, fe, qv);
+  TB_LAUNCH_CHECK();
+  const dim3 pot_grid(nmol, nblk(std::max(b->natmax, b->nshmax), 256));
+  k_potential<<<pot_grid, 256, 0, st>>>(b->Pc, B, qv, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, dflag, b->gtab,
+                                        b->atab);
+  TB_LAUNCH_CHECK();
+  const int gemm_grid = std::min(nt, 148 * 8);
+  k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, nt, b->W, 0, b->W, 1, nullptr, fe, b->kdim, b->F, 1.0,
+                                             0.0, dflag, kGemmSym);
+  TB_LAUNCH_CHECK();
+  TB_CUDA(launch_grad_pairs(b->Pc, B, b->npair, b->pair_i, b->pair_j, b->se, b->P, b->F, b->vsh, b->vat, b->vdp,
+                            b->vqp, dflag, maxsp, items, c->lmask, item, ese, st));
+  ++b->launches;
+  k_grad_pair_reduce<<<(int)std::min<long long>(nblk(b->pair_cap, 256), 148 * 16), 256, 0, st>>>(
+      B, b->npair, b->pair_i, b->pair_j, dflag, maxsp, b->pair_cap, item, G);
+  TB_LAUNCH_CHECK();
+  const dim3 at_grid(nmol, nblk(b->natmax, 128));
+  k_grad_cn<<<at_grid, 128, 0, st>>>(b->Pc, B, dflag, b->P, ese, b->cn, b->mrad, b->qat_out, b->dpat_out,
+                                     b->qpat_out, dcn);
+  TB_LAUNCH_CHECK();
+  k_grad_atoms<<<at_grid, 128, 0, st>>>(b->Pc, B, dflag, G, dcn, b->mrad, b->qsh_out, b->qat_out, b->dpat_out,
+                                        b->qpat_out, b->d_grad);
+  TB_LAUNCH_CHECK();
+  k_grad_sigma<<<nmol, 128, 0, st>>>(B, dflag, b->d_grad, b->d_sigma);
+  TB_LAUNCH_CHECK();
+  b->h_grad_done = flag;
+  return TB_OK;
+}
+
+// Gradient and sigma of the last batch_gradient into host buffers: packed
+// [nat_tot][3] and [nmol][9] (either may be NULL), or per structure into the
+// results whose gradient pointer is set.
+tb_status gradient_copy(tb_batch* b, double* grad, double* sigma, tb_result* out, cudaStream_t st) {
+  const int nmol = b->nmol;
+  std::vector<double> g(3 * (size_t)b->nat_tot), sg(9 * (size_t)nmol);
+  TB_CUDA(cudaMemcpyAsync(g.data(), b->d_grad, g.size() * 8, cudaMemcpyDeviceToHost, st));
+  TB_CUDA(cudaMemcpyAsync(sg.data(), b->d_sigma, sg.size() * 8, cudaMemcpyDeviceToHost, st));
+  TB_CUDA(cudaStreamSynchronize(st));
+  if (grad) std::memcpy(grad, g.data(), g.size() * 8);
+  if (sigma) std::memcpy(sigma, sg.data(), sg.size() * 8);
+  if (out)
+    for (int m = 0; m < nmol; ++m) {
+      if (!out[m].gradient || !b->h_grad_done[m]) continue;
+      const int a0 = b->h_aoff[m], na = b->h_aoff[m + 1] - a0;
+      std::memcpy(out[m].gradient, g.data() + 3 * (size_t)a0, 3 * (size_t)na * 8);
+      std::memcpy(out[m].sigma, sg.data() + 9 * (size_t)m, 9 * 8);
+    }
+  return TB_OK;
+}
+
 // Records with nspin = 2 get tblite's open-shell representation: both spin
 // channels share the orbital energies and coefficients (GFN2 has no
 // spin-dependent potential); per channel the Fermi filling of its electrons
@@ -1614,6 +1718,14 @@ tb_status tb_batch_set_guess(tb_batch* b, const tb_wavefunction* wfn) {
   return batch_set_guess(b, wfn);
 }
 
+tb_status tb_batch_gradient(tb_batch* b, double* grad, double* sigma, void* stream) {
+  if (!b) return fail(TB_BAD_INPUT, "null batch");
+  const std::vector<int> flag(b->nmol, 1);
+  tb_status st = batch_gradient(b, flag, (cudaStream_t)stream);
+  if (st != TB_OK) return st;
+  return gradient_copy(b, grad, sigma, nullptr, (cudaStream_t)stream);
+}
+
 tb_status tb_batch_wavefunction(tb_batch* b, tb_wavefunction* wfn, void* stream) {
   if (!b || !wfn) return fail(TB_BAD_INPUT, "null argument");
   return batch_wavefunction(b, wfn, (cudaStream_t)stream);
@@ -1652,8 +1764,19 @@ tb_status tb_singlepoint_batch(tb_calculator* calc, const tb_structure* mols, in
   }
   st = batch_run(&b, (cudaStream_t)stream);
   if (st != TB_OK) return st;
+  std::vector<int> gflag(nmol, 0);
+  bool any_grad = false;
+  for (int m = 0; m < nmol; ++m) any_grad |= (gflag[m] = out[m].gradient != nullptr) != 0;
+  if (any_grad) {
+    st = batch_gradient(&b, gflag, (cudaStream_t)stream);
+    if (st != TB_OK) return st;
+  }
   const tb_status rs = batch_results(&b, out, (cudaStream_t)stream);
   if (rs == TB_CUDA_ERROR) return rs;
+  if (any_grad) {
+    st = gradient_copy(&b, nullptr, nullptr, out, (cudaStream_t)stream);
+    if (st != TB_OK) return st;
+  }
   if (wfn_inout) {  // also for structures that failed: their records hold their last state
     st = batch_wavefunction(&b, wfn_inout, (cudaStream_t)stream);
     if (st != TB_OK) return st;

@@ -134,6 +134,24 @@ inline size_t oa_smem_bytes(int nmax) {
 __global__ void k_oa_step(DevBatch B, double* G, double* Sm, double* V, double* w, const int* mask,
                           const int* rr_mask);
 
+// nuclear gradient (read-out after the SCF, structures with flag[m] set)
+cudaError_t launch_grad_pairs(const DevParams& P, const DevBatch& B, const int* npair, const int* pair_i,
+                              const int* pair_j, const double* se, const double* Pm, const double* Wm,
+                              const double* vsh, const double* vat, const double* vdp, const double* vqp,
+                              const int* flag, int maxsp, long long items, int lmask, double* item, double* ese_tab,
+                              cudaStream_t st);
+__global__ void k_grad_prep(DevBatch B, const int* flag, const double* focc, const double* w, const double* qsh,
+                            const double* dpat, const double* qpat, double* fe, double* qv);
+__global__ void k_grad_pair_reduce(DevBatch B, const int* npair, const int* pair_i, const int* pair_j,
+                                   const int* flag, int maxsp, long long pair_cap, const double* item, double* G);
+__global__ void k_grad_cn(DevParams P, DevBatch B, const int* flag, const double* Pm, const double* ese_tab,
+                          const double* cn, const double* mrad, const double* qat, const double* dpat,
+                          const double* qpat, double* dEdcn);
+__global__ void k_grad_atoms(DevParams P, DevBatch B, const int* flag, const double* G, const double* dEdcn,
+                             const double* mrad, const double* qsh, const double* qat, const double* dpat,
+                             const double* qpat, double* grad);
+__global__ void k_grad_sigma(DevBatch B, const int* flag, const double* grad, double* sigma);
+
 // SCF
 __global__ void k_scf_init(DevParams P, DevBatch B, const double* charge, const int* uhf, const double* erep,
                            double* n0sh, double* q_in, MolState S);

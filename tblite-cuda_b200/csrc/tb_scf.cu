@@ -686,7 +686,7 @@ __global__ void k_finalize(DevParams P, DevBatch B, const double* __restrict__ c
   }
   err = block_sum(err, red);
   if (tid == 0) {
-    const double elast = S.eelec[m];
+    const double elast = S.eelec[m], prev_error = S.scf_error[m];
     const double eelec = e_band + S.e_ts[m] + e_es2 + e_aes2 + e_es3;
     const double error = sqrt(err / ndim);
     S.eelec[m] = eelec;
@@ -699,11 +699,15 @@ __global__ void k_finalize(DevParams P, DevBatch B, const double* __restrict__ c
     S.iscf[m] = it;
     bool conv = fabs(eelec - elast) < econv && error < pconv;
     if (S.phase) {
-      // mixed-precision form: the mixed phase ends at the loosened test (or
-      // after half the iteration budget), the mixer restarts from the current
-      // point, then at least two FP64 iterations run and the full test decides
+      // mixed-precision form: the mixed phase ends at the loosened test, when
+      // its charge error stops falling (less than halved from the previous
+      // iteration after the third: the FP32 eigenpairs no longer improve the
+      // point), or after half the iteration budget; the mixer restarts from
+      // the current point, then at least two FP64 iterations run and the full
+      // test decides
       if (S.phase[m] == 0) {
-        if ((fabs(eelec - elast) < econv_lo && error < pconv_lo) || 2 * it >= max_iter) {
+        if ((fabs(eelec - elast) < econv_lo && error < pconv_lo) || 2 * it >= max_iter ||
+            (it >= 3 && error > 0.5 * prev_error)) {
           S.phase[m] = 1;
           S.mix_iter[m] = 0;
         }
@@ -853,6 +857,237 @@ __global__ void k_mix_next(DevBatch B, double* __restrict__ q_in, const double* 
     q[i] = v;
   }
   if (tid == 0) S.mix_iter[m] = iter;
+}
+
+// ------------------------------------------------------------ gradient
+// Nuclear gradient and virial (the gradient/sigma outputs of xtb_singlepoint,
+// src/xtb.cu:195-196) of the converged structures with flag[m] set, from the
+// last iteration's density P, coefficients C and orbital energies:
+//   dE/dR = dE_rep/dR + [shell-pair terms: P dH0 - W dS and the Mulliken
+//           moments through dS, dD, dQ, k_grad_pairs_t]
+//         + dE_ES2/dR + dE_AES2/dR at fixed moments + (dE/dCN) dCN/dR,
+// W = C diag(f e) C^T.  Repulsion: get_repulsion_derivs (src/xtb.cu:62-91,
+// quoted); the other terms differentiate the energy expression of the
+// potential and energy kernels above.  Every atom sums its pair terms in a
+// fixed order (no atomics): a structure's gradient is the same alone and in
+// any batch.
+
+// f e (energy-weighted occupations) and the final moments in the mixer layout
+// [qsh, dpat, qpat] (input of k_potential: the potentials dE/dmoment).
+__global__ void k_grad_prep(DevBatch B, const int* __restrict__ flag, const double* __restrict__ focc,
+                            const double* __restrict__ w, const double* __restrict__ qsh,
+                            const double* __restrict__ dpat, const double* __restrict__ qpat, double* __restrict__ fe,
+                            double* __restrict__ qv) {
+  const int m = blockIdx.x;
+  if (!flag[m]) return;
+  const int o0 = B.ooff[m], n = B.ooff[m + 1] - o0;
+  const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0, s0 = B.soff[m], nsh = B.soff[m + 1] - s0;
+  const int mo = B.mixoff[m];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) fe[o0 + i] = focc[o0 + i] * w[o0 + i];
+  for (int i = threadIdx.x; i < nsh; i += blockDim.x) qv[mo + i] = qsh[s0 + i];
+  for (int i = threadIdx.x; i < 3 * nat; i += blockDim.x) qv[mo + nsh + i] = dpat[3 * a0 + i];
+  for (int i = threadIdx.x; i < 6 * nat; i += blockDim.x) qv[mo + nsh + 3 * nat + i] = qpat[6 * a0 + i];
+}
+
+// Sum of a neighbour pair's shell-pair items, in shell-pair order, into the
+// structure's atom-pair table G[i][j] (i > j).
+__global__ void k_grad_pair_reduce(DevBatch B, const int* __restrict__ npair, const int* __restrict__ pair_i,
+                                   const int* __restrict__ pair_j, const int* __restrict__ flag, int maxsp,
+                                   long long pair_cap, const double* __restrict__ item, double* __restrict__ G) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < pair_cap;
+       p += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = B.nmol;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (B.poff[mid] <= p) lo = mid; else hi = mid;
+    }
+    const int m = lo;
+    if (!flag[m] || p - B.poff[m] >= npair[m]) continue;
+    const int nat = B.aoff[m + 1] - B.aoff[m];
+    double g[3] = {0.0, 0.0, 0.0};
+    for (int sp = 0; sp < maxsp; ++sp)
+      for (int x = 0; x < 3; ++x) g[x] += item[3 * (p * maxsp + sp) + x];
+    double* out = G + 3 * (B.a2off[m] + (long long)pair_i[p] * nat + pair_j[p]);
+    for (int x = 0; x < 3; ++x) out[x] = g[x];
+  }
+}
+
+// AES2 energy of the ordered pair (source i, multipole atom j), v = R_i - R_j,
+// and its derivatives along v and with respect to the damping-radius sum
+// (rr = (rad_i + rad_j) / (2 r)):
+//   e = q_i (mu_j.v) g3 f3 + 1/2 [(mu_j.mu_i) g3 - 3 (mu_j.v)(mu_i.v) g5] f5 + q_i (Th_j : tc(v)) g5 f5.
+__device__ inline void aes_pair_grad(const DevParams& P, const double* v, double radi, double radj, double qi,
+                                     const double* mi, const double* mj, const double* tj, double* de,
+                                     double* de_drad) {
+  const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2], r1 = sqrt(r2);
+  const double g1 = 1.0 / r1, g3 = g1 * g1 * g1, g5 = g3 * g1 * g1, g7 = g5 * g1 * g1;
+  const double rr = 0.5 * (radi + radj) * g1, lr = log(rr);
+  const double t3 = 6.0 * exp(P.kdmp3 * lr), t5 = 6.0 * exp(P.kdmp5 * lr);
+  const double f3 = 1.0 / (1.0 + t3), f5 = 1.0 / (1.0 + t5);
+  const double df3 = -P.kdmp3 * t3 / rr * f3 * f3, df5 = -P.kdmp5 * t5 / rr * f5 * f5;
+  const double mjv = mj[0] * v[0] + mj[1] * v[1] + mj[2] * v[2];
+  const double miv = mi[0] * v[0] + mi[1] * v[1] + mi[2] * v[2];
+  const double mm = mj[0] * mi[0] + mj[1] * mi[1] + mj[2] * mi[2];
+  const double tv = tj[0] * v[0] * v[0] + 2.0 * tj[1] * v[0] * v[1] + tj[2] * v[1] * v[1] +
+                    2.0 * tj[3] * v[0] * v[2] + 2.0 * tj[4] * v[1] * v[2] + tj[5] * v[2] * v[2];
+  const double dtv[3] = {2.0 * tj[0] * v[0] + 2.0 * tj[1] * v[1] + 2.0 * tj[3] * v[2],
+                         2.0 * tj[1] * v[0] + 2.0 * tj[2] * v[1] + 2.0 * tj[4] * v[2],
+                         2.0 * tj[3] * v[0] + 2.0 * tj[4] * v[1] + 2.0 * tj[5] * v[2]};
+  const double a_nof = qi * mjv * g3, b_nof = 0.5 * (mm * g3 - 3.0 * mjv * miv * g5), c_nof = qi * tv * g5;
+  for (int k = 0; k < 3; ++k) {
+    const double drr = -rr * v[k] / r2;
+    const double dg3 = -3.0 * g5 * v[k], dg5 = -5.0 * g7 * v[k];
+    const double da = qi * (mj[k] * g3 + mjv * dg3);
+    const double db = 0.5 * (mm * dg3 - 3.0 * (mj[k] * miv + mjv * mi[k]) * g5 - 3.0 * mjv * miv * dg5);
+    const double dc = qi * (dtv[k] * g5 + tv * dg5);
+    de[k] = da * f3 + a_nof * df3 * drr + db * f5 + b_nof * df5 * drr + dc * f5 + c_nof * df5 * drr;
+  }
+  *de_drad = (a_nof * df3 + (b_nof + c_nof) * df5) * g1 * 0.5;
+}
+
+// dE/dCN per atom: its shells' dE/dse (the on-site diagonal of P plus the
+// shell-pair table of k_grad_pairs_t) times dse/dCN = -kcn, and dE/d(damping
+// radius) over all AES2 pairs times dmrad/dCN (get_mrad, src/coulomb.cu:387-398).
+__global__ void k_grad_cn(DevParams P, DevBatch B, const int* __restrict__ flag, const double* __restrict__ Pm,
+                          const double* __restrict__ ese_tab, const double* __restrict__ cn,
+                          const double* __restrict__ mrad, const double* __restrict__ qat,
+                          const double* __restrict__ dpat, const double* __restrict__ qpat,
+                          double* __restrict__ dEdcn) {
+  const int m = blockIdx.x;
+  if (!flag[m]) return;
+  const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0, s0 = B.soff[m], nsh = B.soff[m + 1] - s0;
+  const int o0 = B.ooff[m], n = B.ooff[m + 1] - o0;
+  const long long mo = B.moff[m], so = B.s2off[m];
+  const int A = blockIdx.y * blockDim.x + threadIdx.x;
+  if (A >= nat) return;
+  const SpeciesParam& sa = P.sp[B.id[a0 + A]];
+  const int isa = B.at_ish[a0 + A];
+  double d = 0.0;
+  for (int s = 0; s < sa.nsh; ++s) {
+    const int sh = isa + s;
+    double dse = 0.0;
+    const int i0 = B.sh_iao[s0 + sh], na = msao(P.sh[sa.sh0 + s].ang);
+    for (int x = 0; x < na; ++x) dse += Pm[mo + (long long)(i0 + x) * n + i0 + x];
+    for (int b = 0; b < nsh; ++b) dse += ese_tab[so + (long long)sh * nsh + b];
+    d -= P.sh[sa.sh0 + s].kcn * dse;
+  }
+  const double* xyz = B.xyz + 3 * a0;
+  double drad = 0.0;
+  for (int Bq = 0; Bq < nat; ++Bq) {
+    if (Bq == A) continue;
+    double de[3], dr1, dr2;
+    const double v1[3] = {xyz[3 * A] - xyz[3 * Bq], xyz[3 * A + 1] - xyz[3 * Bq + 1], xyz[3 * A + 2] - xyz[3 * Bq + 2]};
+    const double v2[3] = {-v1[0], -v1[1], -v1[2]};
+    aes_pair_grad(P, v1, mrad[a0 + A], mrad[a0 + Bq], qat[a0 + A], dpat + 3 * (a0 + A), dpat + 3 * (a0 + Bq),
+                  qpat + 6 * (a0 + Bq), de, &dr1);  // source A, multipoles on Bq
+    aes_pair_grad(P, v2, mrad[a0 + Bq], mrad[a0 + A], qat[a0 + Bq], dpat + 3 * (a0 + Bq), dpat + 3 * (a0 + A),
+                  qpat + 6 * (a0 + A), de, &dr2);  // source Bq, multipoles on A
+    drad += dr1 + dr2;
+  }
+  const double t1 = exp(-P.mp_kexp * (cn[a0 + A] - sa.mp_vcn - P.mp_shift));
+  d += drad * (P.mp_rmax - sa.mp_rad) * P.mp_kexp * t1 / ((1.0 + t1) * (1.0 + t1));
+  dEdcn[a0 + A] = d;
+}
+
+// Gradient of atom A: every pair term with A, summed over the other atoms in
+// order -- the shell-pair table G (antisymmetric), repulsion (quoted
+// get_repulsion_derivs), ES2 at fixed shell charges, AES2 at fixed moments
+// (A as source and as multipole atom), and the coordination-number chain.
+__global__ void k_grad_atoms(DevParams P, DevBatch B, const int* __restrict__ flag, const double* __restrict__ G,
+                             const double* __restrict__ dEdcn, const double* __restrict__ mrad,
+                             const double* __restrict__ qsh, const double* __restrict__ qat,
+                             const double* __restrict__ dpat, const double* __restrict__ qpat,
+                             double* __restrict__ grad) {
+  const int m = blockIdx.x;
+  if (!flag[m]) return;
+  const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0, s0 = B.soff[m];
+  const int A = blockIdx.y * blockDim.x + threadIdx.x;
+  if (A >= nat) return;
+  const long long ao = B.a2off[m];
+  const double* xyz = B.xyz + 3 * a0;
+  const SpeciesParam& sa = P.sp[B.id[a0 + A]];
+  const int isa = s0 + B.at_ish[a0 + A];
+  const double ka = 10.0, kb = 20.0, rshift = 2.0;
+  const double cn2 = P.cn_cutoff * P.cn_cutoff, rep2 = P.rep_cutoff * P.rep_cutoff;
+  double g[3] = {0.0, 0.0, 0.0};
+  for (int Bq = 0; Bq < nat; ++Bq) {
+    if (Bq == A) continue;
+    const double v[3] = {xyz[3 * A] - xyz[3 * Bq], xyz[3 * A + 1] - xyz[3 * Bq + 1], xyz[3 * A + 2] - xyz[3 * Bq + 2]};
+    const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    if (r2 < 1.0e-12) continue;
+    const double r1 = sqrt(r2);
+    const SpeciesParam& sb = P.sp[B.id[a0 + Bq]];
+    // shell-pair terms (H0, overlap, Mulliken moments)
+    if (Bq < A) {
+      const double* e = G + 3 * (ao + (long long)A * nat + Bq);
+      for (int k = 0; k < 3; ++k) g[k] += e[k];
+    } else {
+      const double* e = G + 3 * (ao + (long long)Bq * nat + A);
+      for (int k = 0; k < 3; ++k) g[k] -= e[k];
+    }
+    double s = 0.0;  // coefficient of v / r1
+    // repulsion
+    if (r2 <= rep2) {
+      const double alpha = sqrt(sa.rep_alpha * sb.rep_alpha), zeff = sa.rep_zeff * sb.rep_zeff;
+      const double kexp = (sa.z <= 2 && sb.z <= 2) ? P.rep_kexp_light : P.rep_kexp;
+      const double r1k = pow(r1, kexp), r1r = pow(r1, P.rep_rexp);
+      const double dE = zeff * exp(-alpha * r1k) / r1r;
+      s += -(alpha * r1k * kexp + P.rep_rexp) * dE / r1;
+    }
+    // ES2: q_a q_b dgamma/dr over the shells of A and Bq
+    {
+      const int isb = s0 + B.at_ish[a0 + Bq];
+      for (int x = 0; x < sa.nsh; ++x)
+        for (int y = 0; y < sb.nsh; ++y) {
+          const double gam = 0.5 * (P.sh[sa.sh0 + x].hubbard + P.sh[sb.sh0 + y].hubbard);
+          double dg;
+          if (P.gexp == 2.0) {
+            const double b2 = r2 + 1.0 / (gam * gam);
+            dg = -r1 / (b2 * sqrt(b2));
+          } else {
+            const double base = pow(r1, P.gexp) + pow(gam, -P.gexp);
+            dg = -pow(r1, P.gexp - 1.0) * pow(base, -1.0 / P.gexp - 1.0);
+          }
+          s += qsh[isa + x] * qsh[isb + y] * dg;
+        }
+    }
+    // coordination-number chain
+    if (r2 <= cn2) {
+      const double rc = sa.rcov + sb.rcov;
+      const double ea = 1.0 / (1.0 + exp(-ka * (rc / r1 - 1.0)));
+      const double eb = 1.0 / (1.0 + exp(-kb * ((rc + rshift) / r1 - 1.0)));
+      const double dea = -ea * (1.0 - ea) * ka * rc / r2, deb = -eb * (1.0 - eb) * kb * (rc + rshift) / r2;
+      s += (dea * eb + ea * deb) * (dEdcn[a0 + A] + dEdcn[a0 + Bq]);
+    }
+    for (int k = 0; k < 3; ++k) g[k] += s * v[k] / r1;
+    // AES2 at fixed moments: A as source (+), A as multipole atom (-, v = R_Bq - R_A)
+    double de[3], dr;
+    aes_pair_grad(P, v, mrad[a0 + A], mrad[a0 + Bq], qat[a0 + A], dpat + 3 * (a0 + A), dpat + 3 * (a0 + Bq),
+                  qpat + 6 * (a0 + Bq), de, &dr);
+    for (int k = 0; k < 3; ++k) g[k] += de[k];
+    const double vm[3] = {-v[0], -v[1], -v[2]};
+    aes_pair_grad(P, vm, mrad[a0 + Bq], mrad[a0 + A], qat[a0 + Bq], dpat + 3 * (a0 + Bq), dpat + 3 * (a0 + A),
+                  qpat + 6 * (a0 + A), de, &dr);
+    for (int k = 0; k < 3; ++k) g[k] -= de[k];
+  }
+  for (int k = 0; k < 3; ++k) grad[3 * (a0 + A) + k] = g[k];
+}
+
+// Virial sigma[3][3] = sum_A g_A R_A^T per structure (fixed-order block sums).
+__global__ void k_grad_sigma(DevBatch B, const int* __restrict__ flag, const double* __restrict__ grad,
+                             double* __restrict__ sigma) {
+  const int m = blockIdx.x;
+  if (!flag[m]) return;
+  __shared__ double red[32];
+  const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0;
+  for (int ab = 0; ab < 9; ++ab) {
+    const int a = ab / 3, b = ab % 3;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nat; i += blockDim.x) s += grad[3 * (a0 + i) + a] * B.xyz[3 * (a0 + i) + b];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) sigma[9 * m + ab] = s;
+    __syncthreads();
+  }
 }
 
 }  // namespace tb

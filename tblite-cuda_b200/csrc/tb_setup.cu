@@ -462,4 +462,245 @@ cudaError_t launch_integrals(const DevParams& P, const DevBatch& B, const int* n
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- gradient
+// Nuclear gradient, off-site shell pairs (the integral part of the gradient
+// output of xtb_singlepoint, src/xtb.cu:195-196).  The blocks of a shell pair
+// depend on vec = R_i - R_j only; with the moment operator on centre i,
+// d/dvec <phi_j|O_i|phi_i> = <d_r phi_j|O_i|phi_i>: the j function's Cartesian
+// power l along the direction is replaced by l x^(l-1) - 2 a x^(l+1) (the
+// construction of the quoted multipole_grad_3d, src/multipole.cu:326-421,
+// which differentiates the i function with the operator on j).
+
+// 1-D moments of order 0..2 about centre i, powers li <= 2 and lj <= 3.
+__device__ inline void moments_1d_ext(int li, int lj, double rpi, double rpj, const double* s1d, double* v) {
+  double vi[3] = {0, 0, 0}, vj[4] = {0, 0, 0, 0};
+  vi[li] = 1.0;
+  vj[lj] = 1.0;
+  if (li == 1) vi[0] += rpi;
+  if (li == 2) { vi[0] += rpi * rpi; vi[1] += 2.0 * rpi; }
+  if (lj == 1) vj[0] += rpj;
+  if (lj == 2) { vj[0] += rpj * rpj; vj[1] += 2.0 * rpj; }
+  if (lj == 3) { vj[0] += rpj * rpj * rpj; vj[1] += 3.0 * rpj * rpj; vj[2] += 3.0 * rpj; }
+  double vv[6] = {0, 0, 0, 0, 0, 0};
+  for (int x = 0; x <= li; ++x)
+    for (int y = 0; y <= lj; ++y) vv[x + y] += vi[x] * vj[y];
+  double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+  for (int l = 0; l <= li + lj; ++l) {
+    v0 += s1d[l] * vv[l];
+    v1 += (s1d[l + 1] + rpi * s1d[l]) * vv[l];
+    v2 += (s1d[l + 2] + 2.0 * rpi * s1d[l + 1] + rpi * rpi * s1d[l]) * vv[l];
+  }
+  v[0] = v0; v[1] = v1; v[2] = v2;
+}
+
+// Values (t = 0) and vec derivatives (t = 1..3) of one shell pair's blocks:
+// s[t][SI*SJ], d[t][3*SI*SJ], q[t][6*SI*SJ] (spherical, quadrupole traceless).
+template <int LI, int LJ>
+__device__ void multipole_cgto_grad(const ShellParam* __restrict__ ci, const ShellParam* __restrict__ cj, double r2,
+                                    const double* vec, double intcut, double (*s)[(2 * LI + 1) * (2 * LJ + 1)],
+                                    double (*d)[3 * (2 * LI + 1) * (2 * LJ + 1)],
+                                    double (*q)[6 * (2 * LI + 1) * (2 * LJ + 1)]) {
+  constexpr int MI = (LI + 1) * (LI + 2) / 2, MJ = (LJ + 1) * (LJ + 2) / 2;
+  constexpr int SI = 2 * LI + 1, SJ = 2 * LJ + 1;
+  double c3[4][10][MI * MJ];  // [t][s, d(3), q(6)][cartesian pair]
+  for (int t = 0; t < 4; ++t)
+    for (int k = 0; k < 10; ++k)
+      for (int x = 0; x < MI * MJ; ++x) c3[t][k][x] = 0.0;
+  const double sqrtpi3 = 5.568327996831708;
+  for (int ip = 0; ip < ci->nprim; ++ip) {
+    const double ai = ci->alpha[ip], cci = ci->coeff[ip];
+    for (int jp = 0; jp < cj->nprim; ++jp) {
+      const double aj = cj->alpha[jp];
+      const double eab = ai + aj, oab = 1.0 / eab;
+      const double est = ai * aj * r2 * oab;
+      if (est > intcut) continue;
+      const double cc = cci * cj->coeff[jp] * exp(-est) * sqrtpi3 * oab * sqrt(oab);
+      double rpi[3], rpj[3];
+      for (int k = 0; k < 3; ++k) { rpi[k] = -vec[k] * aj * oab; rpj[k] = vec[k] * ai * oab; }
+      const double h = 0.5 * oab;
+      double s1d[8] = {1.0, 0.0, h, 0.0, 3.0 * h * h, 0.0, 15.0 * h * h * h, 0.0};
+      for (int a = 0; a < MI; ++a) {
+        for (int b = 0; b < MJ; ++b) {
+          const int* la = c_lx[lmap(LI) + a];
+          const int* lb = c_lx[lmap(LJ) + b];
+          double v[3][3], g[3][3];
+          for (int k = 0; k < 3; ++k) {
+            moments_1d_ext(la[k], lb[k], rpi[k], rpj[k], s1d, v[k]);
+            double up[3], dn[3] = {0.0, 0.0, 0.0};
+            moments_1d_ext(la[k], lb[k] + 1, rpi[k], rpj[k], s1d, up);
+            if (lb[k] > 0) moments_1d_ext(la[k], lb[k] - 1, rpi[k], rpj[k], s1d, dn);
+            for (int o = 0; o < 3; ++o) g[k][o] = lb[k] * dn[o] - 2.0 * aj * up[o];
+          }
+          const int x = a * MJ + b;
+          for (int t = 0; t < 4; ++t) {
+            const double* fx = (t == 1) ? g[0] : v[0];
+            const double* fy = (t == 2) ? g[1] : v[1];
+            const double* fz = (t == 3) ? g[2] : v[2];
+            c3[t][0][x] += cc * (fx[0] * fy[0] * fz[0]);
+            c3[t][1][x] += cc * (fx[1] * fy[0] * fz[0]);
+            c3[t][2][x] += cc * (fx[0] * fy[1] * fz[0]);
+            c3[t][3][x] += cc * (fx[0] * fy[0] * fz[1]);
+            c3[t][4][x] += cc * (fx[2] * fy[0] * fz[0]);
+            c3[t][5][x] += cc * (fx[1] * fy[1] * fz[0]);
+            c3[t][6][x] += cc * (fx[0] * fy[2] * fz[0]);
+            c3[t][7][x] += cc * (fx[1] * fy[0] * fz[1]);
+            c3[t][8][x] += cc * (fx[0] * fy[1] * fz[1]);
+            c3[t][9][x] += cc * (fx[0] * fy[0] * fz[2]);
+          }
+        }
+      }
+    }
+  }
+  for (int t = 0; t < 4; ++t) {
+    double tmp[SI * SJ];
+    transform0<LI, LJ>(c3[t][0], s[t]);
+    for (int k = 0; k < 3; ++k) {
+      transform0<LI, LJ>(c3[t][1 + k], tmp);
+      for (int x = 0; x < SI * SJ; ++x) d[t][3 * x + k] = tmp[x];
+    }
+    for (int k = 0; k < 6; ++k) {
+      transform0<LI, LJ>(c3[t][4 + k], tmp);
+      for (int x = 0; x < SI * SJ; ++x) q[t][6 * x + k] = tmp[x];
+    }
+    for (int x = 0; x < SI * SJ; ++x) {
+      double* qq = q[t] + 6 * x;
+      const double tr = 0.5 * (qq[0] + qq[2] + qq[5]);
+      qq[0] = 1.5 * qq[0] - tr; qq[1] = 1.5 * qq[1]; qq[2] = 1.5 * qq[2] - tr;
+      qq[3] = 1.5 * qq[3]; qq[4] = 1.5 * qq[4]; qq[5] = 1.5 * qq[5] - tr;
+    }
+  }
+}
+
+// Derivative along vec_x of shift_operator's output (dj, qj) from the
+// derivatives ds, ddi[3], dqi[6] of its inputs along x.
+__device__ inline void shift_operator_grad(const double* vec, int x, double s, const double* di, double ds,
+                                           const double* ddi, const double* dqi, double* ddj, double* dqj) {
+  double e[3] = {0.0, 0.0, 0.0};
+  e[x] = 1.0;
+  for (int k = 0; k < 3; ++k) ddj[k] = ddi[k] + e[k] * s + vec[k] * ds;
+  const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 1, 2, 2, 2};
+  double dt[6];
+  for (int c = 0; c < 6; ++c) {
+    const int a = pa[c], b = pb[c];
+    if (a == b)
+      dt[c] = 2.0 * e[a] * di[a] + 2.0 * vec[a] * ddi[a] + 2.0 * vec[a] * e[a] * s + vec[a] * vec[a] * ds;
+    else
+      dt[c] = e[a] * di[b] + vec[a] * ddi[b] + e[b] * di[a] + vec[b] * ddi[a] + (e[a] * vec[b] + vec[a] * e[b]) * s +
+              vec[a] * vec[b] * ds;
+  }
+  const double tr = 0.5 * (dt[0] + dt[2] + dt[5]);
+  dqj[0] = dqi[0] + 1.5 * dt[0] - tr;
+  dqj[1] = dqi[1] + 1.5 * dt[1];
+  dqj[2] = dqi[2] + 1.5 * dt[2] - tr;
+  dqj[3] = dqi[3] + 1.5 * dt[3];
+  dqj[4] = dqi[4] + 1.5 * dt[4];
+  dqj[5] = dqi[5] + 1.5 * dt[5] - tr;
+}
+
+// One thread per (neighbour pair, shell pair) as k_integrals_t, structures
+// with flag[m] set.  dE/dvec of the pair's blocks:
+//   2 P (h_ij - (v_mu + v_nu)/2) dS - 2 W dS + 2 P S dh_ij (shpoly(rr))
+//   - P (vdp(i) dD_i + vqp(i) dQ_i + vdp(j) dD_j + vqp(j) dQ_j),
+// D_j, Q_j the operator shifted to centre j (shift_operator); written to
+// item[p * maxsp + sp][3].  ese = sum P S hscale shpoly is dE/dse of both
+// shells (written to the structure's shell-pair table at (i, j) and (j, i)).
+template <int LI, int LJ>
+__global__ void k_grad_pairs_t(DevParams P, DevBatch B, const int* __restrict__ npair, const int* __restrict__ pair_i,
+                               const int* __restrict__ pair_j, const double* __restrict__ se,
+                               const double* __restrict__ Pm, const double* __restrict__ Wm,
+                               const double* __restrict__ vsh, const double* __restrict__ vat,
+                               const double* __restrict__ vdp, const double* __restrict__ vqp,
+                               const int* __restrict__ flag, int maxsp, long long total_items,
+                               double* __restrict__ item, double* __restrict__ ese_tab) {
+  constexpr int SI = 2 * LI + 1, SJ = 2 * LJ + 1;
+  for (long long it = blockIdx.x * (long long)blockDim.x + threadIdx.x; it < total_items;
+       it += (long long)gridDim.x * blockDim.x) {
+    const long long p = it / maxsp;
+    const int sp = (int)(it % maxsp);
+    int lo = 0, hi = B.nmol;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (B.poff[mid] <= p) lo = mid; else hi = mid;
+    }
+    const int m = lo;
+    if (!flag[m] || p - B.poff[m] >= npair[m]) continue;
+    const int a0 = B.aoff[m];
+    const int iat = pair_i[p], jat = pair_j[p];
+    const SpeciesParam& spi = P.sp[B.id[a0 + iat]];
+    const SpeciesParam& spj = P.sp[B.id[a0 + jat]];
+    if (sp >= spi.nsh * spj.nsh) continue;
+    const int ish = sp / spj.nsh, jsh = sp % spj.nsh;
+    const int ti = spi.sh0 + ish, tj = spj.sh0 + jsh;
+    const ShellParam* ci = P.sh + ti;
+    const ShellParam* cj = P.sh + tj;
+    if (ci->ang != LI || cj->ang != LJ) continue;
+    const int n = B.ooff[m + 1] - B.ooff[m], o0 = B.ooff[m], s0 = B.soff[m];
+    const long long mo = B.moff[m];
+    const int is = s0 + B.at_ish[a0 + iat], js = s0 + B.at_ish[a0 + jat];
+    const int ii = B.sh_iao[is + ish], jj = B.sh_iao[js + jsh];
+    const double vec[3] = {B.xyz[3 * (a0 + iat)] - B.xyz[3 * (a0 + jat)],
+                           B.xyz[3 * (a0 + iat) + 1] - B.xyz[3 * (a0 + jat) + 1],
+                           B.xyz[3 * (a0 + iat) + 2] - B.xyz[3 * (a0 + jat) + 2]};
+    const double r2 = vec[0] * vec[0] + vec[1] * vec[1] + vec[2] * vec[2];
+    const double r1 = sqrt(r2), radsum = spj.rad + spi.rad;
+    const double rr = sqrt(r1 / radsum);
+    const double shpoly = (1.0 + ci->shpoly * rr) * (1.0 + cj->shpoly * rr);
+    const double dshpoly = ci->shpoly * (1.0 + cj->shpoly * rr) + cj->shpoly * (1.0 + ci->shpoly * rr);
+    const double hs = P.hscale[ti * P.nshtype + tj];
+    const double sesum = 0.5 * (se[is + ish] + se[js + jsh]);
+    const double hij = sesum * hs * shpoly;
+    double s[4][SI * SJ], d[4][3 * SI * SJ], q[4][6 * SI * SJ];
+    multipole_cgto_grad<LI, LJ>(ci, cj, r2, vec, P.intcut, s, d, q);
+    const double* vdi = vdp + 3 * (a0 + iat);
+    const double* vdj = vdp + 3 * (a0 + jat);
+    const double* vqi = vqp + 6 * (a0 + iat);
+    const double* vqj = vqp + 6 * (a0 + jat);
+    double gx[3] = {0.0, 0.0, 0.0}, ese = 0.0;
+    for (int iao = 0; iao < SI; ++iao) {
+      const int nu = ii + iao;
+      const double vnu = vsh[s0 + B.ao_sh[o0 + nu]] + vat[a0 + B.ao_at[o0 + nu]];
+      for (int jao = 0; jao < SJ; ++jao) {
+        const int ij = iao * SJ + jao;
+        const int mu = jj + jao;
+        const long long e1 = mo + (long long)mu * n + nu;
+        const double pij = Pm[e1], wij = Wm[e1];
+        const double vmu = vsh[s0 + B.ao_sh[o0 + mu]] + vat[a0 + B.ao_at[o0 + mu]];
+        ese += pij * s[0][ij] * hs * shpoly;
+        for (int x = 0; x < 3; ++x) {
+          const double drr = 0.5 / rr / radsum * vec[x] / r1;
+          double g = 2.0 * pij * (hij - 0.5 * (vmu + vnu)) * s[1 + x][ij] - 2.0 * wij * s[1 + x][ij];
+          g += 2.0 * pij * s[0][ij] * sesum * hs * dshpoly * drr;
+          double ddj[3], dqj[6];
+          shift_operator_grad(vec, x, s[0][ij], d[0] + 3 * ij, s[1 + x][ij], d[1 + x] + 3 * ij, q[1 + x] + 6 * ij,
+                              ddj, dqj);
+          for (int k = 0; k < 3; ++k) g -= pij * (vdi[k] * d[1 + x][3 * ij + k] + vdj[k] * ddj[k]);
+          for (int c = 0; c < 6; ++c) g -= pij * (vqi[c] * q[1 + x][6 * ij + c] + vqj[c] * dqj[c]);
+          gx[x] += g;
+        }
+      }
+    }
+    for (int x = 0; x < 3; ++x) item[3 * it + x] = gx[x];
+    const int nsh = B.soff[m + 1] - s0;
+    const long long so = B.s2off[m];
+    ese_tab[so + (long long)(is - s0 + ish) * nsh + (js - s0 + jsh)] = ese;
+    ese_tab[so + (long long)(js - s0 + jsh) * nsh + (is - s0 + ish)] = ese;
+  }
+}
+
+cudaError_t launch_grad_pairs(const DevParams& P, const DevBatch& B, const int* npair, const int* pair_i,
+                              const int* pair_j, const double* se, const double* Pm, const double* Wm,
+                              const double* vsh, const double* vat, const double* vdp, const double* vqp,
+                              const int* flag, int maxsp, long long items, int lmask, double* item, double* ese_tab,
+                              cudaStream_t st) {
+  const int grid = (int)std::max(1LL, std::min((items + 127) / 128, 148LL * 16));
+#define TB_LAUNCH_GRAD(A, C)                                                                                   \
+  if ((lmask >> A & 1) && (lmask >> C & 1))                                                                    \
+    k_grad_pairs_t<A, C><<<grid, 128, 0, st>>>(P, B, npair, pair_i, pair_j, se, Pm, Wm, vsh, vat, vdp, vqp, flag, \
+                                               maxsp, items, item, ese_tab);
+  TB_LAUNCH_GRAD(0, 0) TB_LAUNCH_GRAD(0, 1) TB_LAUNCH_GRAD(1, 0) TB_LAUNCH_GRAD(1, 1)
+  TB_LAUNCH_GRAD(0, 2) TB_LAUNCH_GRAD(2, 0) TB_LAUNCH_GRAD(1, 2) TB_LAUNCH_GRAD(2, 1) TB_LAUNCH_GRAD(2, 2)
+#undef TB_LAUNCH_GRAD
+  return cudaGetLastError();
+}
+
 }  // namespace tb

@@ -46,7 +46,7 @@ class Result(C.Structure):
                 ("e_aes2", C.c_double), ("e_es3", C.c_double), ("dipole", C.c_double * 3),
                 ("scf_error", C.c_double), ("iterations", C.c_int32), ("status", C.c_int32),
                 ("nsh", C.c_int32), ("nao", C.c_int32), ("qat", _dp), ("qsh", _dp), ("dpat", _dp),
-                ("qpat", _dp)]
+                ("qpat", _dp), ("gradient", _dp), ("sigma", C.c_double * 9)]
 
 
 class Wavefunction(C.Structure):
@@ -65,7 +65,7 @@ EXPORTS = [
     "tb_atomic_properties", "tb_repulsion", "tb_get_hamiltonian", "tb_coulomb_potential",
     "tb_add_pot_to_h1", "tb_sygvd_batch", "tb_fermi_filling", "tb_batch_profile",
     "tb_server_create", "tb_server_submit", "tb_server_step", "tb_server_poll", "tb_server_destroy",
-    "tb_batch_set_guess", "tb_batch_wavefunction", "tb_sygvd_noalloc",
+    "tb_batch_set_guess", "tb_batch_wavefunction", "tb_batch_gradient", "tb_sygvd_noalloc",
 ]
 
 _lib = None
@@ -136,7 +136,7 @@ _RESULT_DT = _record_dtype(Result, dict(
     {k: np.float64 for k in ("energy", "e_rep", "e_elec", "e_band", "e_ts", "e_es2", "e_aes2", "e_es3",
                              "scf_error")},
     dipole=(np.float64, 3), iterations=np.int32, status=np.int32, nsh=np.int32, nao=np.int32,
-    qat=np.uintp, qsh=np.uintp, dpat=np.uintp, qpat=np.uintp))
+    qat=np.uintp, qsh=np.uintp, dpat=np.uintp, qpat=np.uintp, gradient=np.uintp, sigma=(np.float64, 9)))
 
 
 def _structs(mols):
@@ -198,7 +198,7 @@ class Calculator:
         return load_library().tb_get_cutoff(self.h, C.c_double(accuracy))
 
     def singlepoint_batch(self, mols, stream=None, raise_on_error=False, wavefunction=False, guess=None, nspin=1,
-                          **opts):
+                          gradient=False, **opts):
         """Run xtb_singlepoint for every structure; returns a list of result dicts.
 
         wavefunction=True adds r["wfn"] (the tb_wavefunction record as a dict:
@@ -206,7 +206,8 @@ class Calculator:
         a list (one entry per structure, None for the default start) of dicts
         with qsh, dpat and qpat to start the SCF from, e.g. an earlier result.
         nspin=2 returns the wavefunction in the open-shell representation
-        (leading channel index on every array, see tb_wavefunction)."""
+        (leading channel index on every array, see tb_wavefunction).
+        gradient=True adds r["gradient"] ([nat][3], Eh/Bohr) and r["sigma"] (3x3)."""
         L = load_library()
         arr, keep = _structs(mols)
         o = default_options(**opts)
@@ -228,12 +229,14 @@ class Calculator:
             np.cumsum(nsh[:-1], out=soff[1:])
         na, ns = int(nat.sum()), int(nsh.sum())
         qat, qsh, dpat, qpat = np.zeros(na), np.zeros(ns), np.zeros((na, 3)), np.zeros((na, 6))
+        grad = np.zeros((na, 3)) if gradient else None
         v = np.frombuffer(res, dtype=_RESULT_DT) if n else None
         if n:
             v["qat"] = qat.ctypes.data + 8 * off
             v["qsh"] = qsh.ctypes.data + 8 * soff
             v["dpat"] = dpat.ctypes.data + 24 * off
             v["qpat"] = qpat.ctypes.data + 48 * off
+            v["gradient"] = grad.ctypes.data + 24 * off if gradient else 0
         wfn, wbufs = None, None
         if n and (wavefunction or guess is not None):
             wfn, wbufs = _wavefunction_records(self, mols, guess, wavefunction, nspin)
@@ -255,6 +258,8 @@ class Calculator:
             d = {k: c[i] for k, c in zip(keys, cols)}
             a0, a1 = a0s[i], a1s[i]
             d.update(dipole=dip[i], qat=qat[a0:a1], qsh=qsh[s0s[i]:s1s[i]], dpat=dpat[a0:a1], qpat=qpat[a0:a1])
+            if gradient:
+                d.update(gradient=grad[a0:a1], sigma=v["sigma"][i].reshape(3, 3).copy())
             if wavefunction:
                 w = wfn[i]
                 d["wfn"] = dict(wbufs[i], nspin=w.nspin, nat=w.nat, nsh=w.nsh, nao=w.nao, homo=list(w.homo),
@@ -346,6 +351,15 @@ class Batch:
             nm = names.raw[32 * i:32 * (i + 1)].split(b"\0", 1)[0].decode()
             out[nm] = (int(la[i]), float(ms[i]), float(wk[i]), {0: None, 1: "flop", 2: "byte"}[un[i]])
         return out
+
+    def gradient(self, stream=None):
+        """Analytic gradient of the last run: ([nat_tot][3] packed over the batch, [nmol][3][3] sigma)."""
+        na = sum(m.nat for m in self.mols)
+        g = np.zeros((na, 3))
+        sg = np.zeros((len(self.mols), 3, 3))
+        check(load_library().tb_batch_gradient(self.h, g.ctypes.data_as(_dp), sg.ctypes.data_as(_dp),
+                                                C.c_void_p(stream or 0)), "tb_batch_gradient")
+        return g, sg
 
     def results(self, stream=None):
         L = load_library()
