@@ -157,6 +157,22 @@ void tb_default_options(tb_options* opt);
 /* Text of the last error on this thread. */
 const char* tb_last_error(void);
 
+/* Autotuner (no counterpart in the reference, whose only eigensolver is a
+ * one-thread Jacobi, src/lapack/sygvd.cu:74-133).  The per-size eigensolver
+ * variant is measured once per calculator, on first need: structures of at
+ * most 32 AOs use a one-warp Jacobi solver up to the largest size at which
+ * it is measured faster than the one-CTA solver (Householder + implicit QL
+ * below 64 AOs, + divide and conquer from 64); above 1216 AOs, and above a
+ * size chosen per batch from measured cost models, cuSOLVER Xsyevd (see
+ * tb_options.solver).  The choice depends on the size only, so a structure
+ * gives the same bits alone and in any batch.
+ * tb_calculator_set_small_solver: jacobi_max -1 (default) measured choice,
+ * 0 never, 1..32 fixed bound.  tb_calculator_tuning writes the measurements
+ * and choices as JSON text into buf (NUL-terminated, at most len bytes) and
+ * returns the full length. */
+tb_status tb_calculator_set_small_solver(tb_calculator* calc, int32_t jacobi_max);
+int32_t tb_calculator_tuning(const tb_calculator* calc, char* buf, int32_t len);
+
 /* basis_type sizes (src/basis/type.h:56-73). */
 tb_status tb_basis_size(const tb_calculator* calc, const tb_structure* mol, int32_t* nsh, int32_t* nao);
 

@@ -58,6 +58,7 @@ struct DevBatch {
   const long long* a2off;  // atom-pair table offset (nat^2 per structure), may be null
   int lib_above;         // 0: every structure on the in-house kernels; else structures with N > lib_above
                          // (all of them when -1) are factorised and diagonalised by the library path
+  int jacobi_max;        // structures of N <= jacobi_max use the one-warp Jacobi eigensolver (0: none)
 };
 
 // True when structure size n is handled by the library (cuSOLVER) path.

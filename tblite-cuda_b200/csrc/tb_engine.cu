@@ -226,7 +226,17 @@ struct tb_calculator {
     bool ready = false;
     double a = 0, b = 0;  // in-house latency of one structure: a N^2 + b N^3 seconds
     double c = 0, d = 0;  // one cuSOLVER call: c + d N^3 seconds
+    double t_in[2] = {0, 0}, t_lib[2] = {0, 0};  // the measured points (256/512 and 256/1024 AOs)
   } eig;
+  // small structures: the one-warp Jacobi variant against the one-CTA
+  // eigensolver, measured once per calculator (batched throughput per size)
+  struct SmallModel {
+    bool ready = false;
+    int jacobi_max = 0;              // chosen: Jacobi for N <= jacobi_max
+    std::vector<int> n;              // measured sizes
+    std::vector<double> t_cta, t_warp;  // seconds per structure in a full batch
+  } small;
+  int jacobi_override = -1;  // -1: measured choice; 0: never; 1..32: fixed bound
   std::mutex tune_mu;
   // pinned staging buffer for the batch metadata upload, reused across batches
   std::mutex stage_mu;
@@ -306,6 +316,8 @@ struct tb_batch {
   // nspin = 2 read-out: per-channel occupations (3 x nao_tot) and structure flags
   double* d_fspin = nullptr;
   int* d_wflag = nullptr;
+  int* d_jlist = nullptr;  // structures on the one-warp Jacobi eigensolver
+  int njac = 0;
   int4 *d_tiles64, *d_tiles32, *d_tiles128;
   int2* d_chunks32;
   int* h_nactive = nullptr;  // pinned
@@ -360,6 +372,7 @@ template <typename T>
 T* at(char* base, size_t off) { return reinterpret_cast<T*>(base + off); }
 
 tb_status calibrate_eigensolvers(tb_calculator* c);
+tb_status calibrate_small(tb_calculator* c);
 
 // Automatic eigensolver choice for a batch (tb_options.solver = 0): the k
 // largest structures go to cuSOLVER, the rest to the batched in-house solver,
@@ -547,6 +560,24 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
       b->nmax_in = std::max(b->nmax_in, n);
     }
   }
+  // small structures: the one-warp Jacobi variant up to the measured (or set) bound
+  int jacobi_max = 0;
+  std::vector<int> jlist;
+  {
+    int nmin = 1 << 30;
+    for (int m = 0; m < nmol; ++m) nmin = std::min(nmin, b->h_ooff[m + 1] - b->h_ooff[m]);
+    if (calc->jacobi_override >= 0) {
+      jacobi_max = std::min(calc->jacobi_override, kJacobiMaxN);
+    } else if (nmin <= kJacobiMaxN) {
+      const tb_status ts = calibrate_small(calc);
+      if (ts != TB_OK) return ts;
+      jacobi_max = calc->small.jacobi_max;
+    }
+    for (int m = 0; m < nmol; ++m) {
+      const int n = b->h_ooff[m + 1] - b->h_ooff[m];
+      if (n <= jacobi_max && !(lib_above != 0 && n > lib_above)) jlist.push_back(m);
+    }
+  }
   b->lib_bytes = 0;
   if (!b->big.empty()) {
     const std::string e = b->lib.workspace(nbig_max, &b->lib_bytes);
@@ -572,7 +603,8 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
          o_aosh = L.add(NO * I4), o_t64 = L.add(b->tiles64.size() * sizeof(int4)),
          o_t128 = L.add(b->tiles128.size() * sizeof(int4)),
          o_t32 = L.add(b->tiles32.size() * sizeof(int4)), o_c32 = L.add(b->chunks32.size() * sizeof(int2)),
-         o_charge = L.add(NM * D8), o_uhf = L.add(NM * I4), o_order = L.add(NM * I4);
+         o_charge = L.add(NM * D8), o_uhf = L.add(NM * I4), o_order = L.add(NM * I4),
+         o_jlist = L.add(NM * I4);
   const size_t meta_end = L.total;
   size_t o_gtab = L.add((size_t)b->h_s2off[nmol] * D8), o_atab = L.add((size_t)b->h_a2off[nmol] * 3 * D8);
   size_t o_cn = L.add(NA * D8), o_mrad = L.add(NA * D8), o_erep = L.add(NA * D8), o_se = L.add(NS * D8),
@@ -661,6 +693,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
     return b->h_ooff[a + 1] - b->h_ooff[a] > b->h_ooff[c + 1] - b->h_ooff[c];
   });
   put(o_order, order.data(), NM * I4);
+  if (!jlist.empty()) put(o_jlist, jlist.data(), jlist.size() * I4);
   TB_CUDA(cudaMemcpy(base, blob, meta_end, cudaMemcpyHostToDevice));
 
   DevBatch& d = b->db;
@@ -675,6 +708,9 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   d.ao_sh = at<int>(base, o_aosh);
   d.order = at<int>(base, o_order);
   d.lib_above = lib_above;
+  d.jacobi_max = jacobi_max;
+  b->d_jlist = at<int>(base, o_jlist);
+  b->njac = (int)jlist.size();
   b->lib_work = base + o_lwork;
   b->lib_info = at<int>(base, o_linfo);
   if (b->mixed) {
@@ -826,6 +862,10 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
   // FP64 phase: the FP64 eigensolver (eigenvectors as rows of Z, W as its scratch)
   TB_K("syev", 4.0 * n3_hi, 1,
        k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->W, b->w, b->perm, S.status, hi));
+  if (b->njac > 0)
+    TB_K("syev_jacobi", 0, 0,
+         k_syev_jacobi<<<nblk(b->njac, kJacobiWarps), kJacobiWarps * 32, jacobi_smem_bytes(), st>>>(
+             B, b->F, b->Z, b->w, b->perm, S.status, hi, b->d_jlist, b->njac));
   for (size_t k = 0; k < b->big.size(); ++k) {
     const int m = b->big[k], n = b->h_ooff[m + 1] - b->h_ooff[m];
     if (!b->h_active[m] || b->h_status[m] != kStOk) continue;
@@ -888,7 +928,7 @@ tb_status raise_smem_limits() {
   TB_CUDA(cudaGetDevice(&dev));
   TB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   const void* ks[] = {(const void*)k_syev, (const void*)k_syev_f32, (const void*)k_fermi, (const void*)k_oa_step,
-                      (const void*)k_gemm_tc, (const void*)k_fock};
+                      (const void*)k_gemm_tc, (const void*)k_fock, (const void*)k_syev_jacobi};
   for (const void* k : ks) {
     cudaFuncAttributes a;
     TB_CUDA(cudaFuncGetAttributes(&a, k));
@@ -991,7 +1031,108 @@ tb_status calibrate_eigensolvers(tb_calculator* c) {
   c->eig.b = std::max(0.0, (n1 * n1 * t2 - n2 * n2 * t1) / det);
   c->eig.d = std::max(0.0, (l2 - l1) / (m2 * m2 * m2 - m1 * m1 * m1));
   c->eig.c = std::max(0.0, l1 - c->eig.d * m1 * m1 * m1);
+  c->eig.t_in[0] = t1; c->eig.t_in[1] = t2;
+  c->eig.t_lib[0] = l1; c->eig.t_lib[1] = l2;
   c->eig.ready = true;
+  return TB_OK;
+}
+
+// Measures, once per calculator, the batched throughput of the one-CTA
+// eigensolver (k_syev, implicit QL below 64 AOs) and the one-warp Jacobi
+// variant (k_syev_jacobi) at N = 8, 12, ..., 32: 592 deterministic random
+// symmetric matrices per size (four per SM), the same inputs for both, the
+// faster of two timed launches each.  The warp variant is chosen up to the
+// largest N below which it is faster at every measured size.
+tb_status calibrate_small(tb_calculator* c) {
+  std::lock_guard<std::mutex> lk(c->tune_mu);
+  if (c->small.ready) return TB_OK;
+  {
+    const tb_status ss = raise_smem_limits();
+    if (ss != TB_OK) return ss;
+  }
+  const int cnt = 592, NM = kJacobiMaxN;
+  const size_t nn = (size_t)cnt * NM * NM;
+  Arena ar;
+  Layout L;
+  const size_t oA0 = L.add(nn * 8), oA = L.add(nn * 8), oZ = L.add(nn * 8), oW = L.add(nn * 8),
+               ow = L.add((size_t)cnt * NM * 8), op = L.add((size_t)cnt * NM * 4), os = L.add(cnt * 4),
+               oo = L.add((cnt + 1) * 4), om = L.add((cnt + 1) * 8), ol = L.add(cnt * 4);
+  TB_CUDA(ar.reserve(L.total));
+  char* base = ar.base;
+  std::vector<double> h(nn);
+  std::vector<int> oo_h(cnt + 1), list(cnt);
+  std::vector<long long> om_h(cnt + 1);
+  uint64_t x = 0x2545f4914f6cdd1dull;
+  auto rnd = [&]() {  // xorshift64*, uniform in (-1, 1)
+    x ^= x >> 12; x ^= x << 25; x ^= x >> 27;
+    return (double)((x * 0x2545f4914f6cdd1dull) >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+  };
+  for (int i = 0; i < cnt; ++i) list[i] = i;
+  TB_CUDA(cudaMemcpy(base + ol, list.data(), cnt * 4, cudaMemcpyHostToDevice));
+  cudaEvent_t e0, e1;
+  TB_CUDA(cudaEventCreate(&e0));
+  TB_CUDA(cudaEventCreate(&e1));
+  tb_status st = TB_OK;
+  std::vector<int> sizes = {8, 12, 16, 20, 24, 28, 32};
+  std::vector<double> tc(sizes.size()), tw(sizes.size());
+  for (size_t si = 0; si < sizes.size() && st == TB_OK; ++si) {
+    const int n = sizes[si];
+    for (int k = 0; k < cnt; ++k) {
+      oo_h[k] = k * n;
+      om_h[k] = (long long)k * n * n;
+      double* M = h.data() + (size_t)k * n * n;
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j <= i; ++j) M[(size_t)i * n + j] = M[(size_t)j * n + i] = rnd();
+    }
+    oo_h[cnt] = cnt * n;
+    om_h[cnt] = (long long)cnt * n * n;
+    const size_t bytes = (size_t)cnt * n * n * 8;
+    if (cudaMemcpy(base + oA0, h.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(base + oo, oo_h.data(), (cnt + 1) * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(base + om, om_h.data(), (cnt + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+      st = fail(TB_CUDA_ERROR, "small eigensolver calibration: upload");
+      break;
+    }
+    DevBatch Bk{};
+    Bk.nmol = cnt;
+    Bk.ooff = at<int>(base, oo);
+    Bk.moff = at<long long>(base, om);
+    float best[2] = {1e30f, 1e30f};
+    for (int variant = 0; variant < 2; ++variant)
+      for (int rep = 0; rep < 2; ++rep) {
+        cudaMemcpy(base + oA, base + oA0, bytes, cudaMemcpyDeviceToDevice);
+        cudaMemset(base + os, 0, cnt * 4);
+        cudaEventRecord(e0);
+        if (variant == 0)
+          k_syev<<<cnt, kEigThreads, syev_smem_bytes(n)>>>(Bk, at<double>(base, oA), at<double>(base, oZ),
+                                                           at<double>(base, oW), at<double>(base, ow),
+                                                           at<int>(base, op), at<int>(base, os), nullptr);
+        else
+          k_syev_jacobi<<<nblk(cnt, kJacobiWarps), kJacobiWarps * 32, jacobi_smem_bytes()>>>(
+              Bk, at<double>(base, oA), at<double>(base, oZ), at<double>(base, ow), at<int>(base, op),
+              at<int>(base, os), nullptr, at<int>(base, ol), cnt);
+        cudaEventRecord(e1);
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess ||
+            cudaGetLastError() != cudaSuccess) {
+          st = fail(TB_CUDA_ERROR, "small eigensolver calibration: launch");
+          break;
+        }
+        best[variant] = std::min(best[variant], ms);
+      }
+    tc[si] = best[0] * 1e-3 / cnt;
+    tw[si] = best[1] * 1e-3 / cnt;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != TB_OK) return st;
+  int jmax = 0;
+  for (size_t si = 0; si < sizes.size() && tw[si] < tc[si]; ++si) jmax = sizes[si];
+  c->small.n = sizes;
+  c->small.t_cta = tc;
+  c->small.t_warp = tw;
+  c->small.jacobi_max = jmax;
+  c->small.ready = true;
   return TB_OK;
 }
 
@@ -1143,6 +1284,10 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
     // symmetric eigensolve with vectors: canonical 4 N^3
     TB_K("syev", 4.0 * n3, 1,
          k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->W, b->w, b->perm, S.status, S.active));
+    if (b->njac > 0)
+      TB_K("syev_jacobi", 0, 0,
+           k_syev_jacobi<<<nblk(b->njac, kJacobiWarps), kJacobiWarps * 32, jacobi_smem_bytes(), st>>>(
+               B, b->F, b->Z, b->w, b->perm, S.status, S.active, b->d_jlist, b->njac));
     for (size_t k = 0; k < b->big.size(); ++k) {
       const int m = b->big[k], n = b->h_ooff[m + 1] - b->h_ooff[m];
       if (!b->h_active[m] || b->h_status[m] != kStOk) continue;
@@ -1671,6 +1816,34 @@ tb_status tb_calculator_create(const char* param_file, tb_calculator** out) {
 }
 
 void tb_calculator_destroy(tb_calculator* c) { delete c; }
+
+tb_status tb_calculator_set_small_solver(tb_calculator* c, int32_t jacobi_max) {
+  if (!c) return fail(TB_BAD_INPUT, "null calculator");
+  if (jacobi_max < -1 || jacobi_max > kJacobiMaxN)
+    return fail(TB_BAD_INPUT, "jacobi_max must be -1 (measured), 0 (never) or 1.." + std::to_string(kJacobiMaxN));
+  c->jacobi_override = jacobi_max;
+  return TB_OK;
+}
+
+int32_t tb_calculator_tuning(const tb_calculator* c, char* buf, int32_t len) {
+  if (!c) return 0;
+  std::ostringstream o;
+  o.precision(6);
+  o << "{\"small\": {\"measured\": " << (c->small.ready ? "true" : "false") << ", \"override\": "
+    << c->jacobi_override << ", \"jacobi_max\": " << c->small.jacobi_max << ", \"sizes\": [";
+  for (size_t i = 0; i < c->small.n.size(); ++i) {
+    o << (i ? ", " : "") << "{\"n\": " << c->small.n[i] << ", \"s_per_structure_cta\": " << c->small.t_cta[i]
+      << ", \"s_per_structure_warp_jacobi\": " << c->small.t_warp[i] << "}";
+  }
+  o << "]}, \"large\": {\"measured\": " << (c->eig.ready ? "true" : "false")
+    << ", \"inhouse_s\": {\"256\": " << c->eig.t_in[0] << ", \"512\": " << c->eig.t_in[1] << "}"
+    << ", \"cusolver_s\": {\"256\": " << c->eig.t_lib[0] << ", \"1024\": " << c->eig.t_lib[1] << "}"
+    << ", \"model\": {\"inhouse\": \"" << c->eig.a << " N^2 + " << c->eig.b << " N^3\", \"cusolver\": \""
+    << c->eig.c << " + " << c->eig.d << " N^3\"}, \"inhouse_limit\": " << kSyevMaxN << "}}";
+  const std::string t = o.str();
+  if (buf && len > 0) std::snprintf(buf, (size_t)len, "%s", t.c_str());
+  return (int32_t)t.size();
+}
 int32_t tb_calculator_nspecies(const tb_calculator* c) { return c ? (int32_t)c->hp.sp.size() : 0; }
 
 double tb_get_cutoff(const tb_calculator* c, double accuracy) {

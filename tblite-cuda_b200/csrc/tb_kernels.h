@@ -111,6 +111,15 @@ __global__ void k_syev(DevBatch B, double* Ab, double* Zb, double* Sb, double* w
                        const int* active);
 // the same eigensolver in FP32 (A and Z float, eigenvalues written as double)
 __global__ void k_syev_f32(DevBatch B, float* Ab, float* Zb, double* wout, int* perm, int* status, const int* active);
+// small-structure variant: one warp per structure of N <= kJacobiMaxN (cyclic Jacobi
+// in shared memory), structures list[0..nlist), kJacobiWarps structures per CTA;
+// same outputs as k_syev (w ascending, eigenvector j = row perm[j] of Z)
+constexpr int kJacobiMaxN = 32;
+constexpr int kJacobiWarps = 4;
+constexpr int kJacobiPitch = kJacobiMaxN + 1;
+inline size_t jacobi_smem_bytes() { return (size_t)kJacobiWarps * 2 * kJacobiMaxN * kJacobiPitch * sizeof(double); }
+__global__ void k_syev_jacobi(DevBatch B, double* Ab, double* Zb, double* wout, int* perm, int* status,
+                              const int* active, const int* list, int nlist);
 
 // mixed-precision form (tb_mixed.cu)
 __global__ void k_phase_masks(int nmol, const int* active, const int* phase, int* lo, int* hi);

@@ -1669,6 +1669,7 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
   if (status[m] != kStOk) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
   if (on_library(B, n)) return;
+  if (sizeof(T) == 8 && n <= B.jacobi_max) return;  // the one-warp Jacobi variant (k_syev_jacobi)
   const long long mo = B.moff[m];
   const long long vo = B.ooff[m];
   T* A = Ab + mo;
@@ -1929,6 +1930,126 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
 }
 
 }  // namespace
+
+// ------------------------------------------------ small structures: one-warp Jacobi
+// Cyclic Jacobi (Jacobi 1846; the parallel tournament ordering of Brent and
+// Luk 1985) for structures of at most 32 AOs, one warp per structure, the
+// matrix and the rotation accumulator in shared memory (33-double pitch).
+// A round applies n/2 disjoint rotations: lane t forms the rotation of pair t
+// (symmetric Schur: tau = (a_qq - a_pp)/(2 a_pq), t = sign(tau)/(|tau| +
+// sqrt(1 + tau^2)), c = 1/sqrt(1 + t^2), s = t c, which zeroes a_pq in
+// J^T A J), then lane k updates row k of every pair's two columns (A J, V J)
+// and column k of every pair's two rows (J^T A).  Sweeps stop when the
+// off-diagonal norm is below 1e-14 of the Frobenius norm (at most 50 sweeps,
+// else TB_EIGEN_FAILED).  A one-CTA eigensolver spends most of its 256
+// threads' time waiting at barriers on such small matrices; a warp per
+// structure runs eight times as many structures per SM.
+__global__ void __launch_bounds__(kJacobiWarps * 32) k_syev_jacobi(DevBatch B, double* __restrict__ Ab,
+                                                                  double* __restrict__ Zb,
+                                                                  double* __restrict__ wout,
+                                                                  int* __restrict__ perm, int* __restrict__ status,
+                                                                  const int* __restrict__ active,
+                                                                  const int* __restrict__ list, int nlist) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int li = blockIdx.x * kJacobiWarps + warp;
+  if (li >= nlist) return;
+  const int m = list[li];
+  if ((active && !active[m]) || status[m] != kStOk) return;
+  const int n = B.ooff[m + 1] - B.ooff[m];
+  if (n > kJacobiMaxN) return;
+  constexpr int P = kJacobiPitch;
+  extern __shared__ double jac_smem[];
+  double* a = jac_smem + (size_t)warp * 2 * kJacobiMaxN * P;  // n x n, pitch P
+  double* v = a + kJacobiMaxN * P;
+  __shared__ double rot_c[kJacobiWarps][kJacobiMaxN / 2], rot_s[kJacobiWarps][kJacobiMaxN / 2];
+  __shared__ int rot_p[kJacobiWarps][kJacobiMaxN / 2], rot_q[kJacobiWarps][kJacobiMaxN / 2];
+  const long long mo = B.moff[m], vo = B.ooff[m];
+  const double* A = Ab + mo;
+  if (lane < n)
+    for (int j = 0; j < n; ++j) {
+      a[lane * P + j] = 0.5 * (A[(long long)lane * n + j] + A[(long long)j * n + lane]);
+      v[lane * P + j] = lane == j ? 1.0 : 0.0;
+    }
+  __syncwarp();
+  const int nn = n + (n & 1);  // players; index n (odd n) sits out
+  double fro = 0.0;
+  if (lane < n)
+    for (int j = 0; j < n; ++j) fro += a[lane * P + j] * a[lane * P + j];
+  fro = warp_sum(fro);
+  bool conv = n <= 1;
+  for (int sweep = 0; sweep < 50 && !conv; ++sweep) {
+    double off = 0.0;
+    if (lane < n)
+      for (int j = 0; j < n; ++j)
+        if (j != lane) off += a[lane * P + j] * a[lane * P + j];
+    off = warp_sum(off);
+    if (off <= 1e-28 * fro) { conv = true; break; }
+    for (int r = 0; r < nn - 1; ++r) {
+      if (lane < nn / 2) {
+        int p = lane == 0 ? r : (r + lane) % (nn - 1);
+        int q = lane == 0 ? nn - 1 : (r - lane + nn - 1) % (nn - 1);
+        if (p > q) { const int x = p; p = q; q = x; }
+        double c = 1.0, s = 0.0;
+        if (q < n) {
+          const double apq = a[p * P + q];
+          if (apq != 0.0) {
+            const double tau = (a[q * P + q] - a[p * P + p]) / (2.0 * apq);
+            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+            c = 1.0 / sqrt(1.0 + t * t);
+            s = t * c;
+          }
+        }
+        rot_p[warp][lane] = p;
+        rot_q[warp][lane] = q < n ? q : p;  // the sitting-out pair becomes the identity
+        rot_c[warp][lane] = c;
+        rot_s[warp][lane] = q < n ? s : 0.0;
+      }
+      __syncwarp();
+      // columns: A <- A J and V <- V J, lane k on row k
+      if (lane < n)
+        for (int t = 0; t < nn / 2; ++t) {
+          const int p = rot_p[warp][t], q = rot_q[warp][t];
+          if (p == q) continue;
+          const double c = rot_c[warp][t], s = rot_s[warp][t];
+          const double akp = a[lane * P + p], akq = a[lane * P + q];
+          a[lane * P + p] = c * akp - s * akq;
+          a[lane * P + q] = s * akp + c * akq;
+          const double vkp = v[lane * P + p], vkq = v[lane * P + q];
+          v[lane * P + p] = c * vkp - s * vkq;
+          v[lane * P + q] = s * vkp + c * vkq;
+        }
+      __syncwarp();
+      // rows: A <- J^T A, lane k on column k
+      if (lane < n)
+        for (int t = 0; t < nn / 2; ++t) {
+          const int p = rot_p[warp][t], q = rot_q[warp][t];
+          if (p == q) continue;
+          const double c = rot_c[warp][t], s = rot_s[warp][t];
+          const double apk = a[p * P + lane], aqk = a[q * P + lane];
+          a[p * P + lane] = c * apk - s * aqk;
+          a[q * P + lane] = s * apk + c * aqk;
+        }
+      __syncwarp();
+    }
+  }
+  if (!conv) {
+    if (lane == 0) status[m] = kStEigenFailed;
+    return;
+  }
+  // eigenvector i (column i of v) as row i of Z; ascending order by rank (ties by index)
+  double* Z = Zb + mo;
+  if (lane < n) {
+    for (int k = 0; k < n; ++k) Z[(long long)lane * n + k] = v[k * P + lane];
+    const double di = a[lane * P + lane];
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const double dj = a[j * P + j];
+      rank += (dj < di || (dj == di && j < lane)) ? 1 : 0;
+    }
+    perm[vo + rank] = lane;
+    wout[vo + rank] = di;
+  }
+}
 
 __global__ void __launch_bounds__(kEigThreads, 3) k_syev(DevBatch B, double* __restrict__ Ab, double* __restrict__ Zb,
                                                       double* __restrict__ Sb, double* __restrict__ wout,

@@ -66,6 +66,7 @@ EXPORTS = [
     "tb_add_pot_to_h1", "tb_sygvd_batch", "tb_fermi_filling", "tb_batch_profile",
     "tb_server_create", "tb_server_submit", "tb_server_step", "tb_server_poll", "tb_server_destroy",
     "tb_batch_set_guess", "tb_batch_wavefunction", "tb_batch_gradient", "tb_sygvd_noalloc",
+    "tb_calculator_set_small_solver", "tb_calculator_tuning",
 ]
 
 _lib = None
@@ -101,6 +102,9 @@ def load_library(path: str = LIB_PATH):
     L.tb_server_poll.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.c_void_p]
     L.tb_server_poll.restype = C.c_int32
     L.tb_server_destroy.argtypes = [C.c_void_p]
+    L.tb_calculator_set_small_solver.argtypes = [C.c_void_p, C.c_int32]
+    L.tb_calculator_tuning.argtypes = [C.c_void_p, C.c_char_p, C.c_int32]
+    L.tb_calculator_tuning.restype = C.c_int32
     _lib = L
     return L
 
@@ -193,6 +197,21 @@ class Calculator:
             ns = load_library().tb_calculator_nspecies(self.h)
             self._sp_basis = np.array([self.basis_size(_Atom(z)) for z in range(ns)], np.int64).reshape(-1, 2)
         return self._sp_basis
+
+    def set_small_solver(self, jacobi_max: int):
+        """Eigensolver variant of small structures: -1 measured choice (default),
+        0 never the one-warp Jacobi solver, 1..32 Jacobi up to that many AOs."""
+        check(load_library().tb_calculator_set_small_solver(self.h, C.c_int32(jacobi_max)),
+              "tb_calculator_set_small_solver")
+
+    def tuning(self) -> dict:
+        """The autotuner's measurements and choices (tb_calculator_tuning)."""
+        import json
+        L = load_library()
+        n = L.tb_calculator_tuning(self.h, None, C.c_int32(0))
+        buf = C.create_string_buffer(n + 1)
+        L.tb_calculator_tuning(self.h, buf, C.c_int32(n + 1))
+        return json.loads(buf.value.decode())
 
     def cutoff(self, accuracy=1.0):
         return load_library().tb_get_cutoff(self.h, C.c_double(accuracy))
