@@ -171,6 +171,19 @@ const char* tb_last_error(void);
  * and choices as JSON text into buf (NUL-terminated, at most len bytes) and
  * returns the full length. */
 tb_status tb_calculator_set_small_solver(tb_calculator* calc, int32_t jacobi_max);
+
+/* Checked build (the library built with -DTB_BOUNDS_CHECK, `make check`:
+ * lib/libtblite_b200_check.so; no counterpart in the reference, whose only
+ * checks are device asserts): index guards at the global-memory accesses of
+ * the per-structure kernels skip and record any access outside its
+ * structure's own slice.  tb_bounds_check_build returns 1 in that build, 0
+ * otherwise; tb_bounds_violations returns the number of guarded accesses
+ * skipped since the last reset and the first one's guard site, index and
+ * bounds (all 0 in the normal build), and clears the records when reset is
+ * set.  Needs a CUDA device. */
+int32_t tb_bounds_check_build(void);
+tb_status tb_bounds_violations(int64_t* count, int32_t* site, int64_t* index, int64_t* lo, int64_t* hi,
+                               int32_t reset);
 int32_t tb_calculator_tuning(const tb_calculator* calc, char* buf, int32_t len);
 
 /* basis_type sizes (src/basis/type.h:56-73). */

@@ -68,6 +68,49 @@ __host__ __device__ inline int msao(int l) { return 2 * l + 1; }
 __host__ __device__ inline int mlao(int l) { return (l + 1) * (l + 2) / 2; }
 __host__ __device__ inline int lmap(int l) { return l == 0 ? 0 : (l == 1 ? 1 : 4); }
 
+// ---- checked build (-DTB_BOUNDS_CHECK: `make check`, lib/libtblite_b200_check.so)
+// Index guards at the global-memory accesses of the per-structure kernels: an
+// access outside its structure's own slice (matrix, AO, shell, atom-pair or
+// mixer slice) is skipped and recorded -- the number of violations and the
+// first one's guard site, index and bounds -- in the translation unit's
+// device record, which the host reads back.  No trap, no assert.  In the
+// normal build a guard is the constant true.
+struct OobRecord {
+  unsigned long long count;
+  int site, pad;
+  long long index, lo, hi;
+};
+#ifdef TB_BOUNDS_CHECK
+static __device__ OobRecord g_oob;
+__device__ inline bool tb_guard(int site, long long i, long long lo, long long hi) {
+  if (i >= lo && i < hi) return true;
+  if (atomicAdd(&g_oob.count, 1ULL) == 0ULL) {
+    g_oob.site = site;
+    g_oob.index = i;
+    g_oob.lo = lo;
+    g_oob.hi = hi;
+  }
+  return false;
+}
+#define TB_GUARD(site, i, lo, hi) tb::tb_guard((site), (long long)(i), (long long)(lo), (long long)(hi))
+#define TB_OOB_EXPORT(fn)                                                               \
+  cudaError_t fn(OobRecord* r, bool reset) {                                           \
+    cudaError_t e = cudaMemcpyFromSymbol(r, g_oob, sizeof(OobRecord));                 \
+    if (e == cudaSuccess && reset) {                                                   \
+      OobRecord z{};                                                                   \
+      e = cudaMemcpyToSymbol(g_oob, &z, sizeof(OobRecord));                            \
+    }                                                                                  \
+    return e;                                                                          \
+  }
+#else
+#define TB_GUARD(site, i, lo, hi) true
+#define TB_OOB_EXPORT(fn)                         \
+  cudaError_t fn(OobRecord* r, bool) {           \
+    *r = OobRecord{};                            \
+    return cudaSuccess;                          \
+  }
+#endif
+
 // Status bits per structure (device), mapped to tb_status on the host.
 enum DevStatus : int {
   kStOk = 0, kStBadInput = 1, kStNotSpd = 2, kStScfNotConverged = 3,

@@ -1817,6 +1817,35 @@ tb_status tb_calculator_create(const char* param_file, tb_calculator** out) {
 
 void tb_calculator_destroy(tb_calculator* c) { delete c; }
 
+int32_t tb_bounds_check_build(void) {
+#ifdef TB_BOUNDS_CHECK
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+tb_status tb_bounds_violations(int64_t* count, int32_t* site, int64_t* index, int64_t* lo, int64_t* hi,
+                               int32_t reset) {
+  OobRecord r[3];
+  cudaError_t e = oob_setup(&r[0], reset != 0);
+  if (e == cudaSuccess) e = oob_scf(&r[1], reset != 0);
+  if (e == cudaSuccess) e = oob_linalg(&r[2], reset != 0);
+  if (e != cudaSuccess) return fail(TB_CUDA_ERROR, cudaGetErrorString(e));
+  int64_t total = 0;
+  const OobRecord* first = nullptr;
+  for (const OobRecord& x : r) {
+    total += (int64_t)x.count;
+    if (x.count && !first) first = &x;
+  }
+  if (count) *count = total;
+  if (site) *site = first ? first->site : 0;
+  if (index) *index = first ? first->index : 0;
+  if (lo) *lo = first ? first->lo : 0;
+  if (hi) *hi = first ? first->hi : 0;
+  return TB_OK;
+}
+
 tb_status tb_calculator_set_small_solver(tb_calculator* c, int32_t jacobi_max) {
   if (!c) return fail(TB_BAD_INPUT, "null calculator");
   if (jacobi_max < -1 || jacobi_max > kJacobiMaxN)

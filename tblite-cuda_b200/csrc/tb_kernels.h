@@ -143,6 +143,12 @@ inline size_t oa_smem_bytes(int nmax) {
 __global__ void k_oa_step(DevBatch B, double* G, double* Sm, double* V, double* w, const int* mask,
                           const int* rr_mask);
 
+// records of the checked build's index guards, one per translation unit
+// (all zero in the normal build); reset clears them after the read
+cudaError_t oob_setup(OobRecord* r, bool reset);
+cudaError_t oob_scf(OobRecord* r, bool reset);
+cudaError_t oob_linalg(OobRecord* r, bool reset);
+
 // nuclear gradient (read-out after the SCF, structures with flag[m] set)
 cudaError_t launch_grad_pairs(const DevParams& P, const DevBatch& B, const int* npair, const int* pair_i,
                               const int* pair_j, const double* se, const double* Pm, const double* Wm,

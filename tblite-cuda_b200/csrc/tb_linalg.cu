@@ -283,6 +283,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
         for (int h = 0; h < 2; ++h) {
           const int gj = j0 + wc + 8 * y + 2 * tg + h;
           if (gj >= n) continue;
+          if (!TB_GUARD(8, (long long)gi * n + gj, 0, (long long)n * n)) continue;
           double* c = Cb + mo + (long long)gi * n + gj;
           const double r = beta == 0.0 ? alpha * acc[x][y][h] : alpha * acc[x][y][h] + beta * (*c);
           *c = r;
@@ -1924,12 +1925,15 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
       const T dj = d[j];
       rank += (dj < di || (dj == di && j < i)) ? 1 : 0;
     }
+    if (!TB_GUARD(9, rank, 0, n)) continue;
     perm[vo + rank] = i;
     wout[vo + rank] = di;
   }
 }
 
 }  // namespace
+
+TB_OOB_EXPORT(oob_linalg)
 
 // ------------------------------------------------ small structures: one-warp Jacobi
 // Cyclic Jacobi (Jacobi 1846; the parallel tournament ordering of Brent and
@@ -2038,7 +2042,7 @@ __global__ void __launch_bounds__(kJacobiWarps * 32) k_syev_jacobi(DevBatch B, d
   }
   // eigenvector i (column i of v) as row i of Z; ascending order by rank (ties by index)
   double* Z = Zb + mo;
-  if (lane < n) {
+  if (lane < n && TB_GUARD(10, (long long)lane * n + n - 1, 0, (long long)n * n)) {
     for (int k = 0; k < n; ++k) Z[(long long)lane * n + k] = v[k * P + lane];
     const double di = a[lane * P + lane];
     int rank = 0;

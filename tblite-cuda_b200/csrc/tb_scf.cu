@@ -291,6 +291,7 @@ __global__ void __launch_bounds__(256, 2) k_fock(DevBatch B, const int4* __restr
     mu[r] = r0 + ty + 8 * r;
     ok[r] = mu[r] < n && nu_ok;
     const long long e = mo + (long long)mu[r] * n + nu;
+    if (ok[r] && !TB_GUARD(4, e, mo, mo + nn)) ok[r] = false;
     s_[r] = ok[r] ? S[e] : 0.0;
     h_[r] = ok[r] ? H0[e] : 0.0;
 #pragma unroll
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(256, 2) k_fock(DevBatch B, const int4* __restr
   }
 #pragma unroll
   for (int r = 0; r < 4; ++r)
-    if (ok[r]) F[mo + (long long)mu[r] * n + nu] = acc[r];
+    if (ok[r] && TB_GUARD(5, (long long)mu[r] * n + nu, 0, nn)) F[mo + (long long)mu[r] * n + nu] = acc[r];
   if (r0 != c0) {  // F[c0.., r0..] = this tile transposed
     __syncthreads();
 #pragma unroll
@@ -338,7 +339,8 @@ __global__ void __launch_bounds__(256, 2) k_fock(DevBatch B, const int4* __restr
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
       const int row = c0 + ty + 8 * r, col = r0 + tx;
-      if (row < n && col < n) F[mo + (long long)row * n + col] = fock_T[tx * kFockPitch + ty + 8 * r];
+      if (row < n && col < n && TB_GUARD(5, (long long)row * n + col, 0, nn))
+        F[mo + (long long)row * n + col] = fock_T[tx * kFockPitch + ty + 8 * r];
     }
   }
 }
@@ -528,7 +530,7 @@ __global__ void __launch_bounds__(256) k_mulliken_cols(DevBatch B, const int2* _
   const int nu = ch.y * 32 + tx;
   double acc[11];
   for (int k = 0; k < 11; ++k) acc[k] = 0.0;
-  if (nu < n) {
+  if (nu < n && TB_GUARD(6, (long long)(n - 1) * n + nu, 0, nn)) {  // the column's last element in the slice
     // two rows per step so that 22 independent loads are in flight
     int mu = ty;
     for (; mu + 8 < n; mu += 16) {
@@ -555,7 +557,7 @@ __global__ void __launch_bounds__(256) k_mulliken_cols(DevBatch B, const int2* _
   }
   for (int k = 0; k < 11; ++k) part[ty][k][tx] = acc[k];
   __syncthreads();
-  if (ty == 0 && nu < n) {
+  if (ty == 0 && nu < n && TB_GUARD(7, B.ooff[m] + nu, B.ooff[m], B.ooff[m + 1])) {
     double* out = colred + 12 * (long long)(B.ooff[m] + nu);
     for (int k = 0; k < 11; ++k) {
       double s = 0.0;
@@ -676,6 +678,7 @@ __global__ void k_finalize(DevParams P, DevBatch B, const double* __restrict__ c
   const int mo = B.mixoff[m], ndim = nsh + 9 * nat;
   double err = 0.0;
   for (int i = tid; i < ndim; i += nt) {
+    if (!TB_GUARD(11, mo + i, B.mixoff[m], B.mixoff[m + 1])) continue;
     double out;
     if (i < nsh) out = qsh_out[s0 + i];
     else if (i < nsh + 3 * nat) out = dpat_out[3 * a0 + (i - nsh)];
@@ -859,6 +862,8 @@ __global__ void k_mix_next(DevBatch B, double* __restrict__ q_in, const double* 
   if (tid == 0) S.mix_iter[m] = iter;
 }
 
+TB_OOB_EXPORT(oob_scf)
+
 // ------------------------------------------------------------ gradient
 // Nuclear gradient and virial (the gradient/sigma outputs of xtb_singlepoint,
 // src/xtb.cu:195-196) of the converged structures with flag[m] set, from the
@@ -907,7 +912,9 @@ __global__ void k_grad_pair_reduce(DevBatch B, const int* __restrict__ npair, co
     double g[3] = {0.0, 0.0, 0.0};
     for (int sp = 0; sp < maxsp; ++sp)
       for (int x = 0; x < 3; ++x) g[x] += item[3 * (p * maxsp + sp) + x];
-    double* out = G + 3 * (B.a2off[m] + (long long)pair_i[p] * nat + pair_j[p]);
+    const long long gi = B.a2off[m] + (long long)pair_i[p] * nat + pair_j[p];
+    if (!TB_GUARD(14, gi, B.a2off[m], B.a2off[m + 1])) continue;
+    double* out = G + 3 * gi;
     for (int x = 0; x < 3; ++x) out[x] = g[x];
   }
 }

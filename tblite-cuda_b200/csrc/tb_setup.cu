@@ -342,6 +342,7 @@ __device__ void scatter_block(const MatOut& out, long long mo, int n, int ii, in
       const int ij = iao * SJ + jao;
       const long long mu = jj + jao, nu = ii + iao;
       const long long e1 = mu * n + nu;
+      if (!TB_GUARD(1, e1, 0, nn)) continue;
       out.S[mo + e1] = s[ij];
 #pragma unroll
       for (int k = 0; k < 3; ++k) out.D[3 * mo + k * nn + e1] = d[3 * ij + k];
@@ -352,6 +353,7 @@ __device__ void scatter_block(const MatOut& out, long long mo, int n, int ii, in
         double dj[3], qj[6];
         shift_operator(vec, s[ij], d + 3 * ij, q + 6 * ij, dj, qj);
         const long long e2 = nu * n + mu;
+        if (!TB_GUARD(2, e2, 0, nn)) continue;
         out.S[mo + e2] = s[ij];
         out.H0[mo + e2] = s[ij] * hij;
 #pragma unroll
@@ -439,7 +441,8 @@ __global__ void k_onsite_t(DevParams P, DevBatch B, const double* __restrict__ s
   const double vec[3] = {0.0, 0.0, 0.0};
   pair_block<LI, LJ>(P, out, mo, n, ii, jj, true, 0.0, 0.0, vec, ci, cj);
   if (ish == jsh) {
-    for (int x = 0; x < msao(LI); ++x) out.H0[mo + (long long)(ii + x) * n + ii + x] = se[is + ish];
+    for (int x = 0; x < msao(LI); ++x)
+      if (TB_GUARD(3, ii + x, 0, n)) out.H0[mo + (long long)(ii + x) * n + ii + x] = se[is + ish];
   }
 }
 
@@ -663,6 +666,7 @@ __global__ void k_grad_pairs_t(DevParams P, DevBatch B, const int* __restrict__ 
         const int ij = iao * SJ + jao;
         const int mu = jj + jao;
         const long long e1 = mo + (long long)mu * n + nu;
+        if (!TB_GUARD(12, e1, mo, mo + (long long)n * n)) continue;
         const double pij = Pm[e1], wij = Wm[e1];
         const double vmu = vsh[s0 + B.ao_sh[o0 + mu]] + vat[a0 + B.ao_at[o0 + mu]];
         ese += pij * s[0][ij] * hs * shpoly;
@@ -682,10 +686,14 @@ __global__ void k_grad_pairs_t(DevParams P, DevBatch B, const int* __restrict__ 
     for (int x = 0; x < 3; ++x) item[3 * it + x] = gx[x];
     const int nsh = B.soff[m + 1] - s0;
     const long long so = B.s2off[m];
-    ese_tab[so + (long long)(is - s0 + ish) * nsh + (js - s0 + jsh)] = ese;
-    ese_tab[so + (long long)(js - s0 + jsh) * nsh + (is - s0 + ish)] = ese;
+    const long long x1 = so + (long long)(is - s0 + ish) * nsh + (js - s0 + jsh);
+    const long long x2 = so + (long long)(js - s0 + jsh) * nsh + (is - s0 + ish);
+    if (TB_GUARD(13, x1, so, B.s2off[m + 1])) ese_tab[x1] = ese;
+    if (TB_GUARD(13, x2, so, B.s2off[m + 1])) ese_tab[x2] = ese;
   }
 }
+
+TB_OOB_EXPORT(oob_setup)
 
 cudaError_t launch_grad_pairs(const DevParams& P, const DevBatch& B, const int* npair, const int* pair_i,
                               const int* pair_j, const double* se, const double* Pm, const double* Wm,

@@ -15,6 +15,8 @@ import numpy as np
 
 PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG, "lib", "libtblite_b200.so")
+# the checked build (index guards that skip and record out-of-slice accesses)
+LIB_CHECK_PATH = os.path.join(PKG, "lib", "libtblite_b200_check.so")
 DEFAULT_PARAMS = os.path.join(PKG, "params", "synthetic_hco.tbp")
 
 TB_OK, TB_BAD_INPUT, TB_NOT_SPD, TB_SCF_NOT_CONVERGED = 0, 1, 2, 3
@@ -66,7 +68,7 @@ EXPORTS = [
     "tb_add_pot_to_h1", "tb_sygvd_batch", "tb_fermi_filling", "tb_batch_profile",
     "tb_server_create", "tb_server_submit", "tb_server_step", "tb_server_poll", "tb_server_destroy",
     "tb_batch_set_guess", "tb_batch_wavefunction", "tb_batch_gradient", "tb_sygvd_noalloc",
-    "tb_calculator_set_small_solver", "tb_calculator_tuning",
+    "tb_calculator_set_small_solver", "tb_calculator_tuning", "tb_bounds_check_build", "tb_bounds_violations",
 ]
 
 _lib = None
@@ -103,10 +105,18 @@ def load_library(path: str = LIB_PATH):
     L.tb_server_poll.restype = C.c_int32
     L.tb_server_destroy.argtypes = [C.c_void_p]
     L.tb_calculator_set_small_solver.argtypes = [C.c_void_p, C.c_int32]
+    L.tb_bounds_check_build.restype = C.c_int32
     L.tb_calculator_tuning.argtypes = [C.c_void_p, C.c_char_p, C.c_int32]
     L.tb_calculator_tuning.restype = C.c_int32
     _lib = L
     return L
+
+
+def bounds_violations(reset=True):
+    """(count, site, index, lo, hi) of the checked build's index guards (tb_bounds_violations)."""
+    v = [C.c_int64(), C.c_int32(), C.c_int64(), C.c_int64(), C.c_int64()]
+    check(load_library().tb_bounds_violations(*[C.byref(x) for x in v], C.c_int32(int(reset))), "tb_bounds_violations")
+    return tuple(x.value for x in v)
 
 
 def last_error() -> str:

@@ -49,3 +49,16 @@ def test_params_file_errors_are_reported(tmp_path):
     st = lib.tb_calculator_create(str(bad).encode(), ctypes.byref(h))
     assert st == capi.TB_PARAM_ERROR
     assert "unsupported shell" in capi.last_error()
+
+
+def test_checked_build_exports_and_reports_itself():
+    """The checked build (index guards, -DTB_BOUNDS_CHECK) exports the same
+    boundary and says it is the checked build; the normal build says it is not."""
+    from tblite_b200 import capi
+    if not os.path.exists(capi.LIB_CHECK_PATH):
+        pytest.fail(f"checked library not built: {capi.LIB_CHECK_PATH}")
+    chk = ctypes.CDLL(capi.LIB_CHECK_PATH)
+    missing = [n for n in declared_functions() if not hasattr(chk, n)]
+    assert not missing, missing
+    assert chk.tb_bounds_check_build() == 1
+    assert ctypes.CDLL(capi.LIB_PATH).tb_bounds_check_build() == 0
