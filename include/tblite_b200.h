@@ -235,8 +235,10 @@ void tb_batch_destroy(tb_batch* batch);
  * micro-batch) and advances every resident micro-batch without waiting for
  * any: each runs its SCF iterations on its own stream, so their work overlaps
  * on the device; one whose iteration has finished is collected (structures
- * that converged are retired) and given its next iteration.  A micro-batch's
- * workspace is freed when its last structure finishes.  Call it in a loop.  tb_server_poll hands out finished results in completion
+ * that converged are retired) and given its next iteration.  Once at most half
+ * of a micro-batch is unfinished, the rest moves to a smaller one (see
+ * tb_server_compactions); a micro-batch's workspace returns to the pool when
+ * its last structure finishes.  Call it in a loop.  tb_server_poll hands out finished results in completion
  * order.  Each result equals the one tb_singlepoint_batch gives for the same
  * structure alone (the kernels treat every structure independently).
  * Calls on one server must come from one host thread at a time. */
@@ -253,6 +255,11 @@ tb_status tb_server_step(tb_server* server, int32_t* n_resident, int32_t* n_queu
  * pointers of results[i], when not NULL, receive that structure's qat / qsh /
  * dpat / qpat).  Returns the number written. */
 int32_t tb_server_poll(tb_server* server, int32_t max, int64_t* tickets, tb_result* results);
+/* Number of compactions so far: once at most half of a micro-batch (of 4 or
+ * more structures) is still iterating, its unfinished structures continue in
+ * a new, smaller micro-batch with their SCF state, and the old workspace
+ * returns to the server's pool, where admission can use it at once. */
+int64_t tb_server_compactions(const tb_server* server);
 void tb_server_destroy(tb_server* server);
 
 /* ---- stage entry points (host buffers; one structure each) ---------------- */

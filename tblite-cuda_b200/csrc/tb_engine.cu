@@ -2368,6 +2368,7 @@ struct tb_server {
   // pinned host buffers for the micro-batches' active flags, reused like the
   // streams (pinning host memory is an operating-system call)
   std::vector<std::pair<int*, int>> pinned;
+  int64_t compactions = 0;  // micro-batches moved to their unfinished structures
   // arrivals are collected this long (or until max_batch are queued, or while
   // nothing is resident) so that micro-batches hold more than one request
   double window_s = 0.002;
@@ -2462,6 +2463,78 @@ tb_status server_admit(tb_server* s) {
   L.reqs = std::move(take);
   L.done.assign(L.reqs.size(), 0);
   s->live.push_back(std::move(L));
+  return TB_OK;
+}
+
+// Compaction (continuous batching): once at most half of a micro-batch is
+// still iterating, its unfinished structures continue in a new, smaller
+// micro-batch -- built from their requests, set up (integrals and
+// factorisation recomputed, the same bits), and given their SCF state
+// (k_compact_state) -- and the old workspace returns to the pool, where
+// admission can use it at once.  A structure's iterations and results are
+// unchanged by the move: the kernels treat every structure independently.
+tb_status server_compact(tb_server* s, tb_server::Live& L) {
+  const int nmol = L.b->nmol;
+  std::vector<int> keep;
+  for (int m = 0; m < nmol; ++m)
+    if (L.h_act[m] && !L.done[m]) keep.push_back(m);
+  if (keep.empty() || nmol < 4 || 2 * (int)keep.size() > nmol) return TB_OK;
+  NvtxRange nv("tb.server_compact");
+  const int nk = (int)keep.size();
+  std::vector<tb_structure> mols(nk);
+  std::vector<tb_server::Req> reqs;
+  for (int k = 0; k < nk; ++k) {
+    tb_server::Req& r = L.reqs[keep[k]];
+    mols[k] = {r.nat, r.uhf, r.charge, r.id.data(), r.xyz.data()};
+  }
+  int64_t est = 0;
+  for (int k = 0; k < nk; ++k) est += L.reqs[keep[k]].bytes;
+  std::unique_ptr<Arena> ar;
+  {
+    int best = -1;
+    for (int i = 0; i < (int)s->pool.size(); ++i)
+      if ((int64_t)s->pool[i]->cap >= est && (best < 0 || s->pool[i]->cap < s->pool[best]->cap)) best = i;
+    if (best >= 0) {
+      ar = std::move(s->pool[best]);
+      s->pool.erase(s->pool.begin() + best);
+      s->pooled -= (int64_t)ar->cap;
+    } else {
+      ar.reset(new Arena());
+    }
+  }
+  tb_batch* nb = new tb_batch();
+  tb_status st = batch_build(s->calc, mols.data(), nk, &s->opt, nb, ar.get());
+  if (st == TB_OK) st = batch_setup(nb, L.st);
+  if (st == TB_OK) {
+    tb_batch* ob = L.b;
+    TB_CUDA(cudaMemcpyAsync(nb->d_wflag, keep.data(), nk * sizeof(int), cudaMemcpyHostToDevice, L.st));
+    ScfState so{ob->q_in, ob->dq, ob->dqlast, ob->qlast, ob->df, ob->u, ob->amat, ob->omega, ob->ms};
+    ScfState sn{nb->q_in, nb->dq, nb->dqlast, nb->qlast, nb->df, nb->u, nb->amat, nb->omega, nb->ms};
+    k_compact_state<<<nk, 256, 0, L.st>>>(ob->db, nb->db, nb->d_wflag, so, sn, s->opt.max_iter);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) st = fail(TB_CUDA_ERROR, std::string("compaction: ") + cudaGetErrorString(e));
+    if (st == TB_OK) TB_CUDA(cudaMemcpyAsync(nb->ms.n_active, &nk, sizeof(int), cudaMemcpyHostToDevice, L.st));
+    if (st == TB_OK) TB_CUDA(cudaStreamSynchronize(L.st));  // the old workspace is read until here
+  }
+  if (st != TB_OK) {
+    delete nb;
+    s->pooled += (int64_t)ar->cap;
+    s->pool.push_back(std::move(ar));
+    return st;
+  }
+  nb->it = L.b->it;
+  for (int k = 0; k < nk; ++k) reqs.push_back(std::move(L.reqs[keep[k]]));
+  delete L.b;
+  s->resident -= L.bytes;
+  s->pooled += (int64_t)L.ar->cap;
+  s->pool.push_back(std::move(L.ar));
+  L.b = nb;
+  L.ar = std::move(ar);
+  L.bytes = (int64_t)L.ar->cap;
+  s->resident += L.bytes;
+  L.reqs = std::move(reqs);
+  L.done.assign(nk, 0);
+  s->compactions += 1;
   return TB_OK;
 }
 
@@ -2579,6 +2652,10 @@ tb_status tb_server_step(tb_server* s, int32_t* n_resident, int32_t* n_queued, i
       st = server_collect(s, L);
       if (st != TB_OK) return st;
       L.inflight = false;
+      if (na > 0 && L.b->it < L.b->opt.max_iter) {
+        st = server_compact(s, L);
+        if (st != TB_OK) return st;
+      }
       if (na <= 0 || L.b->it >= L.b->opt.max_iter) {
         delete L.b;
         s->streams.push_back(L.st);
@@ -2605,6 +2682,8 @@ tb_status tb_server_step(tb_server* s, int32_t* n_resident, int32_t* n_queued, i
   if (n_queued) *n_queued = (int32_t)s->queue.size();
   return TB_OK;
 }
+
+int64_t tb_server_compactions(const tb_server* s) { return s ? s->compactions : 0; }
 
 int32_t tb_server_poll(tb_server* s, int32_t max, int64_t* tickets, tb_result* results) {
   if (!s || max <= 0) return 0;

@@ -172,6 +172,13 @@ __global__ void k_scf_init(DevParams P, DevBatch B, const double* charge, const 
                            double* n0sh, double* q_in, MolState S);
 // end of one iteration of the SCF loop graph: counts it and sets the loop condition
 __global__ void k_loop_control(cudaGraphConditionalHandle h, const int* n_active, int* it, int max_iter);
+// SCF state of structure map[k] of batch Bo moved to structure k of batch Bn
+// (serving: compaction of a micro-batch to its unfinished structures)
+struct ScfState {
+  double *q_in, *dq, *dqlast, *qlast, *df, *u, *amat, *omega;
+  MolState S;
+};
+__global__ void k_compact_state(DevBatch Bo, DevBatch Bn, const int* map, ScfState so, ScfState sn, int memory);
 // caller's starting moments (wavefunction guess) into q_in for flagged structures
 __global__ void k_apply_guess(DevBatch B, const double* guess, const int* flag, double* q_in);
 // pair tables of the fixed geometry (gtab: gamma per shell pair, atab: 1/r, f3, f5 per atom pair)

@@ -86,6 +86,53 @@ __global__ void k_scf_init(DevParams P, DevBatch B, const double* __restrict__ c
   }
 }
 
+// Serving: the unfinished structures of a micro-batch continue in a smaller
+// batch (server_compact).  Everything a structure carries from one SCF
+// iteration to the next moves with it: the mixer vectors and its Broyden
+// history slab, the per-structure scalars (iteration counters, energies,
+// phase of the mixed form, status).  Geometry-derived data (integrals, X,
+// pair tables) is recomputed by the new batch's setup, bit for bit the same.
+__global__ void k_compact_state(DevBatch Bo, DevBatch Bn, const int* __restrict__ map, ScfState so, ScfState sn,
+                                int memory) {
+  const int k = blockIdx.x, m = map[k];
+  const int mo = Bo.mixoff[m], mn = Bn.mixoff[k], n = Bo.mixoff[m + 1] - mo;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    sn.q_in[mn + i] = so.q_in[mo + i];
+    sn.dq[mn + i] = so.dq[mo + i];
+    sn.dqlast[mn + i] = so.dqlast[mo + i];
+    sn.qlast[mn + i] = so.qlast[mo + i];
+  }
+  const long long ho = (long long)mo * memory, hn = (long long)mn * memory;
+  for (long long i = threadIdx.x; i < (long long)n * memory; i += blockDim.x) {
+    sn.df[hn + i] = so.df[ho + i];
+    sn.u[hn + i] = so.u[ho + i];
+  }
+  for (int i = threadIdx.x; i < memory * memory; i += blockDim.x)
+    sn.amat[(long long)k * memory * memory + i] = so.amat[(long long)m * memory * memory + i];
+  for (int i = threadIdx.x; i < memory; i += blockDim.x) sn.omega[(long long)k * memory + i] = so.omega[(long long)m * memory + i];
+  if (threadIdx.x == 0) {
+    const MolState& a = so.S;
+    const MolState& b = sn.S;
+    b.e_rep[k] = a.e_rep[m];
+    b.nel[2 * k] = a.nel[2 * m];
+    b.nel[2 * k + 1] = a.nel[2 * m + 1];
+    b.iscf[k] = a.iscf[m];
+    b.mix_iter[k] = a.mix_iter[m];
+    b.eelec[k] = a.eelec[m];
+    b.active[k] = a.active[m];
+    b.status[k] = a.status[m];
+    b.e_ts[k] = a.e_ts[m];
+    b.e_band[k] = a.e_band[m];
+    b.e_es2[k] = a.e_es2[m];
+    b.e_aes2[k] = a.e_aes2[m];
+    b.e_es3[k] = a.e_es3[m];
+    b.scf_error[k] = a.scf_error[m];
+    b.fermi_warn[k] = a.fermi_warn[m];
+    for (int x = 0; x < 3; ++x) b.dipole[3 * k + x] = a.dipole[3 * m + x];
+    if (a.phase && b.phase) { b.phase[k] = a.phase[m]; b.n64[k] = a.n64[m]; }
+  }
+}
+
 // Last node of the body of the SCF loop graph (one graph launch runs the whole
 // loop): counts the iteration and keeps the WHILE node looping while a
 // structure is still active and the iteration budget is not spent (the

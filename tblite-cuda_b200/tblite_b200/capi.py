@@ -69,6 +69,7 @@ EXPORTS = [
     "tb_server_create", "tb_server_submit", "tb_server_step", "tb_server_poll", "tb_server_destroy",
     "tb_batch_set_guess", "tb_batch_wavefunction", "tb_batch_gradient", "tb_sygvd_noalloc",
     "tb_calculator_set_small_solver", "tb_calculator_tuning", "tb_bounds_check_build", "tb_bounds_violations",
+    "tb_server_compactions",
 ]
 
 _lib = None
@@ -104,6 +105,8 @@ def load_library(path: str = LIB_PATH):
     L.tb_server_poll.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.c_void_p]
     L.tb_server_poll.restype = C.c_int32
     L.tb_server_destroy.argtypes = [C.c_void_p]
+    L.tb_server_compactions.argtypes = [C.c_void_p]
+    L.tb_server_compactions.restype = C.c_int64
     L.tb_calculator_set_small_solver.argtypes = [C.c_void_p, C.c_int32]
     L.tb_bounds_check_build.restype = C.c_int32
     L.tb_calculator_tuning.argtypes = [C.c_void_p, C.c_char_p, C.c_int32]
@@ -443,6 +446,10 @@ class Server:
         nr, nq, nb = C.c_int32(), C.c_int32(), C.c_int64()
         check(load_library().tb_server_step(self.h, C.byref(nr), C.byref(nq), C.byref(nb)), "tb_server_step")
         return nr.value, nq.value, nb.value
+
+    def compactions(self) -> int:
+        """Micro-batches moved to their unfinished structures so far (tb_server_compactions)."""
+        return int(load_library().tb_server_compactions(self.h))
 
     def poll(self, max_results: int = 4096):
         L = load_library()

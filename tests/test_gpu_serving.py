@@ -67,3 +67,30 @@ def test_serving_rejects_structure_above_budget(gpu_calc):
     with pytest.raises(capi.TBError) as e:
         srv.submit(g.water_cluster(30, np.random.default_rng(1)))
     assert e.value.status == capi.TB_CAPACITY_EXCEEDED
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_serving_compaction_keeps_results(gpu_calc, precision):
+    """One micro-batch of 8: six alkanes (about 6 SCF iterations) and two water
+    clusters (about 8): once the alkanes are done, the two clusters move to a
+    compacted micro-batch with their SCF state; every result still equals the
+    structure alone, bit for bit, and the old workspace returned to the pool."""
+    rng = np.random.default_rng(91)
+    mols = [g.alkane(n, rng) for n in (4, 6, 8, 10, 12, 14)] + g.water_clusters(2, seed=92, nmin=10, nmax=16)
+    srv = capi.Server(gpu_calc, 8 << 30, max_batch=8, precision=precision)
+    tickets = {srv.submit(m): m for m in mols}
+    got, steps = {}, 0
+    while len(got) < len(mols):
+        srv.step()
+        for t, r in srv.poll():
+            got[t] = r
+        time.sleep(0.0005)
+        steps += 1
+        assert steps < 200000
+    assert srv.compactions() >= 1
+    for t, m in tickets.items():
+        alone = gpu_calc.singlepoint_batch([m], precision=precision)[0]
+        r = got[t]
+        assert r["status"] == alone["status"] == 0
+        assert r["energy"] == alone["energy"] and r["iterations"] == alone["iterations"]
+        np.testing.assert_array_equal(r["qat"], alone["qat"])
