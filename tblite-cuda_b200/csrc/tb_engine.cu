@@ -1172,6 +1172,7 @@ tb_status batch_setup(tb_batch* b, cudaStream_t st) {
   TB_CUDA(cudaMemsetAsync(S.status, 0, nmol * sizeof(int), st));
   TB_CUDA(cudaMemsetAsync(S.fermi_warn, 0, nmol * sizeof(int), st));
   TB_CUDA(cudaMemsetAsync(S.n_active, 0, sizeof(int), st));
+  TB_CUDA(cudaMemsetAsync(b->kdim, 0, nmol * sizeof(int), st));  // no occupied orbitals before k_fermi
   // ---- setup (once per structure)
   TB_K("atoms", 0, 0, k_atoms<<<nblk(B.nat_tot, 128), 128, 0, st>>>(Pc, B, b->cn, b->mrad, b->erep, b->se));
   {
@@ -2515,6 +2516,9 @@ tb_status server_compact(tb_server* s, tb_server::Live& L) {
     if (e != cudaSuccess) st = fail(TB_CUDA_ERROR, std::string("compaction: ") + cudaGetErrorString(e));
     if (st == TB_OK) TB_CUDA(cudaMemcpyAsync(nb->ms.n_active, &nk, sizeof(int), cudaMemcpyHostToDevice, L.st));
     if (st == TB_OK) TB_CUDA(cudaStreamSynchronize(L.st));  // the old workspace is read until here
+    // the host copies of the flags (active, status, phase: the library path
+    // chooses its solver by them) were read by batch_setup before the move
+    if (st == TB_OK) st = read_flags(nb, L.st);
   }
   if (st != TB_OK) {
     delete nb;

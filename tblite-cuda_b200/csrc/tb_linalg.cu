@@ -181,7 +181,8 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
     if (active && !active[m]) continue;
     if ((shape & kGemmSym) && tl.z < tl.y) continue;
     const int n = B.ooff[m + 1] - B.ooff[m];
-    const int K = kdim ? kdim[m] : n;
+    // the reduction length never leaves [0, n], whatever kdim holds
+    const int K = kdim ? min(max(kdim[m], 0), n) : n;
     const long long mo = B.moff[m];
     const long long vo = B.ooff[m];
     const double* A = Ab + mo;

@@ -448,7 +448,9 @@ __global__ void k_fermi(DevBatch B, const double* __restrict__ w, double kt, dou
   const int m = blockIdx.x;
   if (!S.active[m]) return;
   if (S.status[m] != kStOk) {  // eigensolver failure: retire the structure
-    if (threadIdx.x == 0) { S.active[m] = 0; atomicSub(S.n_active, 1); }
+    // (the density GEMMs of the mixed form mask by the phase at the start of
+    // the iteration and still visit it: no orbitals are occupied)
+    if (threadIdx.x == 0) { S.active[m] = 0; atomicSub(S.n_active, 1); kdim[m] = 0; }
     return;
   }
   const int n = B.ooff[m + 1] - B.ooff[m];

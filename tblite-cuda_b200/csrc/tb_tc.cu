@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(DevBatch B, const int
     if (active && !active[m]) continue;
     cur = m;
     const int n = B.ooff[m + 1] - B.ooff[m];
-    const int K = kdim ? kdim[m] : n;
+    const int K = kdim ? min(max(kdim[m], 0), n) : n;  // never outside [0, n], whatever kdim holds
     const long long mo = B.moff[m];
     const long long vo = B.ooff[m];
     const double* A = Ab + mo;

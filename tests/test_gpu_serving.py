@@ -94,3 +94,32 @@ def test_serving_compaction_keeps_results(gpu_calc, precision):
         assert r["status"] == alone["status"] == 0
         assert r["energy"] == alone["energy"] and r["iterations"] == alone["iterations"]
         np.testing.assert_array_equal(r["qat"], alone["qat"])
+
+
+@pytest.mark.parametrize("precision,solver,graphs", [(0, 0, 1), (1, 0, 1), (1, 2, 0), (1, 2, 1)])
+def test_serving_compaction_graphs_and_library(gpu_calc, precision, solver, graphs):
+    """The same compaction with the iteration replayed as a graph and/or every
+    eigensolve on the library path (solver = 2): the compacted micro-batch's
+    host copies of the flags (the mixed form's library path picks its FP32 or
+    FP64 solver by the phase) and its occupied-orbital counts are those of its
+    structures, so every result still equals the structure alone, bit for bit."""
+    rng = np.random.default_rng(91)
+    mols = [g.alkane(n, rng) for n in (4, 6, 8, 10, 12, 14)] + g.water_clusters(2, seed=92, nmin=10, nmax=16)
+    opts = dict(precision=precision, solver=solver, use_graphs=graphs)
+    srv = capi.Server(gpu_calc, 8 << 30, max_batch=8, **opts)
+    tickets = {srv.submit(m): m for m in mols}
+    got, steps = {}, 0
+    while len(got) < len(mols):
+        srv.step()
+        for t, r in srv.poll():
+            got[t] = r
+        time.sleep(0.0005)
+        steps += 1
+        assert steps < 200000
+    assert srv.compactions() >= 1
+    for t, m in tickets.items():
+        alone = gpu_calc.singlepoint_batch([m], precision=precision, solver=solver)[0]
+        r = got[t]
+        assert r["status"] == alone["status"] == 0
+        assert r["energy"] == alone["energy"] and r["iterations"] == alone["iterations"]
+        np.testing.assert_array_equal(r["qat"], alone["qat"])
