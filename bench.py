@@ -389,6 +389,8 @@ def main():
 
     # ---------------- the plain form one structure per call (no batching), for the batching gain
     one = one_per_call(calc, mols, torch, sh) if rank == 0 else None
+    # the same calls with the tridiagonalisation in cluster shared memory (latency-bound calls)
+    one_smem = one_per_call(calc, mols, torch, sh, smem_tridiag=True) if rank == 0 else None
 
     # ---------------- config 2 (256 alkanes, 122-1196 AOs): both forms, errors of the mixed form
     alk = alkanes_summary(capi, calc, torch, stream) if rank == 0 and args.config2 else None
@@ -417,6 +419,7 @@ def main():
         line["alkanes_256"] = alk
     if one is not None:
         line["forms"]["fp64_one_structure_per_call"] = one
+        line["forms"]["fp64_one_structure_per_call_smem_tridiag"] = one_smem
         line["batched_vs_one_per_call"] = value / one["value"]
     iters = [r["iterations"] for r in res]
     line["scf_iterations"] = {"mean": float(np.mean(iters)), "max": int(max(iters))}
@@ -441,20 +444,26 @@ def launches_of(forms, name):
     return int(forms[name]["launches"])
 
 
-def one_per_call(calc, mols, torch, sh, count=48):
+def one_per_call(calc, mols, torch, sh, count=48, smem_tridiag=False):
     """The plain FP64 form without batching: tb_singlepoint_batch called once per
-    structure on an evenly spaced sample of the workload (host buffers)."""
+    structure on an evenly spaced sample of the workload (host buffers);
+    smem_tridiag: with the tridiagonalisation in cluster shared memory."""
     sample = [mols[int(i)] for i in range(0, len(mols), max(1, len(mols) // count))][:count]
-    for m in sample[:4]:
-        calc.singlepoint_batch([m], stream=sh, precision=0)
-    torch.cuda.synchronize()
-    t = time.perf_counter()
-    for m in sample:
-        calc.singlepoint_batch([m], stream=sh, precision=0)
-    torch.cuda.synchronize()
-    dt = time.perf_counter() - t
+    calc.set_smem_tridiag(64 if smem_tridiag else 0)
+    try:
+        for m in sample[:4]:
+            calc.singlepoint_batch([m], stream=sh, precision=0)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for m in sample:
+            calc.singlepoint_batch([m], stream=sh, precision=0)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t
+    finally:
+        calc.set_smem_tridiag(0)
     return {"value": len(sample) / dt, "unit": UNIT, "structures": len(sample),
-            "sample": "evenly spaced structures of the batch, one tb_singlepoint_batch call each"}
+            "sample": "evenly spaced structures of the batch, one tb_singlepoint_batch call each",
+            "smem_tridiag": bool(smem_tridiag)}
 
 
 def alkanes_summary(capi, calc, torch, stream):

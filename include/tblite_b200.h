@@ -172,6 +172,19 @@ const char* tb_last_error(void);
  * returns the full length. */
 tb_status tb_calculator_set_small_solver(tb_calculator* calc, int32_t jacobi_max);
 
+/* Householder tridiagonalisation of the FP64 eigensolver (the dsytrd step of
+ * sygvd_solver::solve, src/lapack/sygvd.cu:223-313) held in the shared memory
+ * of a thread block cluster: structures of 64..560 AOs, one cluster of 1, 2,
+ * 3, 4, 6 or 8 CTAs by size (the choice depends on the size only).  It cuts
+ * the latency of a structure's reduction (a 384-AO one: 4 SMs instead of a
+ * third of one), but spends more SM time per structure, so it pays where
+ * latency bounds the call -- single structures, small batches, the request
+ * loop at low load -- and not for large batches.  min_n: structures of at
+ * least min_n AOs (and 64..560) take it; 0 (default): the one-CTA kernel
+ * reduces every size.  Applies to batches built afterwards.  tb_sygvd_batch
+ * always uses it from 64 AOs. */
+tb_status tb_calculator_set_smem_tridiag(tb_calculator* calc, int32_t min_n);
+
 /* Checked build (the library built with -DTB_BOUNDS_CHECK, `make check`:
  * lib/libtblite_b200_check.so; no counterpart in the reference, whose only
  * checks are device asserts): index guards at the global-memory accesses of

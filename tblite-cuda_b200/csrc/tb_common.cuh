@@ -59,6 +59,9 @@ struct DevBatch {
   int lib_above;         // 0: every structure on the in-house kernels; else structures with N > lib_above
                          // (all of them when -1) are factorised and diagonalised by the library path
   int jacobi_max;        // structures of N <= jacobi_max use the one-warp Jacobi eigensolver (0: none)
+  int trid_min, trid_max;  // FP64 structures of trid_min <= N <= trid_max arrive at k_syev
+                           // tridiagonalised by k_trid_smem (d | e | tau in their scratch slice;
+                           // trid_max 0: none)
 };
 
 // True when structure size n is handled by the library (cuSOLVER) path.

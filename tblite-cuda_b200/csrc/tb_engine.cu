@@ -208,6 +208,38 @@ struct Layout {
   }
 };
 
+// The structures of each k_trid_smem class (cluster size), largest first:
+// every in-house structure of max(min_n, kTridMin)..kTridClassMax[last] AOs
+// (min_n = 0: none), so that k_syev can take DevBatch::trid_min/trid_max as
+// the rule.
+struct TridPlan {
+  std::vector<int> list;
+  int off[kTridClasses + 1] = {0};
+  int nmax[kTridClasses] = {0};
+  int trid_min = 0, trid_max = 0;
+  void build(const std::vector<int>& n, const std::vector<char>& in_house, int min_n) {
+    list.clear();
+    for (int c = 0; c <= kTridClasses; ++c) off[c] = 0;
+    for (int c = 0; c < kTridClasses; ++c) nmax[c] = 0;
+    trid_min = min_n > 0 ? std::max(min_n, kTridMin) : 0;
+    trid_max = min_n > 0 ? kTridClassMax[kTridClasses - 1] : 0;
+    if (min_n <= 0) return;
+    std::vector<std::vector<int>> cls(kTridClasses);
+    for (int m = 0; m < (int)n.size(); ++m) {
+      const int c = in_house[m] && n[m] >= trid_min ? trid_class_of(n[m]) : -1;
+      if (c < 0) continue;
+      cls[c].push_back(m);
+      nmax[c] = std::max(nmax[c], n[m]);
+    }
+    for (int c = 0; c < kTridClasses; ++c) {
+      std::stable_sort(cls[c].begin(), cls[c].end(), [&](int a, int b) { return n[a] > n[b]; });
+      off[c] = (int)list.size();
+      list.insert(list.end(), cls[c].begin(), cls[c].end());
+    }
+    off[kTridClasses] = (int)list.size();
+  }
+};
+
 }  // namespace
 
 // ====================================================================== calculator
@@ -237,6 +269,7 @@ struct tb_calculator {
     std::vector<double> t_cta, t_warp;  // seconds per structure in a full batch
   } small;
   int jacobi_override = -1;  // -1: measured choice; 0: never; 1..32: fixed bound
+  int smem_tridiag = 0;  // FP64 structures of at least this many AOs reduced by k_trid_smem (0: none)
   std::mutex tune_mu;
   // pinned staging buffer for the batch metadata upload, reused across batches
   std::mutex stage_mu;
@@ -318,6 +351,8 @@ struct tb_batch {
   int* d_wflag = nullptr;
   int* d_jlist = nullptr;  // structures on the one-warp Jacobi eigensolver
   int njac = 0;
+  TridPlan trid;            // structures tridiagonalised by k_trid_smem, per class
+  int* d_tlist = nullptr;
   int4 *d_tiles64, *d_tiles32, *d_tiles128;
   int2* d_chunks32;
   int* h_nactive = nullptr;  // pinned
@@ -578,6 +613,15 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
       if (n <= jacobi_max && !(lib_above != 0 && n > lib_above)) jlist.push_back(m);
     }
   }
+  {
+    std::vector<int> sizes(nmol);
+    std::vector<char> in_house(nmol);
+    for (int m = 0; m < nmol; ++m) {
+      sizes[m] = b->h_ooff[m + 1] - b->h_ooff[m];
+      in_house[m] = !(lib_above != 0 && sizes[m] > lib_above);
+    }
+    b->trid.build(sizes, in_house, calc->smem_tridiag);
+  }
   b->lib_bytes = 0;
   if (!b->big.empty()) {
     const std::string e = b->lib.workspace(nbig_max, &b->lib_bytes);
@@ -604,7 +648,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
          o_t128 = L.add(b->tiles128.size() * sizeof(int4)),
          o_t32 = L.add(b->tiles32.size() * sizeof(int4)), o_c32 = L.add(b->chunks32.size() * sizeof(int2)),
          o_charge = L.add(NM * D8), o_uhf = L.add(NM * I4), o_order = L.add(NM * I4),
-         o_jlist = L.add(NM * I4);
+         o_jlist = L.add(NM * I4), o_tlist = L.add(NM * I4);
   const size_t meta_end = L.total;
   size_t o_gtab = L.add((size_t)b->h_s2off[nmol] * D8), o_atab = L.add((size_t)b->h_a2off[nmol] * 3 * D8);
   size_t o_cn = L.add(NA * D8), o_mrad = L.add(NA * D8), o_erep = L.add(NA * D8), o_se = L.add(NS * D8),
@@ -694,6 +738,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   });
   put(o_order, order.data(), NM * I4);
   if (!jlist.empty()) put(o_jlist, jlist.data(), jlist.size() * I4);
+  if (!b->trid.list.empty()) put(o_tlist, b->trid.list.data(), b->trid.list.size() * I4);
   TB_CUDA(cudaMemcpy(base, blob, meta_end, cudaMemcpyHostToDevice));
 
   DevBatch& d = b->db;
@@ -709,7 +754,10 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   d.order = at<int>(base, o_order);
   d.lib_above = lib_above;
   d.jacobi_max = jacobi_max;
+  d.trid_min = b->trid.trid_min;
+  d.trid_max = b->trid.trid_max;
   b->d_jlist = at<int>(base, o_jlist);
+  b->d_tlist = at<int>(base, o_tlist);
   b->njac = (int)jlist.size();
   b->lib_work = base + o_lwork;
   b->lib_info = at<int>(base, o_linfo);
@@ -818,6 +866,24 @@ tb_status prof_collect(tb_batch* b, cudaStream_t st) {
     ++b->launches;                                                                         \
   } while (0)
 
+// k_trid_smem for the structures of the batch's plan (one launch per class;
+// timed with k_syev in the "syev" class), before k_syev
+tb_status launch_trid_plan(tb_batch* b, const int* active, cudaStream_t st) {
+  const TridPlan& tp = b->trid;
+  for (int c = 0; c < kTridClasses; ++c) {
+    const int cnt = tp.off[c + 1] - tp.off[c];
+    if (cnt == 0) continue;
+    cudaEvent_t e0 = nullptr;
+    prof_start(b, st, &e0);
+    const cudaError_t e = launch_trid(b->db, b->F, b->W, b->ms.status, active, b->d_tlist + tp.off[c], cnt,
+                                      kTridClusterSizes[c], tp.nmax[c], st);
+    if (e != cudaSuccess) return fail(TB_CUDA_ERROR, std::string("k_trid_smem: ") + cudaGetErrorString(e));
+    ++b->launches;
+    prof_stop(b, st, "syev", e0, 0.0, 1);
+  }
+  return TB_OK;
+}
+
 // The mixed phase hands over to FP64 once |dE| and the charge error are below
 // this multiple of the final thresholds, but never below the floors: the FP32
 // contractions leave iteration-to-iteration noise of about 1e-6 in charges.
@@ -860,6 +926,10 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
   TB_K("syev_f32", 4.0 * n3_lo, 1,
        k_syev_f32<<<nmol, kEigThreads, smem32, st>>>(B, b->Af, b->Zf, b->w, b->perm, S.status, lo));
   // FP64 phase: the FP64 eigensolver (eigenvectors as rows of Z, W as its scratch)
+  {
+    const tb_status ts = launch_trid_plan(b, hi, st);
+    if (ts != TB_OK) return ts;
+  }
   TB_K("syev", 4.0 * n3_hi, 1,
        k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->W, b->w, b->perm, S.status, hi));
   if (b->njac > 0)
@@ -934,6 +1004,7 @@ tb_status raise_smem_limits() {
     TB_CUDA(cudaFuncGetAttributes(&a, k));
     TB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes));
   }
+  TB_CUDA(trid_raise_limits());
   return TB_OK;
 }
 
@@ -957,7 +1028,8 @@ tb_status calibrate_eigensolvers(tb_calculator* c) {
   if (!we.empty()) return fail(TB_CUDA_ERROR, "eigensolver calibration: " + we);
   Layout L;
   const size_t oA = L.add(nn * 8), oZ = L.add(nn * 8), oW = L.add(nn * 8), ow = L.add(NL * 8), op = L.add(NL * 4), os = L.add(16),
-               oo = L.add(16), om = L.add(16), owk = L.add(std::max<size_t>(wbytes, 16)), oi = L.add(16);
+               oo = L.add(16), om = L.add(16), owk = L.add(std::max<size_t>(wbytes, 16)), oi = L.add(16),
+               ol = L.add(16);
   TB_CUDA(ar.reserve(L.total));
   char* base = ar.base;
   std::vector<double> h(nn);
@@ -985,11 +1057,20 @@ tb_status calibrate_eigensolvers(tb_calculator* c) {
     B.nmol = 1;
     B.ooff = at<int>(base, oo);
     B.moff = at<long long>(base, om);
+    TridPlan tp;  // the eigensolver as a batch runs it
+    tp.build({n}, {1}, c->smem_tridiag);
+    B.trid_min = tp.trid_min;
+    B.trid_max = tp.trid_max;
+    TB_CUDA(cudaMemset(base + ol, 0, 16));
     float ms = 0.f;
     for (int rep = 0; rep < 2; ++rep) {
       const tb_status us = upload(n);
       if (us != TB_OK) return us;
       TB_CUDA(cudaEventRecord(e0));
+      for (int cl = 0; cl < kTridClasses; ++cl)
+        if (tp.off[cl + 1] > tp.off[cl])
+          TB_CUDA(launch_trid(B, at<double>(base, oA), at<double>(base, oW), at<int>(base, os), nullptr,
+                              at<int>(base, ol), 1, kTridClusterSizes[cl], n, 0));
       k_syev<<<1, kEigThreads, syev_smem_bytes(n)>>>(B, at<double>(base, oA), at<double>(base, oZ),
                                                      at<double>(base, oW), at<double>(base, ow), at<int>(base, op),
                                                      at<int>(base, os), nullptr);
@@ -1239,7 +1320,6 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
   const double econv = 1.0e-6 * b->opt.accuracy, pconv = 2.0e-5 * b->opt.accuracy;
   const int ntile64 = (int)b->tiles64.size(), ntile32 = (int)b->tiles32.size(), nchunk = (int)b->chunks32.size();
   const int gemm_grid = std::min(ntile64, 148 * 8);
-  const size_t eig_smem = syev_smem_bytes(std::max(b->nmax_in, 1));
   const size_t fermi_smem = (size_t)b->nmax * sizeof(double);
   const dim3 pot_grid(nmol, nblk(std::max(b->natmax, b->nshmax), 256));
   std::vector<int> act, phase;
@@ -1282,9 +1362,14 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
     TB_K("gemm", 2.0 * n3, 1,
          k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 1, b->W, 0, nullptr, nullptr, nullptr,
                                            b->F, 1.0, 0.0, S.active, kGemmKUpToI | kGemmSym));
-    // symmetric eigensolve with vectors: canonical 4 N^3
+    // symmetric eigensolve with vectors: canonical 4 N^3 (k_trid_smem + k_syev)
+    {
+      const tb_status ts = launch_trid_plan(b, S.active, st);
+      if (ts != TB_OK) return ts;
+    }
     TB_K("syev", 4.0 * n3, 1,
-         k_syev<<<nmol, kEigThreads, eig_smem, st>>>(B, b->F, b->Z, b->W, b->w, b->perm, S.status, S.active));
+         k_syev<<<nmol, kEigThreads, syev_smem_bytes(std::max(b->nmax_in, 1)), st>>>(
+             B, b->F, b->Z, b->W, b->w, b->perm, S.status, S.active));
     if (b->njac > 0)
       TB_K("syev_jacobi", 0, 0,
            k_syev_jacobi<<<nblk(b->njac, kJacobiWarps), kJacobiWarps * 32, jacobi_smem_bytes(), st>>>(
@@ -1855,6 +1940,13 @@ tb_status tb_calculator_set_small_solver(tb_calculator* c, int32_t jacobi_max) {
   return TB_OK;
 }
 
+tb_status tb_calculator_set_smem_tridiag(tb_calculator* c, int32_t min_n) {
+  if (!c) return fail(TB_BAD_INPUT, "null calculator");
+  if (min_n < 0) return fail(TB_BAD_INPUT, "min_n must be 0 (never) or a size in AOs");
+  c->smem_tridiag = min_n;
+  return TB_OK;
+}
+
 int32_t tb_calculator_tuning(const tb_calculator* c, char* buf, int32_t len) {
   if (!c) return 0;
   std::ostringstream o;
@@ -1869,7 +1961,12 @@ int32_t tb_calculator_tuning(const tb_calculator* c, char* buf, int32_t len) {
     << ", \"inhouse_s\": {\"256\": " << c->eig.t_in[0] << ", \"512\": " << c->eig.t_in[1] << "}"
     << ", \"cusolver_s\": {\"256\": " << c->eig.t_lib[0] << ", \"1024\": " << c->eig.t_lib[1] << "}"
     << ", \"model\": {\"inhouse\": \"" << c->eig.a << " N^2 + " << c->eig.b << " N^3\", \"cusolver\": \""
-    << c->eig.c << " + " << c->eig.d << " N^3\"}, \"inhouse_limit\": " << kSyevMaxN << "}}";
+    << c->eig.c << " + " << c->eig.d << " N^3\"}, \"inhouse_limit\": " << kSyevMaxN << "}"
+    << ", \"smem_tridiag\": {\"min_n\": " << c->smem_tridiag << ", \"classes\": [";
+  for (int k = 0; k < kTridClasses; ++k)
+    o << (k ? ", " : "") << "{\"cluster\": " << kTridClusterSizes[k] << ", \"max_n\": " << kTridClassMax[k]
+      << ", \"smem_bytes\": " << trid_smem_bytes(kTridClassMax[k], kTridClusterSizes[k]) << "}";
+  o << "], \"smallest\": " << kTridMin << "}}";
   const std::string t = o.str();
   if (buf && len > 0) std::snprintf(buf, (size_t)len, "%s", t.c_str());
   return (int32_t)t.size();
@@ -2190,7 +2287,9 @@ struct MatBatch {
   void* lib_work = nullptr;
   size_t lib_bytes = 0;
   int* lib_info = nullptr;
-  tb_status build(int nmat, const int32_t* n) {
+  TridPlan trid;
+  int* d_tlist = nullptr;
+  tb_status build(int nmat, const int32_t* n, int smem_tridiag = kTridMin) {
     std::vector<int> ooff(nmat + 1, 0);
     std::vector<long long> moff(nmat + 1, 0);
     for (int m = 0; m < nmat; ++m) {
@@ -2210,6 +2309,12 @@ struct MatBatch {
       const std::string e = lib.workspace(nbig_max, &lib_bytes);
       if (!e.empty()) return fail(TB_CUDA_ERROR, "library eigensolver: " + e);
     }
+    {
+      std::vector<int> sizes(n, n + nmat);
+      std::vector<char> in_house(nmat);
+      for (int m = 0; m < nmat; ++m) in_house[m] = n[m] <= kSyevMaxN;
+      trid.build(sizes, in_house, smem_tridiag);
+    }
     h_moff = moff;
     h_ooff = ooff;
     n2 = moff[nmat];
@@ -2220,7 +2325,8 @@ struct MatBatch {
     size_t o_w = L.add(no * 8), o_f = L.add(no * 8), o_p = L.add(no * 4), o_k = L.add(nmat * 4);
     size_t o_st = L.add(nmat * 4), o_act = L.add(nmat * 4), o_nel = L.add(2 * nmat * 8), o_ets = L.add(nmat * 8),
            o_fw = L.add(nmat * 4), o_ef = L.add(nmat * 8), o_na = L.add(4);
-    size_t o_lw = L.add(std::max<size_t>(lib_bytes, 16)), o_li = L.add((2 * big.size() + 2) * 4);
+    size_t o_lw = L.add(std::max<size_t>(lib_bytes, 16)), o_li = L.add((2 * big.size() + 2) * 4),
+           o_tl = L.add((nmat + 1) * 4);
     TB_CUDA(arena.reserve(L.total));
     char* base = arena.base;
     TB_CUDA(cudaMemset(base, 0, L.total));
@@ -2231,6 +2337,11 @@ struct MatBatch {
     db.ooff = at<int>(base, o_ooff);
     db.moff = at<long long>(base, o_moff);
     db.lib_above = kSyevMaxN;
+    db.trid_min = trid.trid_min;
+    db.trid_max = trid.trid_max;
+    d_tlist = at<int>(base, o_tl);
+    if (!trid.list.empty())
+      TB_CUDA(cudaMemcpy(d_tlist, trid.list.data(), trid.list.size() * 4, cudaMemcpyHostToDevice));
     lib_work = base + o_lw;
     lib_info = at<int>(base, o_li);
     d_tiles = at<int4>(base, o_t);
@@ -2276,6 +2387,12 @@ tb_status tb_sygvd_batch(int32_t nmat, const int32_t* n, const double* H, const 
   {
     const tb_status ss = raise_smem_limits();
     if (ss != TB_OK) return ss;
+  }
+  for (int c = 0; c < kTridClasses; ++c) {
+    const int cnt = mb.trid.off[c + 1] - mb.trid.off[c];
+    if (cnt == 0) continue;
+    TB_CUDA(launch_trid(B, mb.F, mb.W, mb.ms.status, mb.ms.active, mb.d_tlist + mb.trid.off[c], cnt,
+                        kTridClusterSizes[c], mb.trid.nmax[c], 0));
   }
   k_syev<<<nmat, kEigThreads, smem>>>(B, mb.F, mb.Z, mb.W, mb.w, mb.perm, mb.ms.status, mb.ms.active);
   std::vector<int> fstat(nmat, 0);

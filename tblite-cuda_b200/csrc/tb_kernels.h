@@ -34,6 +34,34 @@ inline size_t syev_smem_bytes(int n, size_t elem = sizeof(double)) {
   return v * elem;
 }
 constexpr int kSyevMaxN = 1216;
+// k_trid_smem (tb_trid.cu): the tridiagonalisation of FP64 structures of
+// kTridMin..kTridClassMax[last] AOs held in the shared memory of a thread block
+// cluster of kTridClusterSizes[c] CTAs (class c: up to kTridClassMax[c] AOs,
+// the largest order whose tiles fit 227 KiB per CTA); k_syev then starts from
+// its output (DevBatch::trid_max)
+constexpr int kTridTile = 16;
+constexpr int kTridThreads = 512;
+constexpr int kTridMaxCluster = 8;
+constexpr int kTridClasses = 6;
+constexpr int kTridMin = 64;
+constexpr int kTridClusterSizes[kTridClasses] = {1, 2, 3, 4, 6, 8};
+constexpr int kTridClassMax[kTridClasses] = {208, 288, 352, 400, 480, 560};
+constexpr int kTridMaxN = 560;  // kTridClassMax[kTridClasses - 1]
+inline int trid_class_max(int c) { return kTridClassMax[c]; }
+// class of a structure of n AOs (-1: not handled)
+inline int trid_class_of(int n) {
+  if (n < kTridMin) return -1;
+  for (int c = 0; c < kTridClasses; ++c)
+    if (n <= kTridClassMax[c]) return c;
+  return -1;
+}
+int trid_cluster_for(int n);
+size_t trid_smem_bytes(int n, int C);
+cudaError_t trid_raise_limits();
+// structures list[0..cnt) (all of one class, cluster size C, at most nmax AOs):
+// reflectors into A, d | e | tau into the first 3n doubles of Sb's slice
+cudaError_t launch_trid(const DevBatch& B, double* A, double* Sb, const int* status, const int* active,
+                        const int* list, int cnt, int C, int nmax, cudaStream_t st);
 constexpr int kGemmThreads = 128;  // block size of k_gemm
 
 // cuSOLVER dense path for structures above the in-house size bound

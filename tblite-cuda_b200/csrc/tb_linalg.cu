@@ -1692,22 +1692,34 @@ __device__ __forceinline__ void syev_body(const DevBatch& B, T* __restrict__ Ab,
   __shared__ int q_done[kEigThreads / 32];  // sweeps finished, per consumer warp
   const int tid = threadIdx.x, nt = blockDim.x;
 
-  // symmetrise
-  for (int i = tid >> 5; i < n; i += nt >> 5)
-    for (int j = i + 1 + (tid & 31); j < n; j += 32) {
-      const T s = T(0.5) * (A[(long long)i * n + j] + A[(long long)j * n + i]);
-      A[(long long)i * n + j] = s;
-      A[(long long)j * n + i] = s;
+  if (sizeof(T) == 8 && Sb && B.trid_max > 0 && n >= B.trid_min && n >= kTridMin && n <= B.trid_max) {
+    // tridiagonalised in shared memory by k_trid_smem: reflectors in A's rows,
+    // d | e | tau in the first 3n entries of the scratch slice
+    const T* dte = Sb + mo;
+    for (int i = tid; i < n; i += nt) {
+      d[i] = dte[i];
+      e[i] = i < n - 1 ? dte[n + i] : T(0);
+      tau[i] = i < n - 2 ? dte[2 * n + i] : T(0);
     }
-  for (int i = tid; i < n; i += nt) { e[i] = T(0); tau[i] = T(0); }
-  __syncthreads();
+    __syncthreads();
+  } else {
+    // symmetrise
+    for (int i = tid >> 5; i < n; i += nt >> 5)
+      for (int j = i + 1 + (tid & 31); j < n; j += 32) {
+        const T s = T(0.5) * (A[(long long)i * n + j] + A[(long long)j * n + i]);
+        A[(long long)i * n + j] = s;
+        A[(long long)j * n + i] = s;
+      }
+    for (int i = tid; i < n; i += nt) { e[i] = T(0); tau[i] = T(0); }
+    __syncthreads();
 
-  // d: scratch until the end; the global scratch (8n entries) takes the partial products of symwalk
-  const bool symw = sizeof(T) == 8 && Sb && nt == 256 && n >= kSymMin + 1;
-  tridiagonalise<T>(A, n, e, tau, v, vn, p, w, d, ring, red, sh, symw ? Sb + mo : nullptr);
-  for (int i = tid; i < n; i += nt) d[i] = A[(long long)i * n + i];
-  if (tid == 0 && n >= 2) e[n - 2] = A[(long long)(n - 2) * n + n - 1];
-  __syncthreads();
+    // d: scratch until the end; the global scratch (8n entries) takes the partial products of symwalk
+    const bool symw = sizeof(T) == 8 && Sb && nt == 256 && n >= kSymMin + 1;
+    tridiagonalise<T>(A, n, e, tau, v, vn, p, w, d, ring, red, sh, symw ? Sb + mo : nullptr);
+    for (int i = tid; i < n; i += nt) d[i] = A[(long long)i * n + i];
+    if (tid == 0 && n >= 2) e[n - 2] = A[(long long)(n - 2) * n + n - 1];
+    __syncthreads();
+  }
 
   form_q<T>(A, Z, n, tau, ring, tau + n, Sb ? Sb + mo : nullptr);
 

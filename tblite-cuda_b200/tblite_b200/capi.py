@@ -68,8 +68,8 @@ EXPORTS = [
     "tb_add_pot_to_h1", "tb_sygvd_batch", "tb_fermi_filling", "tb_batch_profile",
     "tb_server_create", "tb_server_submit", "tb_server_step", "tb_server_poll", "tb_server_destroy",
     "tb_batch_set_guess", "tb_batch_wavefunction", "tb_batch_gradient", "tb_sygvd_noalloc",
-    "tb_calculator_set_small_solver", "tb_calculator_tuning", "tb_bounds_check_build", "tb_bounds_violations",
-    "tb_server_compactions",
+    "tb_calculator_set_small_solver", "tb_calculator_set_smem_tridiag", "tb_calculator_tuning",
+    "tb_bounds_check_build", "tb_bounds_violations", "tb_server_compactions",
 ]
 
 _lib = None
@@ -108,6 +108,7 @@ def load_library(path: str = LIB_PATH):
     L.tb_server_compactions.argtypes = [C.c_void_p]
     L.tb_server_compactions.restype = C.c_int64
     L.tb_calculator_set_small_solver.argtypes = [C.c_void_p, C.c_int32]
+    L.tb_calculator_set_smem_tridiag.argtypes = [C.c_void_p, C.c_int32]
     L.tb_bounds_check_build.restype = C.c_int32
     L.tb_calculator_tuning.argtypes = [C.c_void_p, C.c_char_p, C.c_int32]
     L.tb_calculator_tuning.restype = C.c_int32
@@ -216,6 +217,16 @@ class Calculator:
         0 never the one-warp Jacobi solver, 1..32 Jacobi up to that many AOs."""
         check(load_library().tb_calculator_set_small_solver(self.h, C.c_int32(jacobi_max)),
               "tb_calculator_set_small_solver")
+
+    def set_smem_tridiag(self, min_n):
+        """FP64 tridiagonalisation in cluster shared memory (k_trid_smem) for
+        structures of at least min_n AOs (and 64..560): lower latency per
+        structure, more SM time.  True means every size from 64, False or 0
+        none (the default)."""
+        if min_n is True:
+            min_n = 64
+        check(load_library().tb_calculator_set_smem_tridiag(self.h, C.c_int32(int(min_n))),
+              "tb_calculator_set_smem_tridiag")
 
     def tuning(self) -> dict:
         """The autotuner's measurements and choices (tb_calculator_tuning)."""
