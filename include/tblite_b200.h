@@ -80,7 +80,7 @@ typedef struct tb_options {
 /* Per-structure results: the energy/wavefunction outputs of xtb_singlepoint.
  * Array pointers are caller-owned and may be NULL (not written). */
 typedef struct tb_result {
-  double energy;          /* total energy = e_elec + e_rep                     */
+  double energy;          /* total energy = e_elec + e_rep + e_disp            */
   double e_rep;           /* classical repulsion                               */
   double e_elec;          /* electronic: band + (-TS) + ES2 + AES2 + ES3        */
   double e_band, e_ts, e_es2, e_aes2, e_es3;
@@ -98,6 +98,7 @@ typedef struct tb_result {
    * virial sum_A gradient_A R_A^T (row-major 3x3), written with gradient */
   double* gradient;
   double sigma[9];
+  double e_disp;          /* D4 dispersion (0 without a D4 parameter block)     */
 } tb_result;
 
 /* wavefunction_type (src/wavefunction/type.h:81-99) of one structure, as the
@@ -293,6 +294,15 @@ tb_status tb_atomic_properties(const tb_calculator* calc, const tb_structure* mo
 
 /* get_engrad energy part (src/xtb.cu:47-182): erep[nat]. */
 tb_status tb_repulsion(const tb_calculator* calc, const tb_structure* mol, double* erep);
+
+/* dispersion_get_engrad (src/xtb.cu:274-277, a TODO in the reference; tblite
+ * calls dftd4 there): D4 dispersion of the geometry at the neutral reference
+ * charges from the parameter file's D4 block -- edisp[nat] per-atom energies,
+ * gradient[nat][3] and sigma[3][3] (either may be NULL); all zero when the
+ * parameter file has no D4 block.  tb_singlepoint_batch adds the same term to
+ * the energy (tb_result.e_disp) and to the gradient. */
+tb_status tb_dispersion(const tb_calculator* calc, const tb_structure* mol, double* edisp, double* gradient,
+                        double* sigma);
 
 /* get_hamiltonian (src/h0.cu:292-502) incl. on-site blocks: S, H0 [nao][nao],
  * D [3][nao][nao], Q [6][nao][nao]. */

@@ -44,6 +44,11 @@ struct Element {
   double rad = 0, rcov = 0, en = 0, rep_alpha = 0, rep_zeff = 0, mp_rad = 0, mp_vcn = 0;
   double dkernel = 0, qkernel = 0;
   std::vector<Shell> sh;
+  // D4 dispersion (optional block): r4/r2 factor and the reference systems'
+  // coordination numbers and polarizabilities alpha(i w) on the frequency grid
+  double d4_r4r2 = 0;
+  std::vector<double> d4_cn;
+  std::vector<std::vector<double>> d4_alpha;
 };
 
 }  // namespace
@@ -54,6 +59,10 @@ struct orc_params {
   std::map<std::pair<int, int>, double> kpair;
   std::vector<Element> el;
   double min_alpha = 1e300;
+  // D4: frequency grid and quadrature weights (empty: no dispersion), and the
+  // reference C6 of every pair of reference systems, c6ref[(a nel + b) R^2 + i R + j]
+  std::vector<double> d4_freq, d4_wts, d4_c6ref;
+  int d4_nref_max = 0;
   double glob(const char* k) const {
     auto it = g.find(k);
     return it == g.end() ? 0.0 : it->second;
@@ -102,8 +111,19 @@ bool load_params(const char* path, orc_params& P, std::string& err) {
         if (s.ang < 0 || s.ang > kMaxL || s.nprim < 1 || s.nprim > kMaxPrim) { err = "bad shell"; return false; }
         cur->sh.push_back(s); csh = &cur->sh.back(); continue;
       }
+      if (key == "d4_ref") {
+        double cn = 0;
+        is >> cn;
+        std::vector<double> a(P.d4_freq.size());
+        for (double& x : a) is >> x;
+        if (P.d4_freq.empty() || !is) { err = "d4_ref before d4freq or short"; return false; }
+        cur->d4_cn.push_back(cn);
+        cur->d4_alpha.push_back(a);
+        continue;
+      }
       double v; is >> v;
       if (key == "rad") cur->rad = v;
+      else if (key == "d4_r4r2") cur->d4_r4r2 = v;
       else if (key == "rcov") cur->rcov = v;
       else if (key == "en") cur->en = v;
       else if (key == "rep_alpha") cur->rep_alpha = v;
@@ -116,6 +136,15 @@ bool load_params(const char* path, orc_params& P, std::string& err) {
       continue;
     }
     if (key == "global") { std::string k; double v; is >> k >> v; P.g[k] = v; continue; }
+    if (key == "d4freq" || key == "d4wts") {
+      int nf = 0;
+      is >> nf;
+      std::vector<double>& dst = key == "d4freq" ? P.d4_freq : P.d4_wts;
+      dst.resize(nf > 0 ? nf : 0);
+      for (double& x : dst) is >> x;
+      if (nf <= 0 || !is) { err = "bad " + key; return false; }
+      continue;
+    }
     if (key == "kshell") { int a, b; double v; is >> a >> b >> v; P.kshell[a][b] = P.kshell[b][a] = v; continue; }
     if (key == "kpair") { std::string a, b; double v; is >> a >> b >> v; kp.emplace_back(a, b, v); continue; }
     if (key == "element") {
@@ -130,6 +159,27 @@ bool load_params(const char* path, orc_params& P, std::string& err) {
     P.kpair[{a, b}] = P.kpair[{b, a}] = std::get<2>(t);
   }
   for (auto& e : P.el) for (auto& s : e.sh) for (int i = 0; i < s.nprim; ++i) P.min_alpha = std::min(P.min_alpha, s.alpha[i]);
+  if (!P.d4_freq.empty()) {
+    // reference C6 by the Casimir-Polder integral, C6 = 3/pi int alpha_A(iw) alpha_B(iw) dw,
+    // on the file's quadrature
+    if (P.d4_wts.size() != P.d4_freq.size()) { err = "d4wts and d4freq differ in length"; return false; }
+    const int ne = (int)P.el.size();
+    int R = 0;
+    for (auto& e : P.el) {
+      if (e.d4_cn.empty()) { err = "element " + e.sym + " has no d4_ref"; return false; }
+      R = std::max(R, (int)e.d4_cn.size());
+    }
+    P.d4_nref_max = R;
+    P.d4_c6ref.assign((size_t)ne * ne * R * R, 0.0);
+    for (int a = 0; a < ne; ++a)
+      for (int b = 0; b < ne; ++b)
+        for (size_t i = 0; i < P.el[a].d4_cn.size(); ++i)
+          for (size_t j = 0; j < P.el[b].d4_cn.size(); ++j) {
+            double c = 0.0;
+            for (size_t k = 0; k < P.d4_freq.size(); ++k) c += P.d4_wts[k] * P.el[a].d4_alpha[i][k] * P.el[b].d4_alpha[j][k];
+            P.d4_c6ref[((size_t)a * ne + b) * R * R + i * R + j] = 3.0 / M_PI * c;
+          }
+  }
   return !P.el.empty();
 }
 
@@ -541,6 +591,180 @@ void repulsion(const orc_params& P, int nat, const int* id, const double* xyz, d
       erep[jat] += 0.5 * dE;
     }
   }
+}
+
+// ------------------------------------------------------------------ D4 dispersion
+// dispersion_get_engrad (reference src/xtb.cu:274-277, where it is a TODO:
+// tblite calls dftd4, which the reference does not vendor and whose version it
+// does not pin).  Restated from the published D4 model (E. Caldeweyher et al.,
+// J. Chem. Phys. 150, 154122 (2019)) on the parameter file's D4 block, at the
+// neutral reference charges -- the reference's call site precedes the SCF, so
+// no charges exist there; the charge scaling of the reference polarizabilities
+// is therefore the identity:
+//  * CN_A = sum_B f_EN(A, B) (1 + erf(-k0 (r_AB / Rc_AB - 1))) / 2, with
+//    Rc_AB = k1 (rcov_A + rcov_B) and f_EN = k4 exp(-(|EN_A - EN_B| + k5)^2 / k6),
+//    pairs within d4_cn_cut;
+//  * reference weights W_A^i = exp(-wf (CN_A - CN_i)^2) / sum_j exp(-wf (CN_A - CN_j)^2);
+//  * C6_AB = sum_ij W_A^i W_B^j C6ref_ij (Casimir-Polder on the file's grid),
+//    C8_AB = C6_AB q_AB with q_AB = 3 sqrt(r4r2_A r4r2_B), R_AB = a1 sqrt(q_AB) + a2;
+//  * two-body (rational damping), pairs within d4_pair_cut:
+//    E_AB = -C6 (s6 / (r^6 + R^6) + s8 q / (r^8 + R^8));
+//  * three-body (Axilrod-Teller-Muto), triples with all three distances within
+//    d4_atm_cut: E_ABC = s9 sqrt(C6_AB C6_BC C6_CA) (1 + 3 P / (8 u v w)) f / (r_AB r_BC r_CA)^3,
+//    u, v, w the squared distances, P = (u+v-w)(u+w-v)(v+w-u) (so the bracket is
+//    1 + 3 cos a cos b cos c), f = 1 / (1 + 6 t^(alp/3)), t = R_AB R_BC R_CA / (r_AB r_BC r_CA);
+//  * energies split evenly over the atoms of a pair or triple; the analytic
+//    gradient includes the CN dependence of C6 (dW/dCN, dCN/dR).
+struct D4Consts {
+  double s6, s8, a1, a2, s9, alp, wf, k0, k1, k4, k5, k6, cn_cut, atm_cut, pair_cut;
+  explicit D4Consts(const orc_params& P)
+      : s6(P.glob("d4_s6")), s8(P.glob("d4_s8")), a1(P.glob("d4_a1")), a2(P.glob("d4_a2")), s9(P.glob("d4_s9")),
+        alp(P.glob("d4_alp")), wf(P.glob("d4_wf")), k0(P.glob("d4_k0")), k1(P.glob("d4_k1")), k4(P.glob("d4_k4")),
+        k5(P.glob("d4_k5")), k6(P.glob("d4_k6")), cn_cut(P.glob("d4_cn_cut")), atm_cut(P.glob("d4_atm_cut")),
+        pair_cut(P.glob("d4_pair_cut")) {}
+};
+
+// counting function of the D4 coordination number and its derivative in r
+double d4_count(const D4Consts& c, const Element& ea, const Element& eb, double r, double* dcdr) {
+  const double rc = c.k1 * (ea.rcov + eb.rcov);
+  const double den = c.k4 * std::exp(-std::pow(std::fabs(ea.en - eb.en) + c.k5, 2) / c.k6);
+  const double x = c.k0 * (r / rc - 1.0);
+  if (dcdr) *dcdr = den * (-1.0 / std::sqrt(M_PI)) * std::exp(-x * x) * c.k0 / rc;
+  return den * 0.5 * (1.0 + std::erf(-x));
+}
+
+void dispersion(const orc_params& P, int nat, const int* id, const double* xyz, double* e_at, double* grad) {
+  for (int a = 0; a < nat; ++a) e_at[a] = 0.0;
+  if (P.d4_freq.empty() || nat <= 0) return;
+  const D4Consts c(P);
+  const int R = P.d4_nref_max, ne = (int)P.el.size();
+  auto dist = [&](int a, int b, double* v) {
+    for (int k = 0; k < 3; ++k) v[k] = xyz[3 * a + k] - xyz[3 * b + k];
+    return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  };
+  // coordination numbers, weights and their CN derivatives
+  std::vector<double> cn(nat, 0.0), W((size_t)nat * R, 0.0), dW((size_t)nat * R, 0.0), dEdcn(nat, 0.0);
+  for (int a = 0; a < nat; ++a)
+    for (int b = 0; b < nat; ++b) {
+      if (b == a) continue;
+      double v[3];
+      const double r = dist(a, b, v);
+      if (r > c.cn_cut || r < 1.0e-6) continue;
+      cn[a] += d4_count(c, P.el[id[a]], P.el[id[b]], r, nullptr);
+    }
+  for (int a = 0; a < nat; ++a) {
+    const Element& e = P.el[id[a]];
+    const int nr = (int)e.d4_cn.size();
+    double gmax = -1e300;
+    for (int i = 0; i < nr; ++i) gmax = std::max(gmax, -c.wf * std::pow(cn[a] - e.d4_cn[i], 2));
+    double sum = 0.0, gp = 0.0;
+    for (int i = 0; i < nr; ++i) sum += std::exp(-c.wf * std::pow(cn[a] - e.d4_cn[i], 2) - gmax);
+    for (int i = 0; i < nr; ++i) {
+      W[(size_t)a * R + i] = std::exp(-c.wf * std::pow(cn[a] - e.d4_cn[i], 2) - gmax) / sum;
+      gp += W[(size_t)a * R + i] * (-2.0 * c.wf * (cn[a] - e.d4_cn[i]));
+    }
+    for (int i = 0; i < nr; ++i)
+      dW[(size_t)a * R + i] = W[(size_t)a * R + i] * (-2.0 * c.wf * (cn[a] - e.d4_cn[i]) - gp);
+  }
+  // C6 of a pair and its derivatives in CN_a, CN_b
+  auto c6 = [&](int a, int b, double* dca, double* dcb) {
+    const double* t = P.d4_c6ref.data() + ((size_t)id[a] * ne + id[b]) * R * R;
+    const int na = (int)P.el[id[a]].d4_cn.size(), nb = (int)P.el[id[b]].d4_cn.size();
+    double v = 0.0, da = 0.0, db = 0.0;
+    for (int i = 0; i < na; ++i)
+      for (int j = 0; j < nb; ++j) {
+        const double r = t[i * R + j];
+        v += W[(size_t)a * R + i] * W[(size_t)b * R + j] * r;
+        da += dW[(size_t)a * R + i] * W[(size_t)b * R + j] * r;
+        db += W[(size_t)a * R + i] * dW[(size_t)b * R + j] * r;
+      }
+    if (dca) *dca = da;
+    if (dcb) *dcb = db;
+    return v;
+  };
+  auto qpair = [&](int a, int b) { return 3.0 * std::sqrt(P.el[id[a]].d4_r4r2 * P.el[id[b]].d4_r4r2); };
+  auto radius = [&](int a, int b) { return c.a1 * std::sqrt(qpair(a, b)) + c.a2; };
+  auto addg = [&](int a, int b, double dedr, const double* v, double r) {
+    if (!grad) return;
+    for (int k = 0; k < 3; ++k) {
+      grad[3 * a + k] += dedr * v[k] / r;
+      grad[3 * b + k] -= dedr * v[k] / r;
+    }
+  };
+  // two-body
+  for (int a = 0; a < nat; ++a)
+    for (int b = 0; b < a; ++b) {
+      double v[3];
+      const double r = dist(a, b, v);
+      if (r > c.pair_cut || r < 1.0e-6) continue;
+      double dca, dcb;
+      const double C6 = c6(a, b, &dca, &dcb), q = qpair(a, b), Rab = radius(a, b);
+      const double r2 = r * r, r6 = r2 * r2 * r2, r8 = r6 * r2, R2 = Rab * Rab, R6 = R2 * R2 * R2, R8 = R6 * R2;
+      const double h = c.s6 / (r6 + R6) + c.s8 * q / (r8 + R8);
+      const double dh = -c.s6 * 6.0 * r6 / r / ((r6 + R6) * (r6 + R6)) - c.s8 * q * 8.0 * r8 / r / ((r8 + R8) * (r8 + R8));
+      const double e = -C6 * h;
+      e_at[a] += 0.5 * e;
+      e_at[b] += 0.5 * e;
+      dEdcn[a] += -h * dca;
+      dEdcn[b] += -h * dcb;
+      addg(a, b, -C6 * dh, v, r);
+    }
+  // three-body
+  if (c.s9 != 0.0)
+    for (int a = 0; a < nat; ++a)
+      for (int b = 0; b < a; ++b) {
+        double vab[3];
+        const double rab = dist(a, b, vab);
+        if (rab > c.atm_cut || rab < 1.0e-6) continue;
+        for (int d = 0; d < b; ++d) {
+          double vbd[3], vda[3];
+          const double rbd = dist(b, d, vbd), rda = dist(d, a, vda);
+          if (rbd > c.atm_cut || rda > c.atm_cut || rbd < 1.0e-6 || rda < 1.0e-6) continue;
+          double dab_a, dab_b, dbd_b, dbd_d, dda_d, dda_a;
+          const double cab = c6(a, b, &dab_a, &dab_b), cbd = c6(b, d, &dbd_b, &dbd_d), cda = c6(d, a, &dda_d, &dda_a);
+          const double K = c.s9 * std::sqrt(cab * cbd * cda);
+          const double u = rab * rab, vv = rbd * rbd, w = rda * rda;
+          const double f1 = u + vv - w, f2 = u + w - vv, f3 = vv + w - u;
+          const double Pp = f1 * f2 * f3, uvw = u * vv * w;
+          const double ang = 1.0 + 3.0 * Pp / (8.0 * uvw);
+          const double r3 = rab * rbd * rda, r9 = r3 * r3 * r3;
+          const double t = radius(a, b) * radius(b, d) * radius(d, a) / r3, p = c.alp / 3.0, tp = std::pow(t, p);
+          const double fd = 1.0 / (1.0 + 6.0 * tp);
+          const double g = ang * fd / r9;
+          const double E = K * g;
+          e_at[a] += E / 3.0;
+          e_at[b] += E / 3.0;
+          e_at[d] += E / 3.0;
+          // CN dependence through the three C6 (K ~ sqrt of their product)
+          dEdcn[a] += 0.5 * E * (dab_a / cab + dda_a / cda);
+          dEdcn[b] += 0.5 * E * (dab_b / cab + dbd_b / cbd);
+          dEdcn[d] += 0.5 * E * (dbd_d / cbd + dda_d / cda);
+          if (grad) {
+            const double dPu = f2 * f3 + f1 * f3 - f1 * f2, dPv = f2 * f3 - f1 * f3 + f1 * f2,
+                         dPw = -f2 * f3 + f1 * f3 + f1 * f2;
+            const double pre = 3.0 / (8.0 * uvw);
+            const double dang_u = pre * (dPu - Pp / u), dang_v = pre * (dPv - Pp / vv), dang_w = pre * (dPw - Pp / w);
+            const double dfd = 6.0 * p * tp * fd * fd;  // times 1 / r_xy: d fd / d r_xy
+            auto dgdr = [&](double dang_x, double rx) {
+              return K * ((dang_x * 2.0 * rx) * fd / r9 + ang * (dfd / rx) / r9 - 3.0 * ang * fd / (r9 * rx));
+            };
+            addg(a, b, dgdr(dang_u, rab), vab, rab);
+            addg(b, d, dgdr(dang_v, rbd), vbd, rbd);
+            addg(d, a, dgdr(dang_w, rda), vda, rda);
+          }
+        }
+      }
+  // coordination-number chain
+  if (grad)
+    for (int a = 0; a < nat; ++a)
+      for (int b = 0; b < a; ++b) {
+        double v[3];
+        const double r = dist(a, b, v);
+        if (r > c.cn_cut || r < 1.0e-6) continue;
+        double dcdr;
+        d4_count(c, P.el[id[a]], P.el[id[b]], r, &dcdr);
+        addg(a, b, (dEdcn[a] + dEdcn[b]) * dcdr, v, r);
+      }
 }
 
 // ------------------------------------------------------------------ coulomb
@@ -1122,6 +1346,11 @@ int singlepoint(const orc_params& P, int nat, const int* id, const double* xyz, 
   repulsion(P, nat, id, xyz, erep.data());
   double e_rep = 0.0;
   for (double x : erep) e_rep += x;
+  // dispersion (reference src/xtb.cu:274-277; zero without a D4 block)
+  std::vector<double> edisp(nat);
+  dispersion(P, nat, id, xyz, edisp.data(), nullptr);
+  double e_disp = 0.0;
+  for (double x : edisp) e_disp += x;
   // coordination number, Coulomb caches (src/xtb.cu:284-288, :326-331)
   std::vector<double> cn(nat);
   coordination_number(P, nat, id, xyz, cn.data());
@@ -1224,7 +1453,7 @@ int singlepoint(const orc_params& P, int nat, const int* id, const double* xyz, 
     if (opt.verbosity > 0)
       std::printf("%7d %24.13f %16.7e %16.7e\n", iscf, eelec + e_rep, eelec - elast, mixer.error());
   }
-  res.e_rep = e_rep; res.e_elec = eelec; res.energy = eelec + e_rep;
+  res.e_rep = e_rep; res.e_elec = eelec; res.e_disp = e_disp; res.energy = eelec + e_rep + e_disp;
   res.e_band = e_band; res.e_ts = e_ts; res.e_es2 = e_es2; res.e_aes2 = e_aes2; res.e_es3 = e_es3;
   res.iterations = iscf;
   for (int k = 0; k < 3; ++k) {
@@ -1586,6 +1815,10 @@ void singlepoint_gradient(const orc_params& P, int nat, const int* id, const dou
         }
       }
   }
+  {  // dispersion (no-op without a D4 block)
+    std::vector<double> edisp(nat);
+    dispersion(P, nat, id, xyz, edisp.data(), grad);
+  }
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b) {
       double s = 0.0;
@@ -1679,6 +1912,25 @@ int orc_hamiltonian(const orc_params* p, int nat, const int* id, const double* x
   get_hamiltonian(*p, B, id, xyz, se.data(), S, H0, D, Q);
   return ORC_OK;
 }
+int orc_dispersion(const orc_params* p, int nat, const int* id, const double* xyz, double* edisp_at, double* grad,
+                   double* sigma) {
+  if (nat <= 0) return ORC_BAD_INPUT;
+  for (int i = 0; i < nat; ++i)
+    if (id[i] < 0 || id[i] >= (int)p->el.size()) return ORC_BAD_INPUT;
+  std::vector<double> g(3 * (size_t)nat, 0.0);
+  dispersion(*p, nat, id, xyz, edisp_at, g.data());
+  if (grad) std::copy(g.begin(), g.end(), grad);
+  if (sigma)
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double s = 0.0;
+        for (int i = 0; i < nat; ++i) s += g[3 * i + a] * xyz[3 * i + b];
+        sigma[3 * a + b] = s;
+      }
+  return ORC_OK;
+}
+int orc_has_dispersion(const orc_params* p) { return p->d4_freq.empty() ? 0 : 1; }
+
 int orc_repulsion(const orc_params* p, int nat, const int* id, const double* xyz, double* erep_at) {
   repulsion(*p, nat, id, xyz, erep_at);
   return ORC_OK;

@@ -40,13 +40,14 @@ typedef struct orc_options {
 } orc_options;
 
 typedef struct orc_result {
-  double energy;         /* total = e_elec + e_rep */
+  double energy;         /* total = e_elec + e_rep + e_disp */
   double e_rep, e_elec;  /* repulsion; electronic incl. Coulomb and -TS */
   double e_band, e_ts, e_es2, e_aes2, e_es3;
   double dipole[3];
   int iterations;
   int status;            /* 0 ok, see ORC_* below */
   int nsh, nao;
+  double e_disp;         /* D4 dispersion (0 without a D4 block in the parameter file) */
 } orc_result;
 
 enum { ORC_OK = 0, ORC_BAD_INPUT = 1, ORC_NOT_SPD = 2, ORC_SCF_NOT_CONVERGED = 3,
@@ -71,6 +72,13 @@ int orc_selfenergy(const orc_params* p, int nat, const int* id, const double* cn
 int orc_hamiltonian(const orc_params* p, int nat, const int* id, const double* xyz,
                     double* S, double* H0, double* D, double* Q);
 int orc_repulsion(const orc_params* p, int nat, const int* id, const double* xyz, double* erep_at);
+/* dispersion_get_engrad (src/xtb.cu:274-277): D4 at the neutral reference
+ * charges from the parameter file's D4 block; per-atom energies, gradient
+ * grad[nat][3] and virial sigma[3][3] (either may be NULL); all zero without
+ * a D4 block (orc_has_dispersion returns 0). */
+int orc_dispersion(const orc_params* p, int nat, const int* id, const double* xyz, double* edisp_at, double* grad,
+                   double* sigma);
+int orc_has_dispersion(const orc_params* p);
 int orc_coulomb_matrices(const orc_params* p, int nat, const int* id, const double* xyz,
                          double* gamma, double* amat_sd, double* amat_dd, double* amat_sq);
 int orc_coulomb_potential(const orc_params* p, int nat, const int* id, const double* xyz,

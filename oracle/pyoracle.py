@@ -26,7 +26,8 @@ class Result(C.Structure):
     _fields_ = [("energy", C.c_double), ("e_rep", C.c_double), ("e_elec", C.c_double),
                 ("e_band", C.c_double), ("e_ts", C.c_double), ("e_es2", C.c_double),
                 ("e_aes2", C.c_double), ("e_es3", C.c_double), ("dipole", C.c_double * 3),
-                ("iterations", C.c_int), ("status", C.c_int), ("nsh", C.c_int), ("nao", C.c_int)]
+                ("iterations", C.c_int), ("status", C.c_int), ("nsh", C.c_int), ("nao", C.c_int),
+                ("e_disp", C.c_double)]
 
 
 def _d(a):
@@ -63,7 +64,8 @@ def lib():
         for name in ("orc_basis_size", "orc_basis_maps", "orc_coordination_number", "orc_mrad",
                      "orc_selfenergy", "orc_hamiltonian", "orc_repulsion", "orc_coulomb_matrices",
                      "orc_coulomb_potential", "orc_coulomb_energy", "orc_fock", "orc_mulliken",
-                     "orc_singlepoint", "orc_singlepoint_batch", "orc_singlepoint_spin", "orc_singlepoint_gradient", "orc_multipole_cgto", "orc_nspecies"):
+                     "orc_singlepoint", "orc_singlepoint_batch", "orc_singlepoint_spin", "orc_singlepoint_gradient", "orc_multipole_cgto", "orc_nspecies",
+                     "orc_dispersion", "orc_has_dispersion"):
             getattr(L, name).argtypes = None
             getattr(L, name).restype = C.c_int
         L.orc_default_options.argtypes = [C.POINTER(Options)]
@@ -165,6 +167,16 @@ class Oracle:
         lib().orc_repulsion(self.h, C.c_int(len(ids)), _i(ids), _d(xyz), _d(e))
         return e
 
+    def dispersion(self, ids, xyz):
+        """D4 dispersion (orc_dispersion): per-atom energies, gradient [nat][3], virial [3][3]."""
+        ids = np.ascontiguousarray(ids, np.int32); xyz = np.ascontiguousarray(xyz, np.float64)
+        e, g, s = np.zeros(len(ids)), np.zeros((len(ids), 3)), np.zeros((3, 3))
+        lib().orc_dispersion(self.h, C.c_int(len(ids)), _i(ids), _d(xyz), _d(e), _d(g), _d(s))
+        return e, g, s
+
+    def has_dispersion(self):
+        return bool(lib().orc_has_dispersion(self.h))
+
     def coulomb_matrices(self, ids, xyz):
         ids = np.ascontiguousarray(ids, np.int32); xyz = np.ascontiguousarray(xyz, np.float64)
         nsh, _ = self.basis_size(ids)
@@ -243,7 +255,7 @@ class Oracle:
                               C.c_int(mol.uhf), C.byref(o), C.byref(r), *[_d(out[k]) for k in
                               ("qat", "qsh", "dpat", "qpat", "emo", "P")])
         out.update(energy=r.energy, e_rep=r.e_rep, e_elec=r.e_elec, e_band=r.e_band, e_ts=r.e_ts,
-                   e_es2=r.e_es2, e_aes2=r.e_aes2, e_es3=r.e_es3, dipole=np.array(r.dipole[:]),
+                   e_es2=r.e_es2, e_aes2=r.e_aes2, e_es3=r.e_es3, e_disp=r.e_disp, dipole=np.array(r.dipole[:]),
                    iterations=r.iterations, status=r.status)
         return out
 

@@ -9,6 +9,7 @@ namespace tb {
 constexpr int kMaxL = 2;        // s, p, d
 constexpr int kMaxPrim = 12;    // maxg (reference src/limits.h:18)
 constexpr int kMaxShPerAtom = 3;
+constexpr int kD4MaxRef = 4;    // D4 reference systems per element (parameter file)
 
 // One shell type of one species (cgto_type, src/basis/type.h:18-23, plus the
 // per-shell Hamiltonian parameters of tb_hamiltonian, src/h0.h:27-40).
@@ -22,6 +23,10 @@ struct ShellParam {
 struct SpeciesParam {
   int z, nsh, sh0;  // sh0: index of the first ShellParam of this species
   double rad, rcov, en, rep_alpha, rep_zeff, mp_rad, mp_vcn, dkernel, qkernel;
+  // D4 dispersion: r4/r2 factor, reference systems and their coordination numbers
+  double d4_r4r2;
+  int d4_nref;
+  double d4_cn[kD4MaxRef];
 };
 
 // Calculator parameters as seen by kernels (passed by value).
@@ -33,6 +38,13 @@ struct DevParams {
   double gexp, kdmp3, kdmp5, mp_shift, mp_kexp, mp_rmax;
   double rep_kexp, rep_kexp_light, rep_rexp, cn_cutoff, rep_cutoff;
   double intcut, cutoff;  // integral screening (25) and neighbour-list cutoff
+  // D4 dispersion (d4 = 0: the parameter file has no D4 block): reference C6 of
+  // species pair (a, b), references (i, j) at ((a nsp + b) kD4MaxRef + i) kD4MaxRef + j,
+  // and the model's constants (tb_disp.cu)
+  int d4;
+  const double* d4_c6ref;
+  double d4_s6, d4_s8, d4_a1, d4_a2, d4_s9, d4_alp, d4_wf, d4_k0, d4_k1, d4_k4, d4_k5, d4_k6;
+  double d4_cn_cut, d4_atm_cut, d4_pair_cut;
 };
 
 // Per-batch layout: structures packed back to back.  Offsets are [nmol+1].

@@ -63,6 +63,10 @@ struct HostParams {
   std::vector<ShellParam> sh;
   std::vector<std::string> sym;
   double min_alpha = 1e300;
+  // D4 block: frequency grid, quadrature weights, per species the reference
+  // polarizabilities alpha(i w) on the grid (empty grid: no dispersion)
+  std::vector<double> d4_freq, d4_wts;
+  std::vector<std::vector<std::vector<double>>> d4_alpha;
   double glob(const char* k, double dflt = 0.0) const {
     auto it = g.find(k);
     return it == g.end() ? dflt : it->second;
@@ -117,8 +121,20 @@ bool parse_params(const char* path, HostParams& P, std::string& err) {
         csh = (int)shells[cur].size() - 1;
         continue;
       }
+      if (key == "d4_ref") {
+        double cn = 0;
+        std::vector<double> a(P.d4_freq.size());
+        is >> cn;
+        for (double& x : a) is >> x;
+        if (P.d4_freq.empty() || !is) return bad("d4_ref before d4freq, or short");
+        if (e.d4_nref >= kD4MaxRef) return bad("more than " + std::to_string(kD4MaxRef) + " D4 references");
+        e.d4_cn[e.d4_nref++] = cn;
+        P.d4_alpha[cur].push_back(a);
+        continue;
+      }
       double v; if (!(is >> v)) return bad("missing value for " + key);
       if (key == "rad") e.rad = v;
+      else if (key == "d4_r4r2") e.d4_r4r2 = v;
       else if (key == "rcov") e.rcov = v;
       else if (key == "en") e.en = v;
       else if (key == "rep_alpha") e.rep_alpha = v;
@@ -131,6 +147,15 @@ bool parse_params(const char* path, HostParams& P, std::string& err) {
       continue;
     }
     if (key == "global") { std::string k; double v; if (!(is >> k >> v)) return bad("bad global"); P.g[k] = v; continue; }
+    if (key == "d4freq" || key == "d4wts") {
+      int nf = 0;
+      std::vector<double>& dst = key == "d4freq" ? P.d4_freq : P.d4_wts;
+      if (!(is >> nf) || nf <= 0 || nf > 256) return bad("bad " + key);
+      dst.resize(nf);
+      for (double& x : dst) is >> x;
+      if (!is) return bad("short " + key);
+      continue;
+    }
     if (key == "kshell") { int a, b; double v; if (!(is >> a >> b >> v) || a < 0 || b < 0 || a > 2 || b > 2) return bad("bad kshell"); P.kshell[a][b] = P.kshell[b][a] = v; continue; }
     if (key == "kpair") { std::string a, b; double v; if (!(is >> a >> b >> v)) return bad("bad kpair"); kp.emplace_back(a, b, v); continue; }
     if (key == "element") {
@@ -139,6 +164,7 @@ bool parse_params(const char* path, HostParams& P, std::string& err) {
       if (!(is >> sym >> e.z)) return bad("bad element line");
       P.sp.push_back(e);
       P.sym.push_back(sym);
+      P.d4_alpha.emplace_back();
       shells.emplace_back();
       cur = (int)P.sp.size() - 1;
       continue;
@@ -147,6 +173,11 @@ bool parse_params(const char* path, HostParams& P, std::string& err) {
   }
   if (!fmt) { err = "missing or unsupported 'format' line"; return false; }
   if (P.sp.empty()) { err = "no elements"; return false; }
+  if (!P.d4_freq.empty()) {
+    if (P.d4_wts.size() != P.d4_freq.size()) { err = "d4wts and d4freq differ in length"; return false; }
+    for (size_t i = 0; i < P.sp.size(); ++i)
+      if (P.sp[i].d4_nref == 0) { err = "element " + P.sym[i] + " has no d4_ref"; return false; }
+  }
   for (size_t i = 0; i < P.sp.size(); ++i) {
     P.sp[i].nsh = (int)shells[i].size();
     P.sp[i].sh0 = (int)P.sh.size();
@@ -249,6 +280,7 @@ struct tb_calculator {
   SpeciesParam* d_sp = nullptr;
   ShellParam* d_sh = nullptr;
   double* d_hscale = nullptr;
+  double* d_d4c6 = nullptr;  // D4 reference C6 table (DevParams::d4_c6ref)
   int maxsh = 1;
   int lmask = 0;  // bit l set when shells of angular momentum l exist
   std::mutex mu;
@@ -305,6 +337,7 @@ struct tb_calculator {
     if (d_sp) cudaFree(d_sp);
     if (d_sh) cudaFree(d_sh);
     if (d_hscale) cudaFree(d_hscale);
+    if (d_d4c6) cudaFree(d_d4c6);
   }
 };
 
@@ -329,6 +362,10 @@ struct tb_batch {
   long long* inl;
   double *S, *H0, *D, *Q, *X, *W, *F, *Z, *P;
   double *gtab, *atab;  // Coulomb pair tables of the fixed geometry (k_pair_tables)
+  // D4 dispersion of the fixed geometry (setup; only with a D4 parameter block):
+  // per atom cn, W, dW (kD4MaxRef), energy share, dE/dCN, gradient; per structure e_disp
+  double *d4cn = nullptr, *d4w = nullptr, *d4dw = nullptr, *d4e = nullptr, *d4dcn = nullptr, *d4g = nullptr,
+         *e_disp = nullptr;
   double *w, *focc, *vsh, *vat, *vdp, *vqp, *colred, *qsh_out, *qat_out, *dpat_out, *qpat_out;
   int *perm, *kdim;
   double *q_in, *dq, *dqlast, *qlast, *df, *u, *amat, *omega;
@@ -672,6 +709,8 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
          o_ms_nact = L.add(I4), o_itdev = L.add(I4);
   size_t o_guess = L.add(MX * D8), o_gflag = L.add(NM * I4), o_fspin = L.add(3 * NO * D8),
          o_wflag = L.add(NM * I4);
+  size_t o_d4cn = L.add(NA * D8), o_d4w = L.add(kD4MaxRef * NA * D8), o_d4dw = L.add(kD4MaxRef * NA * D8),
+         o_d4e = L.add(NA * D8), o_d4dcn = L.add(NA * D8), o_d4g = L.add(3 * NA * D8), o_edisp = L.add(NM * D8);
   size_t o_lwork = L.add(std::max<size_t>(b->lib_bytes, 16)), o_linfo = L.add((2 * b->big.size() + 2) * I4);
   // mixed-precision form: FP32 eigensolver input/output, refinement buffers, phase state
   const long long MXN2 = b->mixed ? N2 : 0, MXNO = b->mixed ? NO : 0, MXNM = b->mixed ? NM : 0;
@@ -770,6 +809,9 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   b->charge = at<double>(base, o_charge); b->uhf = at<int>(base, o_uhf);
   b->d_guess = at<double>(base, o_guess); b->d_guess_flag = at<int>(base, o_gflag);
   b->d_fspin = at<double>(base, o_fspin); b->d_wflag = at<int>(base, o_wflag);
+  b->d4cn = at<double>(base, o_d4cn); b->d4w = at<double>(base, o_d4w); b->d4dw = at<double>(base, o_d4dw);
+  b->d4e = at<double>(base, o_d4e); b->d4dcn = at<double>(base, o_d4dcn); b->d4g = at<double>(base, o_d4g);
+  b->e_disp = at<double>(base, o_edisp);
   b->h_guess.clear();
   b->h_guess_flag.clear();
   b->any_guess = false;
@@ -1256,6 +1298,16 @@ tb_status batch_setup(tb_batch* b, cudaStream_t st) {
   TB_CUDA(cudaMemsetAsync(b->kdim, 0, nmol * sizeof(int), st));  // no occupied orbitals before k_fermi
   // ---- setup (once per structure)
   TB_K("atoms", 0, 0, k_atoms<<<nblk(B.nat_tot, 128), 128, 0, st>>>(Pc, B, b->cn, b->mrad, b->erep, b->se));
+  // D4 dispersion of the fixed geometry (dispersion_get_engrad, src/xtb.cu:274-277)
+  if (Pc.d4) {
+    cudaEvent_t e0 = nullptr;
+    prof_start(b, st, &e0);
+    TB_CUDA(launch_dispersion(Pc, B, nmol, b->d4cn, b->d4w, b->d4dw, b->d4e, b->d4dcn, b->d4g, b->e_disp, st));
+    b->launches += 5;
+    prof_stop(b, st, "dispersion", e0, 0, 0);
+  } else {
+    TB_CUDA(cudaMemsetAsync(b->e_disp, 0, nmol * sizeof(double), st));
+  }
   {
     const long long mx = std::max((long long)b->nshmax * b->nshmax, (long long)b->natmax * b->natmax);
     TB_K("pair_tables", 0, 0,
@@ -1538,7 +1590,7 @@ tb_status batch_results(tb_batch* b, tb_result* out, cudaStream_t st) {
   // the device results land in the calculator's pinned staging buffer (one
   // copy each at full link speed; pageable destinations would be copied
   // through driver bounce buffers), then go to the caller's records
-  const size_t nd = 11 * (size_t)nmol + 10 * (size_t)NA + (size_t)NS, bytes = 8 * nd + 12 * (size_t)nmol;
+  const size_t nd = 12 * (size_t)nmol + 10 * (size_t)NA + (size_t)NS, bytes = 8 * nd + 12 * (size_t)nmol;
   std::lock_guard<std::mutex> stage_lk(b->calc->stage_mu);
   if (b->calc->stage_bytes < bytes) {
     if (b->calc->stage) cudaFreeHost(b->calc->stage);
@@ -1549,7 +1601,8 @@ tb_status batch_results(tb_batch* b, tb_result* out, cudaStream_t st) {
   }
   double* hd = reinterpret_cast<double*>(b->calc->stage);
   double *erep = hd, *eelec = erep + nmol, *eband = eelec + nmol, *ets = eband + nmol, *e2 = ets + nmol,
-         *ea = e2 + nmol, *e3 = ea + nmol, *err = e3 + nmol, *dip = err + nmol, *qat = dip + 3 * nmol,
+         *ea = e2 + nmol, *e3 = ea + nmol, *err = e3 + nmol, *edisp = err + nmol, *dip = edisp + nmol,
+         *qat = dip + 3 * nmol,
          *qsh = qat + NA, *dp = qsh + NS, *qp = dp + 3 * NA;
   int* hi = reinterpret_cast<int*>(hd + nd);
   int *iscf = hi, *status = iscf + nmol, *fw = status + nmol;
@@ -1561,6 +1614,7 @@ tb_status batch_results(tb_batch* b, tb_result* out, cudaStream_t st) {
   TB_CUDA(cp(eband, S.e_band, nmol * 8)); TB_CUDA(cp(ets, S.e_ts, nmol * 8));
   TB_CUDA(cp(e2, S.e_es2, nmol * 8)); TB_CUDA(cp(ea, S.e_aes2, nmol * 8));
   TB_CUDA(cp(e3, S.e_es3, nmol * 8)); TB_CUDA(cp(err, S.scf_error, nmol * 8));
+  TB_CUDA(cp(edisp, b->e_disp, nmol * 8));
   TB_CUDA(cp(dip, S.dipole, 3 * nmol * 8)); TB_CUDA(cp(iscf, S.iscf, nmol * 4));
   TB_CUDA(cp(status, S.status, nmol * 4)); TB_CUDA(cp(fw, S.fermi_warn, nmol * 4));
   TB_CUDA(cp(qat, b->qat_out, NA * 8)); TB_CUDA(cp(qsh, b->qsh_out, NS * 8));
@@ -1569,7 +1623,7 @@ tb_status batch_results(tb_batch* b, tb_result* out, cudaStream_t st) {
   tb_status first = TB_OK;
   for (int m = 0; m < nmol; ++m) {
     tb_result& r = out[m];
-    r.e_rep = erep[m]; r.e_elec = eelec[m]; r.energy = eelec[m] + erep[m];
+    r.e_rep = erep[m]; r.e_elec = eelec[m]; r.e_disp = edisp[m]; r.energy = eelec[m] + erep[m] + edisp[m];
     r.e_band = eband[m]; r.e_ts = ets[m]; r.e_es2 = e2[m]; r.e_aes2 = ea[m]; r.e_es3 = e3[m];
     r.scf_error = err[m]; r.iterations = iscf[m];
     for (int k = 0; k < 3; ++k) r.dipole[k] = dip[3 * m + k];
@@ -1683,6 +1737,10 @@ tb_status batch_gradient(tb_batch* b, const std::vector<int>& flag, cudaStream_t
   k_grad_atoms<<<at_grid, 128, 0, st>>>(b->Pc, B, dflag, G, dcn, b->mrad, b->qsh_out, b->qat_out, b->dpat_out,
                                         b->qpat_out, b->d_grad);
   TB_LAUNCH_CHECK();
+  if (b->Pc.d4) {  // the dispersion gradient of the setup
+    k_d4_add_grad<<<nblk(B.nat_tot, 128), 128, 0, st>>>(B, dflag, b->d4g, b->d_grad);
+    TB_LAUNCH_CHECK();
+  }
   k_grad_sigma<<<nmol, 128, 0, st>>>(B, dflag, b->d_grad, b->d_sigma);
   TB_LAUNCH_CHECK();
   b->h_grad_done = flag;
@@ -1897,6 +1955,33 @@ tb_status tb_calculator_create(const char* param_file, tb_calculator** out) {
   d.cn_cutoff = P.glob("cn_cutoff", 25.0); d.rep_cutoff = P.glob("rep_cutoff", 25.0);
   d.intcut = integral_cutoff(1.0);
   d.cutoff = std::min(std::sqrt(2.0 * d.intcut / P.min_alpha), 40.0);
+  d.d4 = 0;
+  d.d4_c6ref = nullptr;
+  if (!P.d4_freq.empty()) {
+    // reference C6 of every pair of reference systems, Casimir-Polder on the
+    // file's grid: C6 = 3/pi sum_k wts_k alpha_Ai(i w_k) alpha_Bj(i w_k)
+    const int ns = (int)P.sp.size(), R = kD4MaxRef;
+    std::vector<double> c6((size_t)ns * ns * R * R, 0.0);
+    for (int a = 0; a < ns; ++a)
+      for (int b = 0; b < ns; ++b)
+        for (int i = 0; i < P.sp[a].d4_nref; ++i)
+          for (int j = 0; j < P.sp[b].d4_nref; ++j) {
+            double x = 0.0;
+            for (size_t k = 0; k < P.d4_freq.size(); ++k) x += P.d4_wts[k] * P.d4_alpha[a][i][k] * P.d4_alpha[b][j][k];
+            c6[(((size_t)a * ns + b) * R + i) * R + j] = 3.0 / M_PI * x;
+          }
+    if (cudaMalloc(&c->d_d4c6, c6.size() * sizeof(double)) != cudaSuccess ||
+        cudaMemcpy(c->d_d4c6, c6.data(), c6.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+      delete c;
+      return fail(TB_CUDA_ERROR, "cannot allocate the D4 reference table");
+    }
+    d.d4 = 1;
+    d.d4_c6ref = c->d_d4c6;
+    d.d4_s6 = P.glob("d4_s6"); d.d4_s8 = P.glob("d4_s8"); d.d4_a1 = P.glob("d4_a1"); d.d4_a2 = P.glob("d4_a2");
+    d.d4_s9 = P.glob("d4_s9"); d.d4_alp = P.glob("d4_alp"); d.d4_wf = P.glob("d4_wf"); d.d4_k0 = P.glob("d4_k0");
+    d.d4_k1 = P.glob("d4_k1"); d.d4_k4 = P.glob("d4_k4"); d.d4_k5 = P.glob("d4_k5"); d.d4_k6 = P.glob("d4_k6");
+    d.d4_cn_cut = P.glob("d4_cn_cut"); d.d4_atm_cut = P.glob("d4_atm_cut"); d.d4_pair_cut = P.glob("d4_pair_cut");
+  }
   *out = c;
   return TB_OK;
 }
@@ -2186,6 +2271,35 @@ tb_status tb_repulsion(const tb_calculator* calc, const tb_structure* mol, doubl
   tb_status st = run_setup_to_integrals(&ob.b, false);
   if (st != TB_OK) return st;
   return d2h(erep, ob.b.erep, mol->nat * 8);
+}
+
+tb_status tb_dispersion(const tb_calculator* calc, const tb_structure* mol, double* edisp, double* gradient,
+                        double* sigma) {
+  if (!calc || !mol || !edisp) return fail(TB_BAD_INPUT, "null argument");
+  OneBatch ob(const_cast<tb_calculator*>(calc), mol);
+  if (ob.st != TB_OK) return ob.st;
+  const int nat = mol->nat;
+  std::vector<double> g(3 * (size_t)nat, 0.0);
+  if (calc->dp.d4) {
+    tb_batch& b = ob.b;
+    TB_CUDA(launch_dispersion(calc->dp, b.db, 1, b.d4cn, b.d4w, b.d4dw, b.d4e, b.d4dcn, b.d4g, b.e_disp, 0));
+    TB_CUDA(cudaDeviceSynchronize());
+    const tb_status st = d2h(edisp, b.d4e, nat * 8);
+    if (st != TB_OK) return st;
+    const tb_status sg = d2h(g.data(), b.d4g, g.size() * 8);
+    if (sg != TB_OK) return sg;
+  } else {
+    for (int a = 0; a < nat; ++a) edisp[a] = 0.0;
+  }
+  if (gradient) std::memcpy(gradient, g.data(), g.size() * 8);
+  if (sigma)
+    for (int a = 0; a < 3; ++a)
+      for (int c = 0; c < 3; ++c) {
+        double s = 0.0;
+        for (int i = 0; i < nat; ++i) s += g[3 * i + a] * mol->xyz[3 * i + c];
+        sigma[3 * a + c] = s;
+      }
+  return TB_OK;
 }
 
 tb_status tb_get_hamiltonian(const tb_calculator* calc, const tb_structure* mol, double* S, double* H0, double* D,

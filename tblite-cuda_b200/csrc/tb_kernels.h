@@ -177,6 +177,13 @@ cudaError_t oob_setup(OobRecord* r, bool reset);
 cudaError_t oob_scf(OobRecord* r, bool reset);
 cudaError_t oob_linalg(OobRecord* r, bool reset);
 
+// D4 dispersion (tb_disp.cu; only when DevParams::d4): per atom cn, W and dW
+// (kD4MaxRef each), energy share e_at, dE/dCN and gradient g [3 nat]; per
+// structure e_disp.  Five launches on st.
+cudaError_t launch_dispersion(const DevParams& P, const DevBatch& B, int nmol, double* cn, double* W, double* dW,
+                              double* e_at, double* dEdcn, double* g, double* e_disp, cudaStream_t st);
+__global__ void k_d4_add_grad(DevBatch B, const int* flag, const double* gd, double* grad);
+
 // nuclear gradient (read-out after the SCF, structures with flag[m] set)
 cudaError_t launch_grad_pairs(const DevParams& P, const DevBatch& B, const int* npair, const int* pair_i,
                               const int* pair_j, const double* se, const double* Pm, const double* Wm,

@@ -25,8 +25,11 @@ The file format (``.tbp``) is plain text, one keyword per line:
     global <key> <value>            scalar globals
     kshell <li> <lj> <value>        angular-momentum pair scaling of H0
     kpair <sym_i> <sym_j> <value>   optional element-pair scaling of H0
+    d4freq <n> <n values>           optional D4 block: frequency grid (Eh) and
+    d4wts <n> <n values>            quadrature weights of the Casimir-Polder integral
     element <symbol> <Z>
-      <key> <value>                 element scalars (rad, rcov, en, ...)
+      <key> <value>                 element scalars (rad, rcov, en, ..., d4_r4r2)
+      d4_ref <cn> <n values>        D4 reference: its CN and alpha(i w) on the grid
       shell <ang> <nprim>
         <key> <value>               shell scalars (selfenergy, kcn, ...)
         alpha <nprim values>
@@ -49,6 +52,8 @@ OUT = os.path.join(HERE, "synthetic_hco.tbp")
 # test file with one more element whose shell set includes a d shell, so that
 # the d-shell integral, transformation and Fock paths are exercised
 OUT_D = os.path.join(HERE, "synthetic_hcos.tbp")
+# the H/C/O file plus a synthetic D4 dispersion block (see D4 below)
+OUT_D4 = os.path.join(HERE, "synthetic_hco_d4.tbp")
 
 # radial grid for the fits
 _R = np.linspace(1e-6, 40.0, 40001)
@@ -169,7 +174,75 @@ ELEMENT_S = ("S", 16,
                                    hubbard=0.3000, hubbard_deriv=0.0300))])
 
 
-def write(path, name, title, elements):
+# ---------------------------------------------------------------------------
+# synthetic D4 dispersion data (plausible magnitudes, NOT the dftd4 reference
+# polarizabilities).  Each reference system of an element is a single
+# Lorentzian oscillator, alpha(i w) = alpha0 / (1 + (w / w0)^2), tabulated on a
+# 23-point Gauss-Legendre grid mapped to [0, inf) by w = ws (1 + t) / (1 - t);
+# the C6 of two such oscillators by the Casimir-Polder integral has the London
+# closed form 3/2 a1 a2 w1 w2 / (w1 + w2), against which the grid is checked.
+# ---------------------------------------------------------------------------
+D4_NFREQ = 23
+D4_WS = 0.5
+D4_GLOBALS = {
+    "d4_s6": 1.0,           # two-body C6 scaling
+    "d4_s8": 2.5,           # two-body C8 scaling
+    "d4_a1": 0.5,           # rational damping: R = a1 R0 + a2
+    "d4_a2": 5.0,
+    "d4_s9": 1.0,           # three-body (Axilrod-Teller-Muto) scaling
+    "d4_alp": 16.0,         # three-body damping exponent
+    "d4_wf": 6.0,           # Gaussian weight of the reference CNs
+    "d4_k0": 7.5,           # steepness of the error-function counting
+    "d4_k1": 1.0,           # covalent-radius scaling of the counting
+    "d4_k4": 4.1,           # electronegativity factor k4 exp(-(|dEN| + k5)^2 / k6)
+    "d4_k5": 19.1,
+    "d4_k6": 254.5,
+    "d4_cn_cut": 25.0,      # cutoffs (Bohr): coordination number, three-body, two-body
+    "d4_atm_cut": 25.0,
+    "d4_pair_cut": 60.0,
+}
+# per element: r4/r2 expectation-value factor Q and the references (CN, alpha0, w0)
+D4_ELEMENTS = {
+    "H": (2.00, [(0.0, 4.50, 0.45), (1.0, 3.00, 0.50)]),
+    "C": (3.10, [(0.0, 11.9, 0.40), (2.0, 10.0, 0.42), (3.0, 9.0, 0.44), (4.0, 8.0, 0.46)]),
+    "O": (2.60, [(0.0, 5.40, 0.55), (1.0, 5.00, 0.57), (2.0, 4.60, 0.60)]),
+}
+
+
+def d4_grid():
+    t, wt = np.polynomial.legendre.leggauss(D4_NFREQ)
+    w = D4_WS * (1.0 + t) / (1.0 - t)
+    wts = wt * 2.0 * D4_WS / (1.0 - t) ** 2
+    return w, wts
+
+
+def d4_lines():
+    w, wts = d4_grid()
+    lines = [f"global {k} {v!r}" for k, v in D4_GLOBALS.items()]
+    lines.append(f"d4freq {D4_NFREQ} " + " ".join(f"{x:.17g}" for x in w))
+    lines.append(f"d4wts {D4_NFREQ} " + " ".join(f"{x:.17g}" for x in wts))
+    # quadrature check against the London formula for every pair of references
+    worst = 0.0
+    refs = [r for _, rs in D4_ELEMENTS.values() for r in rs]
+    for _, a1, w1 in refs:
+        for _, a2, w2 in refs:
+            quad = 3.0 / math.pi * float(np.sum(wts * a1 / (1 + (w / w1) ** 2) * a2 / (1 + (w / w2) ** 2)))
+            exact = 1.5 * a1 * a2 * w1 * w2 / (w1 + w2)
+            worst = max(worst, abs(quad - exact) / exact)
+    print(f"D4 grid: largest relative C6 quadrature error {worst:.2e}")
+    return lines
+
+
+def d4_element_lines(sym):
+    w, _ = d4_grid()
+    q, refs = D4_ELEMENTS[sym]
+    lines = [f"  d4_r4r2 {q!r}"]
+    for cn, a0, w0 in refs:
+        lines.append(f"  d4_ref {cn!r} " + " ".join(f"{a0 / (1 + (x / w0) ** 2):.17g}" for x in w))
+    return lines
+
+
+def write(path, name, title, elements, d4=False):
     lines = [
         f"# SYNTHETIC GFN2-shaped parameters for {title}.",
         "# These are NOT the GFN2-xTB parameters; they only have the same fields and",
@@ -179,12 +252,17 @@ def write(path, name, title, elements):
     ]
     for k, v in GLOBALS.items():
         lines.append(f"global {k} {v!r}")
+    if d4:
+        lines.append("# synthetic D4 dispersion block (NOT the dftd4 reference data)")
+        lines += d4_lines()
     for (li, lj), v in sorted(KSHELL.items()):
         lines.append(f"kshell {li} {lj} {v!r}")
     for sym, z, escal, shells in elements:
         lines.append(f"element {sym} {z}")
         for k, v in escal.items():
             lines.append(f"  {k} {v!r}")
+        if d4:
+            lines += d4_element_lines(sym)
         for n, l, zeta, nprim, sscal in shells:
             a, c, ov = fit_sto(n, l, zeta, nprim)
             coeff = [float(ci * sph_prim_factor(ai, l)) for ai, ci in zip(a, c)]
@@ -206,6 +284,8 @@ def main():
     write(OUT, "synthetic-gfn2-shaped-HCO", "H, C, O", ELEMENTS)
     write(OUT_D, "synthetic-gfn2-shaped-HCOS", "H, C, O, S (test file: S has a d shell)",
           ELEMENTS + [ELEMENT_S])
+    write(OUT_D4, "synthetic-gfn2-shaped-HCO-D4", "H, C, O with a synthetic D4 dispersion block", ELEMENTS,
+          d4=True)
 
 
 if __name__ == "__main__":

@@ -48,7 +48,7 @@ class Result(C.Structure):
                 ("e_aes2", C.c_double), ("e_es3", C.c_double), ("dipole", C.c_double * 3),
                 ("scf_error", C.c_double), ("iterations", C.c_int32), ("status", C.c_int32),
                 ("nsh", C.c_int32), ("nao", C.c_int32), ("qat", _dp), ("qsh", _dp), ("dpat", _dp),
-                ("qpat", _dp), ("gradient", _dp), ("sigma", C.c_double * 9)]
+                ("qpat", _dp), ("gradient", _dp), ("sigma", C.c_double * 9), ("e_disp", C.c_double)]
 
 
 class Wavefunction(C.Structure):
@@ -69,7 +69,7 @@ EXPORTS = [
     "tb_server_create", "tb_server_submit", "tb_server_step", "tb_server_poll", "tb_server_destroy",
     "tb_batch_set_guess", "tb_batch_wavefunction", "tb_batch_gradient", "tb_sygvd_noalloc",
     "tb_calculator_set_small_solver", "tb_calculator_set_smem_tridiag", "tb_calculator_tuning",
-    "tb_bounds_check_build", "tb_bounds_violations", "tb_server_compactions",
+    "tb_bounds_check_build", "tb_bounds_violations", "tb_server_compactions", "tb_dispersion",
 ]
 
 _lib = None
@@ -152,7 +152,7 @@ _STRUCT_DT = _record_dtype(Structure, {"nat": np.int32, "uhf": np.int32, "charge
                                        "id": np.uintp, "xyz": np.uintp})
 _RESULT_DT = _record_dtype(Result, dict(
     {k: np.float64 for k in ("energy", "e_rep", "e_elec", "e_band", "e_ts", "e_es2", "e_aes2", "e_es3",
-                             "scf_error")},
+                             "scf_error", "e_disp")},
     dipole=(np.float64, 3), iterations=np.int32, status=np.int32, nsh=np.int32, nao=np.int32,
     qat=np.uintp, qsh=np.uintp, dpat=np.uintp, qpat=np.uintp, gradient=np.uintp, sigma=(np.float64, 9)))
 
@@ -291,7 +291,7 @@ class Calculator:
             return []
         # each field converted once for all structures (numpy scalar access per field is slow)
         keys = ("energy", "e_rep", "e_elec", "e_band", "e_ts", "e_es2", "e_aes2", "e_es3", "scf_error",
-                "iterations", "status", "nsh", "nao")
+                "e_disp", "iterations", "status", "nsh", "nao")
         cols = [v[k].tolist() for k in keys]
         dip = v["dipole"].copy()
         a0s, a1s = off.tolist(), (off + nat).tolist()
@@ -322,7 +322,7 @@ class _Atom:
 
 def _result_dict(r, b):
     d = dict(energy=r.energy, e_rep=r.e_rep, e_elec=r.e_elec, e_band=r.e_band, e_ts=r.e_ts,
-             e_es2=r.e_es2, e_aes2=r.e_aes2, e_es3=r.e_es3, dipole=np.array(r.dipole[:]),
+             e_es2=r.e_es2, e_aes2=r.e_aes2, e_es3=r.e_es3, e_disp=r.e_disp, dipole=np.array(r.dipole[:]),
              scf_error=r.scf_error, iterations=r.iterations, status=r.status, nsh=r.nsh, nao=r.nao)
     d.update(b)
     return d
@@ -532,6 +532,15 @@ def repulsion(calc: Calculator, mol):
     e = np.zeros(mol.nat)
     check(load_library().tb_repulsion(calc.h, C.byref(arr[0]), e.ctypes.data_as(_dp)), "tb_repulsion")
     return e
+
+
+def dispersion(calc: Calculator, mol):
+    """D4 dispersion (tb_dispersion): per-atom energies, gradient [nat][3], virial [3][3]."""
+    arr, keep = _one(mol)
+    e, g, s = np.zeros(mol.nat), np.zeros((mol.nat, 3)), np.zeros((3, 3))
+    check(load_library().tb_dispersion(calc.h, C.byref(arr[0]), e.ctypes.data_as(_dp), g.ctypes.data_as(_dp),
+                                       s.ctypes.data_as(_dp)), "tb_dispersion")
+    return e, g, s
 
 
 def get_hamiltonian(calc: Calculator, mol):
