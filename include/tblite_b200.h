@@ -200,6 +200,19 @@ tb_status tb_bounds_violations(int64_t* count, int32_t* site, int64_t* index, in
                                int32_t reset);
 int32_t tb_calculator_tuning(const tb_calculator* calc, char* buf, int32_t len);
 
+/* Structure input (the structure file I/O of the reference's host-side
+ * plan beside periodic images, src/xtb.cu:342-346): an XYZ file (count line,
+ * comment line, "symbol x y z" per atom in Angstrom; a symbol may also be an
+ * atomic number) into nat, atomic numbers z[nat] and xyz[nat][3] in Bohr;
+ * with more than cap atoms only *nat is set (TB_CAPACITY_EXCEEDED), so a
+ * first call with cap = 0 sizes the buffers.  comment (optional) receives the
+ * second line.  Host only: needs no CUDA device.
+ * tb_calculator_species maps an atomic number to the species index of the
+ * parameter file (tb_structure.id), -1 if it has none. */
+tb_status tb_read_xyz(const char* path, int32_t cap, int32_t* nat, int32_t* z, double* xyz, char* comment,
+                      int32_t comment_len);
+int32_t tb_calculator_species(const tb_calculator* calc, int32_t z);
+
 /* basis_type sizes (src/basis/type.h:56-73). */
 tb_status tb_basis_size(const tb_calculator* calc, const tb_structure* mol, int32_t* nsh, int32_t* nao);
 

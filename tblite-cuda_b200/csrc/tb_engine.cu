@@ -10,7 +10,9 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cctype>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <fstream>
@@ -2023,6 +2025,62 @@ tb_status tb_calculator_set_small_solver(tb_calculator* c, int32_t jacobi_max) {
     return fail(TB_BAD_INPUT, "jacobi_max must be -1 (measured), 0 (never) or 1.." + std::to_string(kJacobiMaxN));
   c->jacobi_override = jacobi_max;
   return TB_OK;
+}
+
+// Structure file input (the structure I/O beside periodic images in the
+// reference's plan, src/xtb.cu:342-346 and src/adjlist.cu:28-29): the XYZ
+// format -- a count line, a comment line, then "symbol x y z" per atom in
+// Angstrom -- into atomic numbers and Bohr.
+tb_status tb_read_xyz(const char* path, int32_t cap, int32_t* nat, int32_t* z, double* xyz, char* comment,
+                      int32_t comment_len) {
+  static const char* kSym[] = {"H",  "He", "Li", "Be", "B",  "C",  "N",  "O",  "F",  "Ne", "Na", "Mg", "Al", "Si", "P",
+                               "S",  "Cl", "Ar", "K",  "Ca", "Sc", "Ti", "V",  "Cr", "Mn", "Fe", "Co", "Ni", "Cu", "Zn",
+                               "Ga", "Ge", "As", "Se", "Br", "Kr", "Rb", "Sr", "Y",  "Zr", "Nb", "Mo", "Tc", "Ru", "Rh",
+                               "Pd", "Ag", "Cd", "In", "Sn", "Sb", "Te", "I",  "Xe", "Cs", "Ba", "La", "Ce", "Pr", "Nd",
+                               "Pm", "Sm", "Eu", "Gd", "Tb", "Dy", "Ho", "Er", "Tm", "Yb", "Lu", "Hf", "Ta", "W",  "Re",
+                               "Os", "Ir", "Pt", "Au", "Hg", "Tl", "Pb", "Bi", "Po", "At", "Rn"};
+  if (!path || !nat) return fail(TB_BAD_INPUT, "null argument");
+  std::ifstream f(path);
+  if (!f) return fail(TB_BAD_INPUT, std::string("cannot open ") + path);
+  std::string line;
+  long long n = -1;
+  if (!std::getline(f, line) || !(std::istringstream(line) >> n) || n <= 0)
+    return fail(TB_BAD_INPUT, "xyz: bad atom count line");
+  *nat = (int32_t)n;
+  std::getline(f, line);
+  if (comment && comment_len > 0) std::snprintf(comment, (size_t)comment_len, "%s", line.c_str());
+  if (n > cap || !z || !xyz) return n > cap ? fail(TB_CAPACITY_EXCEEDED, "xyz: more atoms than cap") : TB_OK;
+  const double bohr = 1.0 / 0.529177210903;
+  for (long long a = 0; a < n; ++a) {
+    if (!std::getline(f, line)) return fail(TB_BAD_INPUT, "xyz: fewer atom lines than the count");
+    std::istringstream is(line);
+    std::string sym;
+    double x, y, w;
+    if (!(is >> sym >> x >> y >> w)) return fail(TB_BAD_INPUT, "xyz: bad atom line " + std::to_string(a + 1));
+    int zz = 0;
+    if (std::isdigit((unsigned char)sym[0])) {
+      zz = std::atoi(sym.c_str());
+    } else {
+      std::string s2 = sym;
+      s2[0] = (char)std::toupper((unsigned char)s2[0]);
+      for (size_t i = 1; i < s2.size(); ++i) s2[i] = (char)std::tolower((unsigned char)s2[i]);
+      for (int k = 0; k < (int)(sizeof(kSym) / sizeof(kSym[0])); ++k)
+        if (s2 == kSym[k]) { zz = k + 1; break; }
+    }
+    if (zz <= 0) return fail(TB_BAD_INPUT, "xyz: unknown element " + sym);
+    z[a] = zz;
+    xyz[3 * a] = x * bohr;
+    xyz[3 * a + 1] = y * bohr;
+    xyz[3 * a + 2] = w * bohr;
+  }
+  return TB_OK;
+}
+
+int32_t tb_calculator_species(const tb_calculator* c, int32_t z) {
+  if (!c) return -1;
+  for (size_t i = 0; i < c->hp.sp.size(); ++i)
+    if (c->hp.sp[i].z == z) return (int32_t)i;
+  return -1;
 }
 
 tb_status tb_calculator_set_smem_tridiag(tb_calculator* c, int32_t min_n) {

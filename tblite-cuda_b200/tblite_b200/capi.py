@@ -70,6 +70,7 @@ EXPORTS = [
     "tb_batch_set_guess", "tb_batch_wavefunction", "tb_batch_gradient", "tb_sygvd_noalloc",
     "tb_calculator_set_small_solver", "tb_calculator_set_smem_tridiag", "tb_calculator_tuning",
     "tb_bounds_check_build", "tb_bounds_violations", "tb_server_compactions", "tb_dispersion",
+    "tb_read_xyz", "tb_calculator_species",
 ]
 
 _lib = None
@@ -227,6 +228,17 @@ class Calculator:
             min_n = 64
         check(load_library().tb_calculator_set_smem_tridiag(self.h, C.c_int32(int(min_n))),
               "tb_calculator_set_smem_tridiag")
+
+    def molecule_from_xyz(self, path: str, charge: float = 0.0, uhf: int = 0):
+        """A structure from an XYZ file, species mapped by this calculator's parameter file."""
+        from .geometry import Molecule
+        z, xyz, comment = read_xyz(path)
+        L = load_library()
+        L.tb_calculator_species.argtypes = [C.c_void_p, C.c_int32]
+        sp = np.array([L.tb_calculator_species(self.h, C.c_int32(int(x))) for x in z], np.int32)
+        if (sp < 0).any():
+            raise TBError(TB_BAD_INPUT, f"{path}: element Z={int(z[sp < 0][0])} is not in the parameter file")
+        return Molecule(sp, xyz, charge=charge, uhf=uhf, label=comment.strip() or os.path.basename(path))
 
     def tuning(self) -> dict:
         """The autotuner's measurements and choices (tb_calculator_tuning)."""
@@ -532,6 +544,22 @@ def repulsion(calc: Calculator, mol):
     e = np.zeros(mol.nat)
     check(load_library().tb_repulsion(calc.h, C.byref(arr[0]), e.ctypes.data_as(_dp)), "tb_repulsion")
     return e
+
+
+def read_xyz(path: str):
+    """An XYZ file through tb_read_xyz: (atomic numbers, coordinates [nat][3] in Bohr, comment line)."""
+    L = load_library()
+    L.tb_read_xyz.argtypes = [C.c_char_p, C.c_int32, C.POINTER(C.c_int32), C.c_void_p, C.c_void_p, C.c_char_p,
+                              C.c_int32]
+    nat = C.c_int32()
+    st = L.tb_read_xyz(path.encode(), 0, C.byref(nat), None, None, None, 0)
+    if st not in (TB_OK, TB_CAPACITY_EXCEEDED):
+        check(st, "tb_read_xyz")
+    z, xyz = np.zeros(nat.value, np.int32), np.zeros((nat.value, 3))
+    comment = C.create_string_buffer(4096)
+    check(L.tb_read_xyz(path.encode(), nat.value, C.byref(nat), z.ctypes.data_as(C.c_void_p),
+                        xyz.ctypes.data_as(C.c_void_p), comment, 4096), "tb_read_xyz")
+    return z, xyz, comment.value.decode(errors="replace")
 
 
 def dispersion(calc: Calculator, mol):

@@ -181,3 +181,12 @@ def request_stream(count: int = 20000, seed: int = 1003, rate: float = 2000.0,
 def water_box(seed: int = 1004) -> Molecule:
     """1000 H2O on a 10x10x10 grid at 3.1 A (3000 atoms)."""
     return water_cluster(1000, np.random.default_rng(seed), grid=10)
+
+
+def write_xyz(mol: Molecule, path: str, symbols=("H", "C", "O")) -> None:
+    """Write a structure in the XYZ format (Angstrom); symbols[i] names species i."""
+    lines = [str(mol.nat), mol.label or "tblite-b200 structure"]
+    for s, (x, y, z) in zip(mol.id, np.asarray(mol.xyz) / ANGSTROM):
+        lines.append(f"{symbols[int(s)]:2s} {x:22.15f} {y:22.15f} {z:22.15f}")
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
