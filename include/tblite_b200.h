@@ -186,6 +186,21 @@ tb_status tb_calculator_set_small_solver(tb_calculator* calc, int32_t jacobi_max
  * always uses it from 64 AOs. */
 tb_status tb_calculator_set_smem_tridiag(tb_calculator* calc, int32_t min_n);
 
+/* FP64 GEMM tile shape (the batched matrix products of every SCF iteration:
+ * X^T F X, C = X V, P = C diag(f) C^T; the reference's get_density_matrix,
+ * src/wavefunction/type.cu:37, is a loop nest per structure with no tiling
+ * choice).  Each structure's products run on 64 x 64 or on 32 x 32 tiles.
+ * The calculator measures both per size (16..384 AOs in steps of 16) on the
+ * first batch that holds a structure of at most 384 AOs; larger structures
+ * always take 64 x 64.  A batch takes the faster shape per structure, but is
+ * split over both kernels only when the modelled saving is at least 5% of the
+ * better single shape (a second launch per product has its own ramp and
+ * tail); tb_calculator_tuning reports the table.  Both shapes accumulate
+ * every element in the same order, so the choice never changes a result's
+ * bits.  max_n32: -1 (default) measured choice, 0 always 64 x 64, N > 0
+ * 32 x 32 up to N AOs.  Applies to batches built afterwards. */
+tb_status tb_calculator_set_gemm_tiles(tb_calculator* calc, int32_t max_n32);
+
 /* Checked build (the library built with -DTB_BOUNDS_CHECK, `make check`:
  * lib/libtblite_b200_check.so; no counterpart in the reference, whose only
  * checks are device asserts): index guards at the global-memory accesses of

@@ -275,6 +275,12 @@ struct TridPlan {
 
 }  // namespace
 
+// largest structure size (AOs) at which the GEMM tile shapes are measured
+constexpr int kTileCalMax = 384;
+// smallest modelled saving (fraction of the single-kernel time) for which a
+// batch's GEMMs are split over both tile shapes
+constexpr double kTileSplitGain = 0.05;
+
 // ====================================================================== calculator
 struct tb_calculator {
   HostParams hp;
@@ -303,6 +309,25 @@ struct tb_calculator {
     std::vector<double> t_cta, t_warp;  // seconds per structure in a full batch
   } small;
   int jacobi_override = -1;  // -1: measured choice; 0: never; 1..32: fixed bound
+  // FP64 GEMM tile shape per structure size: k_gemm32 (32 x 32 tiles) where it
+  // measured faster than k_gemm (64 x 64) on the SCF iteration's four GEMMs.
+  // Sizes are measured in steps of 16 AOs: the tile grids and the K slabs of
+  // both kernels are the same for every N in (n - 16, n], so the measurement
+  // at n stands for that whole interval; above the largest, 64 x 64 tiles.
+  struct TileModel {
+    bool ready = false;
+    std::vector<int> n;              // measured sizes (AOs)
+    std::vector<double> t64, t32;    // seconds per structure in a full batch
+    std::vector<char> use32;         // chosen per measured size
+  } tile;
+  int tile_override = -1;  // -1: measured choice; 0: 64 x 64 always; N > 0: 32 x 32 up to N AOs
+  // index of the measured size that stands for n AOs (-1: above the table)
+  int tile_index(int n) const {
+    if (!tile.ready) return -1;
+    for (size_t i = 0; i < tile.n.size(); ++i)
+      if (n <= tile.n[i]) return (int)i;
+    return -1;
+  }
   int smem_tridiag = 0;  // FP64 structures of at least this many AOs reduced by k_trid_smem (0: none)
   std::mutex tune_mu;
   // pinned staging buffer for the batch metadata upload, reused across batches
@@ -354,6 +379,9 @@ struct tb_batch {
   std::vector<int> h_aoff, h_soff, h_ooff, h_mixoff;
   std::vector<long long> h_moff, h_poff, h_s2off, h_a2off;
   std::vector<int4> tiles64, tiles32, tiles128;  // tiles32: upper 32x32 tiles (t <= u), Fock build
+  // FP64 GEMM tiles by the tile autotuner's choice per structure: 64 x 64
+  // (k_gemm) and 32 x 32 (k_gemm32), largest structures first in each
+  std::vector<int4> gemm64, gemm32;
   std::vector<int2> chunks32;
   std::vector<double> h_xyz;
   // device views
@@ -393,6 +421,8 @@ struct tb_batch {
   TridPlan trid;            // structures tridiagonalised by k_trid_smem, per class
   int* d_tlist = nullptr;
   int4 *d_tiles64, *d_tiles32, *d_tiles128;
+  int4 *d_gemm64 = nullptr, *d_gemm32 = nullptr;
+  int ngemm64 = 0, ngemm32 = 0;
   int2* d_chunks32;
   int* h_nactive = nullptr;  // pinned
   // structures above the in-house size bound: cuSOLVER path (tb_large.cu)
@@ -447,6 +477,7 @@ T* at(char* base, size_t off) { return reinterpret_cast<T*>(base + off); }
 
 tb_status calibrate_eigensolvers(tb_calculator* c);
 tb_status calibrate_small(tb_calculator* c);
+tb_status calibrate_tiles(tb_calculator* c);
 
 // Automatic eigensolver choice for a batch (tb_options.solver = 0): the k
 // largest structures go to cuSOLVER, the rest to the batched in-house solver,
@@ -661,6 +692,60 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
     }
     b->trid.build(sizes, in_house, calc->smem_tridiag);
   }
+  // GEMM tile shape per structure (the measured choice unless overridden)
+  {
+    bool small = false;
+    for (int m = 0; m < nmol && !small; ++m) small = b->h_ooff[m + 1] - b->h_ooff[m] <= kTileCalMax;
+    if (calc->tile_override < 0 && small) {
+      const tb_status ts = calibrate_tiles(calc);
+      if (ts != TB_OK) return ts;
+    }
+    // Measured mode: each structure the faster shape of its size.  A batch
+    // that would then need both kernels pays a second launch per product (its
+    // own ramp and tail; on the 1024-cluster batch a modelled 1.3% saving
+    // measured as a 5% loss), so it is split only when the modelled saving --
+    // the measured per-structure times summed over the batch -- is at least
+    // kTileSplitGain of the better single shape; otherwise the batch takes
+    // that single shape (32 x 32 only when no structure is above the table).
+    std::vector<char> t32(nmol, 0);
+    if (calc->tile_override >= 0) {
+      for (int m = 0; m < nmol; ++m) t32[m] = b->h_ooff[m + 1] - b->h_ooff[m] <= calc->tile_override;
+    } else if (calc->tile.ready) {
+      double s64 = 0, s32 = 0, smin = 0;
+      int n32 = 0, n64 = 0, nbig = 0;
+      for (int m = 0; m < nmol; ++m) {
+        const int i = calc->tile_index(b->h_ooff[m + 1] - b->h_ooff[m]);
+        if (i < 0) { ++nbig; continue; }
+        const double a = calc->tile.t64[i], c = calc->tile.t32[i];
+        s64 += a; s32 += c; smin += std::min(a, c);
+        t32[m] = calc->tile.use32[i];
+        (t32[m] ? n32 : n64) += 1;
+      }
+      if (n32 > 0 && (n64 > 0 || nbig > 0)) {  // the per-structure choice needs both kernels
+        const bool all32 = nbig == 0 && s32 < s64;
+        const double single = all32 ? s32 : s64;
+        if (single - smin < kTileSplitGain * single)
+          for (int m = 0; m < nmol; ++m)
+            t32[m] = all32 && calc->tile_index(b->h_ooff[m + 1] - b->h_ooff[m]) >= 0;
+      }
+    }
+    std::vector<int> ord(nmol);
+    for (int m = 0; m < nmol; ++m) ord[m] = m;
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) {
+      return b->h_ooff[x + 1] - b->h_ooff[x] > b->h_ooff[y + 1] - b->h_ooff[y];
+    });
+    b->gemm64.clear();
+    b->gemm32.clear();
+    for (int m : ord) {
+      const int n = b->h_ooff[m + 1] - b->h_ooff[m];
+      const int nt = t32[m] ? (n + 31) / 32 : (n + 63) / 64;
+      std::vector<int4>& v = t32[m] ? b->gemm32 : b->gemm64;
+      for (int t = 0; t < nt; ++t)
+        for (int u = 0; u < nt; ++u) v.push_back(make_int4(m, t, u, 0));
+    }
+    b->ngemm64 = (int)b->gemm64.size();
+    b->ngemm32 = (int)b->gemm32.size();
+  }
   b->lib_bytes = 0;
   if (!b->big.empty()) {
     const std::string e = b->lib.workspace(nbig_max, &b->lib_bytes);
@@ -686,6 +771,7 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
          o_aosh = L.add(NO * I4), o_t64 = L.add(b->tiles64.size() * sizeof(int4)),
          o_t128 = L.add(b->tiles128.size() * sizeof(int4)),
          o_t32 = L.add(b->tiles32.size() * sizeof(int4)), o_c32 = L.add(b->chunks32.size() * sizeof(int2)),
+         o_g64 = L.add(b->gemm64.size() * sizeof(int4)), o_g32 = L.add(b->gemm32.size() * sizeof(int4)),
          o_charge = L.add(NM * D8), o_uhf = L.add(NM * I4), o_order = L.add(NM * I4),
          o_jlist = L.add(NM * I4), o_tlist = L.add(NM * I4);
   const size_t meta_end = L.total;
@@ -766,6 +852,8 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   put(o_t128, b->tiles128.data(), b->tiles128.size() * sizeof(int4));
   put(o_t32, b->tiles32.data(), b->tiles32.size() * sizeof(int4));
   put(o_c32, b->chunks32.data(), b->chunks32.size() * sizeof(int2));
+  put(o_g64, b->gemm64.data(), b->gemm64.size() * sizeof(int4));
+  put(o_g32, b->gemm32.data(), b->gemm32.size() * sizeof(int4));
   std::vector<double> ch(nmol);
   std::vector<int> uh(nmol);
   for (int m = 0; m < nmol; ++m) { ch[m] = mols[m].charge; uh[m] = mols[m].uhf; }
@@ -808,6 +896,8 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
     b->act_lo = at<int>(base, o_lo); b->act_hi = at<int>(base, o_hi);
   }
   b->d_tiles64 = at<int4>(base, o_t64); b->d_tiles128 = at<int4>(base, o_t128); b->d_tiles32 = at<int4>(base, o_t32); b->d_chunks32 = at<int2>(base, o_c32);
+  b->d_gemm64 = at<int4>(base, o_g64);
+  b->d_gemm32 = at<int4>(base, o_g32);
   b->charge = at<double>(base, o_charge); b->uhf = at<int>(base, o_uhf);
   b->d_guess = at<double>(base, o_guess); b->d_guess_flag = at<int>(base, o_gflag);
   b->d_fspin = at<double>(base, o_fspin); b->d_wflag = at<int>(base, o_wflag);
@@ -928,6 +1018,38 @@ tb_status launch_trid_plan(tb_batch* b, const int* active, cudaStream_t st) {
   return TB_OK;
 }
 
+// One batched FP64 GEMM (k_gemm's operands) over the batch's two GEMM tile
+// lists: k_gemm on the structures given 64 x 64 tiles, k_gemm32 on those given
+// 32 x 32 (the same bits either way).  With a profile name both launches are
+// timed in that class and the algorithmic work is booked once.
+tb_status launch_gemm(tb_batch* b, cudaStream_t st, const char* prof, double work, const double* A, int ta,
+                      const double* Bm, int tb_, const int* perm, const double* ks, const int* kdim, double* C,
+                      double alpha, double beta, const int* active, int shape) {
+  constexpr int kGrid = 148 * 8;
+  bool booked = false;
+  for (int v = 0; v < 2; ++v) {
+    const int nt = v ? b->ngemm32 : b->ngemm64;
+    if (nt == 0) continue;
+    cudaEvent_t e0 = nullptr;
+    if (prof) prof_start(b, st, &e0);
+    if (v == 0)
+      k_gemm<<<std::min(nt, kGrid), kGemmThreads, 0, st>>>(b->db, b->d_gemm64, nt, A, ta, Bm, tb_, perm, ks, kdim, C,
+                                                           alpha, beta, active, shape);
+    else
+      k_gemm32<<<std::min(nt, kGrid), kGemmThreads, 0, st>>>(b->db, b->d_gemm32, nt, A, ta, Bm, tb_, perm, ks, kdim,
+                                                             C, alpha, beta, active, shape);
+    TB_LAUNCH_CHECK();
+    if (prof) prof_stop(b, st, prof, e0, booked ? 0.0 : work, 1);
+    booked = true;
+  }
+  return TB_OK;
+}
+#define TB_GEMM(work, ...)                                                  \
+  do {                                                                      \
+    const tb_status gs_ = launch_gemm(b, st, "gemm", work, __VA_ARGS__);   \
+    if (gs_ != TB_OK) return gs_;                                           \
+  } while (0)
+
 // The mixed phase hands over to FP64 once |dE| and the charge error are below
 // this multiple of the final thresholds, but never below the floors: the FP32
 // contractions leave iteration-to-iteration noise of about 1e-6 in charges.
@@ -957,14 +1079,10 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
   // F' = X^T F X into F (T = F X in W), each phase in its precision
   TB_K("gemm_tc", 2.0 * n3_lo, 1,
        k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, lo, S.status));
-  TB_K("gemm", 2.0 * n3_hi, 1,
-       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi,
-                                                  kGemmKUpToJ));
+  TB_GEMM(2.0 * n3_hi, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, hi, kGemmKUpToJ);
   TB_K("gemm_tc", 2.0 * n3_lo, 1,
        k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, lo, S.status));
-  TB_K("gemm", 2.0 * n3_hi, 1,
-       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, hi,
-                                                  kGemmKUpToI | kGemmSym));
+  TB_GEMM(2.0 * n3_hi, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, hi, kGemmKUpToI | kGemmSym);
   // mixed phase: FP32 eigensolve
   TB_K("convert", 0, 0, k_to_f32<<<gemm_grid, 256, 0, st>>>(B, T, nt, b->F, b->Af, lo));
   TB_K("syev_f32", 4.0 * n3_lo, 1,
@@ -1005,31 +1123,27 @@ tb_status mixed_core(tb_batch* b, cudaStream_t st, double n3_lo, double n3_hi, d
     double* V = b->Z;
     double* Vo = b->Vn;
     const double wk = 2.0 * n3_lo;
-    TB_K("gemm", wk, 1,  // G = V^T V
-         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, V, 1, V, 0, nullptr, nullptr, nullptr, b->G, 1.0, 0.0, lo));
-    TB_K("gemm", wk, 1,  // W = F' V
-         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->F, 0, V, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, lo));
-    TB_K("gemm", wk, 1,  // Sm = V^T W (in P)
-         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, V, 1, b->W, 0, nullptr, nullptr, nullptr, b->P, 1.0, 0.0, lo));
+    TB_GEMM(wk,  // G = V^T V
+            V, 1, V, 0, nullptr, nullptr, nullptr, b->G, 1.0, 0.0, lo, 0);
+    TB_GEMM(wk,  // W = F' V
+            b->F, 0, V, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, lo, 0);
+    TB_GEMM(wk,  // Sm = V^T W (in P)
+            V, 1, b->W, 0, nullptr, nullptr, nullptr, b->P, 1.0, 0.0, lo, 0);
     TB_K("refine", 0, 0, k_oa_step<<<nmol, 256, oa_smem, st>>>(B, b->G, b->P, V, b->w, lo, nullptr));
     TB_CUDA(cudaMemcpyAsync(Vo, V, (size_t)b->n2_tot * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    TB_K("gemm", wk, 1,  // Vo = V + V E
-         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, V, 0, b->G, 0, nullptr, nullptr, nullptr, Vo, 1.0, 1.0, lo));
+    TB_GEMM(wk,  // Vo = V + V E
+            V, 0, b->G, 0, nullptr, nullptr, nullptr, Vo, 1.0, 1.0, lo, 0);
   }
   TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
   // C = X V into W (mixed phase: V after the refinement step, in Vn; FP64
   // phase: the eigenvector rows of Z in ascending order through perm)
   TB_K("gemm_tc", 2.0 * n3_lo, 1,
        k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->X, 0, b->Vn, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, lo, S.status));
-  TB_K("gemm", 2.0 * n3_hi, 1,
-       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr, b->W, 1.0, 0.0, hi,
-                                                  kGemmKFromI));
+  TB_GEMM(2.0 * n3_hi, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr, b->W, 1.0, 0.0, hi, kGemmKFromI);
   // P = C diag(f) C^T
   TB_K("gemm_tc", 2.0 * n2occ_lo, 1,
        k_gemm_tc<<<tc_grid, kTcThreads, tc_smem, st>>>(B, T128, nt128, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.0, 0.0, lo, S.status));
-  TB_K("gemm", 2.0 * n2occ_hi, 1,
-       k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, T, nt, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.0, 0.0, hi,
-                                                  kGemmSym));
+  TB_GEMM(2.0 * n2occ_hi, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.0, 0.0, hi, kGemmSym);
   return TB_OK;
 }
 
@@ -1261,6 +1375,127 @@ tb_status calibrate_small(tb_calculator* c) {
   return TB_OK;
 }
 
+// Measures, once per calculator, the batched FP64 GEMM on both tile shapes
+// (k_gemm, 64 x 64; k_gemm32, 32 x 32) at N = 16, 32, ..., kTileCalMax: the
+// SCF iteration's four GEMM forms (F X with X upper triangular, X^T W into a
+// symmetric result, X Z through a permutation, W diag(f) W^T over the occupied
+// columns), each on floor(E / N^2) structures of N AOs (E = two waves of
+// 64 x 64 tiles on 148 SMs), the same inputs for both shapes, the faster of
+// two timed repetitions after an untimed one.  32 x 32 tiles are chosen at
+// the sizes where they were faster; both shapes give the same bits.
+tb_status calibrate_tiles(tb_calculator* c) {
+  std::lock_guard<std::mutex> lk(c->tune_mu);
+  if (c->tile.ready) return TB_OK;
+  const size_t E = 2ull * 148 * 8 * 64 * 64;  // matrix elements per size
+  const int cmax = (int)(E / (16 * 16));      // structures at the smallest size
+  Arena ar;
+  Layout L;
+  const size_t oA = L.add(E * 8), oB = L.add(E * 8), oC = L.add(E * 8), oK = L.add(E / 16 * 8),
+               oP = L.add(E / 16 * 4), oD = L.add((size_t)cmax * 4), oo = L.add((size_t)(cmax + 1) * 4),
+               om = L.add((size_t)(cmax + 1) * 8), oT = L.add((E / 256 + 1) * sizeof(int4));
+  TB_CUDA(ar.reserve(L.total));
+  char* base = ar.base;
+  {
+    std::vector<double> h(E);
+    uint64_t x = 0x9e3779b97f4a7c15ull;
+    for (size_t i = 0; i < E; ++i) {  // xorshift64*, uniform in (-1, 1)
+      x ^= x >> 12; x ^= x << 25; x ^= x >> 27;
+      h[i] = (double)((x * 0x2545f4914f6cdd1dull) >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+    }
+    TB_CUDA(cudaMemcpy(base + oA, h.data(), E * 8, cudaMemcpyHostToDevice));
+    TB_CUDA(cudaMemcpy(base + oB, h.data(), E * 8, cudaMemcpyHostToDevice));
+    h.assign(E / 16, 0.5);
+    TB_CUDA(cudaMemcpy(base + oK, h.data(), E / 16 * 8, cudaMemcpyHostToDevice));
+  }
+  const double* A = at<double>(base, oA);
+  const double* Bm = at<double>(base, oB);
+  double* C = at<double>(base, oC);
+  const double* ks = at<double>(base, oK);
+  const int* perm = at<int>(base, oP);
+  const int* kdim = at<int>(base, oD);
+  int4* dT = at<int4>(base, oT);
+  cudaEvent_t e0, e1;
+  TB_CUDA(cudaEventCreate(&e0));
+  TB_CUDA(cudaEventCreate(&e1));
+  tb_status st = TB_OK;
+  std::vector<int> sizes;
+  for (int n = 16; n <= kTileCalMax; n += 16) sizes.push_back(n);
+  std::vector<double> t64(sizes.size()), t32(sizes.size());
+  std::vector<int> oo_h, pm_h, kd_h;
+  std::vector<long long> om_h;
+  std::vector<int4> tl;
+  for (size_t si = 0; si < sizes.size() && st == TB_OK; ++si) {
+    const int n = sizes[si], cnt = (int)std::max<size_t>(1, E / ((size_t)n * n));
+    oo_h.resize(cnt + 1);
+    om_h.resize(cnt + 1);
+    pm_h.resize((size_t)cnt * n);
+    kd_h.assign(cnt, n / 2);
+    for (int k = 0; k <= cnt; ++k) {
+      oo_h[k] = k * n;
+      om_h[k] = (long long)k * n * n;
+    }
+    for (int k = 0; k < cnt; ++k)
+      for (int j = 0; j < n; ++j) pm_h[(size_t)k * n + j] = j;
+    if (cudaMemcpy(base + oo, oo_h.data(), (cnt + 1) * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(base + om, om_h.data(), (cnt + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(base + oP, pm_h.data(), (size_t)cnt * n * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(base + oD, kd_h.data(), (size_t)cnt * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+      st = fail(TB_CUDA_ERROR, "GEMM tile calibration: upload");
+      break;
+    }
+    DevBatch Bk{};
+    Bk.nmol = cnt;
+    Bk.ooff = at<int>(base, oo);
+    Bk.moff = at<long long>(base, om);
+    for (int v = 0; v < 2 && st == TB_OK; ++v) {
+      const int tile = v ? 32 : 64, nt1 = (n + tile - 1) / tile;
+      tl.clear();
+      for (int m = 0; m < cnt; ++m)
+        for (int t = 0; t < nt1; ++t)
+          for (int u = 0; u < nt1; ++u) tl.push_back(make_int4(m, t, u, 0));
+      const int nt = (int)tl.size(), grid = std::min(nt, 148 * 8);
+      if (cudaMemcpy(dT, tl.data(), tl.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess) {
+        st = fail(TB_CUDA_ERROR, "GEMM tile calibration: upload");
+        break;
+      }
+      auto launch = [&](const double* a, int ta, const double* bb, int tb_, const int* pm, const double* kv,
+                        const int* kd, int shape) {
+        if (v == 0)
+          k_gemm<<<grid, kGemmThreads>>>(Bk, dT, nt, a, ta, bb, tb_, pm, kv, kd, C, 1.0, 0.0, nullptr, shape);
+        else
+          k_gemm32<<<grid, kGemmThreads>>>(Bk, dT, nt, a, ta, bb, tb_, pm, kv, kd, C, 1.0, 0.0, nullptr, shape);
+      };
+      float best = 1e30f;
+      for (int rep = 0; rep < 3; ++rep) {
+        cudaEventRecord(e0);
+        launch(A, 0, Bm, 0, nullptr, nullptr, nullptr, kGemmKUpToJ);
+        launch(A, 1, Bm, 0, nullptr, nullptr, nullptr, kGemmKUpToI | kGemmSym);
+        launch(A, 0, Bm, 1, perm, nullptr, nullptr, kGemmKFromI);
+        launch(A, 0, A, 1, nullptr, ks, kdim, kGemmSym);
+        cudaEventRecord(e1);
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess ||
+            cudaGetLastError() != cudaSuccess) {
+          st = fail(TB_CUDA_ERROR, "GEMM tile calibration: launch");
+          break;
+        }
+        if (rep > 0) best = std::min(best, ms);
+      }
+      (v ? t32 : t64)[si] = best * 1e-3 / cnt;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != TB_OK) return st;
+  c->tile.n = sizes;
+  c->tile.t64 = t64;
+  c->tile.t32 = t32;
+  c->tile.use32.resize(sizes.size());
+  for (size_t si = 0; si < sizes.size(); ++si) c->tile.use32[si] = t32[si] < t64[si];
+  c->tile.ready = true;
+  return TB_OK;
+}
+
 // Host copy of active/status, read where a run synchronises anyway, so that
 // converged or failed library structures are not diagonalised again.
 tb_status read_flags(tb_batch* b, cudaStream_t st) {
@@ -1410,12 +1645,8 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
                                        b->vqp, b->F, S.active));
   if (!b->mixed) {
     // F' = X^T F X  (T = F X in W, then F' into F): 2 x 2N^3
-    TB_K("gemm", 2.0 * n3, 1,
-         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->F, 0, b->X, 0, nullptr, nullptr, nullptr,
-                                           b->W, 1.0, 0.0, S.active, kGemmKUpToJ));
-    TB_K("gemm", 2.0 * n3, 1,
-         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 1, b->W, 0, nullptr, nullptr, nullptr,
-                                           b->F, 1.0, 0.0, S.active, kGemmKUpToI | kGemmSym));
+    TB_GEMM(2.0 * n3, b->F, 0, b->X, 0, nullptr, nullptr, nullptr, b->W, 1.0, 0.0, S.active, kGemmKUpToJ);
+    TB_GEMM(2.0 * n3, b->X, 1, b->W, 0, nullptr, nullptr, nullptr, b->F, 1.0, 0.0, S.active, kGemmKUpToI | kGemmSym);
     // symmetric eigensolve with vectors: canonical 4 N^3 (k_trid_smem + k_syev)
     {
       const tb_status ts = launch_trid_plan(b, S.active, st);
@@ -1442,12 +1673,8 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
     }
     TB_K("fermi", 0, 0, k_fermi<<<nmol, 128, fermi_smem, st>>>(B, b->w, b->opt.kt, b->focc, b->kdim, S));
     // C = X Z (eigenvectors in ascending order through perm): 2N^3; P = C diag(f) C^T: 2 N^2 n_occ
-    TB_K("gemm", 2.0 * n3, 1,
-         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr,
-                                           b->W, 1.0, 0.0, S.active, kGemmKFromI));
-    TB_K("gemm", 2.0 * n2occ, 1,
-         k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, ntile64, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim,
-                                           b->P, 1.0, 0.0, S.active, kGemmSym));
+    TB_GEMM(2.0 * n3, b->X, 0, b->Z, 1, b->perm, nullptr, nullptr, b->W, 1.0, 0.0, S.active, kGemmKFromI);
+    TB_GEMM(2.0 * n2occ, b->W, 0, b->W, 1, nullptr, b->focc, b->kdim, b->P, 1.0, 0.0, S.active, kGemmSym);
   } else {
     const tb_status ms = mixed_core(b, st, n3_lo, n3_hi, n2occ_lo, n2occ_hi, gemm_grid, fermi_smem);
     if (ms != TB_OK) return ms;
@@ -1722,10 +1949,11 @@ tb_status batch_gradient(tb_batch* b, const std::vector<int>& flag, cudaStream_t
   k_potential<<<pot_grid, 256, 0, st>>>(b->Pc, B, qv, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, dflag, b->gtab,
                                         b->atab);
   TB_LAUNCH_CHECK();
-  const int gemm_grid = std::min(nt, 148 * 8);
-  k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, nt, b->W, 0, b->W, 1, nullptr, fe, b->kdim, b->F, 1.0,
-                                             0.0, dflag, kGemmSym);
-  TB_LAUNCH_CHECK();
+  {
+    const tb_status gs = launch_gemm(b, st, nullptr, 0.0, b->W, 0, b->W, 1, nullptr, fe, b->kdim, b->F, 1.0, 0.0,
+                                     dflag, kGemmSym);
+    if (gs != TB_OK) return gs;
+  }
   TB_CUDA(launch_grad_pairs(b->Pc, B, b->npair, b->pair_i, b->pair_j, b->se, b->P, b->F, b->vsh, b->vat, b->vdp,
                             b->vqp, dflag, maxsp, items, c->lmask, item, ese, st));
   ++b->launches;
@@ -1789,9 +2017,9 @@ tb_status spin_readout(tb_batch* b, const std::vector<int>& flag, cudaStream_t s
   TB_LAUNCH_CHECK();
   double* out[3] = {b->X, b->F, b->Z};  // P_alpha, P_beta, P_alpha - P_beta
   for (int c = 0; c < 3; ++c) {
-    k_gemm<<<gemm_grid, kGemmThreads, 0, st>>>(B, b->d_tiles64, nt, b->W, 0, b->W, 1, nullptr, b->d_fspin + c * NO,
-                                               b->kdim, out[c], 1.0, 0.0, b->d_wflag, kGemmSym);
-    TB_LAUNCH_CHECK();
+    const tb_status gs = launch_gemm(b, st, nullptr, 0.0, b->W, 0, b->W, 1, nullptr, b->d_fspin + c * NO, b->kdim,
+                                     out[c], 1.0, 0.0, b->d_wflag, kGemmSym);
+    if (gs != TB_OK) return gs;
   }
   k_mulliken_cols<<<nchunk, 256, 0, st>>>(B, b->d_chunks32, nchunk, b->Z, b->S, b->H0, b->D, b->Q, b->colred,
                                           b->d_wflag);
@@ -2090,6 +2318,13 @@ tb_status tb_calculator_set_smem_tridiag(tb_calculator* c, int32_t min_n) {
   return TB_OK;
 }
 
+tb_status tb_calculator_set_gemm_tiles(tb_calculator* c, int32_t max_n32) {
+  if (!c) return fail(TB_BAD_INPUT, "null calculator");
+  if (max_n32 < -1) return fail(TB_BAD_INPUT, "max_n32 must be -1 (measured), 0 (64 x 64 always) or a size in AOs");
+  c->tile_override = max_n32;
+  return TB_OK;
+}
+
 int32_t tb_calculator_tuning(const tb_calculator* c, char* buf, int32_t len) {
   if (!c) return 0;
   std::ostringstream o;
@@ -2109,7 +2344,13 @@ int32_t tb_calculator_tuning(const tb_calculator* c, char* buf, int32_t len) {
   for (int k = 0; k < kTridClasses; ++k)
     o << (k ? ", " : "") << "{\"cluster\": " << kTridClusterSizes[k] << ", \"max_n\": " << kTridClassMax[k]
       << ", \"smem_bytes\": " << trid_smem_bytes(kTridClassMax[k], kTridClusterSizes[k]) << "}";
-  o << "], \"smallest\": " << kTridMin << "}}";
+  o << "], \"smallest\": " << kTridMin << "}";
+  o << ", \"gemm_tiles\": {\"measured\": " << (c->tile.ready ? "true" : "false") << ", \"override\": "
+    << c->tile_override << ", \"split_gain\": " << kTileSplitGain << ", \"sizes\": [";
+  for (size_t i = 0; i < c->tile.n.size(); ++i)
+    o << (i ? ", " : "") << "{\"n\": " << c->tile.n[i] << ", \"s_per_structure_64\": " << c->tile.t64[i]
+      << ", \"s_per_structure_32\": " << c->tile.t32[i] << ", \"tile\": " << (c->tile.use32[i] ? 32 : 64) << "}";
+  o << "]}}";
   const std::string t = o.str();
   if (buf && len > 0) std::snprintf(buf, (size_t)len, "%s", t.c_str());
   return (int32_t)t.size();

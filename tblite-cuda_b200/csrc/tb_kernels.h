@@ -133,6 +133,10 @@ constexpr int kGemmKUpToJ = 1, kGemmKUpToI = 2, kGemmKFromI = 4, kGemmSym = 8;
 __global__ void k_gemm(DevBatch B, const int4* tiles, int ntiles, const double* Ab, int ta, const double* Bb, int tb_,
                        const int* perm, const double* ks, const int* kdim, double* Cb, double alpha, double beta,
                        const int* active, int shape = 0);
+// the same GEMM on 32 x 32 tiles (tile list in units of 32; the same bits as k_gemm)
+__global__ void k_gemm32(DevBatch B, const int4* tiles, int ntiles, const double* Ab, int ta, const double* Bb,
+                         int tb_, const int* perm, const double* ks, const int* kdim, double* Cb, double alpha,
+                         double beta, const int* active, int shape = 0);
 // Sb: optional n x n scratch per structure (same offsets as Ab); with it,
 // structures of at least kDcMin (64) AOs take divide and conquer instead of QL
 __global__ void k_syev(DevBatch B, double* Ab, double* Zb, double* Sb, double* wout, int* perm, int* status,

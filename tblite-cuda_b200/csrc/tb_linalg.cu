@@ -133,14 +133,21 @@ __global__ void k_trinv(DevBatch B, const double* __restrict__ W, double* __rest
 // `shape` skips known zeros and redundant tiles: kGemmKUpToJ (op(B) upper
 // triangular: only k < the tile's last column), kGemmKUpToI (op(A) lower
 // triangular: k < its last row), kGemmKFromI (op(A) upper triangular: k >=
-// its first row), kGemmSym (C symmetric: tiles below the diagonal are skipped
-// and every off-diagonal tile is also written transposed).
-// 64 x 64 tiles on the FP64 tensor instruction mma.sync.m8n8k4.f64: four warps,
-// each owning a 32 x 32 quarter as 4 x 4 fragments of 8 x 8 (32 accumulators
-// per lane).  K slabs of 16 are staged by cp.async in a two-stage ring (zero
-// fill past the matrix edge); the shared tiles are padded by 4 doubles so the
-// 64-bit fragment loads of a half-warp hit 16 distinct bank pairs.
-constexpr int GT = 64, GK = 16, GP = GT + 4;
+// its first row), kGemmSym (C symmetric: tiles below the diagonal are
+// skipped, and each element of the upper triangle is computed once and also
+// written to its mirror).
+// TILE x TILE tiles (64 or 32) on the FP64 tensor instruction
+// mma.sync.m8n8k4.f64: four warps, each owning a quarter of the tile as
+// (TILE/16) x (TILE/16) fragments of 8 x 8.  K slabs of 16 are staged by
+// cp.async in a two-stage ring (zero fill past the matrix edge); the shared
+// tiles are padded by 4 doubles so the 64-bit fragment loads of a half-warp
+// hit 16 distinct bank pairs.  Every output element accumulates over k in the
+// same order (slabs starting at multiples of 16, then the four k-steps of the
+// instruction) whatever the tile; the k ranges that only one tile size skips
+// hold exact zeros of the triangular operand, which leave a sum unchanged.
+// So the two tile sizes give the same bits, and the autotuner picks the tile
+// per structure size (k_gemm: 64, k_gemm32: 32).
+constexpr int GK = 16;
 static_assert(kGemmThreads == 128, "k_gemm assumes four warps");
 
 namespace {
@@ -159,22 +166,23 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "+d"(d0), "+d"(d1)
                : "d"(a), "d"(b));
 }
-}  // namespace
 
-__global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* __restrict__ tiles, int ntiles,
-                                                       const double* __restrict__ Ab, int ta,
-                                                       const double* __restrict__ Bb, int tb_,
-                                                       const int* __restrict__ perm, const double* __restrict__ ks,
-                                                       const int* __restrict__ kdim, double* __restrict__ Cb,
-                                                       double alpha, double beta, const int* __restrict__ active,
-                                                       int shape) {
+template <int GT>
+__device__ __forceinline__ void gemm_body(const DevBatch& B, const int4* __restrict__ tiles, int ntiles,
+                                          const double* __restrict__ Ab, int ta, const double* __restrict__ Bb,
+                                          int tb_, const int* __restrict__ perm, const double* __restrict__ ks,
+                                          const int* __restrict__ kdim, double* __restrict__ Cb, double alpha,
+                                          double beta, const int* __restrict__ active, int shape) {
+  constexpr int GP = GT + 4, FX = GT / 16;  // padded row; fragments per warp and dimension
+  constexpr int RA = GT / 8;                // slab elements of op(A) (and of op(B)) per thread
+  constexpr int TSH = GT == 64 ? 6 : 5;     // log2(GT)
   __shared__ __align__(16) double As[2][GK][GP];
   __shared__ __align__(16) double Bs[2][GK][GP];
   __shared__ __align__(16) double Ks[2][GK];
   __shared__ int colS[GT];  // columns of op(B) for this tile (through perm)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, tg = lane & 3;              // fragment coordinates
-  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;  // this warp's quarter of the tile
+  const int g = lane >> 2, tg = lane & 3;                          // fragment coordinates
+  const int wr = (warp >> 1) * (GT / 2), wc = (warp & 1) * (GT / 2);  // this warp's quarter of the tile
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int4 tl = tiles[t];
     const int m = tl.x;
@@ -194,49 +202,50 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
     if (shape & kGemmKUpToJ) khi = min(khi, j0 + GT);
     if (shape & kGemmKUpToI) khi = min(khi, i0 + GT);
     if (shape & kGemmKFromI) klo = min(i0, K);
-    double acc[4][4][2];
+    double acc[FX][FX][2];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < FX; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+      for (int b = 0; b < FX; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
     __syncthreads();  // colS and the ring of the previous tile are free
     if (tid < GT) colS[tid] = pm ? (j0 + tid < n ? pm[j0 + tid] : 0) : j0 + tid;
     __syncthreads();
-    // Element r (0..7) of a slab for this thread:
-    //   op(A) not transposed: kk = tid & 15, ii = (tid >> 4) + 8 r;  transposed: ii = tid & 63, kk = (tid >> 6) + 2 r
-    //   op(B) not transposed: jj = tid & 63, kb = (tid >> 6) + 2 r;  transposed: kb = tid & 15, jj = (tid >> 4) + 8 r
-    const int lo16 = tid & 15, hi8 = tid >> 4, lo64 = tid & 63, hi2 = tid >> 6;
+    // Element r of a slab for this thread:
+    //   op(A) not transposed: kk = tid & 15, ii = (tid >> 4) + 8 r;  transposed: ii = tid & (GT-1), kk = (tid >> log2 GT) + (128/GT) r
+    //   op(B) not transposed: jj = tid & (GT-1), kb = (tid >> log2 GT) + (128/GT) r;  transposed: kb = tid & 15, jj = (tid >> 4) + 8 r
+    const int lo16 = tid & 15, hi8 = tid >> 4, loT = tid & (GT - 1), hiT = tid >> TSH;
+    constexpr int SK = kGemmThreads / GT;  // k step of the transposed loads
     auto issue = [&](int buf, int k0) {
       if (!ta) {
         const int gk = k0 + lo16;
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
+        for (int r = 0; r < RA; ++r) {
           const int gi = i0 + hi8 + 8 * r;
           const bool v = gi < n && gk < K;
           cp_async8(&As[buf][lo16][hi8 + 8 * r], v ? A + (long long)gi * n + gk : A, v);
         }
       } else {
-        const int gi = i0 + lo64;
+        const int gi = i0 + loT;
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          const int gk = k0 + hi2 + 2 * r;
+        for (int r = 0; r < RA; ++r) {
+          const int gk = k0 + hiT + SK * r;
           const bool v = gi < n && gk < K;
-          cp_async8(&As[buf][hi2 + 2 * r][lo64], v ? A + (long long)gk * n + gi : A, v);
+          cp_async8(&As[buf][hiT + SK * r][loT], v ? A + (long long)gk * n + gi : A, v);
         }
       }
       if (!tb_) {
-        const bool vj = j0 + lo64 < n;
-        const int col = colS[lo64];
+        const bool vj = j0 + loT < n;
+        const int col = colS[loT];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          const int gk = k0 + hi2 + 2 * r;
+        for (int r = 0; r < RA; ++r) {
+          const int gk = k0 + hiT + SK * r;
           const bool v = vj && gk < K;
-          cp_async8(&Bs[buf][hi2 + 2 * r][lo64], v ? Bm + (long long)gk * n + col : Bm, v);
+          cp_async8(&Bs[buf][hiT + SK * r][loT], v ? Bm + (long long)gk * n + col : Bm, v);
         }
       } else {
         const int gk = k0 + lo16;
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
+        for (int r = 0; r < RA; ++r) {
           const int jj = hi8 + 8 * r;
           const bool v = j0 + jj < n && gk < K;
           cp_async8(&Bs[buf][lo16][jj], v ? Bm + (long long)colS[jj] * n + gk : Bm, v);
@@ -262,37 +271,61 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* _
       }
 #pragma unroll
       for (int k4 = 0; k4 < GK; k4 += 4) {
-        double af[4], bf[4];
+        double af[FX], bf[FX];
 #pragma unroll
-        for (int x = 0; x < 4; ++x) af[x] = As[cur][k4 + tg][wr + 8 * x + g];
+        for (int x = 0; x < FX; ++x) af[x] = As[cur][k4 + tg][wr + 8 * x + g];
 #pragma unroll
-        for (int y = 0; y < 4; ++y) bf[y] = Bs[cur][k4 + tg][wc + 8 * y + g];
+        for (int y = 0; y < FX; ++y) bf[y] = Bs[cur][k4 + tg][wc + 8 * y + g];
 #pragma unroll
-        for (int x = 0; x < 4; ++x)
+        for (int x = 0; x < FX; ++x)
 #pragma unroll
-          for (int y = 0; y < 4; ++y) dmma(acc[x][y][0], acc[x][y][1], af[x], bf[y]);
+          for (int y = 0; y < FX; ++y) dmma(acc[x][y][0], acc[x][y][1], af[x], bf[y]);
       }
       __syncthreads();  // buffer cur is refilled two slabs later
     }
 #pragma unroll
-    for (int x = 0; x < 4; ++x) {
+    for (int x = 0; x < FX; ++x) {
       const int gi = i0 + wr + 8 * x + g;
       if (gi >= n) continue;
 #pragma unroll
-      for (int y = 0; y < 4; ++y) {
+      for (int y = 0; y < FX; ++y) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int gj = j0 + wc + 8 * y + 2 * tg + h;
           if (gj >= n) continue;
+          // symmetric result: the upper triangle is computed and mirrored, so
+          // no element depends on which tile it fell in
+          if ((shape & kGemmSym) && gi > gj) continue;
           if (!TB_GUARD(8, (long long)gi * n + gj, 0, (long long)n * n)) continue;
           double* c = Cb + mo + (long long)gi * n + gj;
           const double r = beta == 0.0 ? alpha * acc[x][y][h] : alpha * acc[x][y][h] + beta * (*c);
           *c = r;
-          if ((shape & kGemmSym) && i0 != j0) Cb[mo + (long long)gj * n + gi] = r;
+          if ((shape & kGemmSym) && gi != gj) Cb[mo + (long long)gj * n + gi] = r;
         }
       }
     }
   }
+}
+}  // namespace
+
+__global__ void __launch_bounds__(kGemmThreads) k_gemm(DevBatch B, const int4* __restrict__ tiles, int ntiles,
+                                                       const double* __restrict__ Ab, int ta,
+                                                       const double* __restrict__ Bb, int tb_,
+                                                       const int* __restrict__ perm, const double* __restrict__ ks,
+                                                       const int* __restrict__ kdim, double* __restrict__ Cb,
+                                                       double alpha, double beta, const int* __restrict__ active,
+                                                       int shape) {
+  gemm_body<64>(B, tiles, ntiles, Ab, ta, Bb, tb_, perm, ks, kdim, Cb, alpha, beta, active, shape);
+}
+
+__global__ void __launch_bounds__(kGemmThreads) k_gemm32(DevBatch B, const int4* __restrict__ tiles, int ntiles,
+                                                         const double* __restrict__ Ab, int ta,
+                                                         const double* __restrict__ Bb, int tb_,
+                                                         const int* __restrict__ perm, const double* __restrict__ ks,
+                                                         const int* __restrict__ kdim, double* __restrict__ Cb,
+                                                         double alpha, double beta, const int* __restrict__ active,
+                                                         int shape) {
+  gemm_body<32>(B, tiles, ntiles, Ab, ta, Bb, tb_, perm, ks, kdim, Cb, alpha, beta, active, shape);
 }
 
 // ------------------------------------------------------------ eigensolver

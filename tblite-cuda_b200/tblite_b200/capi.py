@@ -70,7 +70,7 @@ EXPORTS = [
     "tb_batch_set_guess", "tb_batch_wavefunction", "tb_batch_gradient", "tb_sygvd_noalloc",
     "tb_calculator_set_small_solver", "tb_calculator_set_smem_tridiag", "tb_calculator_tuning",
     "tb_bounds_check_build", "tb_bounds_violations", "tb_server_compactions", "tb_dispersion",
-    "tb_read_xyz", "tb_calculator_species",
+    "tb_read_xyz", "tb_calculator_species", "tb_calculator_set_gemm_tiles",
 ]
 
 _lib = None
@@ -110,6 +110,7 @@ def load_library(path: str = LIB_PATH):
     L.tb_server_compactions.restype = C.c_int64
     L.tb_calculator_set_small_solver.argtypes = [C.c_void_p, C.c_int32]
     L.tb_calculator_set_smem_tridiag.argtypes = [C.c_void_p, C.c_int32]
+    L.tb_calculator_set_gemm_tiles.argtypes = [C.c_void_p, C.c_int32]
     L.tb_bounds_check_build.restype = C.c_int32
     L.tb_calculator_tuning.argtypes = [C.c_void_p, C.c_char_p, C.c_int32]
     L.tb_calculator_tuning.restype = C.c_int32
@@ -218,6 +219,13 @@ class Calculator:
         0 never the one-warp Jacobi solver, 1..32 Jacobi up to that many AOs."""
         check(load_library().tb_calculator_set_small_solver(self.h, C.c_int32(jacobi_max)),
               "tb_calculator_set_small_solver")
+
+    def set_gemm_tiles(self, max_n32: int):
+        """FP64 GEMM tile shape per structure: -1 the measured choice
+        (default), 0 always 64 x 64, N > 0 32 x 32 tiles up to N AOs.  Both
+        shapes give the same bits."""
+        check(load_library().tb_calculator_set_gemm_tiles(self.h, C.c_int32(max_n32)),
+              "tb_calculator_set_gemm_tiles")
 
     def set_smem_tridiag(self, min_n):
         """FP64 tridiagonalisation in cluster shared memory (k_trid_smem) for

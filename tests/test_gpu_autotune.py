@@ -79,3 +79,65 @@ def test_jacobi_in_mixed_form_fp64_phase(calc, oracle):
 def test_bad_override_rejected(calc):
     with pytest.raises(capi.TBError):
         calc.set_small_solver(33)
+
+
+# ---- FP64 GEMM tile shape (k_gemm 64 x 64 / k_gemm32 32 x 32)
+
+def _tile_mols():
+    rng = np.random.default_rng(43)
+    mols = g.water_clusters(6, seed=44, nmin=2, nmax=40)  # 12..240 AOs
+    mols += [g.alkane(n, rng) for n in (1, 5, 16, 40)]
+    o = g.octane()
+    mols.append(g.Molecule(o.id, o.xyz, charge=1.0, uhf=1))
+    return mols
+
+
+def _same(ra, rb):
+    assert ra["status"] == rb["status"] == 0
+    assert ra["energy"] == rb["energy"] and ra["iterations"] == rb["iterations"]
+    np.testing.assert_array_equal(ra["qat"], rb["qat"])
+    np.testing.assert_array_equal(ra["dipole"], rb["dipole"])
+
+
+def test_gemm_tile_shapes_give_the_same_bits(calc, oracle):
+    mols = _tile_mols()
+    out = {}
+    for shape, setting in (("64", 0), ("32", 100000)):
+        calc.set_gemm_tiles(setting)
+        out[shape] = (calc.singlepoint_batch(mols, gradient=True),
+                      calc.singlepoint_batch(mols, precision=1, accuracy=0.01),
+                      calc.singlepoint_batch(mols[-3:], nspin=2, wavefunction=True))
+    calc.set_gemm_tiles(-1)
+    for a, b in zip(out["64"][0], out["32"][0]):  # plain form with the gradient
+        _same(a, b)
+        np.testing.assert_array_equal(a["gradient"], b["gradient"])
+    for a, b in zip(out["64"][1], out["32"][1]):  # mixed form: FP64 phase and refinement GEMMs
+        _same(a, b)
+    for a, b in zip(out["64"][2], out["32"][2]):  # open-shell density read-out
+        np.testing.assert_array_equal(a["wfn"]["density"], b["wfn"]["density"])
+    for m, r in zip(mols, out["32"][0]):
+        o = oracle.singlepoint(m)
+        assert abs(r["energy"] - o["energy"]) < 1e-9
+        np.testing.assert_allclose(r["qat"], o["qat"], atol=1e-7)
+
+
+def test_gemm_tile_measured_table_and_mixed_batch(calc):
+    calc.set_gemm_tiles(-1)
+    mols = _tile_mols()
+    batch = calc.singlepoint_batch(mols)
+    t = calc.tuning()["gemm_tiles"]
+    assert t["measured"] and t["override"] == -1
+    assert [x["n"] for x in t["sizes"]] == list(range(16, 385, 16))
+    assert all(x["s_per_structure_64"] > 0 and x["s_per_structure_32"] > 0 for x in t["sizes"])
+    assert all(x["tile"] == (32 if x["s_per_structure_32"] < x["s_per_structure_64"] else 64) for x in t["sizes"])
+    # a threshold inside the batch splits it over both kernels: still the same bits
+    calc.set_gemm_tiles(100)
+    split = calc.singlepoint_batch(mols)
+    calc.set_gemm_tiles(-1)
+    for a, b in zip(batch, split):
+        _same(a, b)
+
+
+def test_bad_gemm_tile_override_rejected(calc):
+    with pytest.raises(capi.TBError):
+        calc.set_gemm_tiles(-2)
