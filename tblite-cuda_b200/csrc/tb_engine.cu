@@ -389,6 +389,8 @@ struct tb_batch {
   MolState ms{};
   double *cn, *mrad, *erep, *se, *n0sh;
   int *cnt, *npair, *pair_i, *pair_j;
+  SpLists sp_w{};      // work space of the integral setup (in X..P, see the layout)
+  size_t sp_off[4]{};  // its parts' offsets from X
   long long* inl;
   double *S, *H0, *D, *Q, *X, *W, *F, *Z, *P;
   double *gtab, *atab;  // Coulomb pair tables of the fixed geometry (k_pair_tables)
@@ -778,10 +780,44 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   size_t o_gtab = L.add((size_t)b->h_s2off[nmol] * D8), o_atab = L.add((size_t)b->h_a2off[nmol] * 3 * D8);
   size_t o_cn = L.add(NA * D8), o_mrad = L.add(NA * D8), o_erep = L.add(NA * D8), o_se = L.add(NS * D8),
          o_n0sh = L.add(NS * D8), o_cnt = L.add(NA * I4), o_inl = L.add(NA * 8), o_npair = L.add(NM * I4),
-         o_pi = L.add(b->pair_cap * I4), o_pj = L.add(b->pair_cap * I4);
+         o_pi = L.add(b->pair_cap * I4), o_pj = L.add(b->pair_cap * I4), o_spc = L.add(32 * I4);
   size_t o_S = L.add(N2 * D8), o_H0 = L.add(N2 * D8), o_D = L.add(3 * N2 * D8), o_Q = L.add(6 * N2 * D8);
   size_t o_X = L.add(N2 * D8), o_W = L.add(N2 * D8), o_F = L.add(N2 * D8), o_Z = L.add(N2 * D8),
          o_P = L.add(N2 * D8);
+  // Work space of the integral setup (SpLists: block records, class list,
+  // item index, pair table) in X..P, which the setup fills only after the
+  // integrals; extended here when the batch needs more.  Bounds: every atom
+  // pair i > j of a structure within the cutoff, sum over pairs of
+  // nsh_i nsh_j items and 10 nao_i nao_j + nsh_i nsh_j record doubles.
+  {
+    long long items = 0, rec = 0;
+    for (int m = 0; m < nmol; ++m) {
+      long long sh = 0, sh2 = 0, ao = 0, ao2 = 0;
+      for (int a = b->h_aoff[m]; a < b->h_aoff[m + 1]; ++a) {
+        const SpeciesParam& spa = P.sp[id[a]];
+        long long na = 0;
+        for (int k = 0; k < spa.nsh; ++k) na += msao(P.sh[spa.sh0 + k].ang);
+        sh += spa.nsh; sh2 += (long long)spa.nsh * spa.nsh; ao += na; ao2 += na * na;
+      }
+      const long long it = (sh * sh - sh2) / 2;
+      items += it;
+      rec += 10 * ((ao * ao - ao2) / 2) + it;
+    }
+    const long long idx = b->pair_cap * (long long)calc->maxsh * calc->maxsh;
+    if (items >= (1LL << 31) || b->pair_cap >= (1LL << 31) || nmol >= (1 << 23))
+      return fail(TB_CAPACITY_EXCEEDED, "batch too large for the integral work space (" + std::to_string(items) +
+                                            " shell pairs, " + std::to_string(nmol) + " structures)");
+    auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+    b->sp_w.items = items;
+    b->sp_w.rec_len = rec;
+    b->sp_w.tab_len = b->h_a2off[nmol];
+    b->sp_off[0] = 0;                                            // records
+    b->sp_off[1] = up((size_t)rec * D8);                         // class list
+    b->sp_off[2] = b->sp_off[1] + up((size_t)items * sizeof(int2));  // item index
+    b->sp_off[3] = b->sp_off[2] + up((size_t)idx * I4);          // pair table
+    const size_t need = b->sp_off[3] + (size_t)b->sp_w.tab_len * I4, end = L.add(0);
+    if (end - o_X < need) L.add(need - (end - o_X));
+  }
   size_t o_w = L.add(NO * D8), o_focc = L.add(NO * D8), o_perm = L.add(NO * I4), o_kdim = L.add(NM * I4),
          o_vsh = L.add(NS * D8), o_vat = L.add(NA * D8), o_vdp = L.add(3 * NA * D8), o_vqp = L.add(6 * NA * D8),
          o_col = L.add(12 * NO * D8), o_qsho = L.add(NS * D8), o_qato = L.add(NA * D8), o_dpo = L.add(3 * NA * D8),
@@ -910,6 +946,11 @@ tb_status batch_build(tb_calculator* calc, const tb_structure* mols, int nmol, c
   b->cn = at<double>(base, o_cn); b->mrad = at<double>(base, o_mrad); b->erep = at<double>(base, o_erep);
   b->se = at<double>(base, o_se); b->n0sh = at<double>(base, o_n0sh); b->cnt = at<int>(base, o_cnt);
   b->inl = at<long long>(base, o_inl); b->npair = at<int>(base, o_npair); b->pair_i = at<int>(base, o_pi);
+  b->sp_w.cls = at<int>(base, o_spc);
+  b->sp_w.rec = at<double>(base, o_X + b->sp_off[0]);
+  b->sp_w.list = at<int2>(base, o_X + b->sp_off[1]);
+  b->sp_w.idx = at<int>(base, o_X + b->sp_off[2]);
+  b->sp_w.tab = at<int>(base, o_X + b->sp_off[3]);
   b->pair_j = at<int>(base, o_pj);
   b->S = at<double>(base, o_S); b->H0 = at<double>(base, o_H0); b->D = at<double>(base, o_D);
   b->Q = at<double>(base, o_Q); b->X = at<double>(base, o_X); b->W = at<double>(base, o_W);
@@ -1557,16 +1598,14 @@ tb_status batch_setup(tb_batch* b, cudaStream_t st) {
        k_adj_scan<<<nmol, 256, 0, st>>>(B, b->cnt, b->inl, b->npair);
        TB_LAUNCH_CHECK();
        k_adj_fill<<<nblk((long long)B.nat_tot * 32, 256), 256, 0, st>>>(B, Pc.cutoff, b->inl, b->pair_i, b->pair_j));
-  // S, H0, D, Q are contiguous in the layout: one memset covers 11 N^2
-  TB_CUDA(cudaMemsetAsync(b->S, 0, (size_t)((char*)(b->Q + 6 * b->n2_tot) - (char*)b->S), st));
+  // S, H0, D, Q: every element is written by the integral setup (zeros included)
   {
     MatOut out{b->S, b->H0, b->D, b->Q};
     const int maxsp = c->maxsh * c->maxsh;
-    const long long items = b->pair_cap * maxsp;
     cudaEvent_t e0 = nullptr;
     prof_start(b, st, &e0);
-    TB_CUDA(launch_integrals(Pc, B, b->npair, b->pair_i, b->pair_j, b->se, out, maxsp, items, c->lmask, st,
-                             &b->launches));
+    TB_CUDA(launch_integrals(Pc, B, b->npair, b->pair_i, b->pair_j, b->se, out, maxsp, b->pair_cap, c->lmask,
+                             b->sp_w, st, &b->launches));
     prof_stop(b, st, "integrals", e0, 0, 0);
   }
   TB_K("cholesky", 0, 0, k_cholesky<<<nmol, 256, 0, st>>>(B, b->S, b->W, S.status, nullptr));
@@ -2509,12 +2548,10 @@ tb_status run_setup_to_integrals(tb_batch* b, bool with_integrals) {
   TB_LAUNCH_CHECK();
   k_adj_fill<<<nblk((long long)B.nat_tot * 32, 256), 256>>>(B, P.cutoff, b->inl, b->pair_i, b->pair_j);
   TB_LAUNCH_CHECK();
-  TB_CUDA(cudaMemset(b->S, 0, (size_t)((char*)(b->Q + 6 * b->n2_tot) - (char*)b->S)));
   MatOut out{b->S, b->H0, b->D, b->Q};
   const int maxsp = b->calc->maxsh * b->calc->maxsh;
-  const long long items = b->pair_cap * maxsp;
-  TB_CUDA(launch_integrals(P, B, b->npair, b->pair_i, b->pair_j, b->se, out, maxsp, items, b->calc->lmask, 0,
-                           &b->launches));
+  TB_CUDA(launch_integrals(P, B, b->npair, b->pair_i, b->pair_j, b->se, out, maxsp, b->pair_cap, b->calc->lmask,
+                           b->sp_w, 0, &b->launches));
   TB_CUDA(cudaDeviceSynchronize());
   return TB_OK;
 }
@@ -2925,6 +2962,9 @@ int64_t workspace_estimate(const tb_options& o, int nat, int nsh, int nao) {
   const double n2 = (double)nao * nao;
   double b = 128.0 * n2 + (o.precision == 1 ? 24.0 * n2 : 0.0);
   b += 4.0 * nat * (nat - 1);  // pair_i, pair_j
+  // integral work space beyond X..P: the records' hij, the class list, the
+  // item index (at most 9 shell pairs per atom pair) and the pair table
+  b += 8.0 * nsh * nsh + 22.0 * nat * nat;
   const double mx = nsh + 9.0 * nat;
   b += 8.0 * mx * (4 + 2.0 * o.max_iter) + 8.0 * o.max_iter * o.max_iter;
   b += 8.0 * (30.0 * nao + 30.0 * nat);  // per-AO / per-atom vectors

@@ -121,9 +121,24 @@ __global__ void k_atoms(DevParams P, DevBatch B, double* cn, double* mrad, doubl
 __global__ void k_adj_count(DevBatch B, double cutoff, int* cnt);
 __global__ void k_adj_scan(DevBatch B, const int* cnt, long long* inl, int* npair);
 __global__ void k_adj_fill(DevBatch B, double cutoff, const long long* inl, int* pair_i, int* pair_j);
+// Work space of the integral setup: the shell-pair items sorted by (li, lj)
+// class (list, `items` entries), the item of each (pair slot, shell pair)
+// (idx, pair_cap * maxsp), the computed blocks (rec, `rec_len` doubles:
+// per item s[SI SJ], hij, d[3 SI SJ], q[6 SI SJ]), the pair slot of each
+// atom pair i > j (tab, at a2off, nat^2 per structure) and the class counts
+// and cursors (cls, 32 ints).
+struct SpLists {
+  int2* list;
+  int* idx;
+  double* rec;
+  int* tab;
+  int* cls;
+  long long items, rec_len, tab_len;
+};
+__host__ __device__ constexpr int sp_record(int li, int lj) { return 10 * (2 * li + 1) * (2 * lj + 1) + 1; }
 cudaError_t launch_integrals(const DevParams& P, const DevBatch& B, const int* npair, const int* pair_i,
-                             const int* pair_j, const double* se, const MatOut& out, int maxsp, long long items,
-                             int lmask, cudaStream_t st, int64_t* launches);
+                             const int* pair_j, const double* se, const MatOut& out, int maxsp, long long pair_cap,
+                             int lmask, const SpLists& W, cudaStream_t st, int64_t* launches);
 
 // linear algebra
 __global__ void k_cholesky(DevBatch B, const double* S, double* W, int* status, const int* active);

@@ -374,41 +374,114 @@ __device__ void pair_block(const DevParams& P, const MatOut& out, long long mo, 
   scatter_block<LI, LJ>(out, mo, n, ii, jj, onsite, hij, vec, s, d, q);
 }
 
-// Off-site shell pairs of angular momenta (LI, LJ): one thread per (neighbour
-// pair, shell pair), grid stride over the pair capacity of the whole batch;
-// slots beyond a structure's npair and shell pairs of other (li, lj) are
-// skipped.  One instantiation per (li, lj) keeps the register budget of the
-// s/p kernels independent of the d-shell ones.
-template <int LI, int LJ>
-__global__ void k_integrals_t(DevParams P, DevBatch B, const int* __restrict__ npair, const int* __restrict__ pair_i,
-                              const int* __restrict__ pair_j, const double* __restrict__ se, MatOut out, int maxsp,
-                              long long total_items) {
-  for (long long it = blockIdx.x * (long long)blockDim.x + threadIdx.x; it < total_items;
-       it += (long long)gridDim.x * blockDim.x) {
-    const long long p = it / maxsp;
-    const int sp = (int)(it % maxsp);
-    // structure owning pair slot p (binary search over the capacity offsets)
-    int lo = 0, hi = B.nmol;
+// Item offsets of class c in the sorted list and in the block records.
+__device__ inline void sp_bases(const int* cls, int c, int* off, long long* rbase) {
+  int o = 0;
+  long long r = 0;
+  for (int k = 0; k < c; ++k) {
+    o += cls[k];
+    r += (long long)cls[k] * sp_record(k / (kMaxL + 1), k % (kMaxL + 1));
+  }
+  *off = o;
+  *rbase = r;
+}
+
+// Shell-pair items of the half neighbour list sorted by (li, lj) class
+// c = 3 li + lj, one thread per pair slot.  Pass 0 adds each class's item
+// count to cls[c]; pass 1 places the items into list, class c after the
+// counts of the classes below it, through the cursors cls[16 + c], and
+// records each item's index in idx[p * maxsp + sp].  An item is (pair slot,
+// structure << 8 | shell pair).  The order inside a class follows the
+// atomics and changes no result: every block has its own record.
+__global__ void k_sp_classify(DevParams P, DevBatch B, const int* __restrict__ npair, const int* __restrict__ pair_i,
+                              const int* __restrict__ pair_j, long long pair_cap, int maxsp, int pass, SpLists W) {
+  constexpr int NC = (kMaxL + 1) * (kMaxL + 1), MS = kMaxShPerAtom * kMaxShPerAtom;
+  __shared__ int scnt[NC], sbase[NC];
+  if (threadIdx.x < NC) scnt[threadIdx.x] = 0;
+  __syncthreads();
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  int m = 0, nsp = 0, nshj = 1;
+  int cl[MS], loc[MS];
+  if (p < pair_cap) {
+    int lo = 0, hi = B.nmol;  // structure owning pair slot p
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
       if (B.poff[mid] <= p) lo = mid; else hi = mid;
     }
-    const int m = lo;
-    if (p - B.poff[m] >= npair[m]) continue;
+    m = lo;
+    if (p - B.poff[m] < npair[m]) {
+      const int a0 = B.aoff[m];
+      const SpeciesParam& spi = P.sp[B.id[a0 + pair_i[p]]];
+      const SpeciesParam& spj = P.sp[B.id[a0 + pair_j[p]]];
+      nshj = spj.nsh;
+      nsp = spi.nsh * spj.nsh;
+      for (int sp = 0; sp < nsp; ++sp) {
+        cl[sp] = (kMaxL + 1) * P.sh[spi.sh0 + sp / nshj].ang + P.sh[spj.sh0 + sp % nshj].ang;
+        loc[sp] = atomicAdd(&scnt[cl[sp]], 1);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < NC && scnt[threadIdx.x] > 0) {
+    if (pass == 0) atomicAdd(&W.cls[threadIdx.x], scnt[threadIdx.x]);
+    else sbase[threadIdx.x] = atomicAdd(&W.cls[16 + threadIdx.x], scnt[threadIdx.x]);
+  }
+  if (pass == 0) return;
+  __syncthreads();
+  for (int sp = 0; sp < nsp; ++sp) {
+    int off;
+    long long rb;
+    sp_bases(W.cls, cl[sp], &off, &rb);
+    const int g = off + sbase[cl[sp]] + loc[sp];
+    if (!TB_GUARD(4, g, 0, W.items) || !TB_GUARD(5, p * maxsp + sp, 0, pair_cap * maxsp)) continue;
+    W.list[g] = make_int2((int)p, (m << 8) | sp);
+    W.idx[p * maxsp + sp] = g;
+  }
+}
+
+// Pair slot of every kept atom pair i > j of a structure, at a2off + i nat + j
+// (the table is cleared to -1 first: atom pairs beyond the cutoff).
+__global__ void k_sp_pairtab(DevBatch B, const int* __restrict__ npair, const int* __restrict__ pair_i,
+                             const int* __restrict__ pair_j, long long pair_cap, int* __restrict__ tab) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= pair_cap) return;
+  int lo = 0, hi = B.nmol;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (B.poff[mid] <= p) lo = mid; else hi = mid;
+  }
+  const int m = lo;
+  if (p - B.poff[m] >= npair[m]) return;
+  const int nat = B.aoff[m + 1] - B.aoff[m];
+  const long long x = B.a2off[m] + (long long)pair_i[p] * nat + pair_j[p];
+  if (TB_GUARD(6, x, B.a2off[m], B.a2off[m + 1])) tab[x] = (int)p;
+}
+
+// Off-site shell pairs of angular momenta (LI, LJ): one thread per item of
+// the class's list (k_sp_classify), grid stride; the block goes to the
+// item's record, which consecutive threads write side by side.  One
+// instantiation per (li, lj) keeps the register budget of the s/p kernels
+// independent of the d-shell ones.
+template <int LI, int LJ>
+__global__ void k_integrals_t(DevParams P, DevBatch B, const int* __restrict__ pair_i, const int* __restrict__ pair_j,
+                              const double* __restrict__ se, SpLists W) {
+  constexpr int C = (kMaxL + 1) * LI + LJ, SIJ = (2 * LI + 1) * (2 * LJ + 1), R = sp_record(LI, LJ);
+  int off;
+  long long rbase;
+  sp_bases(W.cls, C, &off, &rbase);
+  const int cnt = W.cls[C];
+  for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < cnt; it += gridDim.x * blockDim.x) {
+    const int2 e = W.list[off + it];
+    const int p = e.x, m = e.y >> 8, sp = e.y & 255;
     const int a0 = B.aoff[m];
     const int iat = pair_i[p], jat = pair_j[p];
     const SpeciesParam& spi = P.sp[B.id[a0 + iat]];
     const SpeciesParam& spj = P.sp[B.id[a0 + jat]];
-    if (sp >= spi.nsh * spj.nsh) continue;
     const int ish = sp / spj.nsh, jsh = sp % spj.nsh;
     const int ti = spi.sh0 + ish, tj = spj.sh0 + jsh;
     const ShellParam* ci = P.sh + ti;
     const ShellParam* cj = P.sh + tj;
-    if (ci->ang != LI || cj->ang != LJ) continue;
-    const int n = B.ooff[m + 1] - B.ooff[m];
-    const long long mo = B.moff[m];
     const int is = B.soff[m] + B.at_ish[a0 + iat], js = B.soff[m] + B.at_ish[a0 + jat];
-    const int ii = B.sh_iao[is + ish], jj = B.sh_iao[js + jsh];
     const double vec[3] = {B.xyz[3 * (a0 + iat)] - B.xyz[3 * (a0 + jat)],
                            B.xyz[3 * (a0 + iat) + 1] - B.xyz[3 * (a0 + jat) + 1],
                            B.xyz[3 * (a0 + iat) + 2] - B.xyz[3 * (a0 + jat) + 2]};
@@ -416,7 +489,90 @@ __global__ void k_integrals_t(DevParams P, DevBatch B, const int* __restrict__ n
     const double rr = sqrt(sqrt(r2) / (spj.rad + spi.rad));
     const double shpoly = (1.0 + ci->shpoly * rr) * (1.0 + cj->shpoly * rr);
     const double hij = 0.5 * (se[is + ish] + se[js + jsh]) * P.hscale[ti * P.nshtype + tj] * shpoly;
-    pair_block<LI, LJ>(P, out, mo, n, ii, jj, false, hij, r2, vec, ci, cj);
+    double sb[SIJ], db[3 * SIJ], qb[6 * SIJ];
+    multipole_cgto<LI, LJ>(ci, cj, r2, vec, P.intcut, sb, db, qb);
+    const long long r0 = rbase + (long long)it * R;
+    if (!TB_GUARD(7, r0 + R - 1, 0, W.rec_len)) continue;
+    double* rec = W.rec + r0;
+#pragma unroll
+    for (int x = 0; x < SIJ; ++x) rec[x] = sb[x];
+    rec[SIJ] = hij;
+#pragma unroll
+    for (int x = 0; x < 3 * SIJ; ++x) rec[SIJ + 1 + x] = db[x];
+#pragma unroll
+    for (int x = 0; x < 6 * SIJ; ++x) rec[4 * SIJ + 1 + x] = qb[x];
+  }
+}
+
+// Dense S, H0, D, Q of every structure from the block records, one warp per
+// AO row, lanes over the columns: each row of the eleven planes is written
+// once, contiguously, zeros included (atom pairs beyond the cutoff, and the
+// on-site blocks, which k_onsite_t writes afterwards).  Element (r, c) with
+// atoms A = atom(r) != Bt = atom(c) belongs to the half-list pair i =
+// max(A, Bt), j = min(A, Bt) (get_hamiltonian's assembly loop,
+// src/h0.cu:306-477, quoted Fortran): for A < Bt it is the block's element
+// [c - first AO of i's shell][r - first AO of j's shell] as computed (operator
+// on centre i); for A > Bt the transposed element [r ...][c ...] with the
+// dipole and quadrupole operators shifted to centre j (shift_operator).
+__global__ void k_sp_assemble(DevParams P, DevBatch B, SpLists W, MatOut out, int maxsp) {
+  const int lane = threadIdx.x & 31;
+  const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  if (row >= B.nao_tot) return;
+  int lo = 0, hi = B.nmol;  // structure owning AO row `row`
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (B.ooff[mid] <= row) lo = mid; else hi = mid;
+  }
+  const int m = lo, o0 = B.ooff[m], n = B.ooff[m + 1] - o0, r = (int)(row - o0);
+  const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0, s0 = B.soff[m];
+  const long long mo = B.moff[m], nn = (long long)n * n;
+  const int A = B.ao_at[o0 + r], shA = B.ao_sh[o0 + r];
+  for (int c = lane; c < n; c += 32) {
+    const long long e = (long long)r * n + c;
+    if (!TB_GUARD(8, e, 0, nn)) continue;
+    double sv = 0.0, hv = 0.0, dv[3] = {0.0, 0.0, 0.0}, qv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const int Bt = B.ao_at[o0 + c];
+    if (Bt != A) {
+      const bool tr = A > Bt;  // row atom is the pair's i
+      const int ia = tr ? A : Bt, ja = tr ? Bt : A;
+      const int p = W.tab[B.a2off[m] + (long long)ia * nat + ja];
+      if (p >= 0) {
+        const int shB = B.ao_sh[o0 + c];
+        const int shi = tr ? shA : shB, shj = tr ? shB : shA;  // local shell indices
+        const int ish = shi - B.at_ish[a0 + ia], jsh = shj - B.at_ish[a0 + ja];
+        const int nshj = P.sp[B.id[a0 + ja]].nsh;
+        const int li = P.sh[B.sh_type[s0 + shi]].ang, lj = P.sh[B.sh_type[s0 + shj]].ang;
+        const int SJ = 2 * lj + 1, SIJ = (2 * li + 1) * SJ;
+        const int iao = (tr ? r : c) - B.sh_iao[s0 + shi], jao = (tr ? c : r) - B.sh_iao[s0 + shj];
+        const int g = W.idx[(long long)p * maxsp + ish * nshj + jsh];
+        int off;
+        long long rbase;
+        sp_bases(W.cls, (kMaxL + 1) * li + lj, &off, &rbase);
+        const double* rec = W.rec + rbase + (long long)(g - off) * sp_record(li, lj);
+        const int ij = iao * SJ + jao;
+        sv = rec[ij];
+        hv = sv * rec[SIJ];
+        const double* d = rec + SIJ + 1 + 3 * ij;
+        const double* q = rec + 4 * SIJ + 1 + 6 * ij;
+        if (tr) {
+          const double vec[3] = {B.xyz[3 * (a0 + ia)] - B.xyz[3 * (a0 + ja)],
+                                 B.xyz[3 * (a0 + ia) + 1] - B.xyz[3 * (a0 + ja) + 1],
+                                 B.xyz[3 * (a0 + ia) + 2] - B.xyz[3 * (a0 + ja) + 2]};
+          shift_operator(vec, sv, d, q, dv, qv);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 3; ++k) dv[k] = d[k];
+#pragma unroll
+          for (int k = 0; k < 6; ++k) qv[k] = q[k];
+        }
+      }
+    }
+    out.S[mo + e] = sv;
+    out.H0[mo + e] = hv;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out.D[3 * mo + k * nn + e] = dv[k];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) out.Q[6 * mo + k * nn + e] = qv[k];
   }
 }
 
@@ -446,22 +602,43 @@ __global__ void k_onsite_t(DevParams P, DevBatch B, const double* __restrict__ s
   }
 }
 
-// Launch the integral kernels for every (li, lj) combination in `lmask`
-// (bit l set when the parameter set has shells of angular momentum l).
+// The integral setup: shell-pair items sorted into (li, lj) classes, the
+// pair table, the off-site blocks of every class present in `lmask` (bit l
+// set when the parameter set has shells of angular momentum l) into their
+// records, the dense planes from the records, then the on-site blocks.
 cudaError_t launch_integrals(const DevParams& P, const DevBatch& B, const int* npair, const int* pair_i,
-                             const int* pair_j, const double* se, const MatOut& out, int maxsp, long long items,
-                             int lmask, cudaStream_t st, int64_t* launches) {
-  const int grid = (int)std::max(1LL, std::min((items + 127) / 128, 148LL * 32));
+                             const int* pair_j, const double* se, const MatOut& out, int maxsp, long long pair_cap,
+                             int lmask, const SpLists& W, cudaStream_t st, int64_t* launches) {
+  const int grid = (int)std::max(1LL, std::min((W.items + 127) / 128, 148LL * 32));
   const int ogrid = (int)std::max(1LL, ((long long)B.nat_tot * maxsp + 127) / 128);
-#define TB_LAUNCH_PAIR(A, C)                                                                              \
-  if ((lmask >> A & 1) && (lmask >> C & 1)) {                                                             \
-    k_integrals_t<A, C><<<grid, 128, 0, st>>>(P, B, npair, pair_i, pair_j, se, out, maxsp, items);        \
-    k_onsite_t<A, C><<<ogrid, 128, 0, st>>>(P, B, se, out, maxsp);                                        \
-    *launches += 2;                                                                                       \
+  const int cgrid = (int)std::max(1LL, (pair_cap + 255) / 256);
+  const int agrid = (int)std::max(1LL, ((long long)B.nao_tot * 32 + 255) / 256);
+  cudaError_t e = cudaMemsetAsync(W.cls, 0, 32 * sizeof(int), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(W.tab, 0xff, (size_t)W.tab_len * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  for (int pass = 0; pass < 2; ++pass)
+    k_sp_classify<<<cgrid, 256, 0, st>>>(P, B, npair, pair_i, pair_j, pair_cap, maxsp, pass, W);
+  k_sp_pairtab<<<cgrid, 256, 0, st>>>(B, npair, pair_i, pair_j, pair_cap, W.tab);
+  *launches += 3;
+#define TB_LAUNCH_PAIR(A, C)                                                           \
+  if ((lmask >> A & 1) && (lmask >> C & 1)) {                                          \
+    k_integrals_t<A, C><<<grid, 128, 0, st>>>(P, B, pair_i, pair_j, se, W);            \
+    *launches += 1;                                                                    \
   }
   TB_LAUNCH_PAIR(0, 0) TB_LAUNCH_PAIR(0, 1) TB_LAUNCH_PAIR(1, 0) TB_LAUNCH_PAIR(1, 1)
   TB_LAUNCH_PAIR(0, 2) TB_LAUNCH_PAIR(2, 0) TB_LAUNCH_PAIR(1, 2) TB_LAUNCH_PAIR(2, 1) TB_LAUNCH_PAIR(2, 2)
 #undef TB_LAUNCH_PAIR
+  k_sp_assemble<<<agrid, 256, 0, st>>>(P, B, W, out, maxsp);
+  *launches += 1;
+#define TB_LAUNCH_ONSITE(A, C)                                                         \
+  if ((lmask >> A & 1) && (lmask >> C & 1)) {                                          \
+    k_onsite_t<A, C><<<ogrid, 128, 0, st>>>(P, B, se, out, maxsp);                     \
+    *launches += 1;                                                                    \
+  }
+  TB_LAUNCH_ONSITE(0, 0) TB_LAUNCH_ONSITE(0, 1) TB_LAUNCH_ONSITE(1, 0) TB_LAUNCH_ONSITE(1, 1)
+  TB_LAUNCH_ONSITE(0, 2) TB_LAUNCH_ONSITE(2, 0) TB_LAUNCH_ONSITE(1, 2) TB_LAUNCH_ONSITE(2, 1)
+  TB_LAUNCH_ONSITE(2, 2)
+#undef TB_LAUNCH_ONSITE
   return cudaGetLastError();
 }
 

@@ -19,8 +19,11 @@ def main(argv=None):
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--solver", type=int, default=1, help="1: in-house eigensolver only (no calibration launches)")
+    ap.add_argument("--gemm-tiles", type=int, default=-1,
+                    help="-1: measured tile choice (its calibration launches come first); 0: 64 x 64 tiles only")
     a = ap.parse_args(argv)
     calc = Calculator()
+    calc.set_gemm_tiles(a.gemm_tiles)
     mols = geometry.water_clusters(a.count, seed=1001, nmin=a.nmin, nmax=a.nmax)
     b = capi.Batch(calc, mols, precision=a.precision, solver=a.solver)
     for _ in range(a.warmup):
