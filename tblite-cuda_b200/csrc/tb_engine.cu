@@ -1061,12 +1061,14 @@ tb_status launch_trid_plan(tb_batch* b, const int* active, cudaStream_t st) {
 
 // One batched FP64 GEMM (k_gemm's operands) over the batch's two GEMM tile
 // lists: k_gemm on the structures given 64 x 64 tiles, k_gemm32 on those given
-// 32 x 32 (the same bits either way).  With a profile name both launches are
-// timed in that class and the algorithmic work is booked once.
+// 32 x 32 (the same bits either way).  One CTA per tile: the block scheduler
+// hands the tiles, largest structures first, to SMs as they free up, which
+// balances tiles of very different K better than a fixed grid stride.  With
+// a profile name both launches are timed in that class and the algorithmic
+// work is booked once.
 tb_status launch_gemm(tb_batch* b, cudaStream_t st, const char* prof, double work, const double* A, int ta,
                       const double* Bm, int tb_, const int* perm, const double* ks, const int* kdim, double* C,
                       double alpha, double beta, const int* active, int shape) {
-  constexpr int kGrid = 148 * 8;
   bool booked = false;
   for (int v = 0; v < 2; ++v) {
     const int nt = v ? b->ngemm32 : b->ngemm64;
@@ -1074,11 +1076,11 @@ tb_status launch_gemm(tb_batch* b, cudaStream_t st, const char* prof, double wor
     cudaEvent_t e0 = nullptr;
     if (prof) prof_start(b, st, &e0);
     if (v == 0)
-      k_gemm<<<std::min(nt, kGrid), kGemmThreads, 0, st>>>(b->db, b->d_gemm64, nt, A, ta, Bm, tb_, perm, ks, kdim, C,
-                                                           alpha, beta, active, shape);
+      k_gemm<<<nt, kGemmThreads, 0, st>>>(b->db, b->d_gemm64, nt, A, ta, Bm, tb_, perm, ks, kdim, C, alpha, beta,
+                                          active, shape);
     else
-      k_gemm32<<<std::min(nt, kGrid), kGemmThreads, 0, st>>>(b->db, b->d_gemm32, nt, A, ta, Bm, tb_, perm, ks, kdim,
-                                                             C, alpha, beta, active, shape);
+      k_gemm32<<<nt, kGemmThreads, 0, st>>>(b->db, b->d_gemm32, nt, A, ta, Bm, tb_, perm, ks, kdim, C, alpha, beta,
+                                            active, shape);
     TB_LAUNCH_CHECK();
     if (prof) prof_stop(b, st, prof, e0, booked ? 0.0 : work, 1);
     booked = true;
@@ -1494,7 +1496,7 @@ tb_status calibrate_tiles(tb_calculator* c) {
       for (int m = 0; m < cnt; ++m)
         for (int t = 0; t < nt1; ++t)
           for (int u = 0; u < nt1; ++u) tl.push_back(make_int4(m, t, u, 0));
-      const int nt = (int)tl.size(), grid = std::min(nt, 148 * 8);
+      const int nt = (int)tl.size(), grid = nt;  // one CTA per tile, as launch_gemm
       if (cudaMemcpy(dT, tl.data(), tl.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess) {
         st = fail(TB_CUDA_ERROR, "GEMM tile calibration: upload");
         break;
@@ -1649,7 +1651,7 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
   const int ntile64 = (int)b->tiles64.size(), ntile32 = (int)b->tiles32.size(), nchunk = (int)b->chunks32.size();
   const int gemm_grid = std::min(ntile64, 148 * 8);
   const size_t fermi_smem = (size_t)b->nmax * sizeof(double);
-  const dim3 pot_grid(nmol, nblk(std::max(b->natmax, b->nshmax), 256));
+  const dim3 pot_grid(nmol, nblk(std::max(b->natmax, b->nshmax), kPotTargets));
   std::vector<int> act, phase;
   // algorithmic work of this iteration over the active structures (profile mode only)
   double n3 = 0, n2 = 0, n2occ = 0, n3_lo = 0, n3_hi = 0, n2occ_lo = 0, n2occ_hi = 0;
@@ -1676,7 +1678,7 @@ tb_status iterate_body(tb_batch* b, cudaStream_t st) {
          k_mix_next<<<nmol, 256, 0, st>>>(B, b->q_in, b->dq, b->dqlast, b->qlast, b->df, b->u, b->amat,
                                           b->omega, b->opt.max_iter, b->opt.mixer_damping, S));
   TB_K("potential", 0, 0,
-       k_potential<<<pot_grid, 256, 0, st>>>(Pc, B, b->q_in, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, S.active,
+       k_potential<<<pot_grid, 32 * kPotTargets, 0, st>>>(Pc, B, b->q_in, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, S.active,
                                              b->gtab, b->atab));
   // Fock build: reads S, H0, D(3), Q(6), writes F -> 12 N^2 doubles
   TB_K("fock", 96.0 * n2, 2,
@@ -1984,8 +1986,8 @@ tb_status batch_gradient(tb_batch* b, const std::vector<int>& flag, cudaStream_t
   TB_CUDA(cudaMemsetAsync(G, 0, (size_t)b->h_a2off[nmol] * 3 * 8, st));
   k_grad_prep<<<nmol, 256, 0, st>>>(B, dflag, b->focc, b->w, b->qsh_out, b->dpat_out, b->qpat_out, fe, qv);
   TB_LAUNCH_CHECK();
-  const dim3 pot_grid(nmol, nblk(std::max(b->natmax, b->nshmax), 256));
-  k_potential<<<pot_grid, 256, 0, st>>>(b->Pc, B, qv, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, dflag, b->gtab,
+  const dim3 pot_grid(nmol, nblk(std::max(b->natmax, b->nshmax), kPotTargets));
+  k_potential<<<pot_grid, 32 * kPotTargets, 0, st>>>(b->Pc, B, qv, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, dflag, b->gtab,
                                         b->atab);
   TB_LAUNCH_CHECK();
   {
@@ -2670,8 +2672,8 @@ tb_status tb_coulomb_potential(const tb_calculator* calc, const tb_structure* mo
   const int one = 1;
   TB_CUDA(cudaMemcpy(b->ms.active, &one, sizeof(int), cudaMemcpyHostToDevice));
   const DevParams P = params_for(calc, 1.0);
-  k_potential<<<dim3(1, nblk(std::max(nat, nsh), 256)), 256>>>(P, b->db, b->q_in, b->mrad, b->vsh, b->vat, b->vdp,
-                                                               b->vqp, b->ms.active, nullptr, nullptr);
+  k_potential<<<dim3(1, nblk(std::max(nat, nsh), kPotTargets)), 32 * kPotTargets>>>(
+      P, b->db, b->q_in, b->mrad, b->vsh, b->vat, b->vdp, b->vqp, b->ms.active, nullptr, nullptr);
   TB_LAUNCH_CHECK();
   if (vsh && d2h(vsh, b->vsh, nsh * 8)) return TB_CUDA_ERROR;
   if (vat && d2h(vat, b->vat, nat * 8)) return TB_CUDA_ERROR;

@@ -238,6 +238,8 @@ __global__ void k_apply_guess(DevBatch B, const double* guess, const int* flag, 
 // pair tables of the fixed geometry (gtab: gamma per shell pair, atab: 1/r, f3, f5 per atom pair)
 __global__ void k_pair_tables(DevParams P, DevBatch B, const double* mrad, double* gtab, double* atab);
 // gtab/atab may be null: the pair terms are then recomputed
+// shells / atoms per CTA of k_potential (one warp each: CTAs of 32 x kPotTargets threads)
+constexpr int kPotTargets = 8;
 __global__ void k_potential(DevParams P, DevBatch B, const double* q_in, const double* mrad, double* vsh, double* vat,
                             double* vdp, double* vqp, const int* active, const double* gtab, const double* atab);
 // dynamic shared memory of k_fock (the nine staged transposed tiles)

@@ -203,8 +203,11 @@ __global__ void k_pair_tables(DevParams P, DevBatch B, const double* __restrict_
 // tb_coulomb::get_potential for the mixed input moments q_in = [qsh, dpat,
 // qpat]: ES2 (vsh += gamma qsh), ES3 (vsh += qsh^2 dGamma), AES2 (the five
 // gemv of the quoted Fortran src/coulomb.cu:665-676) and the on-site kernels
-// (get_kernel_potential, :564-589).  grid = (structure, target chunk).  With
-// the pair tables (gtab, atab non-null) the pair terms are read, not
+// (get_kernel_potential, :564-589).  grid = (structure, target chunk of
+// kPotTargets); one warp per target shell and atom, lanes over the partners
+// (row t of the pair tables, which are symmetric bit for bit, so the lanes
+// read contiguously), partial sums reduced across the warp in a fixed order.
+// With the pair tables (gtab, atab non-null) the pair terms are read, not
 // recomputed; the arithmetic on them is unchanged.
 __global__ void k_potential(DevParams P, DevBatch B, const double* __restrict__ q_in,
                             const double* __restrict__ mrad, double* __restrict__ vsh, double* __restrict__ vat,
@@ -217,37 +220,38 @@ __global__ void k_potential(DevParams P, DevBatch B, const double* __restrict__ 
   const double* qsh = q_in + B.mixoff[m];
   const double* dp = qsh + nsh;
   const double* qp = dp + 3 * nat;
-  const int t = blockIdx.y * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int t = blockIdx.y * kPotTargets + (threadIdx.x >> 5);
   const double* xyz = B.xyz + 3 * a0;
   // shells
   if (t < nsh) {
     const int ta = B.sh_type[s0 + t], A = B.sh_at[s0 + t];
     double v = 0.0;
     if (gtab) {
-      const double* gc = gtab + B.s2off[m] + t;  // column t = row t
-      for (int b = 0; b < nsh; ++b) v += gc[(long long)b * nsh] * qsh[b];
+      const double* gr = gtab + B.s2off[m] + (long long)t * nsh;  // row t = column t
+      for (int b = lane; b < nsh; b += 32) v += gr[b] * qsh[b];
     } else {
-      for (int b = 0; b < nsh; ++b) {
+      for (int b = lane; b < nsh; b += 32) {
         const int Bq = B.sh_at[s0 + b];
         const double dx = xyz[3 * A] - xyz[3 * Bq], dy = xyz[3 * A + 1] - xyz[3 * Bq + 1], dz = xyz[3 * A + 2] - xyz[3 * Bq + 2];
         v += gamma_ab(P, ta, B.sh_type[s0 + b], A == Bq, dx * dx + dy * dy + dz * dz) * qsh[b];
       }
     }
-    v += qsh[t] * qsh[t] * P.sh[ta].hubbard_deriv;
-    vsh[s0 + t] = v;
+    v = warp_sum(v);
+    if (lane == 0) vsh[s0 + t] = v + qsh[t] * qsh[t] * P.sh[ta].hubbard_deriv;
   }
   // atoms
   if (t < nat) {
     const int A = t;
     double va = 0.0, vd[3] = {0, 0, 0}, vq[6] = {0, 0, 0, 0, 0, 0};
     const double rA = mrad[a0 + A];
-    const double* ac = atab ? atab + 3 * (B.a2off[m] + A) : nullptr;  // column A = row A
-    for (int Bq = 0; Bq < nat; ++Bq) {
+    const double* ar = atab ? atab + 3 * (B.a2off[m] + (long long)A * nat) : nullptr;  // row A = column A
+    for (int Bq = lane; Bq < nat; Bq += 32) {
       if (Bq == A) continue;
       const double v[3] = {xyz[3 * Bq] - xyz[3 * A], xyz[3 * Bq + 1] - xyz[3 * A + 1], xyz[3 * Bq + 2] - xyz[3 * A + 2]};
       double g1, f3, f5;
-      if (ac) {
-        const double* e = ac + 3LL * Bq * nat;
+      if (ar) {
+        const double* e = ar + 3LL * Bq;
         g1 = e[0]; f3 = e[1]; f5 = e[2];
       } else {
         const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
@@ -270,12 +274,17 @@ __global__ void k_potential(DevParams P, DevBatch B, const double* __restrict__ 
       for (int c = 0; c < 6; ++c) tq += tc[c] * qpb[c];
       va += -vdb * g3 * f3 + tq * g5 * f5;
     }
-    const SpeciesParam& sp = P.sp[B.id[a0 + A]];
-    for (int k = 0; k < 3; ++k) vd[k] += 2.0 * sp.dkernel * dp[3 * A + k];
-    for (int c = 0; c < 6; ++c) vq[c] += 2.0 * sp.qkernel * qp[6 * A + c] * kMpScale[c];
-    vat[a0 + A] = va;
-    for (int k = 0; k < 3; ++k) vdp[3 * (a0 + A) + k] = vd[k];
-    for (int c = 0; c < 6; ++c) vqp[6 * (a0 + A) + c] = vq[c];
+    va = warp_sum(va);
+    for (int k = 0; k < 3; ++k) vd[k] = warp_sum(vd[k]);
+    for (int c = 0; c < 6; ++c) vq[c] = warp_sum(vq[c]);
+    if (lane == 0) {
+      const SpeciesParam& sp = P.sp[B.id[a0 + A]];
+      for (int k = 0; k < 3; ++k) vd[k] += 2.0 * sp.dkernel * dp[3 * A + k];
+      for (int c = 0; c < 6; ++c) vq[c] += 2.0 * sp.qkernel * qp[6 * A + c] * kMpScale[c];
+      vat[a0 + A] = va;
+      for (int k = 0; k < 3; ++k) vdp[3 * (a0 + A) + k] = vd[k];
+      for (int c = 0; c < 6; ++c) vqp[6 * (a0 + A) + c] = vq[c];
+    }
   }
 }
 
@@ -667,38 +676,44 @@ __global__ void k_finalize(DevParams P, DevBatch B, const double* __restrict__ c
   __syncthreads();
   const double* xyz = B.xyz + 3 * a0;
   const double* qs = qsh_out + s0;
-  // ES2 + ES3
+  // ES2 + ES3 and AES2: one warp per shell (atom), lanes over the partners
+  // (row a of the symmetric pair tables), reduced across the warp in a fixed
+  // order; lane 0 adds the target's energy terms
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
   double e2 = 0.0, e3 = 0.0;
-  for (int a = tid; a < nsh; a += nt) {
+  for (int a = warp; a < nsh; a += nwarp) {
     const int ta = B.sh_type[s0 + a], A = B.sh_at[s0 + a];
     double v = 0.0;
     if (gtab) {
-      const double* gc = gtab + B.s2off[m] + a;  // column a = row a
-      for (int b = 0; b < nsh; ++b) v += gc[(long long)b * nsh] * qs[b];
+      const double* gr = gtab + B.s2off[m] + (long long)a * nsh;  // row a = column a
+      for (int b = lane; b < nsh; b += 32) v += gr[b] * qs[b];
     } else {
-      for (int b = 0; b < nsh; ++b) {
+      for (int b = lane; b < nsh; b += 32) {
         const int Bq = B.sh_at[s0 + b];
         const double dx = xyz[3 * A] - xyz[3 * Bq], dy = xyz[3 * A + 1] - xyz[3 * Bq + 1], dz = xyz[3 * A + 2] - xyz[3 * Bq + 2];
         v += gamma_ab(P, ta, B.sh_type[s0 + b], A == Bq, dx * dx + dy * dy + dz * dz) * qs[b];
       }
     }
-    e2 += 0.5 * v * qs[a];
-    e3 += qs[a] * qs[a] * qs[a] * P.sh[ta].hubbard_deriv / 3.0;
+    v = warp_sum(v);
+    if (lane == 0) {
+      e2 += 0.5 * v * qs[a];
+      e3 += qs[a] * qs[a] * qs[a] * P.sh[ta].hubbard_deriv / 3.0;
+    }
   }
   // AES2: vd = sd q + 0.5 dd dp, vq = sq q; E = dp.vd + qp.vq + kernels
   double ea = 0.0;
-  for (int A = tid; A < nat; A += nt) {
+  for (int A = warp; A < nat; A += nwarp) {
     const double* dA = dpat_out + 3 * (a0 + A);
     const double* qA = qpat_out + 6 * (a0 + A);
     double vd[3] = {0, 0, 0}, vq[6] = {0, 0, 0, 0, 0, 0};
     const double rA = mrad[a0 + A];
-    const double* ac = atab ? atab + 3 * (B.a2off[m] + A) : nullptr;  // column A = row A
-    for (int Bq = 0; Bq < nat; ++Bq) {
+    const double* ar = atab ? atab + 3 * (B.a2off[m] + (long long)A * nat) : nullptr;  // row A = column A
+    for (int Bq = lane; Bq < nat; Bq += 32) {
       if (Bq == A) continue;
       const double v[3] = {xyz[3 * Bq] - xyz[3 * A], xyz[3 * Bq + 1] - xyz[3 * A + 1], xyz[3 * Bq + 2] - xyz[3 * A + 2]};
       double g1, f3, f5;
-      if (ac) {
-        const double* e = ac + 3LL * Bq * nat;
+      if (ar) {
+        const double* e = ar + 3LL * Bq;
         g1 = e[0]; f3 = e[1]; f5 = e[2];
       } else {
         const double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
@@ -714,11 +729,15 @@ __global__ void k_finalize(DevParams P, DevBatch B, const double* __restrict__ c
       for (int k = 0; k < 3; ++k) vd[k] += v[k] * g3 * f3 * qb + 0.5 * (g3 * db[k] - 3.0 * v[k] * vdb * g5) * f5;
       for (int c = 0; c < 6; ++c) vq[c] += tc[c] * g5 * f5 * qb;
     }
-    const SpeciesParam& sp = P.sp[B.id[a0 + A]];
-    double dd = 0.0, qq = 0.0;
-    for (int k = 0; k < 3; ++k) { ea += dA[k] * vd[k]; dd += dA[k] * dA[k]; }
-    for (int c = 0; c < 6; ++c) { ea += qA[c] * vq[c]; qq += qA[c] * qA[c] * kMpScale[c]; }
-    ea += sp.dkernel * dd + sp.qkernel * qq;
+    for (int k = 0; k < 3; ++k) vd[k] = warp_sum(vd[k]);
+    for (int c = 0; c < 6; ++c) vq[c] = warp_sum(vq[c]);
+    if (lane == 0) {
+      const SpeciesParam& sp = P.sp[B.id[a0 + A]];
+      double dd = 0.0, qq = 0.0;
+      for (int k = 0; k < 3; ++k) { ea += dA[k] * vd[k]; dd += dA[k] * dA[k]; }
+      for (int c = 0; c < 6; ++c) { ea += qA[c] * vq[c]; qq += qA[c] * qA[c] * kMpScale[c]; }
+      ea += sp.dkernel * dd + sp.qkernel * qq;
+    }
   }
   const double e_es2 = block_sum(e2, red);
   const double e_es3 = block_sum(e3, red);

@@ -440,6 +440,7 @@ __global__ void k_sp_classify(DevParams P, DevBatch B, const int* __restrict__ n
 }
 
 // Pair slot of every kept atom pair i > j of a structure, at a2off + i nat + j
+// and at a2off + j nat + i, so that a row of the table is read contiguously
 // (the table is cleared to -1 first: atom pairs beyond the cutoff).
 __global__ void k_sp_pairtab(DevBatch B, const int* __restrict__ npair, const int* __restrict__ pair_i,
                              const int* __restrict__ pair_j, long long pair_cap, int* __restrict__ tab) {
@@ -454,7 +455,9 @@ __global__ void k_sp_pairtab(DevBatch B, const int* __restrict__ npair, const in
   if (p - B.poff[m] >= npair[m]) return;
   const int nat = B.aoff[m + 1] - B.aoff[m];
   const long long x = B.a2off[m] + (long long)pair_i[p] * nat + pair_j[p];
+  const long long y = B.a2off[m] + (long long)pair_j[p] * nat + pair_i[p];
   if (TB_GUARD(6, x, B.a2off[m], B.a2off[m + 1])) tab[x] = (int)p;
+  if (TB_GUARD(6, y, B.a2off[m], B.a2off[m + 1])) tab[y] = (int)p;
 }
 
 // Off-site shell pairs of angular momenta (LI, LJ): one thread per item of
@@ -504,6 +507,8 @@ __global__ void k_integrals_t(DevParams P, DevBatch B, const int* __restrict__ p
   }
 }
 
+constexpr int kAsmCols = 4;  // columns per lane and round in k_sp_assemble
+
 // Dense S, H0, D, Q of every structure from the block records, one warp per
 // AO row, lanes over the columns: each row of the eleven planes is written
 // once, contiguously, zeros included (atom pairs beyond the cutoff, and the
@@ -515,6 +520,11 @@ __global__ void k_integrals_t(DevParams P, DevBatch B, const int* __restrict__ p
 // on centre i); for A > Bt the transposed element [r ...][c ...] with the
 // dipole and quadrupole operators shifted to centre j (shift_operator).
 __global__ void k_sp_assemble(DevParams P, DevBatch B, SpLists W, MatOut out, int maxsp) {
+  constexpr int NC = (kMaxL + 1) * (kMaxL + 1);
+  __shared__ int s_off[NC];
+  __shared__ long long s_rbase[NC];
+  if (threadIdx.x < NC) sp_bases(W.cls, threadIdx.x, &s_off[threadIdx.x], &s_rbase[threadIdx.x]);
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   if (row >= B.nao_tot) return;
@@ -527,37 +537,64 @@ __global__ void k_sp_assemble(DevParams P, DevBatch B, SpLists W, MatOut out, in
   const int a0 = B.aoff[m], nat = B.aoff[m + 1] - a0, s0 = B.soff[m];
   const long long mo = B.moff[m], nn = (long long)n * n;
   const int A = B.ao_at[o0 + r], shA = B.ao_sh[o0 + r];
-  for (int c = lane; c < n; c += 32) {
-    const long long e = (long long)r * n + c;
-    if (!TB_GUARD(8, e, 0, nn)) continue;
-    double sv = 0.0, hv = 0.0, dv[3] = {0.0, 0.0, 0.0}, qv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    const int Bt = B.ao_at[o0 + c];
-    if (Bt != A) {
+  // the row's own atom and shell, once per warp
+  const int ishA = shA - B.at_ish[a0 + A], nshA = P.sp[B.id[a0 + A]].nsh;
+  const int lA = P.sh[B.sh_type[s0 + shA]].ang, aoA = r - B.sh_iao[s0 + shA];
+  const double xA[3] = {B.xyz[3 * (a0 + A)], B.xyz[3 * (a0 + A) + 1], B.xyz[3 * (a0 + A) + 2]};
+  const int* trow = W.tab + B.a2off[m] + (long long)A * nat;
+  // kAsmCols columns per lane and round: their index chains (pair table ->
+  // item index -> record) are resolved first, all through the read-only
+  // path, so that several chains are in flight at once
+  constexpr int U = kAsmCols;
+  for (int cb = lane; cb < n; cb += 32 * U) {
+    const double* rec[U];
+    int ij[U], sij[U], bt[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int c = cb + 32 * u;
+      rec[u] = nullptr;
+      ij[u] = sij[u] = 0;
+      bt[u] = A;
+      if (c >= n) continue;
+      const int Bt = __ldg(B.ao_at + o0 + c);
+      bt[u] = Bt;
+      if (Bt == A) continue;
+      const int p = __ldg(trow + Bt);
+      if (p < 0) continue;
       const bool tr = A > Bt;  // row atom is the pair's i
-      const int ia = tr ? A : Bt, ja = tr ? Bt : A;
-      const int p = W.tab[B.a2off[m] + (long long)ia * nat + ja];
-      if (p >= 0) {
-        const int shB = B.ao_sh[o0 + c];
-        const int shi = tr ? shA : shB, shj = tr ? shB : shA;  // local shell indices
-        const int ish = shi - B.at_ish[a0 + ia], jsh = shj - B.at_ish[a0 + ja];
-        const int nshj = P.sp[B.id[a0 + ja]].nsh;
-        const int li = P.sh[B.sh_type[s0 + shi]].ang, lj = P.sh[B.sh_type[s0 + shj]].ang;
-        const int SJ = 2 * lj + 1, SIJ = (2 * li + 1) * SJ;
-        const int iao = (tr ? r : c) - B.sh_iao[s0 + shi], jao = (tr ? c : r) - B.sh_iao[s0 + shj];
-        const int g = W.idx[(long long)p * maxsp + ish * nshj + jsh];
-        int off;
-        long long rbase;
-        sp_bases(W.cls, (kMaxL + 1) * li + lj, &off, &rbase);
-        const double* rec = W.rec + rbase + (long long)(g - off) * sp_record(li, lj);
-        const int ij = iao * SJ + jao;
-        sv = rec[ij];
-        hv = sv * rec[SIJ];
-        const double* d = rec + SIJ + 1 + 3 * ij;
-        const double* q = rec + 4 * SIJ + 1 + 6 * ij;
-        if (tr) {
-          const double vec[3] = {B.xyz[3 * (a0 + ia)] - B.xyz[3 * (a0 + ja)],
-                                 B.xyz[3 * (a0 + ia) + 1] - B.xyz[3 * (a0 + ja) + 1],
-                                 B.xyz[3 * (a0 + ia) + 2] - B.xyz[3 * (a0 + ja) + 2]};
+      const int shB = __ldg(B.ao_sh + o0 + c);
+      const int ishB = shB - __ldg(B.at_ish + a0 + Bt), nshB = P.sp[__ldg(B.id + a0 + Bt)].nsh;
+      const int lB = P.sh[__ldg(B.sh_type + s0 + shB)].ang, aoB = c - __ldg(B.sh_iao + s0 + shB);
+      const int li = tr ? lA : lB, lj = tr ? lB : lA;
+      const int SJ = 2 * lj + 1;
+      const int iao = tr ? aoA : aoB, jao = tr ? aoB : aoA;
+      const int sp = tr ? ishA * nshB + ishB : ishB * nshA + ishA;
+      const int g = __ldg(W.idx + (long long)p * maxsp + sp);
+      const int cl = (kMaxL + 1) * li + lj;
+      rec[u] = W.rec + s_rbase[cl] + (long long)(g - s_off[cl]) * sp_record(li, lj);
+      ij[u] = iao * SJ + jao;
+      sij[u] = (2 * li + 1) * SJ;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int c = cb + 32 * u;
+      if (c >= n) continue;
+      const long long e = (long long)r * n + c;
+      if (!TB_GUARD(8, e, 0, nn)) continue;
+      double sv = 0.0, hv = 0.0, dv[3] = {0.0, 0.0, 0.0}, qv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      if (rec[u]) {
+        const int SIJ = sij[u];
+        sv = __ldg(rec[u] + ij[u]);
+        hv = sv * __ldg(rec[u] + SIJ);
+        double d[3], q[6];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) d[k] = __ldg(rec[u] + SIJ + 1 + 3 * ij[u] + k);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) q[k] = __ldg(rec[u] + 4 * SIJ + 1 + 6 * ij[u] + k);
+        if (A > bt[u]) {
+          const int Bt = bt[u];
+          const double vec[3] = {xA[0] - B.xyz[3 * (a0 + Bt)], xA[1] - B.xyz[3 * (a0 + Bt) + 1],
+                                 xA[2] - B.xyz[3 * (a0 + Bt) + 2]};
           shift_operator(vec, sv, d, q, dv, qv);
         } else {
 #pragma unroll
@@ -566,13 +603,13 @@ __global__ void k_sp_assemble(DevParams P, DevBatch B, SpLists W, MatOut out, in
           for (int k = 0; k < 6; ++k) qv[k] = q[k];
         }
       }
+      out.S[mo + e] = sv;
+      out.H0[mo + e] = hv;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) out.D[3 * mo + k * nn + e] = dv[k];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) out.Q[6 * mo + k * nn + e] = qv[k];
     }
-    out.S[mo + e] = sv;
-    out.H0[mo + e] = hv;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) out.D[3 * mo + k * nn + e] = dv[k];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) out.Q[6 * mo + k * nn + e] = qv[k];
   }
 }
 
