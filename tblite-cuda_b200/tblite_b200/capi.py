@@ -168,9 +168,17 @@ def _structs(mols):
     arr = (Structure * n)()
     if n == 0:
         return arr, ()
-    idl = [np.asarray(m.id, np.int32).ravel() for m in mols]
-    ids = np.ascontiguousarray(np.concatenate(idl))
-    xyz = np.ascontiguousarray(np.concatenate([np.asarray(m.xyz, np.float64).reshape(-1, 3) for m in mols]))
+    idl = [m.id for m in mols]
+    xyl = [m.xyz for m in mols]
+    if all(isinstance(a, np.ndarray) and a.ndim == 1 for a in idl) and \
+            all(isinstance(x, np.ndarray) and x.ndim == 2 and x.shape[1] == 3 for x in xyl):
+        # arrays already shaped as Molecule holds them: one concatenation each
+        ids = np.ascontiguousarray(np.concatenate(idl), dtype=np.int32)
+        xyz = np.ascontiguousarray(np.concatenate(xyl), dtype=np.float64)
+    else:
+        idl = [np.asarray(a, np.int32).ravel() for a in idl]
+        ids = np.ascontiguousarray(np.concatenate(idl))
+        xyz = np.ascontiguousarray(np.concatenate([np.asarray(x, np.float64).reshape(-1, 3) for x in xyl]))
     nat = np.fromiter((len(a) for a in idl), np.int64, n)
     off = np.zeros(n, np.int64)
     np.cumsum(nat[:-1], out=off[1:])
@@ -312,22 +320,26 @@ class Calculator:
         # each field converted once for all structures (numpy scalar access per field is slow)
         keys = ("energy", "e_rep", "e_elec", "e_band", "e_ts", "e_es2", "e_aes2", "e_es3", "scf_error",
                 "e_disp", "iterations", "status", "nsh", "nao")
-        cols = [v[k].tolist() for k in keys]
-        dip = v["dipole"].copy()
+        # (dicts from zipped columns and the per-structure views by list
+        # comprehension: about half the cost of a per-structure loop of dict
+        # comprehensions and slices)
+        out = [dict(zip(keys, vals)) for vals in zip(*[v[k].tolist() for k in keys])]
         a0s, a1s = off.tolist(), (off + nat).tolist()
         s0s, s1s = soff.tolist(), (soff + nsh).tolist()
-        out = []
-        for i in range(n):
-            d = {k: c[i] for k, c in zip(keys, cols)}
-            a0, a1 = a0s[i], a1s[i]
-            d.update(dipole=dip[i], qat=qat[a0:a1], qsh=qsh[s0s[i]:s1s[i]], dpat=dpat[a0:a1], qpat=qpat[a0:a1])
-            if gradient:
-                d.update(gradient=grad[a0:a1], sigma=v["sigma"][i].reshape(3, 3).copy())
-            if wavefunction:
+        views = {"dipole": list(v["dipole"].copy()),
+                 "qat": [qat[a:b] for a, b in zip(a0s, a1s)], "qsh": [qsh[a:b] for a, b in zip(s0s, s1s)],
+                 "dpat": [dpat[a:b] for a, b in zip(a0s, a1s)], "qpat": [qpat[a:b] for a, b in zip(a0s, a1s)]}
+        if gradient:
+            views["gradient"] = [grad[a:b] for a, b in zip(a0s, a1s)]
+            views["sigma"] = list(v["sigma"].reshape(n, 3, 3).copy())
+        for k, col in views.items():
+            for d, x in zip(out, col):
+                d[k] = x
+        if wavefunction:
+            for i, d in enumerate(out):
                 w = wfn[i]
                 d["wfn"] = dict(wbufs[i], nspin=w.nspin, nat=w.nat, nsh=w.nsh, nao=w.nao, homo=list(w.homo),
                                 kt=w.kt, nocc=w.nocc, nuhf=w.nuhf, nel=list(w.nel))
-            out.append(d)
         return out
 
 
