@@ -18,12 +18,16 @@ namespace tb {
 // finished columns k < j0 (each W[k][i] read once per group, the group's
 // entries W[k][j0..] broadcast), then the group is finished column by column
 // with the in-group terms.  Reads of the finished part drop by the group size
-// against a column-at-a-time walk.
+// against a column-at-a-time walk.  The group's entries of the finished
+// columns, which every row needs, are staged in shared memory kFactorChunk
+// columns at a time; the accumulation order is that of a plain loop over k.
 constexpr int kFactorGroup = 16;
+constexpr int kFactorChunk = 128;  // values of k staged in shared memory per round
 
 __global__ void k_cholesky(DevBatch B, const double* __restrict__ S, double* __restrict__ W,
                            int* __restrict__ status, const int* __restrict__ active) {
-  constexpr int G = kFactorGroup;
+  constexpr int G = kFactorGroup, KC = kFactorChunk;
+  __shared__ __align__(16) double ws[KC][G];  // ws[k - kc0][q] = W[k][j0 + q] = L[j0 + q][k]
   const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;
   if (active && !active[m]) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
@@ -38,20 +42,32 @@ __global__ void k_cholesky(DevBatch B, const double* __restrict__ S, double* __r
   __syncthreads();
   for (int j0 = 0; j0 < n; j0 += G) {
     const int gq = min(G, n - j0);
-    for (int i = j0 + tid; i < n; i += nt) {
+    for (int i0 = j0; i0 < n; i0 += nt) {
+      const int i = i0 + tid;  // threads past the last row still stage and wait
       double acc[G];
 #pragma unroll
-      for (int q = 0; q < G; ++q) acc[q] = q < gq ? s[(long long)(j0 + q) * n + i] : 0.0;
-      for (int k = 0; k < j0; ++k) {
-        const double a = w[(long long)k * n + i];
-        const double* wk = w + (long long)k * n + j0;
+      for (int q = 0; q < G; ++q) acc[q] = (q < gq && i < n) ? s[(long long)(j0 + q) * n + i] : 0.0;
+      for (int kc0 = 0; kc0 < j0; kc0 += KC) {
+        const int kn = min(KC, j0 - kc0);
+        __syncthreads();  // the previous chunk has been read
+        for (int e = tid; e < kn * G; e += nt) {
+          const int kk = e / G, q = e - kk * G;
+          ws[kk][q] = q < gq ? w[(long long)(kc0 + kk) * n + j0 + q] : 0.0;
+        }
+        __syncthreads();
+        if (i < n)
+          for (int kk = 0; kk < kn; ++kk) {
+            const double a = w[(long long)(kc0 + kk) * n + i];
+#pragma unroll
+            for (int q = 0; q < G; ++q)
+              if (q < gq) acc[q] -= a * ws[kk][q];
+          }
+      }
+      if (i < n) {
 #pragma unroll
         for (int q = 0; q < G; ++q)
-          if (q < gq) acc[q] -= a * wk[q];
+          if (q < gq) w[(long long)(j0 + q) * n + i] = acc[q];
       }
-#pragma unroll
-      for (int q = 0; q < G; ++q)
-        if (q < gq) w[(long long)(j0 + q) * n + i] = acc[q];
     }
     __syncthreads();
     for (int q = 0; q < gq; ++q) {
@@ -83,11 +99,16 @@ __global__ void k_cholesky(DevBatch B, const double* __restrict__ S, double* __r
 // X = L^-T (upper triangular, row-major): column c solves L^T x = e_c by
 // backward substitution, kFactorGroup rows at a time from the bottom: the
 // group's rows are first reduced with every finished row below it (each
-// X[k][c] read once per group, the group's L entries broadcast), then solved
-// upwards inside the group.  Each thread owns its columns, so no barrier.
+// X[k][c] read once per group), then solved upwards inside the group.  Each
+// thread owns a column; the group's rows of W (the L entries every column
+// needs) are staged in shared memory kFactorChunk values of k at a time, so
+// the inner loop reads them at shared-memory rather than L2 latency.  The
+// accumulation order is that of a plain loop over k, so X does not depend on
+// the staging.
 __global__ void k_trinv(DevBatch B, const double* __restrict__ W, double* __restrict__ X,
                         const int* __restrict__ status) {
-  constexpr int G = kFactorGroup;
+  constexpr int G = kFactorGroup, KC = kFactorChunk;
+  __shared__ double ws[G][KC];  // ws[q][k - kc0] = W[r1 - q][k]
   const int m = B.order ? B.order[blockIdx.x] : blockIdx.x;
   if (status[m] != kStOk) return;
   const int n = B.ooff[m + 1] - B.ooff[m];
@@ -96,19 +117,30 @@ __global__ void k_trinv(DevBatch B, const double* __restrict__ W, double* __rest
   const double* w = W + mo;
   double* x = X + mo;
   for (int c0 = 0; c0 < n; c0 += blockDim.x) {
-    const int c = c0 + threadIdx.x;
-    if (c >= n) continue;
+    const int c = c0 + threadIdx.x;  // threads past the last column still stage and wait
+    const int chi = min(n, c0 + (int)blockDim.x) - 1;  // the round's largest column
     for (int r1 = n - 1; r1 >= 0; r1 -= G) {
       const int gq = min(G, r1 + 1);
       double acc[G];
 #pragma unroll
       for (int q = 0; q < G; ++q) acc[q] = (q < gq && r1 - q == c) ? 1.0 : 0.0;
-      for (int k = r1 + 1; k <= c; ++k) {  // X[k][c] = 0 for k > c
-        const double xk = x[(long long)k * n + c];
+      for (int kc0 = r1 + 1; kc0 <= chi; kc0 += KC) {
+        const int kn = min(KC, chi + 1 - kc0);
+        __syncthreads();  // the previous chunk has been read
+        for (int e = threadIdx.x; e < gq * kn; e += blockDim.x) {
+          const int q = e / kn, kk = e - q * kn;
+          ws[q][kk] = w[(long long)(r1 - q) * n + kc0 + kk];  // W[r][k] = L[k][r]
+        }
+        __syncthreads();
+        const int kend = c < n ? min(kn, c + 1 - kc0) : 0;  // X[k][c] = 0 for k > c
+        for (int kk = 0; kk < kend; ++kk) {
+          const double xk = x[(long long)(kc0 + kk) * n + c];
 #pragma unroll
-        for (int q = 0; q < G; ++q)
-          if (q < gq) acc[q] -= w[(long long)(r1 - q) * n + k] * xk;  // W[r][k] = L[k][r]
+          for (int q = 0; q < G; ++q)
+            if (q < gq) acc[q] -= ws[q][kk] * xk;
+        }
       }
+      if (c >= n) continue;
       double xg[G];
 #pragma unroll
       for (int q = 0; q < G; ++q) {
