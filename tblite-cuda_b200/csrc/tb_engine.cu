@@ -1960,7 +1960,7 @@ tb_status batch_gradient(tb_batch* b, const std::vector<int>& flag, cudaStream_t
   NvtxRange nv("tb.gradient");
   tb_calculator* c = b->calc;
   const DevBatch& B = b->db;
-  const int nmol = b->nmol, nt = (int)b->tiles64.size();
+  const int nmol = b->nmol;
   const long long NA = b->nat_tot, NO = b->nao_tot, NM = nmol, MX = b->mix_tot;
   const int maxsp = c->maxsh * c->maxsh;
   const long long items = b->pair_cap * maxsp;
@@ -2049,8 +2049,7 @@ tb_status gradient_copy(tb_batch* b, double* grad, double* sigma, tb_result* out
 // potential buffers, also free after a run).
 tb_status spin_readout(tb_batch* b, const std::vector<int>& flag, cudaStream_t st) {
   const DevBatch& B = b->db;
-  const int nmol = b->nmol, nt = (int)b->tiles64.size(), nchunk = (int)b->chunks32.size();
-  const int gemm_grid = std::min(nt, 148 * 8);
+  const int nmol = b->nmol, nchunk = (int)b->chunks32.size();
   const long long NO = b->nao_tot;
   TB_CUDA(cudaMemcpyAsync(b->d_wflag, flag.data(), nmol * sizeof(int), cudaMemcpyHostToDevice, st));
   k_spin_occupations<<<nmol, 128, (size_t)b->nmax * sizeof(double), st>>>(B, b->w, b->opt.kt, b->ms.nel, b->d_wflag,
